@@ -1,0 +1,359 @@
+"""Benchmark: Mpix/s to the bit-exact min cut on one (or N) B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config single|batch] [--size 2048]
+
+A step is one solve of one synthetic grid: capacities already resident in HBM (row-major
+int32 planes) -> tile upload -> push-relabel with global relabels -> canonical cut flood
+-> labels in a device buffer + the flow value on the host.  `value` is the whole-job
+throughput (pixels solved by all ranks / max-over-ranks device time), timed with CUDA
+events on the solver's stream; L2 is flushed (256 MiB write) between steps, outside the
+timed region.  `e2e` is the same metric through the public API with host buffers: pinned
+host planes -> GraphCut.upload_capacities -> cut -> labels_host + flow, copies included.
+
+Workload (`--config single`, the default): one 2048x2048 grid per rank built as in the
+synthetic generator (12 blurred ellipses + noise, 2-component GMM t-links, exp n-links),
+seed 1 + rank.  Multi-GPU runs are replicas (one independent grid per rank, weak scaling);
+a single grid is not split across GPUs.
+
+`--impl reference` times the reference schedule restated on the CPU (the oracle's
+ref_tiled: GraphCut.cut + graphcut.cl in int32, OpenMP over tiles) on rank 0 with all host
+threads, on the same workload and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cl-util_b200")
+for _p in (PKG, ROOT):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Mpix/s at bit-exact min cut"
+UNIT = "Mpix/s"
+
+# Algorithmic bytes per tile (32x32 pixels, int32 planes) of each kernel kind; see DESIGN.md.
+ALGO_BYTES_PER_TILE = {
+    "upload": 1024 * 4 * (5 + 7),          # read 5 row-major planes, write 7 tile planes
+    "discharge": 1024 * 4 * (6 + 6) + 4 * 32 * 4,  # read+write excess/height/4 caps, halo
+    "edge_relabel_build": 124 * 4 * 2 + 16,  # edge excess+height, flags
+    "bfs_first": 1024 * 4 * 5 + 1024 * 4 + 6 * 128,  # caps+excess in, distances + masks out
+    "bfs": 5 * 128 + 4 * 128 + 2 * 1024 * 4,          # masks, halo, distances in/out
+    "flood_first": 1024 * 4 + 5 * 128 + 128,
+    "flood": 5 * 128 + 4 * 256 + 128,
+    "compact": 8,
+    "labels": 1024 * 1 + 128,
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="single", choices=["single", "batch"])
+    ap.add_argument("--size", type=int, default=2048)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.lines:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per tile of each kernel kind from the committed ncu summary (or {})."""
+    path = os.path.join(ROOT, "profiles", "traffic_per_tile.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_baseline(graph, threads, budget_s=12.0):
+    """The reference schedule restated (oracle ref_tiled) on the host cores."""
+    from oracle import oracle as O
+    reps, t_total = 0, 0.0
+    while t_total < budget_s and reps < 50:
+        t0 = time.perf_counter()
+        O.ref_tiled(*graph.planes(), bfs=5, threads=threads)
+        t_total += time.perf_counter() - t0
+        reps += 1
+    mpix = graph.width * graph.height / 1e6
+    return {"value": reps * mpix / t_total, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{reps} full solves of the {graph.width}x{graph.height} grid "
+                      f"({t_total:.1f} s), oracle ref_tiled (GraphCut.cut + graphcut.cl "
+                      f"restated, int32, OpenMP)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import synth
+    threads = os.cpu_count() or 1
+    g = synth.make_graph(args.size, args.size, 1)
+    from oracle import oracle as O
+    for _ in range(max(1, args.warmup)):
+        O.ref_tiled(*g.planes(), bfs=5, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.ref_tiled(*g.planes(), bfs=5, threads=threads)
+        times.append(time.perf_counter() - t0)
+    mpix = g.width * g.height / 1e6
+    ms = 1000 * statistics.mean(times)
+    value = mpix / (ms / 1000)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic",
+        "config": {"workload": f"single {args.size}x{args.size} synthetic segmentation grid, seed 1",
+                   "impl": "oracle ref_tiled: the reference schedule (GraphCut.pyx:348-418 + "
+                           "graphcut.cl) restated in int32 C++, OpenMP over tiles"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full solves of the {args.size}^2 grid"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+
+    import synth
+    from GraphCut import GraphCut
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    W = H = args.size
+    g = synth.make_graph(W, H, 1 + rank)
+    dev_planes = [torch.from_numpy(p).cuda() for p in g.planes()]
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    labels = torch.empty((H, W), dtype=torch.uint8, device="cuda")
+    gc = GraphCut(W, H, device=local)
+
+    def step():
+        gc.upload_capacities(*dev_planes, stream=stream)
+        gc.cut(stream=stream)
+        gc.labels(out=labels, stream=stream)
+        return gc.flow
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            flow = step()
+        stream.synchronize()
+        # parity of this workload against the oracle (outside the timed region)
+        lab = labels.cpu().numpy()
+        from oracle import oracle as O
+        f_ref, l_ref = O.maxflow_bk(*g.planes())
+        parity = bool(flow == f_ref and np.array_equal(lab, l_ref))
+
+        gc.set_profile(True)
+        prof_tot = {}
+        step_ms = []
+        clocks = ClockSampler(local)
+        barrier()
+        torch.cuda.synchronize()
+        with clocks:
+            for _ in range(args.steps):
+                flush.fill_(1)
+                ev0 = torch.cuda.Event(enable_timing=True)
+                ev1 = torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                step()
+                ev1.record(stream)
+                ev1.synchronize()
+                step_ms.append(ev0.elapsed_time(ev1))
+                for k, v in gc.profile().items():
+                    acc = prof_tot.setdefault(k, {"launches": 0, "ms": 0.0, "tiles": 0})
+                    for f in acc:
+                        acc[f] += v[f]
+        torch.cuda.synchronize()
+        barrier()
+        gc.set_profile(False)
+        total_ms = sum(step_ms)
+        if world > 1:
+            t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        mpix_all = world * args.steps * W * H / 1e6
+        value = mpix_all / (total_ms / 1000)
+
+        # e2e through the public API with host buffers
+        e2e = None
+        if not args.no_e2e:
+            host = [torch.from_numpy(p).pin_memory().numpy() for p in g.planes()]
+            out_host = torch.empty((H, W), dtype=torch.uint8).pin_memory().numpy()
+            for _ in range(2):
+                gc.upload_capacities(*host, stream=stream)
+                gc.cut(stream=stream)
+                out_host[:] = gc.labels_host(stream=stream)
+            e_ms = []
+            barrier()
+            for _ in range(args.steps):
+                flush.fill_(1)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                gc.upload_capacities(*host, stream=stream)
+                gc.cut(stream=stream)
+                out_host[:] = gc.labels_host(stream=stream)
+                _ = gc.flow
+                e_ms.append(1000 * (time.perf_counter() - t0))
+            e_tot = sum(e_ms)
+            if world > 1:
+                t = torch.tensor([e_tot], dtype=torch.float64, device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                e_tot = float(t.item())
+            e2e = {"value": mpix_all / (e_tot / 1000), "unit": UNIT,
+                   "h2d_bytes_per_step": 5 * 4 * W * H, "d2h_bytes_per_step": W * H + 8,
+                   "ms_per_step": e_tot / args.steps}
+
+    # roofline of the dominant kernel (largest summed event time)
+    peak, peak_kind = measured_peak()
+    dom = max(prof_tot.items(), key=lambda kv: kv[1]["ms"])
+    dname, d = dom
+    algo_bytes = d["tiles"] * ALGO_BYTES_PER_TILE.get(dname, 0)
+    if dname == "compact":
+        algo_bytes = d["launches"] * ((W // 32) * (H // 32)) * 8
+    achieved = algo_bytes / (d["ms"] / 1000) / 1e9 if d["ms"] > 0 else 0.0
+    traffic = None
+    tr = ncu_traffic().get(dname)
+    if tr is not None and d["launches"]:
+        traffic = tr * d["tiles"] / d["launches"]
+    launches = sum(v["launches"] for v in prof_tot.values())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(g, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic",
+            "config": {"workload": f"single {W}x{H} synthetic segmentation grid per GPU "
+                                   "(12 blurred ellipses + N(0,8) noise, 2-component GMM "
+                                   "t-links x100, 50*exp(-beta*dI^2) n-links), seed 1+rank",
+                       "l2": "flushed between steps (256 MiB write, outside the timed region)",
+                       "parallelism": f"replicas x{world}",
+                       "solver": {"discharge_iters": gc.opts.discharge_iters,
+                                  "pulses_per_relabel": gc.opts.pulses_per_relabel,
+                                  "initial_relabel": gc.opts.initial_relabel}},
+            "parity": parity,
+            "flow": flow,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "algo_bytes_per_launch": algo_bytes / max(1, d["launches"]),
+                         "avg_launch_us": 1000 * d["ms"] / max(1, d["launches"])},
+            "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "tiles": v["tiles"]}
+                        for k, v in prof_tot.items() if v["launches"]},
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+            "solve_stats": gc.stats(),
+        }
+        print(json.dumps(line), flush=True)
+    gc.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

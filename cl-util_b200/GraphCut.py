@@ -1,0 +1,212 @@
+"""GraphCut: the solver class of the reference (GraphCut.pyx:29-437) on libgcut.
+
+The reference class is built from an OpenCL context and an RGBA image and derives its
+n-link capacities on the device (``GraphCut(context, devices, dImg, lamda)``,
+GraphCut.pyx:80; load_tiles, graphcut.cl:1033-1132); its ``cut(dExcess, bfs)`` mutates the
+excess buffer in place and returns nothing (GraphCut.pyx:348-418).  Here the capacities are
+uploaded (int32 planes, see include/gcut.h), and the solve yields the max-flow value and
+the canonical minimum cut:
+
+    gc = GraphCut(width, height)
+    gc.upload_capacities(up, down, left, right, excess)   # torch CUDA int32 or numpy int32
+    gc.cut()
+    gc.flow, gc.labels()                                   # int, torch.uint8 [H, W] on device
+
+The reference's stepping methods keep their names: ``push``, ``relabel``, ``startBfs``,
+``isCompleted``; its read-only device planes ``dUp, dDown, dLeft, dRight, dHeight`` and
+``dExcess`` are materialised as row-major tensors on access.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+import _gcut
+from _gcut import check, lib, ptr, stream_handle
+
+BFS_DEFAULT = 5  # GraphCut.pyx:27
+
+
+def _as_i32_device(a, device):
+    import torch
+    if isinstance(a, torch.Tensor):
+        if a.dtype != torch.int32:
+            raise TypeError("capacity planes must be int32")
+        return a.to(device).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.int32)).to(device)
+
+
+class GraphCut:
+    """Tiled push-relabel graph cut on one width x height 4-connected grid."""
+
+    def __init__(self, width: int, height: int, device: int = 0, bfs: int | None = None,
+                 discharge_iters: int | None = None, initial_relabel: bool | None = None,
+                 max_cycles: int | None = None, max_bfs_rounds: int | None = None):
+        import torch
+        self.width, self.height = int(width), int(height)
+        self.device = torch.device("cuda", device)
+        opts = _gcut.default_opts(device=device, discharge_iters=discharge_iters,
+                                  pulses_per_relabel=bfs,
+                                  initial_relabel=None if initial_relabel is None else int(initial_relabel),
+                                  max_cycles=max_cycles, max_bfs_rounds=max_bfs_rounds)
+        self.opts = opts
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(lib().gc_create(self.width, self.height, ctypes.byref(opts), ctypes.byref(h)))
+        self._h = h
+        self._solved = False
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- input ------------------------------------------------------------------
+    def upload_capacities(self, up, down, left, right, excess, stream=None):
+        """Uploads the capacity planes; torch CUDA tensors are read in place, anything else
+        is copied to the device first.  Resets the residual graph."""
+        import torch
+        planes = (up, down, left, right, excess)
+        for p in planes:
+            if tuple(p.shape) != (self.height, self.width):
+                raise ValueError(f"plane shape {tuple(p.shape)} != {(self.height, self.width)}")
+        if all(isinstance(p, torch.Tensor) and p.is_cuda for p in planes):
+            dev = [_as_i32_device(p, self.device) for p in planes]
+            check(lib().gc_upload(self._h, *[ptr(d) for d in dev], stream_handle(stream)))
+            self._keep = dev  # the upload kernel reads them asynchronously
+        else:
+            host = [np.ascontiguousarray(p.cpu().numpy() if isinstance(p, torch.Tensor) else p,
+                                         dtype=np.int32) for p in planes]
+            with torch.cuda.device(self.device):
+                check(lib().gc_upload_host(self._h, *[ptr(a) for a in host], stream_handle(stream)))
+        self._solved = False
+
+    # ---- solve ------------------------------------------------------------------
+    def cut(self, stream=None):
+        """Runs push-relabel to the final cut (GraphCut.cut, GraphCut.pyx:348-418)."""
+        with __import__("torch").cuda.device(self.device):
+            check(lib().gc_solve(self._h, stream_handle(stream)))
+        self._solved = True
+        return self
+
+    def push(self, stream=None):
+        check(lib().gc_push(self._h, stream_handle(stream)))
+
+    def relabel(self, stream=None):
+        check(lib().gc_relabel(self._h, stream_handle(stream)))
+
+    def startBfs(self, stream=None):
+        check(lib().gc_start_bfs(self._h, stream_handle(stream)))
+
+    def isCompleted(self, stream=None) -> bool:
+        done = ctypes.c_int(0)
+        check(lib().gc_is_completed(self._h, ctypes.byref(done), stream_handle(stream)))
+        if done.value:
+            self._solved = True
+        return bool(done.value)
+
+    # ---- results ----------------------------------------------------------------
+    @property
+    def flow(self) -> int:
+        f = ctypes.c_int64(0)
+        check(lib().gc_flow(self._h, ctypes.byref(f)))
+        return int(f.value)
+
+    def labels(self, out=None, stream=None):
+        """Canonical cut: uint8 [H, W] device tensor, 1 = source side."""
+        import torch
+        if out is None:
+            out = torch.empty((self.height, self.width), dtype=torch.uint8, device=self.device)
+        check(lib().gc_labels(self._h, ptr(out), stream_handle(stream)))
+        return out
+
+    def labels_host(self, stream=None) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.uint8)
+        check(lib().gc_labels_host(self._h, ptr(out), stream_handle(stream)))
+        return out
+
+    def stats(self) -> dict:
+        st = _gcut.GcStats()
+        check(lib().gc_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def set_profile(self, on: bool):
+        """Per-kernel CUDA-event timing and tile counters for the following calls."""
+        check(lib().gc_set_profile(self._h, int(on)))
+
+    def profile(self) -> dict:
+        return _gcut.kernel_profile(lib().gc_get_profile, self._h)
+
+    def set_collect_stats(self, on: bool):
+        check(lib().gc_set_collect_stats(self._h, int(on)))
+
+    # ---- warm start -------------------------------------------------------------
+    def edit_tlinks(self, idx, values, stream=None):
+        """Sets t-links of pixels idx (flat y*W+x, distinct) to values; warm-starts cut()."""
+        import torch
+        idx = torch.as_tensor(np.asarray(idx.cpu() if isinstance(idx, torch.Tensor) else idx),
+                              dtype=torch.int32).to(self.device).contiguous()
+        vals = torch.as_tensor(np.asarray(values.cpu() if isinstance(values, torch.Tensor) else values),
+                               dtype=torch.int32).to(self.device).contiguous()
+        if idx.numel() != vals.numel():
+            raise ValueError("idx and values differ in length")
+        check(lib().gc_edit_tlinks(self._h, ptr(idx), ptr(vals), int(idx.numel()),
+                                   stream_handle(stream)))
+        self._keep_edit = (idx, vals)
+        self._solved = False
+
+    def edit_stroke(self, xs, ys, radius: int, value: int, stream=None):
+        """Every pixel within `radius` of the polyline gets t-link `value` (device raster)."""
+        xs = np.ascontiguousarray(xs, dtype=np.int32)
+        ys = np.ascontiguousarray(ys, dtype=np.int32)
+        if xs.shape != ys.shape or xs.ndim != 1:
+            raise ValueError("xs and ys must be 1-D arrays of the same length")
+        check(lib().gc_edit_stroke(self._h, ptr(xs), ptr(ys), int(xs.shape[0]), int(radius),
+                                   int(value), stream_handle(stream)))
+        self._solved = False
+
+    # ---- read-only planes (GraphCut.pyx:57-79) ----------------------------------
+    def _plane(self, which: int):
+        import torch
+        out = torch.empty((self.height, self.width), dtype=torch.int32, device=self.device)
+        args = [None] * 6
+        args[which] = ptr(out)
+        check(lib().gc_download_state(self._h, *args, stream_handle(None)))
+        return out
+
+    @property
+    def dExcess(self):
+        return self._plane(0)
+
+    @property
+    def dHeight(self):
+        return self._plane(1)
+
+    @property
+    def dUp(self):
+        return self._plane(2)
+
+    @property
+    def dDown(self):
+        return self._plane(3)
+
+    @property
+    def dLeft(self):
+        return self._plane(4)
+
+    @property
+    def dRight(self):
+        return self._plane(5)

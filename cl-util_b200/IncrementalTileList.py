@@ -1,0 +1,170 @@
+"""IncrementalTileList, StreamCompact and PrefixSum on libgcut's single-pass scan.
+
+Mirrors of the reference classes beneath GraphCut (IncrementalTileList.pyx:26-208,
+StreamCompact.pyx:22-82, PrefixSum.pyx:121-226) with the same method names, argument
+meaning and ValueError on capacity overflow.  Buffers are torch int32 CUDA tensors; every
+build / compact / scan is one kernel launch (decoupled look-back) instead of the
+reference's flag + copy + 1-3 scan launches + scatter.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import _gcut
+from _gcut import check, lib, ptr, stream_handle
+
+
+class Operator:
+    """Stamp comparisons (IncrementalTileList.pyx:26-31)."""
+    EQUAL = 0
+    GT = 1
+    LT = 2
+    GTE = 3
+    LTE = 4
+
+
+class Logical:
+    """Combination of two predicates (IncrementalTileList.pyx:33-35)."""
+    AND = 0
+    OR = 1
+
+
+def _i32(n, device):
+    import torch
+    return torch.zeros(max(1, n), dtype=torch.int32, device=device)
+
+
+def _pow2gt(x: int) -> int:
+    """Smallest power of two >= x (clutil.pyx:15-20)."""
+    i = 1
+    while i < x:
+        i <<= 1
+    return i
+
+
+class PrefixSum:
+    """Exclusive int32 scan (PrefixSum.pyx:121-226, prefixsum.cl)."""
+
+    def __init__(self, capacity: int, device=0):
+        import torch
+        self.capacity = int(capacity)
+        self.device = torch.device("cuda", device) if isinstance(device, int) else device
+
+    def factory(self, length=None):
+        """A scan buffer; its size is rounded up to a power of two (PrefixSum.pyx:168-176)."""
+        if length is None:
+            length = self.capacity
+        elif length > self.capacity:
+            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
+        return _i32(_pow2gt(length), self.device)
+
+    def scan(self, dArray, dTotal, length=None, stream=None):
+        """In-place exclusive scan of dArray[:length]; the sum goes to dTotal[0]."""
+        if length is None:
+            length = dArray.numel()
+        if length > self.capacity:
+            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
+        check(lib().gc_scan_exclusive(ptr(dArray), ptr(dArray), ptr(dTotal), int(length),
+                                      stream_handle(stream)))
+
+
+class StreamCompact:
+    """Stream compaction of int32 flags (StreamCompact.pyx:22-82)."""
+
+    def __init__(self, capacity: int, device=0):
+        import torch
+        self.capacity = int(capacity)
+        self.device = torch.device("cuda", device) if isinstance(device, int) else device
+
+    def flagFactory(self, length=None):
+        if length is None:
+            length = self.capacity
+        elif length > self.capacity:
+            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
+        return _i32(length, self.device)
+
+    def listFactory(self, length=None):
+        if length is None:
+            length = self.capacity
+        elif length > self.capacity:
+            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
+        return _i32(_pow2gt(length), self.device)
+
+    def compact(self, dFlags, dList, dLength, length=None, stream=None):
+        """dList[:n] = indices of the non-zero flags (increasing), dLength[0] = n."""
+        if length is None:
+            length = dFlags.numel()
+        elif length > self.capacity:
+            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
+        check(lib().gc_compact(ptr(dFlags), ptr(dList), ptr(dLength), int(length),
+                               stream_handle(stream)))
+
+
+class IncrementalTileList:
+    """Per-tile iteration stamps and the compacted list of tiles matching a predicate
+    (IncrementalTileList.pyx:37-208)."""
+
+    def __init__(self, global_dim, tiles_dim, device=0):
+        import torch
+        self.global_dim = tuple(int(v) for v in global_dim)
+        self.tiles_dim = tuple(int(v) for v in tiles_dim)
+        self.dim = (self.global_dim[0] // self.tiles_dim[0], self.global_dim[1] // self.tiles_dim[1])
+        self.device = torch.device("cuda", device) if isinstance(device, int) else device
+        n = self.dim[0] * self.dim[1]
+        self.d_tiles = torch.zeros((self.dim[1], self.dim[0]), dtype=torch.int32, device=self.device)
+        self.d_list = _i32(n, self.device)
+        self.d_length = _i32(1, self.device)
+        self.init_iteration = -1
+        self.is_dirty = True
+        self._length = 0
+        self.reset()
+
+    @property
+    def n_tiles(self) -> int:
+        return self.dim[0] * self.dim[1]
+
+    @property
+    def length(self) -> int:
+        """Number of tiles in d_list (one device->host read when dirty)."""
+        if self.is_dirty:
+            self._length = int(self.d_length[0].item())
+            self.is_dirty = False
+        return self._length
+
+    def increment(self) -> int:
+        self.iteration += 1
+        return self.iteration
+
+    def build(self, operator=None, operand=None, stream=None):
+        """d_list = row-major ids of tiles with `stamp operator operand` (default: EQUAL to
+        the current iteration)."""
+        if operator is None:
+            operator = Operator.EQUAL
+        if operand is None:
+            operand = self.iteration
+        check(lib().gc_tiles_build(ptr(self.d_tiles), int(operator), int(operand),
+                                   ptr(self.d_list), ptr(self.d_length), self.n_tiles,
+                                   stream_handle(stream)))
+        self.is_dirty = True
+
+    def incorporate(self, d_tiles2, operator1, operand1, operator2, operand2, logical,
+                    stream=None):
+        """Stamps the current iteration where (stamp op1 a1) LOGICAL (tiles2 op2 a2)."""
+        check(lib().gc_tiles_incorporate(ptr(self.d_tiles), ptr(d_tiles2), int(operator1),
+                                         int(operand1), int(operator2), int(operand2),
+                                         int(logical), int(self.iteration), self.n_tiles,
+                                         stream_handle(stream)))
+
+    def buildLogical(self, d_tiles2, operator1, operand1, operator2, operand2, logical,
+                     stream=None):
+        check(lib().gc_tiles_build_logical(ptr(self.d_tiles), ptr(d_tiles2), int(operator1),
+                                           int(operand1), int(operator2), int(operand2),
+                                           int(logical), ptr(self.d_list), ptr(self.d_length),
+                                           self.n_tiles, stream_handle(stream)))
+        self.is_dirty = True
+
+    def reset(self, stream=None):
+        self.iteration = self.init_iteration + 1
+        check(lib().gc_tiles_fill(ptr(self.d_tiles), int(self.init_iteration), self.n_tiles,
+                                  stream_handle(stream)))
+        self.is_dirty = True

@@ -1,0 +1,159 @@
+"""ctypes binding of libgcut.so (the C ABI declared in include/gcut.h).
+
+The library must have been built (``python cl-util_b200/gcut_build.py``); loading fails loudly
+otherwise - there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgcut.so")
+
+GC_OK, GC_ERR_INVALID, GC_ERR_OOM, GC_ERR_NOT_CONVERGED, GC_ERR_CUDA, GC_ERR_INTERNAL, \
+    GC_ERR_STATE = range(7)
+
+ERROR_NAMES = {
+    GC_ERR_INVALID: "GC_ERR_INVALID", GC_ERR_OOM: "GC_ERR_OOM",
+    GC_ERR_NOT_CONVERGED: "GC_ERR_NOT_CONVERGED", GC_ERR_CUDA: "GC_ERR_CUDA",
+    GC_ERR_INTERNAL: "GC_ERR_INTERNAL", GC_ERR_STATE: "GC_ERR_STATE",
+}
+
+
+class GCError(RuntimeError):
+    """A non-zero status returned by libgcut."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class GcOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("discharge_iters", ctypes.c_int),
+                ("pulses_per_relabel", ctypes.c_int), ("initial_relabel", ctypes.c_int),
+                ("max_cycles", ctypes.c_int), ("max_bfs_rounds", ctypes.c_int)]
+
+
+class GcStats(ctypes.Structure):
+    _fields_ = [("cycles", ctypes.c_int64), ("pulses", ctypes.c_int64),
+                ("bfs_rounds", ctypes.c_int64), ("flood_rounds", ctypes.c_int64),
+                ("launches", ctypes.c_int64), ("tiles_discharged", ctypes.c_int64)]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
+class GcKernelProf(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_int64), ("ms", ctypes.c_double), ("tiles", ctypes.c_int64)]
+
+
+GC_NKERN = 9
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I32 = ctypes.c_int32
+
+# name -> argument types (all functions return int unless listed in _RESTYPE)
+SIGNATURES = {
+    "gc_opts_default": [_P],
+    "gc_create": [_I, _I, _P, _P],
+    "gc_destroy": [_P],
+    "gc_size": [_P, _P, _P],
+    "gc_upload": [_P] * 6 + [_P],
+    "gc_upload_host": [_P] * 6 + [_P],
+    "gc_solve": [_P, _P],
+    "gc_push": [_P, _P],
+    "gc_relabel": [_P, _P],
+    "gc_start_bfs": [_P, _P],
+    "gc_is_completed": [_P, _P, _P],
+    "gc_flow": [_P, _P],
+    "gc_labels": [_P, _P, _P],
+    "gc_labels_host": [_P, _P, _P],
+    "gc_edit_tlinks": [_P, _P, _P, _I, _P],
+    "gc_edit_stroke": [_P, _P, _P, _I, _I, _I32, _P],
+    "gc_download_state": [_P] * 7 + [_P],
+    "gc_get_stats": [_P, _P],
+    "gc_set_collect_stats": [_P, _I],
+    "gc_set_profile": [_P, _I],
+    "gc_get_profile": [_P, _P, _I],
+    "gc_kernel_name": [_I],
+    "gc_last_error": [],
+    "gc_scan_exclusive": [_P, _P, _P, _I, _P],
+    "gc_compact": [_P, _P, _P, _I, _P],
+    "gc_tiles_build": [_P, _I, _I32, _P, _P, _I, _P],
+    "gc_tiles_build_logical": [_P, _P, _I, _I32, _I, _I32, _I, _P, _P, _I, _P],
+    "gc_tiles_incorporate": [_P, _P, _I, _I32, _I, _I32, _I, _I32, _I, _P],
+    "gc_tiles_fill": [_P, _I32, _I, _P],
+    "gcb_create": [_I, _P, _P, _P, _P],
+    "gcb_destroy": [_P],
+    "gcb_upload": [_P, _I] + [_P] * 5 + [_P],
+    "gcb_solve": [_P, _P],
+    "gcb_flow": [_P, _I, _P],
+    "gcb_labels": [_P, _I, _P, _P],
+    "gcb_get_stats": [_P, _P],
+    "gcb_set_profile": [_P, _I],
+    "gcb_get_profile": [_P, _P, _I],
+}
+_RESTYPE = {"gc_last_error": ctypes.c_char_p, "gc_kernel_name": ctypes.c_char_p}
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with "
+                               "`python cl-util_b200/gcut_build.py` (no fallback exists)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPE.get(name, ctypes.c_int)
+        _lib = L
+    return _lib
+
+
+def check(rc: int):
+    if rc != GC_OK:
+        msg = lib().gc_last_error()
+        raise GCError(rc, msg.decode() if msg else "")
+
+
+def default_opts(**overrides) -> GcOpts:
+    o = GcOpts()
+    check(lib().gc_opts_default(ctypes.byref(o)))
+    for k, v in overrides.items():
+        if v is not None:
+            setattr(o, k, int(v))
+    return o
+
+
+def stream_handle(stream=None):
+    """cudaStream_t of a torch stream (current stream when None) as a ctypes pointer."""
+    import torch
+    s = torch.cuda.current_stream() if stream is None else stream
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def ptr(t):
+    """Device/host address of a tensor or numpy array."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return ctypes.c_void_p(t.data_ptr())
+    return t.ctypes.data_as(ctypes.c_void_p)
+
+
+def kernel_profile(get_fn, handle) -> dict:
+    """{kernel name: {launches, ms, tiles}} from gc_get_profile / gcb_get_profile."""
+    arr = (GcKernelProf * GC_NKERN)()
+    check(get_fn(handle, arr, GC_NKERN))
+    out = {}
+    for k in range(GC_NKERN):
+        name = lib().gc_kernel_name(k).decode()
+        out[name] = {"launches": int(arr[k].launches), "ms": float(arr[k].ms),
+                     "tiles": int(arr[k].tiles)}
+    return out

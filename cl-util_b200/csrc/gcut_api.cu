@@ -1,0 +1,774 @@
+// C ABI of libgcut.so: tile pools, the solve loop and the data-parallel primitives.
+//
+// The host loop mirrors GraphCut.cut (GraphCut.pyx:348-418) at a coarser grain: where the
+// reference enqueues ~30 kernels and blocks on ~5 device->host reads per push iteration,
+// a cycle here is `pulses_per_relabel` x {discharge, edge-relabel + list rebuild} and one
+// exact global relabel, all enqueued without a host wait; the host reads one int (the
+// active-tile count) per cycle and one per few BFS rounds.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "gcut_internal.h"
+
+using namespace gcut;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  g_err = std::string(where) + ": " + cudaGetErrorString(e);
+  return GC_ERR_CUDA;
+}
+
+#define CK(call)                                   \
+  do {                                             \
+    cudaError_t _e = (call);                       \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+
+#define RK(call)                                   \
+  do {                                             \
+    int _r = (call);                               \
+    if (_r != GC_OK) {                             \
+      if (g_err.empty()) g_err = #call;            \
+      return _r;                                   \
+    }                                              \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n) {
+  return cudaMalloc((void**)p, n * sizeof(T) + 16);
+}
+
+struct ScanBuffers {
+  ScanState st{};
+  cudaError_t alloc(int max_chunks) {
+    cudaError_t e;
+    if ((e = cudaMalloc((void**)&st.status, sizeof(unsigned long long) * max_chunks))) return e;
+    if ((e = cudaMalloc((void**)&st.ticket, 4 * sizeof(int32_t)))) return e;
+    st.done = st.ticket + 1;
+    st.err = st.ticket + 2;
+    st.seq = (uint32_t*)(st.ticket + 3);
+    st.max_chunks = max_chunks;
+    if ((e = cudaMemset(st.status, 0, sizeof(unsigned long long) * max_chunks))) return e;
+    if ((e = cudaMemset(st.ticket, 0, 4 * sizeof(int32_t)))) return e;
+    uint32_t one = 1;
+    return cudaMemcpy(st.seq, &one, sizeof(one), cudaMemcpyHostToDevice);
+  }
+  void release() {
+    if (st.status) cudaFree(st.status);
+    if (st.ticket) cudaFree(st.ticket);
+    st = ScanState{};
+  }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// Tile pool: one or more images, all solved together.
+// ------------------------------------------------------------------------------------
+struct Pool {
+  int device = 0;
+  gc_opts opts{};
+  std::vector<ImageDesc> imgs;
+  int nt = 0;
+  PoolView P{};
+  int32_t* tl = nullptr;       // current t-links per pixel (tile planes)
+  int32_t* list = nullptr;     // active / frontier tile list
+  int32_t* counts = nullptr;   // [0] list length
+  ImageAcc* acc = nullptr;     // per image
+  ScanBuffers scan;
+  int32_t* h_count = nullptr;  // pinned
+  ImageAcc* h_acc = nullptr;   // pinned
+  int grid_dis = 0, grid_warps = 0;
+  bool uploaded = false, solved = false, edited = false, collect = false;
+  bool list_valid = false, bfs_fresh = false;
+  gc_stats stats{};
+  // profiling: event pairs around every launch, tiles processed per kernel kind
+  bool prof = false;
+  unsigned long long* ktiles = nullptr;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, size_t>> ev_used;   // (kind, index of the start event)
+  gc_kernel_prof kprof[GC_NKERN]{};
+
+  template <class F>
+  int timed(int kind, cudaStream_t s, F&& launch) {
+    kprof[kind].launches++;
+    stats.launches++;
+    if (!prof) return launch();
+    size_t i = ev_used.size() * 2;
+    while (ev_pool.size() < i + 2) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      ev_pool.push_back(e);
+    }
+    CK(cudaEventRecord(ev_pool[i], s));
+    int r = launch();
+    CK(cudaEventRecord(ev_pool[i + 1], s));
+    ev_used.push_back({kind, i});
+    return r;
+  }
+  int prof_begin(cudaStream_t s) {
+    for (auto& k : kprof) k = gc_kernel_prof{};
+    ev_used.clear();
+    if (prof) {
+      CK(cudaMemsetAsync(ktiles, 0, sizeof(unsigned long long) * GC_NKERN, s));
+      P.ktiles = ktiles;
+    } else {
+      P.ktiles = nullptr;
+    }
+    return GC_OK;
+  }
+  int prof_end(cudaStream_t s) {
+    if (!prof) return GC_OK;
+    CK(cudaStreamSynchronize(s));
+    for (auto& u : ev_used) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev_pool[u.second], ev_pool[u.second + 1]));
+      kprof[u.first].ms += ms;
+    }
+    unsigned long long t[GC_NKERN];
+    CK(cudaMemcpy(t, ktiles, sizeof(t), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < GC_NKERN; ++k) kprof[k].tiles = (int64_t)t[k];
+    ev_used.clear();
+    return GC_OK;
+  }
+  // staging for host uploads / label reads (single-image handles)
+  int32_t* stage = nullptr;
+  uint8_t* lstage = nullptr;
+  int32_t* pts = nullptr;      // stroke points (device)
+
+  ~Pool() { release(); }
+
+  void release() {
+    int32_t* bufs[] = {P.exc, P.hgt, P.cap[0], P.cap[1], P.cap[2], P.cap[3], tl, list, counts,
+                       P.touched, P.act_int, P.mark, P.tact, P.img_of, stage, pts};
+    for (auto* b : bufs) if (b) cudaFree(b);
+    if (P.nbr) cudaFree(P.nbr);
+    if (P.mcan) cudaFree(P.mcan);
+    if (P.msink) cudaFree(P.msink);
+    if (P.mexc) cudaFree(P.mexc);
+    if (P.mreach) cudaFree(P.mreach);
+    if (acc) cudaFree(acc);
+    if (lstage) cudaFree(lstage);
+    if (h_count) cudaFreeHost(h_count);
+    if (h_acc) cudaFreeHost(h_acc);
+    if (ktiles) cudaFree(ktiles);
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    ev_pool.clear();
+    ktiles = nullptr;
+    scan.release();
+    P = PoolView{};
+    tl = list = counts = stage = pts = nullptr;
+    acc = nullptr; lstage = nullptr; h_count = nullptr; h_acc = nullptr;
+  }
+
+  int create(int n, const int* W, const int* H, const gc_opts* o) {
+    if (n <= 0 || !W || !H) return fail(GC_ERR_INVALID, "no images");
+    opts = *o;
+    device = opts.device;
+    nt = 0;
+    for (int i = 0; i < n; ++i) {
+      if (W[i] <= 0 || H[i] <= 0 || W[i] > (1 << 16) || H[i] > (1 << 16))
+        return fail(GC_ERR_INVALID, "image size out of range");
+      ImageDesc d{W[i], H[i], (W[i] + 31) / 32, (H[i] + 31) / 32, nt};
+      long long tiles = (long long)d.tw * d.th;
+      if (nt + tiles > (1 << 26)) return fail(GC_ERR_INVALID, "pool too large");
+      nt += (int)tiles;
+      imgs.push_back(d);
+    }
+    CK(cudaSetDevice(device));
+    const size_t px = (size_t)nt * GC_TILE_PX;
+    P.nt = nt;
+    cudaError_t e = cudaSuccess;
+    int32_t** planes[] = {&P.exc, &P.hgt, &P.cap[0], &P.cap[1], &P.cap[2], &P.cap[3], &tl};
+    for (auto** p : planes) if (!e) e = dalloc(p, px);
+    if (!e) e = dalloc(&P.nbr, nt);
+    if (!e) e = dalloc(&P.mcan, (size_t)nt * 128);
+    if (!e) e = dalloc(&P.msink, (size_t)nt * 32);
+    if (!e) e = dalloc(&P.mexc, (size_t)nt * 32);
+    if (!e) e = dalloc(&P.mreach, (size_t)nt * 32);
+    int32_t** small[] = {&P.touched, &P.act_int, &P.mark, &P.tact, &P.img_of, &list};
+    for (auto** p : small) if (!e) e = dalloc(p, nt);
+    if (!e) e = dalloc(&counts, 4);
+    if (!e) e = dalloc(&acc, imgs.size());
+    if (!e) e = dalloc(&ktiles, GC_NKERN);
+    if (!e) e = scan.alloc(scan_chunks(nt) > nt / 256 + 1 ? scan_chunks(nt) : nt / 256 + 1);
+    if (!e) e = cudaMallocHost((void**)&h_count, 4 * sizeof(int32_t));
+    if (!e) e = cudaMallocHost((void**)&h_acc, imgs.size() * sizeof(ImageAcc));
+    if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); release(); return fail(GC_ERR_OOM, "device allocation failed"); }
+    if (e) { release(); return cuda_fail(e, "pool allocation"); }
+    std::vector<int4> nb(nt);
+    for (const auto& d : imgs)
+      for (int ty = 0; ty < d.th; ++ty)
+        for (int tx = 0; tx < d.tw; ++tx) {
+          int t = d.tile0 + ty * d.tw + tx;
+          nb[t] = make_int4(ty > 0 ? t - d.tw : -1, ty < d.th - 1 ? t + d.tw : -1,
+                            tx > 0 ? t - 1 : -1, tx < d.tw - 1 ? t + 1 : -1);
+        }
+    CK(cudaMemcpy(P.nbr, nb.data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
+    CK(cudaMemset(P.touched, 0, sizeof(int32_t) * nt));
+    CK(cudaMemset(P.mark, 0, sizeof(int32_t) * nt));
+    CK(cudaMemset(P.act_int, 0, sizeof(int32_t) * nt));
+    CK(cudaMemset(P.tact, 0, sizeof(int32_t) * nt));
+    CK(cudaMemset(acc, 0, sizeof(ImageAcc) * imgs.size()));
+    grid_dis = occupancy_discharge(device);
+    grid_warps = occupancy_warps(device);
+    return GC_OK;
+  }
+
+  int upload(int i, const int32_t* up, const int32_t* down, const int32_t* left,
+             const int32_t* right, const int32_t* excess, cudaStream_t s) {
+    if (i < 0 || i >= (int)imgs.size()) return fail(GC_ERR_INVALID, "image index");
+    if (!up || !down || !left || !right || !excess) return fail(GC_ERR_INVALID, "null plane");
+    CK(cudaSetDevice(device));
+    CK(cudaMemsetAsync(acc + i, 0, sizeof(ImageAcc), s));
+    P.ktiles = nullptr;
+    RK(timed(K_UPLOAD, s, [&] { return launch_upload(P, imgs[i], i, up, down, left, right, excess, tl, acc, s); }));
+    uploaded = true;
+    solved = false;
+    edited = false;
+    list_valid = false;
+    bfs_fresh = false;
+    return GC_OK;
+  }
+
+  // exact BFS distances to the sink pixels (global relabel); sets tact
+  int global_relabel(cudaStream_t s) {
+    RK(timed(K_BFS_FIRST, s, [&] { return launch_bfs_round(P, list, counts, 1, grid_warps, s); }));
+    stats.bfs_rounds++;
+    return frontier_rounds(s, /*flood=*/false);
+  }
+
+  // repeat {compact marks -> list; round over list} until a round had no tiles
+  int frontier_rounds(cudaStream_t s, bool flood) {
+    int batch = 4;
+    long long rounds = 0;
+    while (true) {
+      for (int k = 0; k < batch; ++k) {
+        RK(compact(P.mark, P.mark, s));
+        if (flood) RK(timed(K_FLOOD, s, [&] { return launch_flood_round(P, list, counts, 0, acc, grid_warps, s); }));
+        else RK(timed(K_BFS, s, [&] { return launch_bfs_round(P, list, counts, 0, grid_warps, s); }));
+      }
+      rounds += batch;
+      int n;
+      RK(read_count(s, &n));
+      if (flood) stats.flood_rounds += batch; else stats.bfs_rounds += batch;
+      if (n == 0) break;
+      if (rounds >= opts.max_bfs_rounds) return fail(GC_ERR_NOT_CONVERGED, "BFS round cap reached");
+      batch = batch < 32 ? batch * 2 : 32;
+    }
+    return GC_OK;
+  }
+
+  int compact(const int32_t* flags, int32_t* clear, cudaStream_t s) {
+    return timed(K_COMPACT, s, [&] {
+      return launch_scan(GC_SCAN_MODE_COMPACT, flags, nullptr, clear, nullptr, list, counts, nt,
+                         0, 0, 0, 0, 0, scan.st, s);
+    });
+  }
+
+  int read_count(cudaStream_t s, int* n) {
+    CK(cudaMemcpyAsync(h_count, counts, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *n = h_count[0];
+    return GC_OK;
+  }
+
+  int check_device_error(cudaStream_t s) {
+    int32_t err = 0;
+    CK(cudaMemcpyAsync(&h_count[1], scan.st.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    err = h_count[1];
+    if (err) {
+      cudaMemsetAsync(scan.st.err, 0, sizeof(int32_t), s);
+      return fail(GC_ERR_INTERNAL, "a bounded device-side wait gave up");
+    }
+    return GC_OK;
+  }
+
+  int solve(cudaStream_t s) {
+    if (!uploaded) return fail(GC_ERR_STATE, "solve before upload");
+    CK(cudaSetDevice(device));
+    stats = gc_stats{};
+    RK(prof_begin(s));
+    int n = 0;
+    const bool relabel_first = opts.initial_relabel || edited || solved;
+    if (relabel_first) RK(global_relabel(s));
+    RK(compact(P.tact, nullptr, s));
+    if (relabel_first) {
+      RK(read_count(s, &n));
+      if (n == 0) return finish(s);
+    }
+    for (int cycle = 0; cycle < opts.max_cycles; ++cycle) {
+      stats.cycles++;
+      for (int p = 0; p < opts.pulses_per_relabel; ++p) {
+        RK(timed(K_DISCHARGE, s, [&] { return launch_discharge(P, list, counts, opts.discharge_iters, grid_dis, s); }));
+        RK(timed(K_EDGE_BUILD, s, [&] { return launch_edge_relabel_build(P, list, counts, scan.st, s); }));
+        stats.pulses++;
+        if (collect) { int m; RK(read_count(s, &m)); stats.tiles_discharged += m; }
+      }
+      RK(global_relabel(s));
+      RK(compact(P.tact, nullptr, s));
+      RK(read_count(s, &n));
+      if (n == 0) return finish(s);
+    }
+    return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
+  }
+
+  // canonical cut (flood from excess pixels) and the flow sums
+  int finish(cudaStream_t s) {
+    for (size_t i = 0; i < imgs.size(); ++i)
+      CK(cudaMemsetAsync(&acc[i].sumpos_e, 0, sizeof(unsigned long long), s));
+    RK(timed(K_FLOOD_FIRST, s, [&] { return launch_flood_round(P, list, counts, 1, acc, grid_warps, s); }));
+    stats.flood_rounds++;
+    RK(frontier_rounds(s, /*flood=*/true));
+    CK(cudaMemcpyAsync(h_acc, acc, sizeof(ImageAcc) * imgs.size(), cudaMemcpyDeviceToHost, s));
+    RK(check_device_error(s));
+    for (size_t i = 0; i < imgs.size(); ++i)
+      if (h_acc[i].bad_caps) return fail(GC_ERR_INVALID, "negative capacity in the upload");
+    RK(prof_end(s));
+    solved = true;
+    edited = false;
+    return GC_OK;
+  }
+
+  // manual stepping (gc_push / gc_relabel / gc_start_bfs / gc_is_completed)
+  int step_push(cudaStream_t s) {
+    if (!uploaded) return fail(GC_ERR_STATE, "push before upload");
+    if (!list_valid) {
+      RK(compact(P.tact, nullptr, s));
+      list_valid = true;
+    }
+    solved = false;
+    bfs_fresh = false;
+    return launch_discharge(P, list, counts, opts.discharge_iters, grid_dis, s);
+  }
+  int step_relabel(cudaStream_t s) {
+    if (!uploaded) return fail(GC_ERR_STATE, "relabel before upload");
+    solved = false;
+    bfs_fresh = false;
+    list_valid = true;
+    return launch_edge_relabel_build(P, list, counts, scan.st, s);
+  }
+  int step_start_bfs(cudaStream_t s) {
+    if (!uploaded) return fail(GC_ERR_STATE, "startBfs before upload");
+    RK(global_relabel(s));
+    RK(compact(P.tact, nullptr, s));
+    list_valid = true;
+    bfs_fresh = true;
+    return GC_OK;
+  }
+  int step_is_completed(int* done, cudaStream_t s) {
+    if (!bfs_fresh) return fail(GC_ERR_STATE, "isCompleted is valid right after startBfs");
+    int n;
+    RK(read_count(s, &n));
+    *done = n == 0;
+    if (*done) RK(finish(s));
+    return GC_OK;
+  }
+
+  int flow(int i, int64_t* out) {
+    if (!solved) return fail(GC_ERR_STATE, "flow before solve");
+    if (i < 0 || i >= (int)imgs.size() || !out) return fail(GC_ERR_INVALID, "bad argument");
+    *out = (int64_t)(h_acc[i].sumpos_t - h_acc[i].sumpos_e);
+    return GC_OK;
+  }
+
+  int labels(int i, uint8_t* out, cudaStream_t s) {
+    if (!solved) return fail(GC_ERR_STATE, "labels before solve");
+    if (i < 0 || i >= (int)imgs.size() || !out) return fail(GC_ERR_INVALID, "bad argument");
+    CK(cudaSetDevice(device));
+    return timed(K_LABELS, s, [&] { return launch_labels_out(P, imgs[i], out, s); });
+  }
+};
+
+struct gc_handle {
+  Pool pool;
+};
+
+struct gcb_handle {
+  Pool pool;
+};
+
+// ------------------------------------------------------------------------------------
+// Per-device look-back state for the stand-alone primitives.
+// ------------------------------------------------------------------------------------
+namespace {
+std::mutex g_scan_mu;
+std::unordered_map<int, ScanBuffers> g_scan;
+
+int device_scan_state(ScanState* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e) return cuda_fail(e, "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(g_scan_mu);
+  auto it = g_scan.find(dev);
+  if (it == g_scan.end()) {
+    ScanBuffers b;
+    e = b.alloc(1 << 16);
+    if (e) { b.release(); return e == cudaErrorMemoryAllocation ? fail(GC_ERR_OOM, "scan state") : cuda_fail(e, "scan state"); }
+    it = g_scan.emplace(dev, b).first;
+  }
+  *out = it->second.st;
+  return GC_OK;
+}
+}  // namespace
+
+extern "C" {
+
+const char* gc_last_error(void) { return g_err.c_str(); }
+
+int gc_opts_default(gc_opts* o) {
+  if (!o) return fail(GC_ERR_INVALID, "null opts");
+  o->device = 0;
+  o->discharge_iters = 32;
+  o->pulses_per_relabel = 2;
+  o->initial_relabel = 0;
+  o->max_cycles = 100000;
+  o->max_bfs_rounds = 1 << 20;
+  return GC_OK;
+}
+
+static int check_opts(const gc_opts* o) {
+  if (o->discharge_iters < 1 || o->pulses_per_relabel < 0 || o->max_cycles < 1 || o->max_bfs_rounds < 1)
+    return fail(GC_ERR_INVALID, "invalid options");
+  return GC_OK;
+}
+
+int gc_create(int width, int height, const gc_opts* opts, gc_handle** out) {
+  g_err.clear();
+  if (!out) return fail(GC_ERR_INVALID, "null out");
+  *out = nullptr;
+  gc_opts o;
+  if (opts) o = *opts; else gc_opts_default(&o);
+  RK(check_opts(&o));
+  gc_handle* h = new (std::nothrow) gc_handle();
+  if (!h) return fail(GC_ERR_OOM, "host allocation");
+  int w[1] = {width}, hh[1] = {height};
+  int r = h->pool.create(1, w, hh, &o);
+  if (r) { delete h; return r; }
+  *out = h;
+  return GC_OK;
+}
+
+int gc_destroy(gc_handle* h) {
+  if (!h) return GC_OK;
+  cudaSetDevice(h->pool.device);
+  delete h;
+  return GC_OK;
+}
+
+int gc_size(const gc_handle* h, int* w, int* hh) {
+  if (!h || !w || !hh) return fail(GC_ERR_INVALID, "null argument");
+  *w = h->pool.imgs[0].W;
+  *hh = h->pool.imgs[0].H;
+  return GC_OK;
+}
+
+int gc_upload(gc_handle* h, const int32_t* up, const int32_t* down, const int32_t* left,
+              const int32_t* right, const int32_t* excess, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  return h->pool.upload(0, up, down, left, right, excess, (cudaStream_t)stream);
+}
+
+int gc_upload_host(gc_handle* h, const int32_t* up, const int32_t* down, const int32_t* left,
+                   const int32_t* right, const int32_t* excess, void* stream) {
+  g_err.clear();
+  if (!h || !up || !down || !left || !right || !excess) return fail(GC_ERR_INVALID, "null argument");
+  Pool& p = h->pool;
+  CK(cudaSetDevice(p.device));
+  const size_t n = (size_t)p.imgs[0].W * p.imgs[0].H;
+  if (!p.stage) {
+    cudaError_t e = cudaMalloc((void**)&p.stage, 5 * n * sizeof(int32_t));
+    if (e) { p.stage = nullptr; cudaGetLastError(); return fail(GC_ERR_OOM, "staging buffer"); }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const int32_t* src[5] = {up, down, left, right, excess};
+  for (int k = 0; k < 5; ++k)
+    CK(cudaMemcpyAsync(p.stage + k * n, src[k], n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  int r = p.upload(0, p.stage, p.stage + n, p.stage + 2 * n, p.stage + 3 * n, p.stage + 4 * n, s);
+  if (r) return r;
+  CK(cudaStreamSynchronize(s));
+  return GC_OK;
+}
+
+int gc_solve(gc_handle* h, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  return h->pool.solve((cudaStream_t)stream);
+}
+
+int gc_flow(gc_handle* h, int64_t* flow) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  return h->pool.flow(0, flow);
+}
+
+int gc_labels(gc_handle* h, uint8_t* labels, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  return h->pool.labels(0, labels, (cudaStream_t)stream);
+}
+
+int gc_labels_host(gc_handle* h, uint8_t* labels, void* stream) {
+  g_err.clear();
+  if (!h || !labels) return fail(GC_ERR_INVALID, "null argument");
+  Pool& p = h->pool;
+  CK(cudaSetDevice(p.device));
+  const size_t n = (size_t)p.imgs[0].W * p.imgs[0].H;
+  if (!p.lstage) {
+    cudaError_t e = cudaMalloc((void**)&p.lstage, n);
+    if (e) { p.lstage = nullptr; cudaGetLastError(); return fail(GC_ERR_OOM, "label staging"); }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  RK(p.labels(0, p.lstage, s));
+  CK(cudaMemcpyAsync(labels, p.lstage, n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return GC_OK;
+}
+
+int gc_edit_tlinks(gc_handle* h, const int32_t* idx, const int32_t* value, int n, void* stream) {
+  g_err.clear();
+  if (!h || n < 0 || (n > 0 && (!idx || !value))) return fail(GC_ERR_INVALID, "bad argument");
+  Pool& p = h->pool;
+  if (!p.uploaded) return fail(GC_ERR_STATE, "edit before upload");
+  CK(cudaSetDevice(p.device));
+  RK(launch_edit(p.P, p.imgs[0], 0, idx, value, n, p.tl, p.acc, (cudaStream_t)stream));
+  p.edited = true;
+  p.bfs_fresh = false;
+  return GC_OK;
+}
+
+int gc_edit_stroke(gc_handle* h, const int32_t* xs, const int32_t* ys, int npts, int radius,
+                   int32_t value, void* stream) {
+  g_err.clear();
+  if (!h || !xs || !ys || npts < 1 || npts > 1024 || radius < 0 || radius > 4096)
+    return fail(GC_ERR_INVALID, "bad stroke");
+  Pool& p = h->pool;
+  if (!p.uploaded) return fail(GC_ERR_STATE, "edit before upload");
+  CK(cudaSetDevice(p.device));
+  if (!p.pts) {
+    cudaError_t e = cudaMalloc((void**)&p.pts, 2 * 1024 * sizeof(int32_t));
+    if (e) { p.pts = nullptr; cudaGetLastError(); return fail(GC_ERR_OOM, "stroke buffer"); }
+  }
+  std::vector<int32_t> pts(2 * npts);
+  for (int k = 0; k < npts; ++k) { pts[2 * k] = xs[k]; pts[2 * k + 1] = ys[k]; }
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(p.pts, pts.data(), pts.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  RK(launch_stroke(p.P, p.imgs[0], 0, p.pts, pts.data(), npts, radius, value, p.tl, p.acc, s));
+  CK(cudaStreamSynchronize(s));  // pts (host vector) must outlive the copy
+  p.edited = true;
+  p.bfs_fresh = false;
+  return GC_OK;
+}
+
+int gc_download_state(gc_handle* h, int32_t* excess, int32_t* height, int32_t* up,
+                      int32_t* down, int32_t* left, int32_t* right, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  Pool& p = h->pool;
+  CK(cudaSetDevice(p.device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const int32_t* planes[6] = {p.P.exc, p.P.hgt, p.P.cap[0], p.P.cap[1], p.P.cap[2], p.P.cap[3]};
+  int32_t* outs[6] = {excess, height, up, down, left, right};
+  for (int k = 0; k < 6; ++k)
+    if (outs[k]) RK(launch_state_out(p.P, p.imgs[0], planes[k], outs[k], s));
+  return GC_OK;
+}
+
+int gc_push(gc_handle* h, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  return h->pool.step_push((cudaStream_t)stream);
+}
+
+int gc_relabel(gc_handle* h, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  return h->pool.step_relabel((cudaStream_t)stream);
+}
+
+int gc_start_bfs(gc_handle* h, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  return h->pool.step_start_bfs((cudaStream_t)stream);
+}
+
+int gc_is_completed(gc_handle* h, int* completed, void* stream) {
+  g_err.clear();
+  if (!h || !completed) return fail(GC_ERR_INVALID, "null argument");
+  return h->pool.step_is_completed(completed, (cudaStream_t)stream);
+}
+
+int gc_get_stats(const gc_handle* h, gc_stats* st) {
+  if (!h || !st) return fail(GC_ERR_INVALID, "null argument");
+  *st = h->pool.stats;
+  return GC_OK;
+}
+
+int gc_set_profile(gc_handle* h, int on) {
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  h->pool.prof = on != 0;
+  return GC_OK;
+}
+
+int gc_get_profile(const gc_handle* h, gc_kernel_prof* out, int n) {
+  if (!h || !out || n < 0) return fail(GC_ERR_INVALID, "bad argument");
+  for (int k = 0; k < n && k < GC_NKERN; ++k) out[k] = h->pool.kprof[k];
+  return GC_OK;
+}
+
+const char* gc_kernel_name(int kind) {
+  static const char* names[GC_NKERN] = {"upload", "discharge", "edge_relabel_build", "bfs_first",
+                                        "bfs", "flood_first", "flood", "compact", "labels"};
+  return kind >= 0 && kind < GC_NKERN ? names[kind] : "";
+}
+
+int gc_set_collect_stats(gc_handle* h, int on) {
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  h->pool.collect = on != 0;
+  return GC_OK;
+}
+
+// ---- primitives -------------------------------------------------------------------
+int gc_scan_exclusive(const int32_t* in, int32_t* out, int32_t* total, int n, void* stream) {
+  g_err.clear();
+  if (n < 0 || (n > 0 && (!in || !out)) || !total) return fail(GC_ERR_INVALID, "bad argument");
+  ScanState st;
+  RK(device_scan_state(&st));
+  return launch_scan(GC_SCAN_MODE_SCAN, in, nullptr, nullptr, out, nullptr, total, n, 0, 0, 0,
+                     0, 0, st, (cudaStream_t)stream);
+}
+
+int gc_compact(const int32_t* flags, int32_t* list, int32_t* length, int n, void* stream) {
+  g_err.clear();
+  if (n < 0 || (n > 0 && (!flags || !list)) || !length) return fail(GC_ERR_INVALID, "bad argument");
+  if (n > 0 && flags == list) return fail(GC_ERR_INVALID, "list must not alias flags");
+  ScanState st;
+  RK(device_scan_state(&st));
+  return launch_scan(GC_SCAN_MODE_COMPACT, flags, nullptr, nullptr, nullptr, list, length, n, 0,
+                     0, 0, 0, 0, st, (cudaStream_t)stream);
+}
+
+int gc_tiles_build(const int32_t* tiles, int op, int32_t operand, int32_t* list,
+                   int32_t* length, int n, void* stream) {
+  g_err.clear();
+  if (n < 0 || (n > 0 && (!tiles || !list)) || !length || op < 0 || op > 4)
+    return fail(GC_ERR_INVALID, "bad argument");
+  ScanState st;
+  RK(device_scan_state(&st));
+  return launch_scan(GC_SCAN_MODE_FLAG, tiles, nullptr, nullptr, nullptr, list, length, n, op,
+                     operand, 0, 0, 0, st, (cudaStream_t)stream);
+}
+
+int gc_tiles_build_logical(const int32_t* tiles, const int32_t* tiles2, int op1, int32_t a1,
+                           int op2, int32_t a2, int logical, int32_t* list, int32_t* length,
+                           int n, void* stream) {
+  g_err.clear();
+  if (n < 0 || (n > 0 && (!tiles || !tiles2 || !list)) || !length || op1 < 0 || op1 > 4 ||
+      op2 < 0 || op2 > 4 || logical < 0 || logical > 1)
+    return fail(GC_ERR_INVALID, "bad argument");
+  ScanState st;
+  RK(device_scan_state(&st));
+  return launch_scan(GC_SCAN_MODE_LOGICAL, tiles, tiles2, nullptr, nullptr, list, length, n, op1,
+                     a1, op2, a2, logical, st, (cudaStream_t)stream);
+}
+
+int gc_tiles_incorporate(int32_t* tiles, const int32_t* tiles2, int op1, int32_t a1, int op2,
+                         int32_t a2, int logical, int32_t iteration, int n, void* stream) {
+  g_err.clear();
+  if (n < 0 || (n > 0 && (!tiles || !tiles2)) || op1 < 0 || op1 > 4 || op2 < 0 || op2 > 4 ||
+      logical < 0 || logical > 1)
+    return fail(GC_ERR_INVALID, "bad argument");
+  return launch_increment_logical(tiles, tiles2, tiles, n, op1, op2, a1, a2, logical, iteration,
+                                  (cudaStream_t)stream);
+}
+
+int gc_tiles_fill(int32_t* tiles, int32_t value, int n, void* stream) {
+  g_err.clear();
+  if (n < 0 || (n > 0 && !tiles)) return fail(GC_ERR_INVALID, "bad argument");
+  return launch_fill(tiles, n, value, (cudaStream_t)stream);
+}
+
+// ---- batch ------------------------------------------------------------------------
+int gcb_create(int n, const int* widths, const int* heights, const gc_opts* opts,
+               gcb_handle** out) {
+  g_err.clear();
+  if (!out) return fail(GC_ERR_INVALID, "null out");
+  *out = nullptr;
+  gc_opts o;
+  if (opts) o = *opts; else gc_opts_default(&o);
+  RK(check_opts(&o));
+  gcb_handle* b = new (std::nothrow) gcb_handle();
+  if (!b) return fail(GC_ERR_OOM, "host allocation");
+  int r = b->pool.create(n, widths, heights, &o);
+  if (r) { delete b; return r; }
+  *out = b;
+  return GC_OK;
+}
+
+int gcb_destroy(gcb_handle* b) {
+  if (!b) return GC_OK;
+  cudaSetDevice(b->pool.device);
+  delete b;
+  return GC_OK;
+}
+
+int gcb_upload(gcb_handle* b, int i, const int32_t* up, const int32_t* down,
+               const int32_t* left, const int32_t* right, const int32_t* excess, void* stream) {
+  g_err.clear();
+  if (!b) return fail(GC_ERR_INVALID, "null handle");
+  Pool& p = b->pool;
+  int r = p.upload(i, up, down, left, right, excess, (cudaStream_t)stream);
+  return r;
+}
+
+int gcb_solve(gcb_handle* b, void* stream) {
+  g_err.clear();
+  if (!b) return fail(GC_ERR_INVALID, "null handle");
+  return b->pool.solve((cudaStream_t)stream);
+}
+
+int gcb_flow(gcb_handle* b, int i, int64_t* flow) {
+  g_err.clear();
+  if (!b) return fail(GC_ERR_INVALID, "null handle");
+  return b->pool.flow(i, flow);
+}
+
+int gcb_labels(gcb_handle* b, int i, uint8_t* labels, void* stream) {
+  g_err.clear();
+  if (!b) return fail(GC_ERR_INVALID, "null handle");
+  return b->pool.labels(i, labels, (cudaStream_t)stream);
+}
+
+int gcb_set_profile(gcb_handle* b, int on) {
+  if (!b) return fail(GC_ERR_INVALID, "null handle");
+  b->pool.prof = on != 0;
+  return GC_OK;
+}
+
+int gcb_get_profile(const gcb_handle* b, gc_kernel_prof* out, int n) {
+  if (!b || !out || n < 0) return fail(GC_ERR_INVALID, "bad argument");
+  for (int k = 0; k < n && k < GC_NKERN; ++k) out[k] = b->pool.kprof[k];
+  return GC_OK;
+}
+
+int gcb_get_stats(const gcb_handle* b, gc_stats* st) {
+  if (!b || !st) return fail(GC_ERR_INVALID, "null argument");
+  *st = b->pool.stats;
+  return GC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,152 @@
+// Shared definitions for the sm_100a tiled push-relabel graph cut.
+//
+// Data layout in HBM (tile-major "tile pool"):
+//   A pool holds NT tiles of 32x32 pixels, possibly from several images.  Every per-pixel
+//   plane is stored tile after tile: plane[t * 1024 + r * 32 + c] is pixel (r, c) of tile t,
+//   so one tile of one plane is a contiguous 4 KiB block and a warp reading a tile row reads
+//   one 128-byte line.  Planes: excess (signed t-link + net inflow), height, and the four
+//   residual capacities cap_up/down/left/right (edge from the pixel to that neighbour).
+//   Per tile: its four neighbour tile ids (-1 outside the image), 32-bit row masks used by
+//   the bit-parallel BFS (residual edge present per direction, sink pixels, excess pixels,
+//   reachable pixels) and small int flags.
+//
+// All arithmetic is int32 (int64 for the flow sums); heights use HINF for "cannot reach a
+// sink pixel".
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define GC_TILE 32
+#define GC_TILE_PX 1024
+#define GC_HINF 0x3fffffff
+
+namespace gcut {
+
+enum { DUP = 0, DDOWN = 1, DLEFT = 2, DRIGHT = 3 };
+
+// Device view of a tile pool.  All pointers are device pointers.
+struct PoolView {
+  int nt;                 // tiles in the pool
+  int32_t* exc;           // [nt][1024]
+  int32_t* hgt;           // [nt][1024]
+  int32_t* cap[4];        // [nt][1024] each: up, down, left, right
+  int4* nbr;              // [nt] neighbour tile ids (up, down, left, right), -1 if none
+  uint32_t* mcan;         // [nt][4][32] residual-edge row masks (up, down, left, right)
+  uint32_t* msink;        // [nt][32]   excess < 0
+  uint32_t* mexc;         // [nt][32]   excess > 0
+  uint32_t* mreach;       // [nt][32]   reachable from an excess pixel (canonical cut)
+  int32_t* touched;       // [nt] tile was discharged or received cross-tile flow
+  int32_t* act_int;       // [nt] tile has an active interior pixel after its discharge
+  int32_t* mark;          // [nt] BFS / flood-fill frontier marks
+  int32_t* tact;          // [nt] tile has an active pixel (excess > 0, height < HINF)
+  int32_t* img_of;        // [nt] image index of the tile
+  unsigned long long* ktiles;  // [K_COUNT] tiles processed per kernel kind (profiling)
+};
+
+// Kernel kinds for profiling (launch counts, event time, tiles processed).
+enum KernelKind { K_UPLOAD = 0, K_DISCHARGE, K_EDGE_BUILD, K_BFS_FIRST, K_BFS, K_FLOOD_FIRST,
+                  K_FLOOD, K_COMPACT, K_LABELS, K_COUNT };
+
+// Decoupled look-back bookkeeping (single-pass scan).  status[] words are tagged with the
+// launch sequence number, so no reset is needed between launches.
+struct ScanState {
+  unsigned long long* status;  // [max chunks]
+  int32_t* ticket;             // dynamic chunk ids (reset by the last CTA)
+  int32_t* done;               // finished CTAs (reset by the last CTA)
+  uint32_t* seq;               // launch sequence tag (bumped by the last CTA)
+  int32_t* err;                // set when a look-back wait gives up
+  int max_chunks;
+};
+
+enum ScanStateFlag : unsigned { SS_NONE = 0, SS_AGG = 1, SS_PREFIX = 2 };
+
+__device__ __forceinline__ unsigned long long ss_pack(uint32_t tag, unsigned st, int32_t v) {
+  return ((unsigned long long)(tag & 0x3fffffffu) << 34) | ((unsigned long long)st << 32) |
+         (unsigned long long)(uint32_t)v;
+}
+
+// Spin limit for look-back waits: after this many polls the wait gives up, records an
+// error and continues, so a scheduling anomaly can never hang the GPU.
+#define GC_SPIN_LIMIT (1 << 22)
+
+// Called by one thread (thread 0) of the CTA owning chunk `chunk` after it knows its own
+// aggregate.  Publishes the aggregate, walks back over predecessors and returns the
+// exclusive prefix of the chunk.  Chunks are numbered by arrival ticket, so every
+// predecessor belongs to a CTA that is already running.
+__device__ __forceinline__ int32_t lookback_exclusive(const ScanState& st, uint32_t tag,
+                                                      int chunk, int32_t aggregate) {
+  volatile unsigned long long* status = st.status;
+  if (chunk == 0) {
+    __threadfence();
+    status[0] = ss_pack(tag, SS_PREFIX, aggregate);
+    return 0;
+  }
+  status[chunk] = ss_pack(tag, SS_AGG, aggregate);
+  __threadfence();
+  int32_t excl = 0;
+  int j = chunk - 1;
+  int spins = 0;
+  while (j >= 0) {
+    unsigned long long s = status[j];
+    uint32_t stag = (uint32_t)(s >> 34);
+    unsigned sst = (unsigned)((s >> 32) & 3u);
+    if (stag != (tag & 0x3fffffffu) || sst == SS_NONE) {
+      if (++spins > GC_SPIN_LIMIT) {
+        atomicExch(st.err, 1);
+        break;
+      }
+      __nanosleep(32);
+      continue;
+    }
+    excl += (int32_t)(uint32_t)(s & 0xffffffffull);
+    if (sst == SS_PREFIX) break;
+    --j;
+  }
+  __threadfence();
+  status[chunk] = ss_pack(tag, SS_PREFIX, excl + aggregate);
+  return excl;
+}
+
+// Last CTA to finish resets the tickets and bumps the tag for the next launch.
+__device__ __forceinline__ void scan_finish(const ScanState& st, int nchunks) {
+  __threadfence();
+  int d = atomicAdd(st.done, 1);
+  if (d == nchunks - 1) {
+    *st.ticket = 0;
+    *st.done = 0;
+    uint32_t s = *st.seq + 1;
+    if ((s & 0x3fffffffu) == 0) s = 1;
+    *st.seq = s;
+    __threadfence();
+  }
+}
+
+// Block-wide exclusive scan of one int per thread (blockDim.x multiple of 32, <= 1024).
+// Returns the exclusive prefix; *total gets the block sum.  `sm` needs 32 ints.
+__device__ __forceinline__ int32_t block_exclusive_scan(int32_t v, int32_t* sm, int32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int32_t w = lane < nw ? sm[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int32_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    sm[lane] = w;  // inclusive warp prefix
+  }
+  __syncthreads();
+  int32_t base = warp ? sm[warp - 1] : 0;
+  *total = sm[nw - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+}  // namespace gcut

@@ -1,0 +1,74 @@
+// Internal interfaces between the translation units of libgcut.so.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/gcut.h"
+#include "gcut_common.cuh"
+
+static_assert(gcut::K_COUNT == GC_NKERN, "kernel kinds");
+
+namespace gcut {
+
+enum ScanMode {
+  GC_SCAN_MODE_SCAN = 0,     // exclusive scan of values
+  GC_SCAN_MODE_COMPACT = 1,  // indices of non-zero values
+  GC_SCAN_MODE_FLAG = 2,     // indices where op1(in, a1)
+  GC_SCAN_MODE_LOGICAL = 3,  // indices where op1(in, a1) AND/OR op2(in2, a2)
+};
+
+int scan_chunks(int n);
+int launch_scan(int mode, const int32_t* in, const int32_t* in2, int32_t* clear,
+                int32_t* scan_out, int32_t* list_out, int32_t* total_out, int n, int op1,
+                int32_t a1, int op2, int32_t a2, int logical, const ScanState& st,
+                cudaStream_t s);
+int launch_increment_logical(const int32_t* in1, const int32_t* in2, int32_t* out, int n,
+                             int op1, int op2, int32_t a1, int32_t a2, int logical,
+                             int32_t iteration, cudaStream_t s);
+int launch_fill(int32_t* p, int n, int32_t v, cudaStream_t s);
+
+// One image inside a tile pool.
+struct ImageDesc {
+  int W, H;      // pixel size
+  int tw, th;    // tile grid
+  int tile0;     // first tile id; tiles are row-major from there
+};
+
+// Per-image accumulators on the device.
+struct ImageAcc {
+  unsigned long long sumpos_t;   // sum max(t-link, 0)  (two's complement int64)
+  unsigned long long sumpos_e;   // sum max(excess, 0) at the end of a solve
+  int32_t bad_caps;              // negative capacities seen at upload
+  int32_t pad;
+};
+
+// Solver kernels (gcut_solver.cu).
+struct Launch {
+  int grid_discharge;   // persistent CTAs for the discharge kernel
+  int grid_warps;       // CTAs (4 warps each) for the per-tile warp kernels
+};
+
+int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t* up,
+                  const int32_t* down, const int32_t* left, const int32_t* right,
+                  const int32_t* excess, int32_t* tl, ImageAcc* acc, cudaStream_t s);
+int launch_discharge(const PoolView& P, const int32_t* list, const int32_t* count, int iters,
+                     int grid, cudaStream_t s);
+int launch_edge_relabel_build(const PoolView& P, int32_t* list, int32_t* count,
+                              const ScanState& st, cudaStream_t s);
+int launch_bfs_round(const PoolView& P, const int32_t* list, const int32_t* count, int first,
+                     int grid, cudaStream_t s);
+int launch_flood_round(const PoolView& P, const int32_t* list, const int32_t* count, int first,
+                       ImageAcc* acc, int grid, cudaStream_t s);
+int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s);
+int launch_state_out(const PoolView& P, const ImageDesc& im, const int32_t* plane,
+                     int32_t* out, cudaStream_t s);
+int launch_edit(const PoolView& P, const ImageDesc& im, int img, const int32_t* idx,
+                const int32_t* val, int n, int32_t* tl, ImageAcc* acc, cudaStream_t s);
+// pts_dev / pts_host: the same (x, y) pairs on the device and on the host (for the bounds).
+int launch_stroke(const PoolView& P, const ImageDesc& im, int img, const int32_t* pts_dev,
+                  const int32_t* pts_host, int npts, int radius, int32_t value, int32_t* tl,
+                  ImageAcc* acc, cudaStream_t s);
+int occupancy_discharge(int device);
+int occupancy_warps(int device);
+
+}  // namespace gcut

@@ -1,0 +1,143 @@
+// Single-pass decoupled look-back scan and stream compaction (sm_100a).
+//
+// Replaces the reference's multi-launch Blelloch scan (prefixsum.cl:81-212, driven by
+// PrefixSum.pyx:83-129), the scatter of streamcompact.cl:1-14 (StreamCompact.pyx:66-82)
+// and the stamp predicates of incremental_tile_list.cl:40-154 (IncrementalTileList.pyx:
+// 119-176).  One launch per scan/compaction: each CTA takes a chunk of 4096 items by
+// arrival ticket, reduces it, publishes its aggregate and looks back over its
+// predecessors' published prefixes.  The predicate is evaluated while loading, so the
+// "flag" kernel of the reference disappears into the scan.  Compaction writes to a list
+// separate from the flags (the reference scans in place into the list and then scatters
+// into the same buffer, StreamCompact.pyx:72-81).
+#include "gcut_common.cuh"
+#include "gcut_internal.h"
+
+namespace gcut {
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 16;
+constexpr int SCAN_CHUNK = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ bool op_apply(int op, int32_t v, int32_t a) {
+  switch (op) {
+    case 0: return v == a;   // OPERATOR_EQUAL
+    case 1: return v > a;    // OPERATOR_GT
+    case 2: return v < a;    // OPERATOR_LT
+    case 3: return v >= a;   // OPERATOR_GTE
+    default: return v <= a;  // OPERATOR_LTE
+  }
+}
+
+struct ScanArgs {
+  const int32_t* in;
+  const int32_t* in2;
+  int32_t* clear;        // optional: zeroed after reading (consumed flags)
+  int32_t* scan_out;     // MODE_SCAN: exclusive scan
+  int32_t* list_out;     // compaction modes: selected indices
+  int32_t* total_out;    // scan total / list length
+  int n;
+  int mode;
+  int op1, op2;
+  int32_t a1, a2;
+  int logical;           // 0 AND, 1 OR
+};
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan(ScanArgs a, ScanState st) {
+  __shared__ int32_t sm[32];
+  __shared__ int32_t s_chunk, s_excl;
+  __shared__ uint32_t s_tag;
+  if (threadIdx.x == 0) {
+    s_chunk = atomicAdd(st.ticket, 1);
+    s_tag = *((volatile uint32_t*)st.seq);
+  }
+  __syncthreads();
+  const int chunk = s_chunk;
+  const int nchunks = (a.n + SCAN_CHUNK - 1) / SCAN_CHUNK > 0 ? (a.n + SCAN_CHUNK - 1) / SCAN_CHUNK : 1;
+  const long long base = (long long)chunk * SCAN_CHUNK + (long long)threadIdx.x * SCAN_ITEMS;
+
+  int32_t v[SCAN_ITEMS];
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    long long i = base + k;
+    int32_t x = 0;
+    if (i < a.n) {
+      int32_t raw = a.in[i];
+      switch (a.mode) {
+        case GC_SCAN_MODE_SCAN: x = raw; break;
+        case GC_SCAN_MODE_COMPACT: x = raw != 0; break;
+        case GC_SCAN_MODE_FLAG: x = op_apply(a.op1, raw, a.a1); break;
+        default: {
+          bool f1 = op_apply(a.op1, raw, a.a1), f2 = op_apply(a.op2, a.in2[i], a.a2);
+          x = a.logical == 0 ? (f1 && f2) : (f1 || f2);
+        }
+      }
+      if (a.clear) a.clear[i] = 0;
+    }
+    v[k] = x;
+  }
+  int32_t tsum = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) tsum += v[k];
+  int32_t agg;
+  int32_t tex = block_exclusive_scan(tsum, sm, &agg);
+  if (threadIdx.x == 0) s_excl = lookback_exclusive(st, s_tag, chunk, agg);
+  __syncthreads();
+  int32_t run = s_excl + tex;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; ++k) {
+    long long i = base + k;
+    if (i < a.n) {
+      if (a.mode == GC_SCAN_MODE_SCAN) a.scan_out[i] = run;
+      else if (v[k]) a.list_out[run] = (int32_t)i;
+    }
+    run += v[k];
+  }
+  if (chunk == nchunks - 1 && threadIdx.x == 0 && a.total_out) *a.total_out = s_excl + agg;
+  if (threadIdx.x == 0) scan_finish(st, nchunks);
+}
+
+// IncrementalTileList.incorporate (incremental_tile_list.cl:110-154): stamp `iteration`
+// where the combined predicate holds.
+__global__ void k_increment_logical(const int32_t* in1, const int32_t* in2, int32_t* out,
+                                    int n, int op1, int op2, int32_t a1, int32_t a2,
+                                    int logical, int32_t iteration) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  bool f1 = op_apply(op1, in1[i], a1), f2 = op_apply(op2, in2[i], a2);
+  if (logical == 0 ? (f1 && f2) : (f1 || f2)) out[i] = iteration;
+}
+
+__global__ void k_fill(int32_t* p, int n, int32_t v) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+int scan_chunks(int n) { return n <= 0 ? 1 : (n + SCAN_CHUNK - 1) / SCAN_CHUNK; }
+
+int launch_scan(int mode, const int32_t* in, const int32_t* in2, int32_t* clear,
+                int32_t* scan_out, int32_t* list_out, int32_t* total_out, int n, int op1,
+                int32_t a1, int op2, int32_t a2, int logical, const ScanState& st,
+                cudaStream_t s) {
+  int nch = scan_chunks(n);
+  if (nch > st.max_chunks) return GC_ERR_INVALID;
+  ScanArgs a{in, in2, clear, scan_out, list_out, total_out, n, mode, op1, op2, a1, a2, logical};
+  k_scan<<<nch, SCAN_THREADS, 0, s>>>(a, st);
+  return cudaGetLastError() == cudaSuccess ? GC_OK : GC_ERR_CUDA;
+}
+
+int launch_increment_logical(const int32_t* in1, const int32_t* in2, int32_t* out, int n,
+                             int op1, int op2, int32_t a1, int32_t a2, int logical,
+                             int32_t iteration, cudaStream_t s) {
+  if (n <= 0) return GC_OK;
+  k_increment_logical<<<(n + 255) / 256, 256, 0, s>>>(in1, in2, out, n, op1, op2, a1, a2,
+                                                       logical, iteration);
+  return cudaGetLastError() == cudaSuccess ? GC_OK : GC_ERR_CUDA;
+}
+
+int launch_fill(int32_t* p, int n, int32_t v, cudaStream_t s) {
+  if (n <= 0) return GC_OK;
+  k_fill<<<(n + 255) / 256, 256, 0, s>>>(p, n, v);
+  return cudaGetLastError() == cudaSuccess ? GC_OK : GC_ERR_CUDA;
+}
+
+}  // namespace gcut

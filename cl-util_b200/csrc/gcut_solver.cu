@@ -1,0 +1,759 @@
+// Tiled push-relabel kernels for sm_100a.
+//
+// Reference path: GraphCut.cut (GraphCut.pyx:348-418) driving graphcut.cl.  The reference
+// runs one OpenCL kernel per push direction (push_down/up/right/left, graphcut.cl:158-536)
+// with an 8-pixel wave per work-item, merges tile overspill with add_border (:114-156),
+// relabels the whole image with a Jacobi pass (:538-577) and computes the global relabel
+// with init_bfs/bfs_intratile/bfs_intertile (:582-1016) over compacted tile lists.  Here:
+//
+//  * k_discharge   one CTA per active tile (persistent over the device-side list): the tile's
+//                  excess, height and four residual planes are loaded with int4 loads into
+//                  registers/shared memory together with the halo heights, and the CTA runs
+//                  `iters` rounds of {push along every admissible edge (all 4 directions),
+//                  Jacobi relabel of interior pixels}.  Flow leaving the tile is added to
+//                  the neighbour's excess and reverse residual with atomics (no border
+//                  buffer, no add_border launch).  Tile-edge pixels keep their height during
+//                  the launch, so every cross-tile push sees the true height of its target.
+//  * k_edge_relabel_build   relabels the active tile-edge pixels (Jacobi) and rebuilds the
+//                  active-tile list with the single-pass decoupled look-back compaction in
+//                  the same launch (IncrementalTileList.build + StreamCompact + PrefixSum).
+//  * k_bfs_round   exact global relabel: per tile, one warp runs a bit-parallel multi-source
+//                  BFS (32-bit row masks of residual edges, lane = row) seeded by sink
+//                  pixels and by the halo distances, and marks neighbours whose edge
+//                  distances changed; the marked tiles form the next frontier.
+//  * k_flood_round canonical cut: the same tile rounds flood the set reachable from excess
+//                  pixels over residual edges (the minimal source set).
+#include <cstdio>
+
+#include "gcut_common.cuh"
+#include "gcut_internal.h"
+
+namespace gcut {
+
+constexpr int DIS_THREADS = 256;
+
+__device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+
+// ------------------------------------------------------------------------------------
+// Upload: row-major planes -> tile planes; boundary capacities zeroed; padding pixels are
+// isolated (all zero).  Heights start at 0 for sink pixels and 1 otherwise (a valid
+// labelling).  Replaces init_gc + load_tiles (graphcut.cl:63-112, 1033-1132).
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(DIS_THREADS)
+k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
+         const int32_t* __restrict__ down, const int32_t* __restrict__ left,
+         const int32_t* __restrict__ right, const int32_t* __restrict__ excess,
+         int32_t* __restrict__ tl, ImageAcc* acc) {
+  const int bt = blockIdx.x;
+  const int tx = bt % im.tw, ty = bt / im.tw;
+  const int t = im.tile0 + bt;
+  const int r = threadIdx.x >> 3, c0 = (threadIdx.x & 7) * 4;
+  const int y = ty * GC_TILE + r;
+  int e[4], h[4], cu[4], cd[4], cl[4], cr[4];
+  long long pos = 0;
+  int bad = 0, anypos = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int x = tx * GC_TILE + c0 + j;
+    e[j] = cu[j] = cd[j] = cl[j] = cr[j] = 0;
+    if (x < im.W && y < im.H) {
+      const long long i = (long long)y * im.W + x;
+      e[j] = excess[i];
+      cu[j] = y > 0 ? up[i] : 0;
+      cd[j] = y < im.H - 1 ? down[i] : 0;
+      cl[j] = x > 0 ? left[i] : 0;
+      cr[j] = x < im.W - 1 ? right[i] : 0;
+      bad |= (cu[j] | cd[j] | cl[j] | cr[j]) < 0;
+    }
+    h[j] = e[j] < 0 ? 0 : 1;
+    pos += e[j] > 0 ? e[j] : 0;
+    anypos |= e[j] > 0;
+  }
+  const long long off = (long long)t * GC_TILE_PX + r * GC_TILE + c0;
+  *(int4*)(P.exc + off) = make_int4(e[0], e[1], e[2], e[3]);
+  *(int4*)(tl + off) = make_int4(e[0], e[1], e[2], e[3]);
+  *(int4*)(P.hgt + off) = make_int4(h[0], h[1], h[2], h[3]);
+  *(int4*)(P.cap[DUP] + off) = make_int4(cu[0], cu[1], cu[2], cu[3]);
+  *(int4*)(P.cap[DDOWN] + off) = make_int4(cd[0], cd[1], cd[2], cd[3]);
+  *(int4*)(P.cap[DLEFT] + off) = make_int4(cl[0], cl[1], cl[2], cl[3]);
+  *(int4*)(P.cap[DRIGHT] + off) = make_int4(cr[0], cr[1], cr[2], cr[3]);
+  // block reductions
+#pragma unroll
+  for (int o = 16; o; o >>= 1) pos += __shfl_xor_sync(0xffffffffu, pos, o);
+  bad = __syncthreads_or(bad);
+  anypos = __syncthreads_or(anypos);
+  if ((threadIdx.x & 31) == 0 && pos) atomicAdd(&acc[img].sumpos_t, (unsigned long long)pos);
+  if (threadIdx.x == 0) {
+    if (bad) atomicAdd(&acc[img].bad_caps, 1);
+    P.tact[t] = anypos;
+    P.touched[t] = 0;
+    P.act_int[t] = 0;
+    P.mark[t] = 0;
+    P.img_of[t] = img;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Discharge.  Thread (r, q) owns pixels (r, 4q .. 4q+3) of the tile.
+// ------------------------------------------------------------------------------------
+struct DisSmem {
+  int32_t hs[GC_TILE_PX];   // heights
+  int32_t fu[GC_TILE_PX];   // flow pushed up by each pixel this round
+  int32_t fd[GC_TILE_PX];   // flow pushed down
+  int32_t fl[GC_TILE * 8];  // flow pushed left by the first pixel of each 4-pixel strip
+  int32_t fr[GC_TILE * 8];  // flow pushed right by the last pixel of each strip
+  int32_t hu[GC_TILE], hd[GC_TILE], hl[GC_TILE], hr[GC_TILE];  // halo heights
+};
+
+__global__ void __launch_bounds__(DIS_THREADS)
+k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restrict__ count,
+            int iters) {
+  __shared__ DisSmem S;
+  const int tid = threadIdx.x;
+  const int r = tid >> 3, q = tid & 7, c0 = q * 4;
+  const int n = *count;
+  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+    const int t = list[li];
+    const int4 nb = P.nbr[t];
+    const long long off = (long long)t * GC_TILE_PX + r * GC_TILE + c0;
+    int e[4], h[4], cu[4], cd[4], cl[4], cr[4];
+    {
+      int4 v = *(const int4*)(P.exc + off); e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w;
+      v = *(const int4*)(P.hgt + off); h[0] = v.x; h[1] = v.y; h[2] = v.z; h[3] = v.w;
+      v = *(const int4*)(P.cap[DUP] + off); cu[0] = v.x; cu[1] = v.y; cu[2] = v.z; cu[3] = v.w;
+      v = *(const int4*)(P.cap[DDOWN] + off); cd[0] = v.x; cd[1] = v.y; cd[2] = v.z; cd[3] = v.w;
+      v = *(const int4*)(P.cap[DLEFT] + off); cl[0] = v.x; cl[1] = v.y; cl[2] = v.z; cl[3] = v.w;
+      v = *(const int4*)(P.cap[DRIGHT] + off); cr[0] = v.x; cr[1] = v.y; cr[2] = v.z; cr[3] = v.w;
+    }
+    int e0[4], cu0[4], cd0[4], cl0, cr0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) { e0[j] = e[j]; cu0[j] = cu[j]; cd0[j] = cd[j]; }
+    cl0 = cl[0];
+    cr0 = cr[3];
+    *(int4*)(S.hs + r * GC_TILE + c0) = make_int4(h[0], h[1], h[2], h[3]);
+    if (tid < 32) S.hu[tid] = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + tid] : GC_HINF;
+    else if (tid < 64) S.hd[tid - 32] = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + (tid - 32)] : GC_HINF;
+    else if (tid < 96) S.hl[tid - 64] = nb.z >= 0 ? P.hgt[(long long)nb.z * GC_TILE_PX + (tid - 64) * GC_TILE + 31] : GC_HINF;
+    else if (tid < 128) S.hr[tid - 96] = nb.w >= 0 ? P.hgt[(long long)nb.w * GC_TILE_PX + (tid - 96) * GC_TILE] : GC_HINF;
+    int xu[4] = {0, 0, 0, 0}, xd[4] = {0, 0, 0, 0}, xl = 0, xr = 0;  // cross-tile flow
+    __syncthreads();
+
+    for (int it = 0; it < iters; ++it) {
+      // neighbour heights (fixed during the push phase)
+      int hnu[4], hnd[4], hnl[4], hnr[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = c0 + j;
+        hnu[j] = r > 0 ? S.hs[(r - 1) * GC_TILE + c] : S.hu[c];
+        hnd[j] = r < 31 ? S.hs[(r + 1) * GC_TILE + c] : S.hd[c];
+      }
+      hnl[0] = c0 > 0 ? S.hs[r * GC_TILE + c0 - 1] : S.hl[r];
+      hnl[1] = h[0]; hnl[2] = h[1]; hnl[3] = h[2];
+      hnr[0] = h[1]; hnr[1] = h[2]; hnr[2] = h[3];
+      hnr[3] = c0 < 28 ? S.hs[r * GC_TILE + c0 + 4] : S.hr[r];
+
+      // push phase
+      int ou[4], od[4], ol[4], orr[4];
+      int changed = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        ou[j] = od[j] = ol[j] = orr[j] = 0;
+        int ej = e[j];
+        if (ej > 0 && h[j] < GC_HINF) {
+          if (cd[j] > 0 && h[j] == hnd[j] + 1) { int f = imin(ej, cd[j]); ej -= f; cd[j] -= f; od[j] = f; }
+          if (ej > 0 && cu[j] > 0 && h[j] == hnu[j] + 1) { int f = imin(ej, cu[j]); ej -= f; cu[j] -= f; ou[j] = f; }
+          if (ej > 0 && cr[j] > 0 && h[j] == hnr[j] + 1) { int f = imin(ej, cr[j]); ej -= f; cr[j] -= f; orr[j] = f; }
+          if (ej > 0 && cl[j] > 0 && h[j] == hnl[j] + 1) { int f = imin(ej, cl[j]); ej -= f; cl[j] -= f; ol[j] = f; }
+          changed |= ej != e[j];
+          e[j] = ej;
+        }
+      }
+      // flow leaving the tile is delivered at the end of the launch
+      if (r == 0) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { xu[j] += ou[j]; ou[j] = 0; }
+      }
+      if (r == 31) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) { xd[j] += od[j]; od[j] = 0; }
+      }
+      if (q == 0) { xl += ol[0]; ol[0] = 0; }
+      if (q == 7) { xr += orr[3]; orr[3] = 0; }
+      *(int4*)(S.fu + r * GC_TILE + c0) = make_int4(ou[0], ou[1], ou[2], ou[3]);
+      *(int4*)(S.fd + r * GC_TILE + c0) = make_int4(od[0], od[1], od[2], od[3]);
+      S.fl[r * 8 + q] = ol[0];
+      S.fr[r * 8 + q] = orr[3];
+      __syncthreads();
+      // gather inflow; a pixel receiving flow gains the reverse residual
+      {
+        int4 a = r < 31 ? *(const int4*)(S.fu + (r + 1) * GC_TILE + c0) : make_int4(0, 0, 0, 0);
+        int4 b = r > 0 ? *(const int4*)(S.fd + (r - 1) * GC_TILE + c0) : make_int4(0, 0, 0, 0);
+        int fb[4] = {a.x, a.y, a.z, a.w}, fa[4] = {b.x, b.y, b.z, b.w};
+        int fromleft[4], fromright[4];
+        fromleft[0] = q > 0 ? S.fr[r * 8 + q - 1] : 0;
+        fromleft[1] = orr[0]; fromleft[2] = orr[1]; fromleft[3] = orr[2];
+        fromright[0] = ol[1]; fromright[1] = ol[2]; fromright[2] = ol[3];
+        fromright[3] = q < 7 ? S.fl[r * 8 + q + 1] : 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          e[j] += fb[j] + fa[j] + fromleft[j] + fromright[j];
+          cd[j] += fb[j];
+          cu[j] += fa[j];
+          cl[j] += fromleft[j];
+          cr[j] += fromright[j];
+        }
+      }
+      // relabel phase (interior pixels; tile-edge pixels keep their height in this launch)
+      int nh[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        nh[j] = h[j];
+        const int c = c0 + j;
+        const bool interior = r > 0 && r < 31 && c > 0 && c < 31;
+        if (interior && e[j] > 0 && h[j] < GC_HINF) {
+          const bool adm = (cd[j] > 0 && h[j] == hnd[j] + 1) || (cu[j] > 0 && h[j] == hnu[j] + 1) ||
+                           (cr[j] > 0 && h[j] == hnr[j] + 1) || (cl[j] > 0 && h[j] == hnl[j] + 1);
+          if (!adm) {
+            int m = GC_HINF;
+            if (cd[j] > 0) m = imin(m, hnd[j] + 1);
+            if (cu[j] > 0) m = imin(m, hnu[j] + 1);
+            if (cr[j] > 0) m = imin(m, hnr[j] + 1);
+            if (cl[j] > 0) m = imin(m, hnl[j] + 1);
+            nh[j] = imin(m, GC_HINF);
+            changed |= nh[j] != h[j];
+          }
+        }
+      }
+      __syncthreads();  // all reads of S.hs / flow buffers of this round are done
+#pragma unroll
+      for (int j = 0; j < 4; ++j) h[j] = nh[j];
+      *(int4*)(S.hs + r * GC_TILE + c0) = make_int4(h[0], h[1], h[2], h[3]);
+      if (!__syncthreads_or(changed)) break;
+    }
+
+    // write back: interior values are owned by this CTA; tile-edge excess and the
+    // outward residual of edge pixels also receive atomics from neighbouring tiles, so
+    // they are written as deltas.
+    const bool edge_row = (r == 0) || (r == 31);
+    if (!edge_row && q > 0 && q < 7) {
+      *(int4*)(P.exc + off) = make_int4(e[0], e[1], e[2], e[3]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = c0 + j;
+        if (edge_row || c == 0 || c == 31) {
+          if (e[j] != e0[j]) atomicAdd(P.exc + off + j, e[j] - e0[j]);
+        } else {
+          P.exc[off + j] = e[j];
+        }
+      }
+    }
+    *(int4*)(P.hgt + off) = make_int4(h[0], h[1], h[2], h[3]);
+    if (r == 0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) if (cu[j] != cu0[j]) atomicAdd(P.cap[DUP] + off + j, cu[j] - cu0[j]);
+    } else {
+      *(int4*)(P.cap[DUP] + off) = make_int4(cu[0], cu[1], cu[2], cu[3]);
+    }
+    if (r == 31) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) if (cd[j] != cd0[j]) atomicAdd(P.cap[DDOWN] + off + j, cd[j] - cd0[j]);
+    } else {
+      *(int4*)(P.cap[DDOWN] + off) = make_int4(cd[0], cd[1], cd[2], cd[3]);
+    }
+    if (q == 0) {
+      if (cl[0] != cl0) atomicAdd(P.cap[DLEFT] + off, cl[0] - cl0);
+      P.cap[DLEFT][off + 1] = cl[1]; P.cap[DLEFT][off + 2] = cl[2]; P.cap[DLEFT][off + 3] = cl[3];
+    } else {
+      *(int4*)(P.cap[DLEFT] + off) = make_int4(cl[0], cl[1], cl[2], cl[3]);
+    }
+    if (q == 7) {
+      if (cr[3] != cr0) atomicAdd(P.cap[DRIGHT] + off + 3, cr[3] - cr0);
+      P.cap[DRIGHT][off] = cr[0]; P.cap[DRIGHT][off + 1] = cr[1]; P.cap[DRIGHT][off + 2] = cr[2];
+    } else {
+      *(int4*)(P.cap[DRIGHT] + off) = make_int4(cr[0], cr[1], cr[2], cr[3]);
+    }
+    // deliver cross-tile flow: excess of the neighbour pixel and its reverse residual
+    int sent_u = 0, sent_d = 0, sent_l = 0, sent_r = 0;
+    if (r == 0 && nb.x >= 0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) if (xu[j]) {
+        long long o = (long long)nb.x * GC_TILE_PX + 31 * GC_TILE + c0 + j;
+        atomicAdd(P.exc + o, xu[j]); atomicAdd(P.cap[DDOWN] + o, xu[j]); sent_u = 1;
+      }
+    }
+    if (r == 31 && nb.y >= 0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) if (xd[j]) {
+        long long o = (long long)nb.y * GC_TILE_PX + c0 + j;
+        atomicAdd(P.exc + o, xd[j]); atomicAdd(P.cap[DUP] + o, xd[j]); sent_d = 1;
+      }
+    }
+    if (q == 0 && xl && nb.z >= 0) {
+      long long o = (long long)nb.z * GC_TILE_PX + r * GC_TILE + 31;
+      atomicAdd(P.exc + o, xl); atomicAdd(P.cap[DRIGHT] + o, xl); sent_l = 1;
+    }
+    if (q == 7 && xr && nb.w >= 0) {
+      long long o = (long long)nb.w * GC_TILE_PX + r * GC_TILE;
+      atomicAdd(P.exc + o, xr); atomicAdd(P.cap[DLEFT] + o, xr); sent_r = 1;
+    }
+    if (sent_u) P.touched[nb.x] = 1;
+    if (sent_d) P.touched[nb.y] = 1;
+    if (sent_l) P.touched[nb.z] = 1;
+    if (sent_r) P.touched[nb.w] = 1;
+    int act = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + j;
+      act |= (r > 0 && r < 31 && c > 0 && c < 31 && e[j] > 0 && h[j] < GC_HINF);
+    }
+    act = __syncthreads_or(act);
+    if (tid == 0) {
+      P.touched[t] = 1;
+      P.act_int[t] = act;
+      if (P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Edge relabel + active-tile list (one launch).  CTA = 256 tiles by arrival ticket; warp w
+// walks 32 of them.  A tile is active when an interior pixel was active after its
+// discharge or a tile-edge pixel is active after this relabel.
+// ------------------------------------------------------------------------------------
+constexpr int EB_THREADS = 256;
+constexpr int EB_TILES = 256;
+
+__device__ __forceinline__ int edge_relabel_pixel(const PoolView& P, int t, int4 nb, int r,
+                                                  int c) {
+  const long long o = (long long)t * GC_TILE_PX + r * GC_TILE + c;
+  const int e = P.exc[o];
+  const int h = P.hgt[o];
+  if (!(e > 0 && h < GC_HINF)) return 0;
+  const int cu = P.cap[DUP][o], cd = P.cap[DDOWN][o], cl = P.cap[DLEFT][o], cr = P.cap[DRIGHT][o];
+  int hu = GC_HINF, hd = GC_HINF, hl = GC_HINF, hr = GC_HINF;
+  if (r > 0) hu = P.hgt[o - GC_TILE]; else if (nb.x >= 0) hu = P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + c];
+  if (r < 31) hd = P.hgt[o + GC_TILE]; else if (nb.y >= 0) hd = P.hgt[(long long)nb.y * GC_TILE_PX + c];
+  if (c > 0) hl = P.hgt[o - 1]; else if (nb.z >= 0) hl = P.hgt[(long long)nb.z * GC_TILE_PX + r * GC_TILE + 31];
+  if (c < 31) hr = P.hgt[o + 1]; else if (nb.w >= 0) hr = P.hgt[(long long)nb.w * GC_TILE_PX + r * GC_TILE];
+  const bool adm = (cu > 0 && h == hu + 1) || (cd > 0 && h == hd + 1) || (cl > 0 && h == hl + 1) ||
+                   (cr > 0 && h == hr + 1);
+  if (adm) return 1;
+  int m = GC_HINF;
+  if (cu > 0) m = imin(m, hu + 1);
+  if (cd > 0) m = imin(m, hd + 1);
+  if (cl > 0) m = imin(m, hl + 1);
+  if (cr > 0) m = imin(m, hr + 1);
+  m = imin(m, GC_HINF);
+  if (m != h) P.hgt[o] = m;
+  return m < GC_HINF;
+}
+
+__global__ void __launch_bounds__(EB_THREADS)
+k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
+  __shared__ int32_t sm[32];
+  __shared__ int32_t s_chunk, s_excl;
+  __shared__ uint32_t s_tag;
+  __shared__ int32_t flag[EB_TILES];
+  if (threadIdx.x == 0) {
+    s_chunk = atomicAdd(st.ticket, 1);
+    s_tag = *((volatile uint32_t*)st.seq);
+  }
+  __syncthreads();
+  const int chunk = s_chunk;
+  const int nchunks = (P.nt + EB_TILES - 1) / EB_TILES;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < 32; ++k) {
+    const int slot = warp * 32 + k;
+    const int t = chunk * EB_TILES + slot;
+    int active = 0;
+    if (t < P.nt && P.touched[t]) {
+      const int4 nb = P.nbr[t];
+      int a = edge_relabel_pixel(P, t, nb, 0, lane);
+      a |= edge_relabel_pixel(P, t, nb, 31, lane);
+      if (lane > 0 && lane < 31) {
+        a |= edge_relabel_pixel(P, t, nb, lane, 0);
+        a |= edge_relabel_pixel(P, t, nb, lane, 31);
+      }
+      active = __any_sync(0xffffffffu, a) | P.act_int[t];
+      if (lane == 0) {
+        P.touched[t] = 0;
+        if (P.ktiles) atomicAdd(&P.ktiles[K_EDGE_BUILD], 1ull);
+      }
+    }
+    if (lane == 0) flag[slot] = active;
+  }
+  __syncthreads();
+  const int v = flag[threadIdx.x];
+  int32_t agg;
+  const int32_t ex = block_exclusive_scan(v, sm, &agg);
+  if (threadIdx.x == 0) s_excl = lookback_exclusive(st, s_tag, chunk, agg);
+  __syncthreads();
+  if (v) list[s_excl + ex] = chunk * EB_TILES + threadIdx.x;
+  if (chunk == nchunks - 1 && threadIdx.x == 0) *count = s_excl + agg;
+  if (threadIdx.x == 0) scan_finish(st, nchunks);
+}
+
+// ------------------------------------------------------------------------------------
+// Global relabel: bit-parallel BFS per tile, one warp per tile, lane = row.
+// ------------------------------------------------------------------------------------
+constexpr int WARPS_PER_CTA = 4;
+
+// Loads 32 rows of a per-pixel predicate as row masks: lane r receives the mask of row r.
+template <class F>
+__device__ __forceinline__ uint32_t rows_ballot(const int32_t* __restrict__ plane, int lane, F f) {
+  uint32_t mine = 0;
+#pragma unroll 4
+  for (int rr = 0; rr < 32; ++rr) {
+    const uint32_t b = __ballot_sync(0xffffffffu, f(plane[rr * GC_TILE + lane]));
+    if (lane == rr) mine = b;
+  }
+  return mine;
+}
+
+__device__ __forceinline__ int warp_min(int v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v = imin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Multi-source BFS inside a tile: d[] holds the seeds (GC_HINF elsewhere); on return d[]
+// holds the exact distances given the seeds, where an edge u -> v of the residual graph
+// lets u take d(v) + 1.
+__device__ __forceinline__ void tile_bfs(int (&d)[32], uint32_t canU, uint32_t canD,
+                                         uint32_t canL, uint32_t canR, int lane) {
+  uint32_t vis = 0;
+  for (int guard = 0; guard < 2 * GC_TILE_PX + 2; ++guard) {
+    int m = GC_HINF;
+#pragma unroll
+    for (int c = 0; c < 32; ++c) if (!((vis >> c) & 1u)) m = imin(m, d[c]);
+    m = warp_min(m);
+    if (m >= GC_HINF) break;
+    uint32_t F = 0;
+#pragma unroll
+    for (int c = 0; c < 32; ++c) F |= (uint32_t)(d[c] == m) << c;
+    F &= ~vis;
+    vis |= F;
+    uint32_t Fu = __shfl_up_sync(0xffffffffu, F, 1);
+    uint32_t Fd = __shfl_down_sync(0xffffffffu, F, 1);
+    if (lane == 0) Fu = 0;
+    if (lane == 31) Fd = 0;
+    uint32_t N = ((F >> 1) & canR) | ((F << 1) & canL) | (Fu & canU) | (Fd & canD);
+    N &= ~vis;
+    if (N) {
+#pragma unroll
+      for (int c = 0; c < 32; ++c) if ((N >> c) & 1u) d[c] = imin(d[c], m + 1);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(WARPS_PER_CTA * 32)
+k_bfs_round(PoolView P, const int32_t* __restrict__ list, const int32_t* __restrict__ count,
+            int first) {
+  __shared__ int32_t tr[WARPS_PER_CTA][32 * 33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n = first ? P.nt : *count;
+  int32_t* T = tr[warp];
+  for (int w = blockIdx.x * WARPS_PER_CTA + warp; w < n; w += gridDim.x * WARPS_PER_CTA) {
+    const int t = first ? w : list[w];
+    const int4 nb = P.nbr[t];
+    const long long base = (long long)t * GC_TILE_PX;
+    uint32_t canU, canD, canL, canR, sink;
+    if (first) {
+      canU = rows_ballot(P.cap[DUP] + base, lane, [](int v) { return v > 0; });
+      canD = rows_ballot(P.cap[DDOWN] + base, lane, [](int v) { return v > 0; });
+      canL = rows_ballot(P.cap[DLEFT] + base, lane, [](int v) { return v > 0; });
+      canR = rows_ballot(P.cap[DRIGHT] + base, lane, [](int v) { return v > 0; });
+      sink = rows_ballot(P.exc + base, lane, [](int v) { return v < 0; });
+      const uint32_t pos = rows_ballot(P.exc + base, lane, [](int v) { return v > 0; });
+      uint32_t* mc = P.mcan + (long long)t * 128;
+      mc[lane] = canU; mc[32 + lane] = canD; mc[64 + lane] = canL; mc[96 + lane] = canR;
+      P.msink[(long long)t * 32 + lane] = sink;
+      P.mexc[(long long)t * 32 + lane] = pos;
+    } else {
+      const uint32_t* mc = P.mcan + (long long)t * 128;
+      canU = mc[lane]; canD = mc[32 + lane]; canL = mc[64 + lane]; canR = mc[96 + lane];
+      sink = P.msink[(long long)t * 32 + lane];
+    }
+    int d[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) d[c] = ((sink >> c) & 1u) ? 0 : GC_HINF;
+    if (!first) {
+      // halo seeds: an edge pixel with a residual edge into the neighbour tile
+      int vu = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + lane] : GC_HINF;
+      int vd = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + lane] : GC_HINF;
+      const int vl = nb.z >= 0 ? P.hgt[(long long)nb.z * GC_TILE_PX + lane * GC_TILE + 31] : GC_HINF;
+      const int vr = nb.w >= 0 ? P.hgt[(long long)nb.w * GC_TILE_PX + lane * GC_TILE] : GC_HINF;
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        const int a = __shfl_sync(0xffffffffu, vu, c);
+        const int b = __shfl_sync(0xffffffffu, vd, c);
+        if (lane == 0 && ((canU >> c) & 1u) && a < GC_HINF) d[c] = imin(d[c], a + 1);
+        if (lane == 31 && ((canD >> c) & 1u) && b < GC_HINF) d[c] = imin(d[c], b + 1);
+      }
+      if ((canL & 1u) && vl < GC_HINF) d[0] = imin(d[0], vl + 1);
+      if ((canR >> 31) && vr < GC_HINF) d[31] = imin(d[31], vr + 1);
+    }
+    tile_bfs(d, canU, canD, canL, canR, lane);
+    // transpose through shared memory and write the distances back (coalesced rows)
+#pragma unroll
+    for (int c = 0; c < 32; ++c) T[lane * 33 + c] = d[c];
+    __syncwarp();
+    int chU = 0, chD = 0, chL = 0, chR = 0;
+    uint32_t fin = 0;
+#pragma unroll
+    for (int c = 0; c < 32; ++c) fin |= (uint32_t)(d[c] < GC_HINF) << c;
+    for (int rr = 0; rr < 32; ++rr) {
+      const int nv = T[rr * 33 + lane];
+      int* p = P.hgt + base + rr * GC_TILE + lane;
+      if (first) {
+        *p = nv;
+        const int fv = nv < GC_HINF;
+        chU |= (rr == 0) & fv; chD |= (rr == 31) & fv; chL |= (lane == 0) & fv; chR |= (lane == 31) & fv;
+      } else {
+        const int ov = *p;
+        if (nv != ov) *p = nv;
+        const int dec = nv < ov;
+        chU |= (rr == 0) & dec; chD |= (rr == 31) & dec; chL |= (lane == 0) & dec; chR |= (lane == 31) & dec;
+      }
+    }
+    __syncwarp();
+    chU = __any_sync(0xffffffffu, chU); chD = __any_sync(0xffffffffu, chD);
+    chL = __any_sync(0xffffffffu, chL); chR = __any_sync(0xffffffffu, chR);
+    const uint32_t pos = P.mexc[(long long)t * 32 + lane];
+    const int act = __any_sync(0xffffffffu, (pos & fin) != 0);
+    if (lane == 0) {
+      P.tact[t] = act;
+      if (P.ktiles) atomicAdd(&P.ktiles[first ? K_BFS_FIRST : K_BFS], 1ull);
+      if (chU && nb.x >= 0) P.mark[nb.x] = 1;
+      if (chD && nb.y >= 0) P.mark[nb.y] = 1;
+      if (chL && nb.z >= 0) P.mark[nb.z] = 1;
+      if (chR && nb.w >= 0) P.mark[nb.w] = 1;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Canonical cut: flood from excess pixels over residual edges (forward direction).
+// Round 1 also sums max(excess, 0) per image for the flow value.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(WARPS_PER_CTA * 32)
+k_flood_round(PoolView P, const int32_t* __restrict__ list, const int32_t* __restrict__ count,
+              int first, ImageAcc* acc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int n = first ? P.nt : *count;
+  for (int w = blockIdx.x * WARPS_PER_CTA + warp; w < n; w += gridDim.x * WARPS_PER_CTA) {
+    const int t = first ? w : list[w];
+    const int4 nb = P.nbr[t];
+    const uint32_t* mc = P.mcan + (long long)t * 128;
+    const uint32_t canU = mc[lane], canD = mc[32 + lane], canL = mc[64 + lane], canR = mc[96 + lane];
+    uint32_t R, R0;
+    if (first) {
+      R = P.mexc[(long long)t * 32 + lane];
+      R0 = 0;
+      long long s = 0;
+      const int32_t* ep = P.exc + (long long)t * GC_TILE_PX;
+#pragma unroll 4
+      for (int rr = 0; rr < 32; ++rr) { const int v = ep[rr * GC_TILE + lane]; s += v > 0 ? v : 0; }
+#pragma unroll
+      for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0 && s) atomicAdd(&acc[P.img_of[t]].sumpos_e, (unsigned long long)s);
+    } else {
+      R = R0 = P.mreach[(long long)t * 32 + lane];
+      if (lane == 0 && nb.x >= 0)
+        R |= P.mreach[(long long)nb.x * 32 + 31] & P.mcan[(long long)nb.x * 128 + 32 + 31];
+      if (lane == 31 && nb.y >= 0)
+        R |= P.mreach[(long long)nb.y * 32] & P.mcan[(long long)nb.y * 128 + 0];
+      if (nb.z >= 0 && ((P.mreach[(long long)nb.z * 32 + lane] & P.mcan[(long long)nb.z * 128 + 96 + lane]) >> 31))
+        R |= 1u;
+      if (nb.w >= 0 && ((P.mreach[(long long)nb.w * 32 + lane] & P.mcan[(long long)nb.w * 128 + 64 + lane]) & 1u))
+        R |= 0x80000000u;
+    }
+    for (int guard = 0; guard < GC_TILE_PX + 1; ++guard) {
+      uint32_t dn = __shfl_up_sync(0xffffffffu, R & canD, 1);   // row r-1 flows down into r
+      uint32_t up = __shfl_down_sync(0xffffffffu, R & canU, 1); // row r+1 flows up into r
+      if (lane == 0) dn = 0;
+      if (lane == 31) up = 0;
+      const uint32_t N = R | ((R & canR) << 1) | ((R & canL) >> 1) | dn | up;
+      if (!__any_sync(0xffffffffu, N != R)) break;
+      R = N;
+    }
+    P.mreach[(long long)t * 32 + lane] = R;
+    const uint32_t nw = first ? R : (R & ~R0);
+    const int sU = __any_sync(0xffffffffu, lane == 0 && (nw & canU));
+    const int sD = __any_sync(0xffffffffu, lane == 31 && (nw & canD));
+    const int sL = __any_sync(0xffffffffu, (nw & canL & 1u) != 0);
+    const int sR = __any_sync(0xffffffffu, ((nw & canR) >> 31) != 0);
+    if (lane == 0) {
+      if (P.ktiles) atomicAdd(&P.ktiles[first ? K_FLOOD_FIRST : K_FLOOD], 1ull);
+      if (sU && nb.x >= 0) P.mark[nb.x] = 1;
+      if (sD && nb.y >= 0) P.mark[nb.y] = 1;
+      if (sL && nb.z >= 0) P.mark[nb.z] = 1;
+      if (sR && nb.w >= 0) P.mark[nb.w] = 1;
+    }
+  }
+}
+
+// Labels of one image, row-major, padding excluded.
+__global__ void k_labels_out(PoolView P, ImageDesc im, uint8_t* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)im.W * im.H) return;
+  const int y = (int)(i / im.W), x = (int)(i % im.W);
+  const int t = im.tile0 + (y >> 5) * im.tw + (x >> 5);
+  out[i] = (uint8_t)((P.mreach[(long long)t * 32 + (y & 31)] >> (x & 31)) & 1u);
+}
+
+// One plane of one image back to row-major.
+__global__ void k_state_out(ImageDesc im, const int32_t* __restrict__ plane, int32_t* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)im.W * im.H) return;
+  const int y = (int)(i / im.W), x = (int)(i % im.W);
+  const int t = im.tile0 + (y >> 5) * im.tw + (x >> 5);
+  out[i] = plane[(long long)t * GC_TILE_PX + (y & 31) * GC_TILE + (x & 31)];
+}
+
+// T-link edits: excess moves by (new - old) t-link; the running sum of max(t, 0) follows.
+__device__ __forceinline__ void apply_tlink(const PoolView& P, const ImageDesc& im, int img,
+                                            int x, int y, int32_t v, int32_t* tl, ImageAcc* acc) {
+  const int t = im.tile0 + (y >> 5) * im.tw + (x >> 5);
+  const long long o = (long long)t * GC_TILE_PX + (y & 31) * GC_TILE + (x & 31);
+  const int32_t old = tl[o];
+  if (old == v) return;
+  tl[o] = v;
+  atomicAdd(P.exc + o, v - old);
+  const long long dpos = (long long)(v > 0 ? v : 0) - (long long)(old > 0 ? old : 0);
+  if (dpos) atomicAdd(&acc[img].sumpos_t, (unsigned long long)dpos);
+}
+
+__global__ void k_edit(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ idx,
+                       const int32_t* __restrict__ val, int n, int32_t* tl, ImageAcc* acc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = idx[i];
+  if (p < 0 || p >= im.W * im.H) return;
+  apply_tlink(P, im, img, p % im.W, p / im.W, val[i], tl, acc);
+}
+
+// Stroke: pixels within `radius` of the polyline get t-link `value`.  Exact integer test:
+// with a = p - A, b = B - A, L = b.b, s = a.b: inside iff |p - A|^2 <= r^2 (s <= 0),
+// |p - B|^2 <= r^2 (s >= L), else |a|^2 L - s^2 <= r^2 L.
+__device__ __forceinline__ bool in_stroke(int px, int py, const int32_t* pts, int npts, int r) {
+  const long long r2 = (long long)r * r;
+  for (int k = 0; k < (npts > 1 ? npts - 1 : 1); ++k) {
+    const long long ax = pts[2 * k], ay = pts[2 * k + 1];
+    const long long bx = npts > 1 ? pts[2 * k + 2] : ax, by = npts > 1 ? pts[2 * k + 3] : ay;
+    const long long dx = px - ax, dy = py - ay, ux = bx - ax, uy = by - ay;
+    const long long L = ux * ux + uy * uy, s = dx * ux + dy * uy;
+    if (L == 0 || s <= 0) { if (dx * dx + dy * dy <= r2) return true; continue; }
+    if (s >= L) { const long long ex = px - bx, ey = py - by; if (ex * ex + ey * ey <= r2) return true; continue; }
+    if ((dx * dx + dy * dy) * L - s * s <= r2 * L) return true;
+  }
+  return false;
+}
+
+__global__ void k_stroke(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ pts,
+                         int npts, int radius, int32_t value, int x0, int y0, int bw, int bh,
+                         int32_t* tl, ImageAcc* acc) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)bw * bh) return;
+  const int x = x0 + (int)(i % bw), y = y0 + (int)(i / bw);
+  if (x < 0 || y < 0 || x >= im.W || y >= im.H) return;
+  if (!in_stroke(x, y, pts, npts, radius)) return;
+  apply_tlink(P, im, img, x, y, value, tl, acc);
+}
+
+// ------------------------------------------------------------------------------------
+// Launchers
+// ------------------------------------------------------------------------------------
+static inline int ok() { return cudaGetLastError() == cudaSuccess ? GC_OK : GC_ERR_CUDA; }
+
+int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t* up,
+                  const int32_t* down, const int32_t* left, const int32_t* right,
+                  const int32_t* excess, int32_t* tl, ImageAcc* acc, cudaStream_t s) {
+  k_upload<<<im.tw * im.th, DIS_THREADS, 0, s>>>(P, im, img, up, down, left, right, excess, tl, acc);
+  return ok();
+}
+
+int launch_discharge(const PoolView& P, const int32_t* list, const int32_t* count, int iters,
+                     int grid, cudaStream_t s) {
+  k_discharge<<<grid, DIS_THREADS, 0, s>>>(P, list, count, iters);
+  return ok();
+}
+
+int launch_edge_relabel_build(const PoolView& P, int32_t* list, int32_t* count,
+                              const ScanState& st, cudaStream_t s) {
+  const int nch = (P.nt + EB_TILES - 1) / EB_TILES;
+  if (nch > st.max_chunks) return GC_ERR_INVALID;
+  k_edge_relabel_build<<<nch, EB_THREADS, 0, s>>>(P, list, count, st);
+  return ok();
+}
+
+int launch_bfs_round(const PoolView& P, const int32_t* list, const int32_t* count, int first,
+                     int grid, cudaStream_t s) {
+  k_bfs_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, list, count, first);
+  return ok();
+}
+
+int launch_flood_round(const PoolView& P, const int32_t* list, const int32_t* count, int first,
+                       ImageAcc* acc, int grid, cudaStream_t s) {
+  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, list, count, first, acc);
+  return ok();
+}
+
+int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s) {
+  const long long n = (long long)im.W * im.H;
+  k_labels_out<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, im, out);
+  return ok();
+}
+
+int launch_state_out(const PoolView& P, const ImageDesc& im, const int32_t* plane,
+                     int32_t* out, cudaStream_t s) {
+  (void)P;
+  const long long n = (long long)im.W * im.H;
+  k_state_out<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(im, plane, out);
+  return ok();
+}
+
+int launch_edit(const PoolView& P, const ImageDesc& im, int img, const int32_t* idx,
+                const int32_t* val, int n, int32_t* tl, ImageAcc* acc, cudaStream_t s) {
+  if (n <= 0) return GC_OK;
+  k_edit<<<(n + 255) / 256, 256, 0, s>>>(P, im, img, idx, val, n, tl, acc);
+  return ok();
+}
+
+int launch_stroke(const PoolView& P, const ImageDesc& im, int img, const int32_t* pts_dev,
+                  const int32_t* pts_host, int npts, int radius, int32_t value, int32_t* tl,
+                  ImageAcc* acc, cudaStream_t s) {
+  int xmin = pts_host[0], xmax = pts_host[0], ymin = pts_host[1], ymax = pts_host[1];
+  for (int k = 1; k < npts; ++k) {
+    xmin = xmin < pts_host[2 * k] ? xmin : pts_host[2 * k];
+    xmax = xmax > pts_host[2 * k] ? xmax : pts_host[2 * k];
+    ymin = ymin < pts_host[2 * k + 1] ? ymin : pts_host[2 * k + 1];
+    ymax = ymax > pts_host[2 * k + 1] ? ymax : pts_host[2 * k + 1];
+  }
+  int x0 = xmin - radius, y0 = ymin - radius, x1 = xmax + radius, y1 = ymax + radius;
+  x0 = x0 < 0 ? 0 : x0; y0 = y0 < 0 ? 0 : y0;
+  x1 = x1 > im.W - 1 ? im.W - 1 : x1; y1 = y1 > im.H - 1 ? im.H - 1 : y1;
+  if (x1 < x0 || y1 < y0) return GC_OK;
+  const int bw = x1 - x0 + 1, bh = y1 - y0 + 1;
+  const long long n = (long long)bw * bh;
+  k_stroke<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, im, img, pts_dev, npts, radius, value,
+                                                     x0, y0, bw, bh, tl, acc);
+  return ok();
+}
+
+int occupancy_discharge(int device) {
+  int per_sm = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_discharge, DIS_THREADS, 0);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+}
+
+int occupancy_warps(int device) {
+  int per_sm = 0, sms = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_round, WARPS_PER_CTA * 32, 0);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+}
+
+}  // namespace gcut

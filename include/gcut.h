@@ -1,0 +1,201 @@
+/* gcut.h - C ABI of the sm_100a tiled push-relabel graph cut (libgcut.so).
+ *
+ * Drop-in boundary for the path GraphCut.pyx -> graphcut.cl of rheiland/cl-util, with the
+ * IncrementalTileList / StreamCompact / PrefixSum layer beneath it.  Plain C types only:
+ * device buffers are passed as pointers, streams as `void*` (a cudaStream_t, NULL for the
+ * legacy default stream).  Every function returns a status code (GC_OK == 0); no C++
+ * exception crosses the boundary.  gc_last_error() describes the last failure of the
+ * calling thread.
+ *
+ * Graph convention (all int32, row-major [height][width], pitch = width):
+ *   up[y][x]    residual capacity of the edge (x,y) -> (x,y-1)
+ *   down[y][x]  ... (x,y) -> (x,y+1)
+ *   left[y][x]  ... (x,y) -> (x-1,y)
+ *   right[y][x] ... (x,y) -> (x+1,y)
+ *   excess[y][x] signed t-link: > 0 source capacity, < 0 sink capacity.
+ * Capacities pointing out of the image are ignored (treated as 0), as the reference zeroes
+ * them (graphcut.cl:1107-1108, 1125-1127).  Capacities must be >= 0; every value must
+ * satisfy |excess| + 4 * max(cap(u->v) + cap(v->u)) < 2^31.
+ *
+ * Result: the max-flow value (int64) and the canonical minimum cut, i.e. the set of pixels
+ * reachable from the source in the final residual graph (label 1), which is unique for a
+ * given graph.  The reference exposes neither directly: GraphCut.cut mutates dExcess and
+ * leaves BFS distances in dHeight (GraphCut.pyx:348-418).
+ */
+#ifndef GCUT_H
+#define GCUT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define GC_OK 0
+#define GC_ERR_INVALID 1        /* bad argument (sizes, null pointers, negative capacity) */
+#define GC_ERR_OOM 2            /* device allocation failed */
+#define GC_ERR_NOT_CONVERGED 3  /* iteration cap reached before the cut was final */
+#define GC_ERR_CUDA 4           /* a CUDA call failed */
+#define GC_ERR_INTERNAL 5       /* a bounded device-side wait gave up */
+#define GC_ERR_STATE 6          /* call out of order (e.g. labels before a solve) */
+
+/* Stamp predicates of IncrementalTileList (IncrementalTileList.pyx:26-35). */
+#define GC_OPERATOR_EQUAL 0
+#define GC_OPERATOR_GT 1
+#define GC_OPERATOR_LT 2
+#define GC_OPERATOR_GTE 3
+#define GC_OPERATOR_LTE 4
+#define GC_LOGICAL_AND 0
+#define GC_LOGICAL_OR 1
+
+typedef struct gc_opts {
+  int device;              /* CUDA device ordinal */
+  int discharge_iters;     /* push + interior-relabel iterations inside a tile per launch */
+  int pulses_per_relabel;  /* discharge launches between global relabels (reference: bfs=5,
+                              GraphCut.pyx:27) */
+  int initial_relabel;     /* 1: exact global relabel before the first push; 0: start from
+                              heights 0 (sink pixels) / 1 (others) */
+  int max_cycles;          /* cap on global-relabel cycles; exceeded -> GC_ERR_NOT_CONVERGED */
+  int max_bfs_rounds;      /* cap on tile rounds of one BFS / flood fill */
+} gc_opts;
+
+typedef struct gc_stats {
+  int64_t cycles;          /* global-relabel cycles of the last solve */
+  int64_t pulses;          /* discharge launches */
+  int64_t bfs_rounds;      /* tile rounds over all global relabels */
+  int64_t flood_rounds;    /* tile rounds of the canonical-cut flood fill */
+  int64_t launches;        /* kernels launched by the last solve */
+  int64_t tiles_discharged;/* sum over pulses of the active-list length (host-visible
+                              only when stats collection is on) */
+} gc_stats;
+
+typedef struct gc_handle gc_handle;
+
+/* Fills opts with defaults. */
+int gc_opts_default(gc_opts* opts);
+
+/* One solver for one width x height grid (any size >= 1; padded internally to 32).
+   Replaces GraphCut.__init__ (GraphCut.pyx:80-154). */
+int gc_create(int width, int height, const gc_opts* opts, gc_handle** out);
+int gc_destroy(gc_handle* h);
+int gc_size(const gc_handle* h, int* width, int* height);
+
+/* Capacity upload from DEVICE buffers (row-major, see above).  Replaces init_gc +
+   load_tiles (graphcut.cl:63-112, 1033-1132), which built n-links from an image.
+   Resets the residual graph to these capacities. */
+int gc_upload(gc_handle* h, const int32_t* up, const int32_t* down, const int32_t* left,
+              const int32_t* right, const int32_t* excess, void* stream);
+/* Same from HOST buffers (copied through a pinned staging buffer owned by the handle).
+   Synchronous with respect to the host buffers. */
+int gc_upload_host(gc_handle* h, const int32_t* up, const int32_t* down, const int32_t* left,
+                   const int32_t* right, const int32_t* excess, void* stream);
+
+/* Max-flow to the final cut.  Replaces GraphCut.cut (GraphCut.pyx:348-418); warm-starts
+   from the current residual graph when called again after gc_edit_tlinks.  Blocks the
+   calling host thread until the solve is done (it polls the active-tile count). */
+int gc_solve(gc_handle* h, void* stream);
+
+/* Manual stepping, mirroring the reference methods a caller can drive one at a time (the
+   GUI buttons of test_GraphCut.py:81-83).  gc_push = one discharge launch over the active
+   tiles (GraphCut.push, GraphCut.pyx:242-323, all four directions plus the in-tile local
+   relabel); gc_relabel = relabel of active tile-edge pixels and the active-tile list
+   rebuild (GraphCut.relabel, GraphCut.pyx:224-240); gc_start_bfs = exact global relabel
+   and the active-tile list from it (GraphCut.startBfs, GraphCut.pyx:187-222);
+   gc_is_completed = 1 when no pixel with excess > 0 can reach a sink pixel, valid right
+   after gc_start_bfs (GraphCut.isCompleted, GraphCut.pyx:328-346); it also computes the
+   canonical cut and the flow when it returns 1. */
+int gc_push(gc_handle* h, void* stream);
+int gc_relabel(gc_handle* h, void* stream);
+int gc_start_bfs(gc_handle* h, void* stream);
+int gc_is_completed(gc_handle* h, int* completed, void* stream);
+
+/* Flow value of the last solve (int64). */
+int gc_flow(gc_handle* h, int64_t* flow);
+/* Canonical labels (1 = source side) into a DEVICE buffer [height][width] uint8. */
+int gc_labels(gc_handle* h, uint8_t* labels, void* stream);
+/* Same into a HOST buffer (synchronous). */
+int gc_labels_host(gc_handle* h, uint8_t* labels, void* stream);
+
+/* Sets the signed t-link of n pixels (flat indices y*width+x, DEVICE arrays) to value[i];
+   the excess changes by value - previous t-link, which warm-starts the next gc_solve from
+   the previous flow.  Indices must be distinct within one call. */
+int gc_edit_tlinks(gc_handle* h, const int32_t* idx, const int32_t* value, int n, void* stream);
+/* Stroke edit: every pixel within `radius` of the polyline (xs[i], ys[i]), i < npts (host
+   arrays, integer pixel centres) gets t-link `value`.  Rasterised on the device. */
+int gc_edit_stroke(gc_handle* h, const int32_t* xs, const int32_t* ys, int npts, int radius,
+                   int32_t value, void* stream);
+
+/* Residual state back to row-major DEVICE buffers (any pointer may be NULL): excess,
+   height, residual capacities.  Inspection and tests. */
+int gc_download_state(gc_handle* h, int32_t* excess, int32_t* height, int32_t* up,
+                      int32_t* down, int32_t* left, int32_t* right, void* stream);
+int gc_get_stats(const gc_handle* h, gc_stats* stats);
+/* Per-pulse host readback of the active-tile count (diagnostics; slows the solve). */
+int gc_set_collect_stats(gc_handle* h, int on);
+
+/* Per-kernel profile of the last solve (and the upload / labels calls around it):
+   launches, summed CUDA-event time of each launch on the caller's stream, and tiles
+   processed (device counters).  Kinds 0..GC_NKERN-1, named by gc_kernel_name. */
+#define GC_NKERN 9
+typedef struct gc_kernel_prof {
+  int64_t launches;
+  double ms;
+  int64_t tiles;
+} gc_kernel_prof;
+int gc_set_profile(gc_handle* h, int on);
+int gc_get_profile(const gc_handle* h, gc_kernel_prof* out, int n);
+const char* gc_kernel_name(int kind);
+
+/* Message of the last error on this thread ("" if none). */
+const char* gc_last_error(void);
+
+/* ---- data-parallel primitives beneath IncrementalTileList ---------------------------
+   All pointers are DEVICE pointers; n items; one launch each.  The library keeps the
+   look-back state per device. */
+
+/* PrefixSum.scan (PrefixSum.pyx:83-129, prefixsum.cl): exclusive scan of in[0..n) into
+   out (may alias in) and the sum into *total (int32 wrap-around). */
+int gc_scan_exclusive(const int32_t* in, int32_t* out, int32_t* total, int n, void* stream);
+/* StreamCompact.compact (StreamCompact.pyx:66-82, streamcompact.cl): indices i with
+   flags[i] != 0, increasing, into list; their number into *length.  list must not alias
+   flags. */
+int gc_compact(const int32_t* flags, int32_t* list, int32_t* length, int n, void* stream);
+/* IncrementalTileList.build(operator, operand) (IncrementalTileList.pyx:119-136,
+   incremental_tile_list.cl:40-64 + compaction). */
+int gc_tiles_build(const int32_t* tiles, int op, int32_t operand, int32_t* list,
+                   int32_t* length, int n, void* stream);
+/* IncrementalTileList.buildLogical (IncrementalTileList.pyx:157-176,
+   incremental_tile_list.cl:66-108 + compaction). */
+int gc_tiles_build_logical(const int32_t* tiles, const int32_t* tiles2, int op1, int32_t a1,
+                           int op2, int32_t a2, int logical, int32_t* list, int32_t* length,
+                           int n, void* stream);
+/* IncrementalTileList.incorporate (IncrementalTileList.pyx:138-155,
+   incremental_tile_list.cl:110-154): tiles[i] = iteration where the predicate holds. */
+int gc_tiles_incorporate(int32_t* tiles, const int32_t* tiles2, int op1, int32_t a1, int op2,
+                         int32_t a2, int logical, int32_t iteration, int n, void* stream);
+/* IncrementalTileList.reset (IncrementalTileList.pyx:178-189, init_incremental
+   incremental_tile_list.cl:26-38): tiles[i] = value. */
+int gc_tiles_fill(int32_t* tiles, int32_t value, int n, void* stream);
+
+/* ---- batched solver: many independent grids in one tile pool ------------------------ */
+typedef struct gcb_handle gcb_handle;
+int gcb_create(int n, const int* widths, const int* heights, const gc_opts* opts,
+               gcb_handle** out);
+int gcb_destroy(gcb_handle* b);
+/* Upload grid i from DEVICE buffers (layout as gc_upload). */
+int gcb_upload(gcb_handle* b, int i, const int32_t* up, const int32_t* down,
+               const int32_t* left, const int32_t* right, const int32_t* excess, void* stream);
+/* Solves every grid of the pool together (one tile queue over all grids). */
+int gcb_solve(gcb_handle* b, void* stream);
+int gcb_flow(gcb_handle* b, int i, int64_t* flow);
+int gcb_labels(gcb_handle* b, int i, uint8_t* labels, void* stream);
+int gcb_get_stats(const gcb_handle* b, gc_stats* stats);
+int gcb_set_profile(gcb_handle* b, int on);
+int gcb_get_profile(const gcb_handle* b, gc_kernel_prof* out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GCUT_H */

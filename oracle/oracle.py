@@ -1,0 +1,148 @@
+"""CPU oracle wrapper.  TEST INFRASTRUCTURE ONLY.
+
+The parity tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use
+this module as the checker; the product never imports it.
+
+* ``maxflow_bk``      exact max-flow (Boykov-Kolmogorov, TPAMI 2004), canonical labels.
+* ``ref_tiled``       int32 restatement of the reference schedule (GraphCut.pyx:348-418 +
+                      graphcut.cl), OpenMP over tiles; the CPU baseline.
+* ``canonical``       canonical cut + flow of a residual state.
+* ``cut_capacity``    capacity of a labelled cut from the original capacities.
+* ``exclusive_scan``, ``compact``, ``flag``, ``flag_logical``, ``increment_logical``:
+  restatements of prefixsum.cl (exclusive Blelloch scan, total in a separate word),
+  streamcompact.cl:1-14 (``out[scan[i]] = i`` for flagged i) and
+  incremental_tile_list.cl:40-154 (stamp predicates).  Pinned by the reference's own
+  known-answer checks (test_PrefixSum.py:35, test_StreamCompact.py:40-41,
+  test_IncrementalTileList.py:38-40) in tests/test_oracle.py.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+OPERATOR_EQUAL, OPERATOR_GT, OPERATOR_LT, OPERATOR_GTE, OPERATOR_LTE = range(5)
+LOGICAL_AND, LOGICAL_OR = 0, 1
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _LIB = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        _LIB.orc_maxflow_bk.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 5 + [P, P, P]
+        _LIB.orc_canonical.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 6 + [P, P]
+        _LIB.orc_cut_capacity.argtypes = [ctypes.c_int, ctypes.c_int] + [P] * 6
+        _LIB.orc_cut_capacity.restype = ctypes.c_int64
+        _LIB.orc_ref_tiled.argtypes = ([ctypes.c_int, ctypes.c_int] + [P] * 5 +
+                                       [ctypes.c_int, ctypes.c_longlong, ctypes.c_int, P, P, P])
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def maxflow_bk(up, down, left, right, excess, return_excess=False):
+    """Exact max-flow of the grid graph: (flow:int, labels:uint8[H,W][, final excess])."""
+    up, down, left, right, excess = map(_i32, (up, down, left, right, excess))
+    h, w = excess.shape
+    flow = np.zeros(1, np.int64)
+    labels = np.zeros((h, w), np.uint8)
+    fe = np.zeros((h, w), np.int64) if return_excess else None
+    rc = lib().orc_maxflow_bk(w, h, _p(up), _p(down), _p(left), _p(right), _p(excess),
+                              _p(flow), _p(labels), _p(fe) if fe is not None else None)
+    if rc != 0:
+        raise RuntimeError(f"orc_maxflow_bk failed ({rc})")
+    return (int(flow[0]), labels, fe) if return_excess else (int(flow[0]), labels)
+
+
+def ref_tiled(up, down, left, right, excess, bfs=5, max_iters=10 ** 7, threads=0):
+    """The reference schedule restated: (flow, labels, stats[iterations, relabels, bfs])."""
+    up, down, left, right, excess = map(_i32, (up, down, left, right, excess))
+    h, w = excess.shape
+    flow = np.zeros(1, np.int64)
+    labels = np.zeros((h, w), np.uint8)
+    stats = np.zeros(3, np.int64)
+    rc = lib().orc_ref_tiled(w, h, _p(up), _p(down), _p(left), _p(right), _p(excess), bfs,
+                             max_iters, threads, _p(flow), _p(labels), _p(stats))
+    if rc != 0:
+        raise RuntimeError(f"orc_ref_tiled failed ({rc})")
+    return int(flow[0]), labels, stats
+
+
+def canonical(rup, rdown, rleft, rright, exc, t0):
+    rup, rdown, rleft, rright, exc, t0 = map(_i32, (rup, rdown, rleft, rright, exc, t0))
+    h, w = exc.shape
+    flow = np.zeros(1, np.int64)
+    labels = np.zeros((h, w), np.uint8)
+    lib().orc_canonical(w, h, _p(rup), _p(rdown), _p(rleft), _p(rright), _p(exc), _p(t0),
+                        _p(flow), _p(labels))
+    return int(flow[0]), labels
+
+
+def cut_capacity(up, down, left, right, excess, labels):
+    up, down, left, right, excess = map(_i32, (up, down, left, right, excess))
+    labels = np.ascontiguousarray(labels, dtype=np.uint8)
+    h, w = excess.shape
+    return int(lib().orc_cut_capacity(w, h, _p(up), _p(down), _p(left), _p(right), _p(excess),
+                                      _p(labels)))
+
+
+# --- data-parallel primitives beneath IncrementalTileList --------------------------------
+
+def exclusive_scan(a):
+    """prefixsum.cl: exclusive scan of int32 values and the total (int32 wrap-around)."""
+    a = np.asarray(a, dtype=np.int64)
+    out = np.zeros(a.shape[0], np.int64)
+    if a.shape[0]:
+        np.cumsum(a[:-1], out=out[1:])
+    total = int(a.sum())
+    wrap = lambda v: ((v + 2 ** 31) % 2 ** 32) - 2 ** 31
+    return wrap(out).astype(np.int32), int(wrap(np.int64(total)))
+
+
+def compact(flags):
+    """StreamCompact.compact: ids of the non-zero flags in increasing order, and count."""
+    ids = np.flatnonzero(np.asarray(flags) != 0).astype(np.int32)
+    return ids, int(ids.shape[0])
+
+
+def _pred(op, v, operand):
+    v = np.asarray(v, dtype=np.int64)
+    return {OPERATOR_EQUAL: v == operand, OPERATOR_GT: v > operand, OPERATOR_LT: v < operand,
+            OPERATOR_GTE: v >= operand, OPERATOR_LTE: v <= operand}[op]
+
+
+def flag(tiles, op, operand):
+    """incremental_tile_list.cl:40-64."""
+    return _pred(op, tiles, operand).astype(np.int32)
+
+
+def flag_logical(t1, t2, op1, op2, a1, a2, logical):
+    """incremental_tile_list.cl:66-108."""
+    f1, f2 = _pred(op1, t1, a1), _pred(op2, t2, a2)
+    return ((f1 & f2) if logical == LOGICAL_AND else (f1 | f2)).astype(np.int32)
+
+
+def increment_logical(t1, t2, op1, op2, a1, a2, logical, iteration):
+    """incremental_tile_list.cl:110-154: stamp ``iteration`` where the predicate holds."""
+    out = np.array(t1, dtype=np.int32, copy=True)
+    out[flag_logical(t1, t2, op1, op2, a1, a2, logical) != 0] = iteration
+    return out

@@ -1,0 +1,58 @@
+"""The C-ABI library loads without a GPU and exports every function include/gcut.h
+declares; the Python binding declares exactly those functions."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "gcut.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gcb?_[a-z_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def libgcut():
+    import _gcut
+    if not os.path.exists(_gcut.LIB_PATH):
+        import gcut_build
+        gcut_build.build()
+    return ctypes.CDLL(_gcut.LIB_PATH)
+
+
+def test_header_declares_functions():
+    names = header_functions()
+    assert "gc_solve" in names and "gc_compact" in names and "gcb_solve" in names
+    assert len(names) >= 30
+
+
+def test_library_exports_every_declared_symbol(libgcut):
+    missing = [n for n in header_functions() if not hasattr(libgcut, n)]
+    assert not missing, missing
+
+
+def test_binding_matches_header():
+    import _gcut
+    assert sorted(_gcut.SIGNATURES) == header_functions()
+
+
+def test_calls_without_gpu_fail_cleanly(libgcut):
+    """No CUDA device here: creating a solver returns an error code, never crashes."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import _gcut
+    L = _gcut.lib()
+    h = ctypes.c_void_p()
+    rc = L.gc_create(64, 64, None, ctypes.byref(h))
+    assert rc != 0 and not h.value
+    assert L.gc_last_error()
+    # invalid arguments are rejected before any CUDA call
+    assert L.gc_create(0, 64, None, ctypes.byref(h)) == _gcut.GC_ERR_INVALID
+    assert L.gc_solve(None, None) == _gcut.GC_ERR_INVALID
+    o = _gcut.GcOpts()
+    assert L.gc_opts_default(ctypes.byref(o)) == 0 and o.discharge_iters > 0

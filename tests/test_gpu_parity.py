@@ -1,0 +1,201 @@
+"""Parity of the CUDA solver with the oracle (bit-exact flow value and canonical cut).
+
+Every case calls libgcut through the C ABI (via the GraphCut class) and compares with the
+Boykov-Kolmogorov oracle on the same seeded inputs; at the benchmark size (2048^2) the
+oracle still finishes in well under a second, so the comparison is direct, plus the
+size-independent certificate flow == capacity(cut).
+"""
+import numpy as np
+import pytest
+
+import synth
+import strokes
+from GraphCut import GraphCut
+from GraphCutBatch import GraphCutBatch
+
+pytestmark = pytest.mark.gpu
+
+
+def solve_gpu(g, **kw):
+    with GraphCut(g.width, g.height, **kw) as gc:
+        gc.upload_capacities(*g.planes())
+        gc.cut()
+        return gc.flow, gc.labels().cpu().numpy(), gc.stats()
+
+
+def check(g, oracle, **kw):
+    f_ref, l_ref = oracle.maxflow_bk(*g.planes())
+    f, lab, st = solve_gpu(g, **kw)
+    assert f == f_ref, (f, f_ref, st)
+    assert np.array_equal(lab, l_ref), (int((lab != l_ref).sum()), st)
+    return st
+
+
+@pytest.mark.parametrize("w,h,seed", [(512, 512, 0), (512, 512, 1), (256, 384, 2), (64, 96, 3),
+                                      (32, 32, 4), (1024, 512, 5)])
+def test_synthetic_matches_oracle(cuda, oracle, w, h, seed):
+    check(synth.make_graph(w, h, seed), oracle)
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (1, 7), (7, 1), (33, 31), (100, 37), (300, 211)])
+def test_ragged_sizes(cuda, oracle, w, h):
+    check(synth.random_graph(w, h, w * 1000 + h, cap_max=30, tlink_max=60), oracle)
+
+
+@pytest.mark.parametrize("seed,sym,sparsity", [(0, True, 0.0), (1, False, 0.0), (2, True, 0.4),
+                                               (3, False, 0.6), (4, True, 0.9)])
+def test_random_graphs(cuda, oracle, seed, sym, sparsity):
+    g = synth.random_graph(256, 192, seed, cap_max=100, tlink_max=150, sparsity=sparsity,
+                           symmetric=sym)
+    check(g, oracle)
+
+
+@pytest.mark.parametrize("iters,pulses,init", [(1, 1, 0), (4, 1, 1), (64, 5, 0), (32, 0, 1)])
+def test_schedules_agree(cuda, oracle, iters, pulses, init):
+    g = synth.random_graph(160, 128, 11, cap_max=80, tlink_max=120, symmetric=False)
+    check(g, oracle, discharge_iters=iters, bfs=pulses, initial_relabel=bool(init))
+
+
+def test_edge_cases_zero_and_uniform(cuda, oracle):
+    w, h = 96, 64
+    z = np.zeros((h, w), np.int32)
+    g = synth.Graph(w, h, z, z, z, z, z)
+    f, lab, _ = solve_gpu(g)
+    assert f == 0 and lab.sum() == 0
+    # all source, no sink: no flow, everything on the source side
+    g = synth.Graph(w, h, *synth.planes_from_weights(np.full((h - 1, w), 5, np.int32),
+                                                     np.full((h, w - 1), 5, np.int32), z),
+                    np.full((h, w), 7, np.int32))
+    f, lab, _ = solve_gpu(g)
+    assert f == 0 and lab.all()
+    # single sink pixel in the middle: everything drains into it up to the cut
+    e = np.full((h, w), 3, np.int32)
+    e[h // 2, w // 2] = -10 ** 6
+    g = synth.Graph(w, h, *synth.planes_from_weights(np.full((h - 1, w), 2, np.int32),
+                                                     np.full((h, w - 1), 2, np.int32), e), e)
+    check(g, oracle)
+
+
+def test_benchmark_size_2048(cuda, oracle):
+    g = synth.make_graph(2048, 2048, 1)
+    st = check(g, oracle)
+    assert st["cycles"] >= 1
+
+
+def test_flow_equals_cut_capacity(cuda, oracle):
+    g = synth.make_graph(1024, 1024, 7)
+    f, lab, _ = solve_gpu(g)
+    assert oracle.cut_capacity(*g.planes(), lab) == f
+
+
+def test_manual_stepping_matches(cuda, oracle):
+    g = synth.random_graph(128, 96, 5, cap_max=60, tlink_max=90)
+    f_ref, l_ref = oracle.maxflow_bk(*g.planes())
+    with GraphCut(g.width, g.height) as gc:
+        gc.upload_capacities(*g.planes())
+        done = False
+        for _ in range(10000):
+            for _ in range(3):
+                gc.push()
+                gc.relabel()
+            gc.startBfs()
+            if gc.isCompleted():
+                done = True
+                break
+        assert done
+        assert gc.flow == f_ref
+        assert np.array_equal(gc.labels().cpu().numpy(), l_ref)
+
+
+def test_warm_start_strokes_match_cold(cuda, oracle):
+    g = synth.make_graph(512, 512, 3)
+    rng = np.random.default_rng(0)
+    t = g.excess.copy()
+    with GraphCut(g.width, g.height) as gc:
+        gc.upload_capacities(*g.planes())
+        gc.cut()
+        for k in range(6):
+            s = strokes.random_stroke(rng, g.width, g.height)
+            gc.edit_stroke(s.xs, s.ys, s.radius, s.value)
+            t = strokes.apply(t, s)
+            gc.cut()
+            f_ref, l_ref = oracle.maxflow_bk(g.up, g.down, g.left, g.right, t)
+            assert gc.flow == f_ref, k
+            assert np.array_equal(gc.labels().cpu().numpy(), l_ref), k
+
+
+def test_edit_tlinks_match_cold(cuda, oracle):
+    g = synth.random_graph(200, 150, 9, cap_max=50, tlink_max=80)
+    rng = np.random.default_rng(1)
+    t = g.excess.copy()
+    with GraphCut(g.width, g.height) as gc:
+        gc.upload_capacities(*g.planes())
+        gc.cut()
+        for k in range(4):
+            idx = rng.choice(g.width * g.height, 500, replace=False)
+            vals = rng.integers(-200, 201, 500).astype(np.int32)
+            gc.edit_tlinks(idx, vals)
+            t.reshape(-1)[idx] = vals
+            gc.cut()
+            f_ref, l_ref = oracle.maxflow_bk(g.up, g.down, g.left, g.right, t)
+            assert gc.flow == f_ref
+            assert np.array_equal(gc.labels().cpu().numpy(), l_ref)
+
+
+def test_stroke_raster_matches_host(cuda):
+    g = synth.random_graph(300, 200, 2, cap_max=5, tlink_max=5)
+    rng = np.random.default_rng(5)
+    with GraphCut(g.width, g.height) as gc:
+        gc.upload_capacities(*g.planes())
+        t = g.excess.copy()
+        for _ in range(5):
+            s = strokes.random_stroke(rng, g.width, g.height)
+            gc.edit_stroke(s.xs, s.ys, s.radius, s.value)
+            t = strokes.apply(t, s)
+        # the excess plane before any solve is exactly the edited t-links
+        assert np.array_equal(gc.dExcess.cpu().numpy(), t)
+
+
+def test_batch_matches_per_image(cuda, oracle):
+    shapes = synth.batch_shapes(12, seed=3, lo=128, hi=512, step=64)
+    graphs = [synth.make_graph(w, h, 100 + i) for i, (w, h) in enumerate(shapes)]
+    b = GraphCutBatch(shapes)
+    for i, g in enumerate(graphs):
+        b.upload(i, *g.planes())
+    b.cut()
+    for i, g in enumerate(graphs):
+        f_ref, l_ref = oracle.maxflow_bk(*g.planes())
+        assert b.flow(i) == f_ref, i
+        assert np.array_equal(b.labels(i).cpu().numpy(), l_ref), i
+    b.close()
+
+
+def test_negative_capacity_rejected(cuda):
+    import _gcut
+    g = synth.random_graph(64, 64, 0)
+    g.up[5, 5] = -1
+    with GraphCut(64, 64) as gc:
+        gc.upload_capacities(*g.planes())
+        with pytest.raises(_gcut.GCError) as ei:
+            gc.cut()
+        assert ei.value.code == _gcut.GC_ERR_INVALID
+
+
+def test_cycle_cap_reports_not_converged(cuda):
+    import _gcut
+    g = synth.random_graph(256, 256, 3, cap_max=100, tlink_max=100)
+    with GraphCut(256, 256, max_cycles=1, bfs=1, discharge_iters=1) as gc:
+        gc.upload_capacities(*g.planes())
+        with pytest.raises(_gcut.GCError) as ei:
+            gc.cut()
+        assert ei.value.code == _gcut.GC_ERR_NOT_CONVERGED
+
+
+def test_state_errors(cuda):
+    import _gcut
+    with GraphCut(64, 64) as gc:
+        with pytest.raises(_gcut.GCError) as ei:
+            gc.cut()
+        assert ei.value.code == _gcut.GC_ERR_STATE
+        with pytest.raises(_gcut.GCError):
+            _ = gc.flow

@@ -1,0 +1,125 @@
+"""Scan / compaction / tile-list primitives (PrefixSum, StreamCompact, IncrementalTileList)
+through the C ABI, against the oracle restatements and the reference's own checks
+(test_PrefixSum.py:35, test_StreamCompact.py:40-41, test_IncrementalTileList.py:38-40)."""
+import numpy as np
+import pytest
+
+from IncrementalTileList import IncrementalTileList, Logical, Operator, PrefixSum, StreamCompact
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a, torch):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.int32)).cuda()
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 511, 512, 513, 4095, 4096, 4097, 65536, 1 << 20, 3000017])
+def test_prefix_sum(cuda, oracle, n):
+    torch = cuda
+    rng = np.random.default_rng(n)
+    h = rng.integers(0, 20, n).astype(np.int32)
+    ps = PrefixSum(max(n, 1))
+    d = ps.factory(max(n, 1))
+    d[:n] = _dev(h, torch)
+    tot = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ps.scan(d, tot, n)
+    ref, ref_tot = oracle.exclusive_scan(h)
+    assert int(tot.item()) == h.sum() == ref_tot            # test_PrefixSum.py:35
+    assert np.array_equal(d[:n].cpu().numpy(), ref)          # element-wise (stronger)
+
+
+def test_prefix_sum_negative_values(cuda, oracle):
+    torch = cuda
+    h = np.random.default_rng(3).integers(-1000, 1000, 100000).astype(np.int32)
+    d = _dev(h, torch)
+    tot = torch.zeros(1, dtype=torch.int32, device="cuda")
+    PrefixSum(h.size).scan(d, tot, h.size)
+    ref, ref_tot = oracle.exclusive_scan(h)
+    assert np.array_equal(d.cpu().numpy(), ref) and int(tot.item()) == ref_tot
+
+
+@pytest.mark.parametrize("n", [0, 1, 4096, 4097, 65536, 1000003])
+def test_stream_compact(cuda, oracle, n):
+    torch = cuda
+    flags = np.random.default_rng(n + 1).integers(0, 2, n).astype(np.int32)
+    sc = StreamCompact(max(n, 1))
+    dF = sc.flagFactory(max(n, 1)); dF[:n] = _dev(flags, torch)
+    dL = sc.listFactory(max(n, 1))
+    dN = torch.zeros(1, dtype=torch.int32, device="cuda")
+    sc.compact(dF, dL, dN, n)
+    m = int(dN.item())
+    ref, ref_n = oracle.compact(flags)
+    assert m == ref_n
+    assert np.array_equal(np.where(flags == 1)[0], dL[:m].cpu().numpy())  # test_StreamCompact.py:40
+
+
+def test_stream_compact_capacity_error(cuda):
+    sc = StreamCompact(100)
+    with pytest.raises(ValueError):
+        sc.flagFactory(101)
+    with pytest.raises(ValueError):
+        sc.listFactory(101)
+
+
+def test_tile_list_reference_check(cuda):
+    """test_IncrementalTileList.py:18-40: 4096^2 image, 16^2 tiles, stamps in [0,20),
+    build(GTE, 10) == row-major ids of np.where(tiles >= 10)."""
+    torch = cuda
+    tl = IncrementalTileList((4096, 4096), (16, 16))
+    dim = tl.dim
+    h = np.random.default_rng(0).integers(0, 20, (dim[1], dim[0])).astype(np.int32)
+    tl.d_tiles.copy_(_dev(h, torch))
+    tl.build(Operator.GTE, 10)
+    ys, xs = np.where(h >= 10)
+    ref = ys * dim[0] + xs
+    assert tl.length == ref.size
+    assert np.array_equal(ref, tl.d_list[:tl.length].cpu().numpy())
+
+
+@pytest.mark.parametrize("op", [Operator.EQUAL, Operator.GT, Operator.LT, Operator.GTE, Operator.LTE])
+def test_tile_list_operators(cuda, oracle, op):
+    torch = cuda
+    tl = IncrementalTileList((2048, 1024), (32, 32))
+    h = np.random.default_rng(op).integers(-3, 4, (tl.dim[1], tl.dim[0])).astype(np.int32)
+    tl.d_tiles.copy_(_dev(h, torch))
+    tl.build(op, 1)
+    ref, n = oracle.compact(oracle.flag(h.reshape(-1), op, 1))
+    assert tl.length == n and np.array_equal(tl.d_list[:n].cpu().numpy(), ref)
+
+
+def test_tile_list_incorporate_and_logical(cuda, oracle):
+    torch = cuda
+    tl = IncrementalTileList((1024, 1024), (32, 32))
+    rng = np.random.default_rng(7)
+    a = rng.integers(-2, 6, (tl.dim[1], tl.dim[0])).astype(np.int32)
+    b = rng.integers(0, 30, (tl.dim[1], tl.dim[0])).astype(np.int32)
+    tl.d_tiles.copy_(_dev(a, torch))
+    d2 = _dev(b, torch)
+    it = tl.increment()
+    tl.incorporate(d2, Operator.LTE, 0, Operator.GTE, 12, Logical.AND)
+    ref = oracle.increment_logical(a.reshape(-1), b.reshape(-1), Operator.LTE, Operator.GTE,
+                                   0, 12, Logical.AND, it)
+    assert np.array_equal(tl.d_tiles.cpu().numpy().reshape(-1), ref)
+    tl.buildLogical(d2, Operator.EQUAL, it, Operator.LT, 20, Logical.OR)
+    refl, n = oracle.compact(oracle.flag_logical(ref, b.reshape(-1), Operator.EQUAL, Operator.LT,
+                                                 it, 20, Logical.OR))
+    assert tl.length == n and np.array_equal(tl.d_list[:n].cpu().numpy(), refl)
+    tl.reset()
+    assert (tl.d_tiles.cpu().numpy() == -1).all() and tl.iteration == 0
+
+
+def test_repeated_calls_reuse_lookback_state(cuda, oracle):
+    """Many back-to-back launches: the look-back tags must not leak between launches."""
+    torch = cuda
+    rng = np.random.default_rng(11)
+    sc = StreamCompact(200000)
+    dL = sc.listFactory()
+    dN = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for k in range(50):
+        n = int(rng.integers(1, 200000))
+        f = (rng.random(n) < rng.random()).astype(np.int32)
+        dF = _dev(f, torch)
+        sc.compact(dF, dL, dN, n)
+        m = int(dN.item())
+        assert m == int(f.sum())
+        assert np.array_equal(np.flatnonzero(f), dL[:m].cpu().numpy())
