@@ -152,7 +152,8 @@ struct Pool {
 
   void release() {
     int32_t* bufs[] = {P.exc, P.hgt, P.cap[0], P.cap[1], P.cap[2], P.cap[3], tl, list, counts,
-                       P.touched, P.act_int, P.mark, P.tact, P.img_of, stage, pts};
+                       P.touched, P.act_int, P.mark[0], P.mark[1], P.rcnt, P.tact, P.img_of,
+                       stage, pts};
     for (auto* b : bufs) if (b) cudaFree(b);
     if (P.nbr) cudaFree(P.nbr);
     if (P.mcan) cudaFree(P.mcan);
@@ -198,12 +199,14 @@ struct Pool {
     if (!e) e = dalloc(&P.msink, (size_t)nt * 32);
     if (!e) e = dalloc(&P.mexc, (size_t)nt * 32);
     if (!e) e = dalloc(&P.mreach, (size_t)nt * 32);
-    int32_t** small[] = {&P.touched, &P.act_int, &P.mark, &P.tact, &P.img_of, &list};
+    int32_t** small[] = {&P.touched, &P.act_int, &P.mark[0], &P.mark[1], &P.tact, &P.img_of, &list};
     for (auto** p : small) if (!e) e = dalloc(p, nt);
+    if (!e) e = dalloc(&P.rcnt, 2);
     if (!e) e = dalloc(&counts, 4);
     if (!e) e = dalloc(&acc, imgs.size());
     if (!e) e = dalloc(&ktiles, GC_NKERN);
-    if (!e) e = scan.alloc(scan_chunks(nt) > nt / 256 + 1 ? scan_chunks(nt) : nt / 256 + 1);
+    // look-back slots: the scan uses one per 4096 items, the list rebuild one per 8 tiles
+    if (!e) e = scan.alloc(scan_chunks(nt) > nt / 8 + 1 ? scan_chunks(nt) : nt / 8 + 1);
     if (!e) e = cudaMallocHost((void**)&h_count, 4 * sizeof(int32_t));
     if (!e) e = cudaMallocHost((void**)&h_acc, imgs.size() * sizeof(ImageAcc));
     if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); release(); return fail(GC_ERR_OOM, "device allocation failed"); }
@@ -218,7 +221,9 @@ struct Pool {
         }
     CK(cudaMemcpy(P.nbr, nb.data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
     CK(cudaMemset(P.touched, 0, sizeof(int32_t) * nt));
-    CK(cudaMemset(P.mark, 0, sizeof(int32_t) * nt));
+    CK(cudaMemset(P.mark[0], 0, sizeof(int32_t) * nt));
+    CK(cudaMemset(P.mark[1], 0, sizeof(int32_t) * nt));
+    CK(cudaMemset(P.rcnt, 0, sizeof(int32_t) * 2));
     CK(cudaMemset(P.act_int, 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.tact, 0, sizeof(int32_t) * nt));
     CK(cudaMemset(acc, 0, sizeof(ImageAcc) * imgs.size()));
@@ -245,26 +250,27 @@ struct Pool {
 
   // exact BFS distances to the sink pixels (global relabel); sets tact
   int global_relabel(cudaStream_t s) {
-    RK(timed(K_BFS_FIRST, s, [&] { return launch_bfs_round(P, list, counts, 1, grid_warps, s); }));
+    RK(timed(K_BFS_FIRST, s, [&] { return launch_bfs_round(P, 1, 0, grid_warps, s); }));
     stats.bfs_rounds++;
     return frontier_rounds(s, /*flood=*/false);
   }
 
-  // repeat {compact marks -> list; round over list} until a round had no tiles
+  // rounds over the marked tiles until a round finds none; the host reads the per-round
+  // tile counter once per batch of rounds
   int frontier_rounds(cudaStream_t s, bool flood) {
     int batch = 4;
     long long rounds = 0;
+    int rnd = 1;
     while (true) {
-      for (int k = 0; k < batch; ++k) {
-        RK(compact(P.mark, P.mark, s));
-        if (flood) RK(timed(K_FLOOD, s, [&] { return launch_flood_round(P, list, counts, 0, acc, grid_warps, s); }));
-        else RK(timed(K_BFS, s, [&] { return launch_bfs_round(P, list, counts, 0, grid_warps, s); }));
+      for (int k = 0; k < batch; ++k, ++rnd) {
+        if (flood) RK(timed(K_FLOOD, s, [&] { return launch_flood_round(P, 0, rnd, acc, grid_warps, s); }));
+        else RK(timed(K_BFS, s, [&] { return launch_bfs_round(P, 0, rnd, grid_warps, s); }));
       }
       rounds += batch;
-      int n;
-      RK(read_count(s, &n));
       if (flood) stats.flood_rounds += batch; else stats.bfs_rounds += batch;
-      if (n == 0) break;
+      CK(cudaMemcpyAsync(h_count, P.rcnt + ((rnd - 1) & 1), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      if (h_count[0] == 0) break;
       if (rounds >= opts.max_bfs_rounds) return fail(GC_ERR_NOT_CONVERGED, "BFS round cap reached");
       batch = batch < 32 ? batch * 2 : 32;
     }
@@ -330,7 +336,7 @@ struct Pool {
   int finish(cudaStream_t s) {
     for (size_t i = 0; i < imgs.size(); ++i)
       CK(cudaMemsetAsync(&acc[i].sumpos_e, 0, sizeof(unsigned long long), s));
-    RK(timed(K_FLOOD_FIRST, s, [&] { return launch_flood_round(P, list, counts, 1, acc, grid_warps, s); }));
+    RK(timed(K_FLOOD_FIRST, s, [&] { return launch_flood_round(P, 1, 0, acc, grid_warps, s); }));
     stats.flood_rounds++;
     RK(frontier_rounds(s, /*flood=*/true));
     CK(cudaMemcpyAsync(h_acc, acc, sizeof(ImageAcc) * imgs.size(), cudaMemcpyDeviceToHost, s));
@@ -432,8 +438,8 @@ const char* gc_last_error(void) { return g_err.c_str(); }
 int gc_opts_default(gc_opts* o) {
   if (!o) return fail(GC_ERR_INVALID, "null opts");
   o->device = 0;
-  o->discharge_iters = 32;
-  o->pulses_per_relabel = 2;
+  o->discharge_iters = 2;     // autotuned on 2048^2 and 4096^2 synthetic grids
+  o->pulses_per_relabel = 4;
   o->initial_relabel = 0;
   o->max_cycles = 100000;
   o->max_bfs_rounds = 1 << 20;
@@ -441,7 +447,7 @@ int gc_opts_default(gc_opts* o) {
 }
 
 static int check_opts(const gc_opts* o) {
-  if (o->discharge_iters < 1 || o->pulses_per_relabel < 0 || o->max_cycles < 1 || o->max_bfs_rounds < 1)
+  if (o->discharge_iters < 1 || o->pulses_per_relabel < 1 || o->max_cycles < 1 || o->max_bfs_rounds < 1)
     return fail(GC_ERR_INVALID, "invalid options");
   return GC_OK;
 }

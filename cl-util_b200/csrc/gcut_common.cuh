@@ -37,7 +37,8 @@ struct PoolView {
   uint32_t* mreach;       // [nt][32]   reachable from an excess pixel (canonical cut)
   int32_t* touched;       // [nt] tile was discharged or received cross-tile flow
   int32_t* act_int;       // [nt] tile has an active interior pixel after its discharge
-  int32_t* mark;          // [nt] BFS / flood-fill frontier marks
+  int32_t* mark[2];       // [nt] BFS / flood-fill frontier marks, alternating by round
+  int32_t* rcnt;          // [2] tiles processed by the current / next frontier round
   int32_t* tact;          // [nt] tile has an active pixel (excess > 0, height < HINF)
   int32_t* img_of;        // [nt] image index of the tile
   unsigned long long* ktiles;  // [K_COUNT] tiles processed per kernel kind (profiling)
@@ -104,6 +105,57 @@ __device__ __forceinline__ int32_t lookback_exclusive(const ScanState& st, uint3
   }
   __threadfence();
   status[chunk] = ss_pack(tag, SS_PREFIX, excl + aggregate);
+  return excl;
+}
+
+// Warp-parallel variant, executed by all 32 lanes of one warp: each step inspects the
+// status words of 32 predecessors at once.  Returns the exclusive prefix to every lane.
+__device__ __forceinline__ int32_t lookback_exclusive_warp(const ScanState& st, uint32_t tag,
+                                                           int chunk, int32_t aggregate) {
+  const int lane = threadIdx.x & 31;
+  volatile unsigned long long* status = st.status;
+  const uint32_t tg = tag & 0x3fffffffu;
+  if (chunk == 0) {
+    if (lane == 0) { __threadfence(); status[0] = ss_pack(tag, SS_PREFIX, aggregate); }
+    return 0;
+  }
+  if (lane == 0) { status[chunk] = ss_pack(tag, SS_AGG, aggregate); __threadfence(); }
+  __syncwarp();
+  int32_t excl = 0;
+  int j = chunk - 1;
+  int spins = 0;
+  bool gave_up = false;
+  while (j >= 0) {
+    const int idx = j - lane;
+    unsigned long long s = 0;
+    unsigned sst = SS_PREFIX;
+    int32_t v = 0;
+    bool ready = true;
+    if (idx >= 0) {
+      s = status[idx];
+      sst = (unsigned)((s >> 32) & 3u);
+      ready = (uint32_t)(s >> 34) == tg && sst != SS_NONE;
+      v = (int32_t)(uint32_t)(s & 0xffffffffull);
+    }
+    if (!__all_sync(0xffffffffu, ready)) {
+      if (++spins > GC_SPIN_LIMIT) { gave_up = true; break; }
+      __nanosleep(32);
+      continue;
+    }
+    const unsigned pm = __ballot_sync(0xffffffffu, idx >= 0 && sst == SS_PREFIX);
+    const int stop = pm ? __ffs(pm) - 1 : 31;      // nearest predecessor with a prefix
+    int32_t w = (lane <= stop && idx >= 0) ? v : 0;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+    excl += w;
+    if (pm || j - 31 < 0) break;
+    j -= 32;
+  }
+  if (lane == 0) {
+    if (gave_up) atomicExch(st.err, 1);
+    __threadfence();
+    status[chunk] = ss_pack(tag, SS_PREFIX, excl + aggregate);
+  }
   return excl;
 }
 

@@ -56,18 +56,38 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(ScanArgs a, ScanState st)
   const long long base = (long long)chunk * SCAN_CHUNK + (long long)threadIdx.x * SCAN_ITEMS;
 
   int32_t v[SCAN_ITEMS];
+  int32_t raw[SCAN_ITEMS], raw2[SCAN_ITEMS];
+  const bool vec = base + SCAN_ITEMS <= a.n && ((reinterpret_cast<uintptr_t>(a.in) & 15) == 0) &&
+                   (a.mode != GC_SCAN_MODE_LOGICAL || (reinterpret_cast<uintptr_t>(a.in2) & 15) == 0);
+  if (vec) {
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k += 4) {
+      const int4 q = *reinterpret_cast<const int4*>(a.in + base + k);
+      raw[k] = q.x; raw[k + 1] = q.y; raw[k + 2] = q.z; raw[k + 3] = q.w;
+      if (a.mode == GC_SCAN_MODE_LOGICAL) {
+        const int4 q2 = *reinterpret_cast<const int4*>(a.in2 + base + k);
+        raw2[k] = q2.x; raw2[k + 1] = q2.y; raw2[k + 2] = q2.z; raw2[k + 3] = q2.w;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+      const long long i = base + k;
+      raw[k] = i < a.n ? a.in[i] : 0;
+      raw2[k] = (i < a.n && a.mode == GC_SCAN_MODE_LOGICAL) ? a.in2[i] : 0;
+    }
+  }
 #pragma unroll
   for (int k = 0; k < SCAN_ITEMS; ++k) {
-    long long i = base + k;
+    const long long i = base + k;
     int32_t x = 0;
     if (i < a.n) {
-      int32_t raw = a.in[i];
       switch (a.mode) {
-        case GC_SCAN_MODE_SCAN: x = raw; break;
-        case GC_SCAN_MODE_COMPACT: x = raw != 0; break;
-        case GC_SCAN_MODE_FLAG: x = op_apply(a.op1, raw, a.a1); break;
+        case GC_SCAN_MODE_SCAN: x = raw[k]; break;
+        case GC_SCAN_MODE_COMPACT: x = raw[k] != 0; break;
+        case GC_SCAN_MODE_FLAG: x = op_apply(a.op1, raw[k], a.a1); break;
         default: {
-          bool f1 = op_apply(a.op1, raw, a.a1), f2 = op_apply(a.op2, a.in2[i], a.a2);
+          const bool f1 = op_apply(a.op1, raw[k], a.a1), f2 = op_apply(a.op2, raw2[k], a.a2);
           x = a.logical == 0 ? (f1 && f2) : (f1 || f2);
         }
       }
@@ -80,7 +100,10 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(ScanArgs a, ScanState st)
   for (int k = 0; k < SCAN_ITEMS; ++k) tsum += v[k];
   int32_t agg;
   int32_t tex = block_exclusive_scan(tsum, sm, &agg);
-  if (threadIdx.x == 0) s_excl = lookback_exclusive(st, s_tag, chunk, agg);
+  if (threadIdx.x < 32) {
+    const int32_t ex = lookback_exclusive_warp(st, s_tag, chunk, agg);
+    if (threadIdx.x == 0) s_excl = ex;
+  }
   __syncthreads();
   int32_t run = s_excl + tex;
 #pragma unroll

@@ -88,7 +88,8 @@ k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
     P.tact[t] = anypos;
     P.touched[t] = 0;
     P.act_int[t] = 0;
-    P.mark[t] = 0;
+    P.mark[0][t] = 0;
+    P.mark[1][t] = 0;
     P.img_of[t] = img;
   }
 }
@@ -322,39 +323,59 @@ k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
 // discharge or a tile-edge pixel is active after this relabel.
 // ------------------------------------------------------------------------------------
 constexpr int EB_THREADS = 256;
-constexpr int EB_TILES = 256;
+constexpr int EB_TILES = EB_THREADS / 32;   // one warp per tile
 
-__device__ __forceinline__ int edge_relabel_pixel(const PoolView& P, int t, int4 nb, int r,
-                                                  int c) {
-  const long long o = (long long)t * GC_TILE_PX + r * GC_TILE + c;
-  const int e = P.exc[o];
-  const int h = P.hgt[o];
-  if (!(e > 0 && h < GC_HINF)) return 0;
-  const int cu = P.cap[DUP][o], cd = P.cap[DDOWN][o], cl = P.cap[DLEFT][o], cr = P.cap[DRIGHT][o];
-  int hu = GC_HINF, hd = GC_HINF, hl = GC_HINF, hr = GC_HINF;
-  if (r > 0) hu = P.hgt[o - GC_TILE]; else if (nb.x >= 0) hu = P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + c];
-  if (r < 31) hd = P.hgt[o + GC_TILE]; else if (nb.y >= 0) hd = P.hgt[(long long)nb.y * GC_TILE_PX + c];
-  if (c > 0) hl = P.hgt[o - 1]; else if (nb.z >= 0) hl = P.hgt[(long long)nb.z * GC_TILE_PX + r * GC_TILE + 31];
-  if (c < 31) hr = P.hgt[o + 1]; else if (nb.w >= 0) hr = P.hgt[(long long)nb.w * GC_TILE_PX + r * GC_TILE];
-  const bool adm = (cu > 0 && h == hu + 1) || (cd > 0 && h == hd + 1) || (cl > 0 && h == hl + 1) ||
-                   (cr > 0 && h == hr + 1);
-  if (adm) return 1;
-  int m = GC_HINF;
-  if (cu > 0) m = imin(m, hu + 1);
-  if (cd > 0) m = imin(m, hd + 1);
-  if (cl > 0) m = imin(m, hl + 1);
-  if (cr > 0) m = imin(m, hr + 1);
-  m = imin(m, GC_HINF);
-  if (m != h) P.hgt[o] = m;
-  return m < GC_HINF;
+// Relabels up to four tile-edge pixels of one lane (Jacobi: neighbour heights are read
+// as they are, a concurrent update only makes them larger, which keeps the labelling
+// valid).  Returns whether one of them is active afterwards.
+__device__ __forceinline__ int edge_relabel_lane(const PoolView& P, int t, int4 nb, int lane) {
+  int rr[4] = {0, 31, lane, lane}, cc[4] = {lane, lane, 0, 31};
+  const bool use[4] = {true, true, lane > 0 && lane < 31, lane > 0 && lane < 31};
+  const long long base = (long long)t * GC_TILE_PX;
+  int e[4], h[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const long long o = base + rr[k] * GC_TILE + cc[k];
+    e[k] = use[k] ? P.exc[o] : 0;
+    h[k] = use[k] ? P.hgt[o] : GC_HINF;
+  }
+  int act = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (!(e[k] > 0 && h[k] < GC_HINF)) continue;
+    const int r = rr[k], c = cc[k];
+    const long long o = base + r * GC_TILE + c;
+    const int cu = P.cap[DUP][o], cd = P.cap[DDOWN][o], cl = P.cap[DLEFT][o], cr = P.cap[DRIGHT][o];
+    int hu = GC_HINF, hd = GC_HINF, hl = GC_HINF, hr = GC_HINF;
+    if (r > 0) hu = P.hgt[o - GC_TILE]; else if (nb.x >= 0) hu = P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + c];
+    if (r < 31) hd = P.hgt[o + GC_TILE]; else if (nb.y >= 0) hd = P.hgt[(long long)nb.y * GC_TILE_PX + c];
+    if (c > 0) hl = P.hgt[o - 1]; else if (nb.z >= 0) hl = P.hgt[(long long)nb.z * GC_TILE_PX + r * GC_TILE + 31];
+    if (c < 31) hr = P.hgt[o + 1]; else if (nb.w >= 0) hr = P.hgt[(long long)nb.w * GC_TILE_PX + r * GC_TILE];
+    const int hh = h[k];
+    const bool adm = (cu > 0 && hh == hu + 1) || (cd > 0 && hh == hd + 1) || (cl > 0 && hh == hl + 1) ||
+                     (cr > 0 && hh == hr + 1);
+    if (adm) { act = 1; continue; }
+    int m = GC_HINF;
+    if (cu > 0) m = imin(m, hu + 1);
+    if (cd > 0) m = imin(m, hd + 1);
+    if (cl > 0) m = imin(m, hl + 1);
+    if (cr > 0) m = imin(m, hr + 1);
+    m = imin(m, GC_HINF);
+    if (m != hh) P.hgt[o] = m;
+    act |= m < GC_HINF;
+  }
+  return act;
 }
 
+// Edge relabel + active-tile list (one launch).  A CTA owns EB_TILES consecutive tiles (one
+// warp each) by arrival ticket; a tile is active when an interior pixel was active after its
+// discharge or a tile-edge pixel is active after this relabel.  The active tiles are
+// compacted in tile order with a warp-parallel decoupled look-back.
 __global__ void __launch_bounds__(EB_THREADS)
 k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
-  __shared__ int32_t sm[32];
+  __shared__ int32_t flag[EB_TILES];
   __shared__ int32_t s_chunk, s_excl;
   __shared__ uint32_t s_tag;
-  __shared__ int32_t flag[EB_TILES];
   if (threadIdx.x == 0) {
     s_chunk = atomicAdd(st.ticket, 1);
     s_tag = *((volatile uint32_t*)st.seq);
@@ -363,35 +384,33 @@ k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
   const int chunk = s_chunk;
   const int nchunks = (P.nt + EB_TILES - 1) / EB_TILES;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int k = 0; k < 32; ++k) {
-    const int slot = warp * 32 + k;
-    const int t = chunk * EB_TILES + slot;
-    int active = 0;
-    if (t < P.nt && P.touched[t]) {
-      const int4 nb = P.nbr[t];
-      int a = edge_relabel_pixel(P, t, nb, 0, lane);
-      a |= edge_relabel_pixel(P, t, nb, 31, lane);
-      if (lane > 0 && lane < 31) {
-        a |= edge_relabel_pixel(P, t, nb, lane, 0);
-        a |= edge_relabel_pixel(P, t, nb, lane, 31);
-      }
-      active = __any_sync(0xffffffffu, a) | P.act_int[t];
-      if (lane == 0) {
-        P.touched[t] = 0;
-        if (P.ktiles) atomicAdd(&P.ktiles[K_EDGE_BUILD], 1ull);
-      }
+  const int t = chunk * EB_TILES + warp;
+  int active = 0;
+  if (t < P.nt && P.touched[t]) {
+    const int4 nb = P.nbr[t];
+    const int a = edge_relabel_lane(P, t, nb, lane);
+    active = __any_sync(0xffffffffu, a) | P.act_int[t];
+    if (lane == 0) {
+      P.touched[t] = 0;
+      if (P.ktiles) atomicAdd(&P.ktiles[K_EDGE_BUILD], 1ull);
     }
-    if (lane == 0) flag[slot] = active;
   }
+  if (lane == 0) flag[warp] = active;
   __syncthreads();
-  const int v = flag[threadIdx.x];
-  int32_t agg;
-  const int32_t ex = block_exclusive_scan(v, sm, &agg);
-  if (threadIdx.x == 0) s_excl = lookback_exclusive(st, s_tag, chunk, agg);
-  __syncthreads();
-  if (v) list[s_excl + ex] = chunk * EB_TILES + threadIdx.x;
-  if (chunk == nchunks - 1 && threadIdx.x == 0) *count = s_excl + agg;
-  if (threadIdx.x == 0) scan_finish(st, nchunks);
+  if (warp == 0) {
+    const int v = lane < EB_TILES ? flag[lane] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    const int agg = __shfl_sync(0xffffffffu, x, 31);
+    const int excl = lookback_exclusive_warp(st, s_tag, chunk, agg);
+    if (v) list[excl + x - v] = chunk * EB_TILES + lane;
+    if (chunk == nchunks - 1 && lane == 0) *count = excl + agg;
+    if (lane == 0) scan_finish(st, nchunks);
+  }
 }
 
 // ------------------------------------------------------------------------------------
@@ -447,15 +466,29 @@ __device__ __forceinline__ void tile_bfs(int (&d)[32], uint32_t canU, uint32_t c
   }
 }
 
+// Frontier rounds: round `rnd` processes the tiles marked in mark[rnd & 1] (every tile when
+// `first`), marks neighbours in mark[(rnd + 1) & 1] and counts its tiles in rcnt[rnd & 1];
+// it zeroes rcnt for the next round.
+__device__ __forceinline__ void frontier_round_begin(const PoolView& P, int in) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) P.rcnt[in ^ 1] = 0;
+}
+
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
-k_bfs_round(PoolView P, const int32_t* __restrict__ list, const int32_t* __restrict__ count,
-            int first) {
+k_bfs_round(PoolView P, int first, int rnd) {
   __shared__ int32_t tr[WARPS_PER_CTA][32 * 33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int n = first ? P.nt : *count;
+  const int in = rnd & 1, out = in ^ 1;
+  int32_t* const markin = P.mark[in];
+  int32_t* const markout = P.mark[out];
+  frontier_round_begin(P, in);
   int32_t* T = tr[warp];
-  for (int w = blockIdx.x * WARPS_PER_CTA + warp; w < n; w += gridDim.x * WARPS_PER_CTA) {
-    const int t = first ? w : list[w];
+  int done = 0;
+  for (int t = blockIdx.x * WARPS_PER_CTA + warp; t < P.nt; t += gridDim.x * WARPS_PER_CTA) {
+    if (!first) {
+      if (!markin[t]) continue;
+      if (lane == 0) markin[t] = 0;
+    }
+    ++done;
     const int4 nb = P.nbr[t];
     const long long base = (long long)t * GC_TILE_PX;
     uint32_t canU, canD, canL, canR, sink;
@@ -524,12 +557,15 @@ k_bfs_round(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
     const int act = __any_sync(0xffffffffu, (pos & fin) != 0);
     if (lane == 0) {
       P.tact[t] = act;
-      if (P.ktiles) atomicAdd(&P.ktiles[first ? K_BFS_FIRST : K_BFS], 1ull);
-      if (chU && nb.x >= 0) P.mark[nb.x] = 1;
-      if (chD && nb.y >= 0) P.mark[nb.y] = 1;
-      if (chL && nb.z >= 0) P.mark[nb.z] = 1;
-      if (chR && nb.w >= 0) P.mark[nb.w] = 1;
+      if (chU && nb.x >= 0) markout[nb.x] = 1;
+      if (chD && nb.y >= 0) markout[nb.y] = 1;
+      if (chL && nb.z >= 0) markout[nb.z] = 1;
+      if (chR && nb.w >= 0) markout[nb.w] = 1;
     }
+  }
+  if (lane == 0 && done) {
+    atomicAdd(&P.rcnt[in], done);
+    if (P.ktiles) atomicAdd(&P.ktiles[first ? K_BFS_FIRST : K_BFS], (unsigned long long)done);
   }
 }
 
@@ -538,12 +574,19 @@ k_bfs_round(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
 // Round 1 also sums max(excess, 0) per image for the flow value.
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
-k_flood_round(PoolView P, const int32_t* __restrict__ list, const int32_t* __restrict__ count,
-              int first, ImageAcc* acc) {
+k_flood_round(PoolView P, int first, int rnd, ImageAcc* acc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int n = first ? P.nt : *count;
-  for (int w = blockIdx.x * WARPS_PER_CTA + warp; w < n; w += gridDim.x * WARPS_PER_CTA) {
-    const int t = first ? w : list[w];
+  const int in = rnd & 1, out = in ^ 1;
+  int32_t* const markin = P.mark[in];
+  int32_t* const markout = P.mark[out];
+  frontier_round_begin(P, in);
+  int done = 0;
+  for (int t = blockIdx.x * WARPS_PER_CTA + warp; t < P.nt; t += gridDim.x * WARPS_PER_CTA) {
+    if (!first) {
+      if (!markin[t]) continue;
+      if (lane == 0) markin[t] = 0;
+    }
+    ++done;
     const int4 nb = P.nbr[t];
     const uint32_t* mc = P.mcan + (long long)t * 128;
     const uint32_t canU = mc[lane], canD = mc[32 + lane], canL = mc[64 + lane], canR = mc[96 + lane];
@@ -585,12 +628,15 @@ k_flood_round(PoolView P, const int32_t* __restrict__ list, const int32_t* __res
     const int sL = __any_sync(0xffffffffu, (nw & canL & 1u) != 0);
     const int sR = __any_sync(0xffffffffu, ((nw & canR) >> 31) != 0);
     if (lane == 0) {
-      if (P.ktiles) atomicAdd(&P.ktiles[first ? K_FLOOD_FIRST : K_FLOOD], 1ull);
-      if (sU && nb.x >= 0) P.mark[nb.x] = 1;
-      if (sD && nb.y >= 0) P.mark[nb.y] = 1;
-      if (sL && nb.z >= 0) P.mark[nb.z] = 1;
-      if (sR && nb.w >= 0) P.mark[nb.w] = 1;
+      if (sU && nb.x >= 0) markout[nb.x] = 1;
+      if (sD && nb.y >= 0) markout[nb.y] = 1;
+      if (sL && nb.z >= 0) markout[nb.z] = 1;
+      if (sR && nb.w >= 0) markout[nb.w] = 1;
     }
+  }
+  if (lane == 0 && done) {
+    atomicAdd(&P.rcnt[in], done);
+    if (P.ktiles) atomicAdd(&P.ktiles[first ? K_FLOOD_FIRST : K_FLOOD], (unsigned long long)done);
   }
 }
 
@@ -688,15 +734,14 @@ int launch_edge_relabel_build(const PoolView& P, int32_t* list, int32_t* count,
   return ok();
 }
 
-int launch_bfs_round(const PoolView& P, const int32_t* list, const int32_t* count, int first,
-                     int grid, cudaStream_t s) {
-  k_bfs_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, list, count, first);
+int launch_bfs_round(const PoolView& P, int first, int rnd, int grid, cudaStream_t s) {
+  k_bfs_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, first, rnd);
   return ok();
 }
 
-int launch_flood_round(const PoolView& P, const int32_t* list, const int32_t* count, int first,
-                       ImageAcc* acc, int grid, cudaStream_t s) {
-  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, list, count, first, acc);
+int launch_flood_round(const PoolView& P, int first, int rnd, ImageAcc* acc, int grid,
+                       cudaStream_t s) {
+  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, first, rnd, acc);
   return ok();
 }
 

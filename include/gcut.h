@@ -52,8 +52,8 @@ extern "C" {
 typedef struct gc_opts {
   int device;              /* CUDA device ordinal */
   int discharge_iters;     /* push + interior-relabel iterations inside a tile per launch */
-  int pulses_per_relabel;  /* discharge launches between global relabels (reference: bfs=5,
-                              GraphCut.pyx:27) */
+  int pulses_per_relabel;  /* discharge launches between global relabels, >= 1 (reference:
+                              bfs=5 push iterations, GraphCut.pyx:27) */
   int initial_relabel;     /* 1: exact global relabel before the first push; 0: start from
                               heights 0 (sink pixels) / 1 (others) */
   int max_cycles;          /* cap on global-relabel cycles; exceeded -> GC_ERR_NOT_CONVERGED */

@@ -50,7 +50,7 @@ def test_random_graphs(cuda, oracle, seed, sym, sparsity):
     check(g, oracle)
 
 
-@pytest.mark.parametrize("iters,pulses,init", [(1, 1, 0), (4, 1, 1), (64, 5, 0), (32, 0, 1)])
+@pytest.mark.parametrize("iters,pulses,init", [(1, 1, 0), (4, 1, 1), (64, 5, 0), (32, 1, 1)])
 def test_schedules_agree(cuda, oracle, iters, pulses, init):
     g = synth.random_graph(160, 128, 11, cap_max=80, tlink_max=120, symmetric=False)
     check(g, oracle, discharge_iters=iters, bfs=pulses, initial_relabel=bool(init))
@@ -189,6 +189,14 @@ def test_cycle_cap_reports_not_converged(cuda):
         with pytest.raises(_gcut.GCError) as ei:
             gc.cut()
         assert ei.value.code == _gcut.GC_ERR_NOT_CONVERGED
+
+
+def test_invalid_options_rejected(cuda):
+    import _gcut
+    for kw in ({"bfs": 0}, {"discharge_iters": 0}, {"max_cycles": 0}):
+        with pytest.raises(_gcut.GCError) as ei:
+            GraphCut(64, 64, **kw)
+        assert ei.value.code == _gcut.GC_ERR_INVALID
 
 
 def test_state_errors(cuda):
