@@ -42,14 +42,16 @@ class GraphCut:
 
     def __init__(self, width: int, height: int, device: int = 0, bfs: int | None = None,
                  discharge_iters: int | None = None, initial_relabel: bool | None = None,
-                 max_cycles: int | None = None, max_bfs_rounds: int | None = None):
+                 max_cycles: int | None = None, max_bfs_rounds: int | None = None,
+                 use_graph: bool | None = None):
         import torch
         self.width, self.height = int(width), int(height)
         self.device = torch.device("cuda", device)
         opts = _gcut.default_opts(device=device, discharge_iters=discharge_iters,
                                   pulses_per_relabel=bfs,
                                   initial_relabel=None if initial_relabel is None else int(initial_relabel),
-                                  max_cycles=max_cycles, max_bfs_rounds=max_bfs_rounds)
+                                  max_cycles=max_cycles, max_bfs_rounds=max_bfs_rounds,
+                                  use_graph=None if use_graph is None else int(use_graph))
         self.opts = opts
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):

@@ -20,14 +20,16 @@ from _gcut import check, lib, ptr, stream_handle
 
 class GraphCutBatch:
     def __init__(self, shapes, device: int = 0, bfs=None, discharge_iters=None,
-                 initial_relabel=None, max_cycles=None, max_bfs_rounds=None):
+                 initial_relabel=None, max_cycles=None, max_bfs_rounds=None,
+                 use_graph=None):
         import torch
         self.shapes = [(int(w), int(h)) for (w, h) in shapes]
         self.device = torch.device("cuda", device)
         opts = _gcut.default_opts(device=device, discharge_iters=discharge_iters,
                                   pulses_per_relabel=bfs,
                                   initial_relabel=None if initial_relabel is None else int(initial_relabel),
-                                  max_cycles=max_cycles, max_bfs_rounds=max_bfs_rounds)
+                                  max_cycles=max_cycles, max_bfs_rounds=max_bfs_rounds,
+                                  use_graph=None if use_graph is None else int(use_graph))
         n = len(self.shapes)
         ws = (ctypes.c_int * n)(*[w for w, _ in self.shapes])
         hs = (ctypes.c_int * n)(*[h for _, h in self.shapes])

@@ -32,7 +32,8 @@ class GCError(RuntimeError):
 class GcOpts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("discharge_iters", ctypes.c_int),
                 ("pulses_per_relabel", ctypes.c_int), ("initial_relabel", ctypes.c_int),
-                ("max_cycles", ctypes.c_int), ("max_bfs_rounds", ctypes.c_int)]
+                ("max_cycles", ctypes.c_int), ("max_bfs_rounds", ctypes.c_int),
+                ("use_graph", ctypes.c_int)]
 
 
 class GcStats(ctypes.Structure):

@@ -89,6 +89,8 @@ struct Pool {
   ImageAcc* acc = nullptr;     // per image
   ScanBuffers scan;
   int32_t* h_count = nullptr;  // pinned
+  int32_t* h_ctl = nullptr;    // pinned copy of the control words
+  bool use_graph = true;
   ImageAcc* h_acc = nullptr;   // pinned
   int grid_dis = 0, grid_warps = 0;
   bool uploaded = false, solved = false, edited = false, collect = false;
@@ -152,8 +154,8 @@ struct Pool {
 
   void release() {
     int32_t* bufs[] = {P.exc, P.hgt, P.cap[0], P.cap[1], P.cap[2], P.cap[3], tl, list, counts,
-                       P.touched, P.act_int, P.mark[0], P.mark[1], P.rcnt, P.tact, P.img_of,
-                       stage, pts};
+                       P.touched, P.act_int, P.mark[0], P.mark[1], P.rcnt, P.ctl, P.tact,
+                       P.img_of, stage, pts};
     for (auto* b : bufs) if (b) cudaFree(b);
     if (P.nbr) cudaFree(P.nbr);
     if (P.mcan) cudaFree(P.mcan);
@@ -162,7 +164,10 @@ struct Pool {
     if (P.mreach) cudaFree(P.mreach);
     if (acc) cudaFree(acc);
     if (lstage) cudaFree(lstage);
+    release_graphs();
     if (h_count) cudaFreeHost(h_count);
+    if (h_ctl) cudaFreeHost(h_ctl);
+    h_ctl = nullptr;
     if (h_acc) cudaFreeHost(h_acc);
     if (ktiles) cudaFree(ktiles);
     for (auto e : ev_pool) cudaEventDestroy(e);
@@ -178,6 +183,7 @@ struct Pool {
     if (n <= 0 || !W || !H) return fail(GC_ERR_INVALID, "no images");
     opts = *o;
     device = opts.device;
+    use_graph = opts.use_graph != 0;
     nt = 0;
     for (int i = 0; i < n; ++i) {
       if (W[i] <= 0 || H[i] <= 0 || W[i] > (1 << 16) || H[i] > (1 << 16))
@@ -208,6 +214,8 @@ struct Pool {
     // look-back slots: the scan uses one per 4096 items, the list rebuild one per 8 tiles
     if (!e) e = scan.alloc(scan_chunks(nt) > nt / 8 + 1 ? scan_chunks(nt) : nt / 8 + 1);
     if (!e) e = cudaMallocHost((void**)&h_count, 4 * sizeof(int32_t));
+    if (!e) e = cudaMallocHost((void**)&h_ctl, CTL_N * sizeof(int32_t));
+    if (!e) e = dalloc(&P.ctl, CTL_N);
     if (!e) e = cudaMallocHost((void**)&h_acc, imgs.size() * sizeof(ImageAcc));
     if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); release(); return fail(GC_ERR_OOM, "device allocation failed"); }
     if (e) { release(); return cuda_fail(e, "pool allocation"); }
@@ -224,6 +232,7 @@ struct Pool {
     CK(cudaMemset(P.mark[0], 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.mark[1], 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.rcnt, 0, sizeof(int32_t) * 2));
+    CK(cudaMemset(P.ctl, 0, sizeof(int32_t) * CTL_N));
     CK(cudaMemset(P.act_int, 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.tact, 0, sizeof(int32_t) * nt));
     CK(cudaMemset(acc, 0, sizeof(ImageAcc) * imgs.size()));
@@ -248,32 +257,33 @@ struct Pool {
     return GC_OK;
   }
 
-  // exact BFS distances to the sink pixels (global relabel); sets tact
+  // exact BFS distances to the sink pixels (global relabel); sets tact.  h: condition
+  // handle when captured into a graph (0: host-driven rounds)
   int global_relabel(cudaStream_t s) {
     RK(timed(K_BFS_FIRST, s, [&] { return launch_bfs_round(P, 1, 0, grid_warps, s); }));
-    stats.bfs_rounds++;
     return frontier_rounds(s, /*flood=*/false);
   }
 
-  // rounds over the marked tiles until a round finds none; the host reads the per-round
-  // tile counter once per batch of rounds
+  // host-driven rounds over the marked tiles until a round finds none; the host reads
+  // the control words once per batch of rounds
   int frontier_rounds(cudaStream_t s, bool flood) {
     int batch = 4;
-    long long rounds = 0;
-    int rnd = 1;
     while (true) {
-      for (int k = 0; k < batch; ++k, ++rnd) {
-        if (flood) RK(timed(K_FLOOD, s, [&] { return launch_flood_round(P, 0, rnd, acc, grid_warps, s); }));
-        else RK(timed(K_BFS, s, [&] { return launch_bfs_round(P, 0, rnd, grid_warps, s); }));
+      for (int k = 0; k < batch; ++k) {
+        if (flood) RK(timed(K_FLOOD, s, [&] { return launch_flood_round(P, 0, 0, acc, grid_warps, s); }));
+        else RK(timed(K_BFS, s, [&] { return launch_bfs_round(P, 0, 0, grid_warps, s); }));
       }
-      rounds += batch;
-      if (flood) stats.flood_rounds += batch; else stats.bfs_rounds += batch;
-      CK(cudaMemcpyAsync(h_count, P.rcnt + ((rnd - 1) & 1), sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      if (h_count[0] == 0) break;
-      if (rounds >= opts.max_bfs_rounds) return fail(GC_ERR_NOT_CONVERGED, "BFS round cap reached");
+      RK(read_ctl(s));
+      if (h_ctl[CTL_ERR] == 1) return fail(GC_ERR_NOT_CONVERGED, "BFS round cap reached");
+      if (h_ctl[CTL_LASTCNT] == 0) break;
       batch = batch < 32 ? batch * 2 : 32;
     }
+    return GC_OK;
+  }
+
+  int read_ctl(cudaStream_t s) {
+    CK(cudaMemcpyAsync(h_ctl, P.ctl, sizeof(int32_t) * CTL_N, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     return GC_OK;
   }
 
@@ -307,16 +317,26 @@ struct Pool {
     if (!uploaded) return fail(GC_ERR_STATE, "solve before upload");
     CK(cudaSetDevice(device));
     stats = gc_stats{};
-    RK(prof_begin(s));
-    int n = 0;
     const bool relabel_first = opts.initial_relabel || edited || solved;
+    int r = (prof || collect || !use_graph) ? solve_host(s, relabel_first) : solve_graph(s, relabel_first);
+    if (r) return r;
+    return finish_check(s);
+  }
+
+  // Host-driven solve (profiling, stats collection): same kernels, host decides the loops.
+  int solve_host(cudaStream_t s, bool relabel_first) {
+    RK(prof_begin(s));
+    RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, s));
+    int n = 0;
     if (relabel_first) RK(global_relabel(s));
     RK(compact(P.tact, nullptr, s));
+    bool go = true;
     if (relabel_first) {
       RK(read_count(s, &n));
-      if (n == 0) return finish(s);
+      go = n > 0;
     }
-    for (int cycle = 0; cycle < opts.max_cycles; ++cycle) {
+    for (int cycle = 0; go; ++cycle) {
+      if (cycle >= opts.max_cycles) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
       stats.cycles++;
       for (int p = 0; p < opts.pulses_per_relabel; ++p) {
         RK(timed(K_DISCHARGE, s, [&] { return launch_discharge(P, list, counts, opts.discharge_iters, grid_dis, s); }));
@@ -327,23 +347,163 @@ struct Pool {
       RK(global_relabel(s));
       RK(compact(P.tact, nullptr, s));
       RK(read_count(s, &n));
-      if (n == 0) return finish(s);
+      go = n > 0;
     }
-    return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
-  }
-
-  // canonical cut (flood from excess pixels) and the flow sums
-  int finish(cudaStream_t s) {
-    for (size_t i = 0; i < imgs.size(); ++i)
-      CK(cudaMemsetAsync(&acc[i].sumpos_e, 0, sizeof(unsigned long long), s));
+    RK(launch_acc_reset(acc, (int)imgs.size(), s));
     RK(timed(K_FLOOD_FIRST, s, [&] { return launch_flood_round(P, 1, 0, acc, grid_warps, s); }));
-    stats.flood_rounds++;
     RK(frontier_rounds(s, /*flood=*/true));
     CK(cudaMemcpyAsync(h_acc, acc, sizeof(ImageAcc) * imgs.size(), cudaMemcpyDeviceToHost, s));
+    RK(read_ctl(s));
+    RK(prof_end(s));
+    return GC_OK;
+  }
+
+  // ---- CUDA graph solve: the whole solve is one graph launch.  The loops are WHILE nodes
+  // whose conditions are set on the device (frontier rounds by their last CTA, cycles by
+  // k_ctl_cycle), so the host waits once, at the end.
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};   // [relabel_first]
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+
+  template <class F>
+  int capture(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves, F&& fn) {
+    CK(cudaStreamBeginCaptureToGraph(cap_stream, g, leaves.empty() ? nullptr : leaves.data(),
+                                     nullptr, leaves.size(), cudaStreamCaptureModeThreadLocal));
+    const int r = fn(cap_stream);
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    const cudaError_t e1 = cudaStreamGetCaptureInfo(cap_stream, &st, nullptr, nullptr, &deps, &nd);
+    std::vector<cudaGraphNode_t> nl(deps, deps + (e1 == cudaSuccess ? nd : 0));
+    cudaGraph_t out = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(cap_stream, &out);
+    if (r) return r;
+    if (e1) return cuda_fail(e1, "cudaStreamGetCaptureInfo");
+    if (e2) return cuda_fail(e2, "cudaStreamEndCapture");
+    if (!nl.empty()) leaves = nl;
+    return GC_OK;
+  }
+
+  int add_while(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves,
+                cudaGraphConditionalHandle h, cudaGraph_t* body) {
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, leaves.empty() ? nullptr : leaves.data(), leaves.size(), &p));
+    *body = p.conditional.phGraph_out[0];
+    leaves.assign(1, node);
+    return GC_OK;
+  }
+
+  int build_graph(int variant) {
+    if (!cap_stream) CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0));
+    graph[variant] = g;
+    std::vector<cudaGraphNode_t> L;
+    cudaGraphConditionalHandle hmain, hflood;
+    CK(cudaGraphConditionalHandleCreate(&hmain, g, 0, 0));
+    CK(cudaGraphConditionalHandleCreate(&hflood, g, 0, 0));
+    RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, cs); }));
+    if (variant) {  // exact global relabel before the first push
+      cudaGraphConditionalHandle h0;
+      CK(cudaGraphConditionalHandleCreate(&h0, g, 0, 0));
+      RK(capture(g, L, [&](cudaStream_t cs) { return launch_bfs_round(P, 1, h0, grid_warps, cs); }));
+      cudaGraph_t b0;
+      RK(add_while(g, L, h0, &b0));
+      std::vector<cudaGraphNode_t> Lb;
+      RK(capture(b0, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, h0, grid_warps, cs); }));
+    }
+    RK(capture(g, L, [&](cudaStream_t cs) {
+      RK(launch_scan(GC_SCAN_MODE_COMPACT, P.tact, nullptr, nullptr, nullptr, list, counts, nt, 0, 0, 0, 0, 0, scan.st, cs));
+      return launch_ctl_cycle(P, counts, 0, hmain, cs);
+    }));
+    cudaGraph_t bm;
+    RK(add_while(g, L, hmain, &bm));
+    {
+      std::vector<cudaGraphNode_t> Lm;
+      cudaGraphConditionalHandle hb;
+      CK(cudaGraphConditionalHandleCreate(&hb, bm, 0, 0));
+      RK(capture(bm, Lm, [&](cudaStream_t cs) {
+        for (int p = 0; p < opts.pulses_per_relabel; ++p) {
+          RK(launch_discharge(P, list, counts, opts.discharge_iters, grid_dis, cs));
+          RK(launch_edge_relabel_build(P, list, counts, scan.st, cs));
+        }
+        return launch_bfs_round(P, 1, hb, grid_warps, cs);
+      }));
+      cudaGraph_t bb;
+      RK(add_while(bm, Lm, hb, &bb));
+      std::vector<cudaGraphNode_t> Lb;
+      RK(capture(bb, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, hb, grid_warps, cs); }));
+      RK(capture(bm, Lm, [&](cudaStream_t cs) {
+        RK(launch_scan(GC_SCAN_MODE_COMPACT, P.tact, nullptr, nullptr, nullptr, list, counts, nt, 0, 0, 0, 0, 0, scan.st, cs));
+        return launch_ctl_cycle(P, counts, 1, hmain, cs);
+      }));
+    }
+    RK(capture(g, L, [&](cudaStream_t cs) {
+      RK(launch_acc_reset(acc, (int)imgs.size(), cs));
+      return launch_flood_round(P, 1, hflood, acc, grid_warps, cs);
+    }));
+    cudaGraph_t bf;
+    RK(add_while(g, L, hflood, &bf));
+    {
+      std::vector<cudaGraphNode_t> Lf;
+      RK(capture(bf, Lf, [&](cudaStream_t cs) { return launch_flood_round(P, 0, hflood, acc, grid_warps, cs); }));
+    }
+    RK(capture(g, L, [&](cudaStream_t cs) {
+      CK(cudaMemcpyAsync(h_acc, acc, sizeof(ImageAcc) * imgs.size(), cudaMemcpyDeviceToHost, cs));
+      CK(cudaMemcpyAsync(h_ctl, P.ctl, sizeof(int32_t) * CTL_N, cudaMemcpyDeviceToHost, cs));
+      return GC_OK;
+    }));
+    CK(cudaGraphInstantiate(&gexec[variant], g, 0));
+    return GC_OK;
+  }
+
+  int solve_graph(cudaStream_t s, bool relabel_first) {
+    const int v = relabel_first ? 1 : 0;
+    if (!gexec[v]) {
+      const int r = build_graph(v);
+      if (r) {
+        if (graph[v]) { cudaGraphDestroy(graph[v]); graph[v] = nullptr; }
+        return r;
+      }
+    }
+    P.ktiles = nullptr;
+    CK(cudaGraphLaunch(gexec[v], s));
+    CK(cudaStreamSynchronize(s));
+    stats.launches = -1;  // inside the graph; see gc_stats
+    return GC_OK;
+  }
+
+  void release_graphs() {
+    for (int v = 0; v < 2; ++v) {
+      if (gexec[v]) cudaGraphExecDestroy(gexec[v]);
+      if (graph[v]) cudaGraphDestroy(graph[v]);
+      gexec[v] = nullptr;
+      graph[v] = nullptr;
+    }
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    cap_stream = nullptr;
+  }
+
+  // errors and results common to both paths (h_acc / h_ctl are filled and synchronised)
+  int finish_check(cudaStream_t s) {
     RK(check_device_error(s));
+    if (h_ctl[CTL_ERR] == 1) return fail(GC_ERR_NOT_CONVERGED, "BFS round cap reached");
+    if (h_ctl[CTL_ERR] == 2) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
     for (size_t i = 0; i < imgs.size(); ++i)
       if (h_acc[i].bad_caps) return fail(GC_ERR_INVALID, "negative capacity in the upload");
-    RK(prof_end(s));
+    stats.bfs_rounds = h_ctl[CTL_BFS_TOTAL];
+    stats.flood_rounds = h_ctl[CTL_FLOOD_TOTAL];
+    if (stats.launches < 0) {  // graph solve: count the kernel nodes that ran
+      stats.cycles = h_ctl[CTL_CYCLES];
+      stats.pulses = stats.cycles * opts.pulses_per_relabel;
+      stats.launches = 3 + stats.cycles * (2LL * opts.pulses_per_relabel + 2) + stats.bfs_rounds +
+                       1 + stats.flood_rounds;
+    }
     solved = true;
     edited = false;
     return GC_OK;
@@ -369,6 +529,7 @@ struct Pool {
   }
   int step_start_bfs(cudaStream_t s) {
     if (!uploaded) return fail(GC_ERR_STATE, "startBfs before upload");
+    RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, s));
     RK(global_relabel(s));
     RK(compact(P.tact, nullptr, s));
     list_valid = true;
@@ -380,7 +541,14 @@ struct Pool {
     int n;
     RK(read_count(s, &n));
     *done = n == 0;
-    if (*done) RK(finish(s));
+    if (*done) {
+      RK(launch_acc_reset(acc, (int)imgs.size(), s));
+      RK(launch_flood_round(P, 1, 0, acc, grid_warps, s));
+      RK(frontier_rounds(s, /*flood=*/true));
+      CK(cudaMemcpyAsync(h_acc, acc, sizeof(ImageAcc) * imgs.size(), cudaMemcpyDeviceToHost, s));
+      RK(read_ctl(s));
+      RK(finish_check(s));
+    }
     return GC_OK;
   }
 
@@ -443,6 +611,7 @@ int gc_opts_default(gc_opts* o) {
   o->initial_relabel = 0;
   o->max_cycles = 100000;
   o->max_bfs_rounds = 1 << 20;
+  o->use_graph = 1;
   return GC_OK;
 }
 

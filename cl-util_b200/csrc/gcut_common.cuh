@@ -39,9 +39,27 @@ struct PoolView {
   int32_t* act_int;       // [nt] tile has an active interior pixel after its discharge
   int32_t* mark[2];       // [nt] BFS / flood-fill frontier marks, alternating by round
   int32_t* rcnt;          // [2] tiles processed by the current / next frontier round
+  int32_t* ctl;           // [CTL_N] device-side loop control (see CtlSlot)
   int32_t* tact;          // [nt] tile has an active pixel (excess > 0, height < HINF)
   int32_t* img_of;        // [nt] image index of the tile
   unsigned long long* ktiles;  // [K_COUNT] tiles processed per kernel kind (profiling)
+};
+
+// Device-side loop control words.  The last CTA of every frontier round advances the round
+// parity and decides whether another round follows; in a CUDA graph it also sets the
+// condition of the enclosing WHILE node, so no host round trip is needed per round.
+enum CtlSlot {
+  CTL_RND = 0,        // frontier round number (its parity selects the mark buffer)
+  CTL_DONE = 1,       // CTAs finished in the current round
+  CTL_LASTCNT = 2,    // tiles processed by the last finished round
+  CTL_ROUNDS = 3,     // rounds of the current frontier loop
+  CTL_BFS_TOTAL = 4,  // BFS rounds of the solve
+  CTL_FLOOD_TOTAL = 5,
+  CTL_CYCLES = 6,     // global-relabel cycles of the solve
+  CTL_ERR = 7,        // 1: round cap reached, 2: cycle cap reached
+  CTL_MAXROUNDS = 8,
+  CTL_MAXCYCLES = 9,
+  CTL_N = 16
 };
 
 // Kernel kinds for profiling (launch counts, event time, tiles processed).

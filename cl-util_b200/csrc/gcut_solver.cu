@@ -374,7 +374,7 @@ __device__ __forceinline__ int edge_relabel_lane(const PoolView& P, int t, int4 
 __global__ void __launch_bounds__(EB_THREADS)
 k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
   __shared__ int32_t flag[EB_TILES];
-  __shared__ int32_t s_chunk, s_excl;
+  __shared__ int32_t s_chunk;
   __shared__ uint32_t s_tag;
   if (threadIdx.x == 0) {
     s_chunk = atomicAdd(st.ticket, 1);
@@ -467,20 +467,74 @@ __device__ __forceinline__ void tile_bfs(int (&d)[32], uint32_t canU, uint32_t c
 }
 
 // Frontier rounds: round `rnd` processes the tiles marked in mark[rnd & 1] (every tile when
-// `first`), marks neighbours in mark[(rnd + 1) & 1] and counts its tiles in rcnt[rnd & 1];
-// it zeroes rcnt for the next round.
-__device__ __forceinline__ void frontier_round_begin(const PoolView& P, int in) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) P.rcnt[in ^ 1] = 0;
+// `first`), marks neighbours in mark[(rnd + 1) & 1] and counts its tiles in rcnt[rnd & 1].
+// The round number lives in device memory (ctl[CTL_RND]); the last CTA of a round consumes
+// the count, advances the round and, inside a CUDA graph, sets the WHILE condition.
+__device__ __forceinline__ int frontier_round_number(const PoolView& P, int first) {
+  return first ? 0 : *((volatile int32_t*)&P.ctl[CTL_RND]);
+}
+
+__device__ __forceinline__ void frontier_round_end(const PoolView& P, int first, int in,
+                                                   int total_slot, cudaGraphConditionalHandle h) {
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  __threadfence();
+  const int d = atomicAdd(&P.ctl[CTL_DONE], 1);
+  if (d != (int)gridDim.x - 1) return;
+  __threadfence();
+  volatile int32_t* ctl = P.ctl;
+  const int cnt = *((volatile int32_t*)&P.rcnt[in]);
+  P.rcnt[in] = 0;
+  ctl[CTL_LASTCNT] = cnt;
+  ctl[CTL_RND] = first ? 1 : ctl[CTL_RND] + 1;
+  const int rounds = first ? 1 : ctl[CTL_ROUNDS] + 1;
+  ctl[CTL_ROUNDS] = rounds;
+  ctl[total_slot] = ctl[total_slot] + 1;
+  ctl[CTL_DONE] = 0;
+  bool more = cnt > 0;
+  if (more && rounds >= ctl[CTL_MAXROUNDS]) {
+    ctl[CTL_ERR] = 1;
+    more = false;
+  }
+  __threadfence();
+  if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+// Solve prologue: reset the control words.
+__global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles) {
+  if (threadIdx.x < CTL_N) P.ctl[threadIdx.x] = 0;
+  if (threadIdx.x == 0) {
+    P.ctl[CTL_MAXROUNDS] = max_rounds;
+    P.ctl[CTL_MAXCYCLES] = max_cycles;
+    P.rcnt[0] = 0;
+    P.rcnt[1] = 0;
+  }
+}
+
+// After the active-tile compaction: another cycle runs while tiles are active and the cycle
+// cap is not reached (`count_cycle` counts this check as a finished cycle).
+__global__ void k_ctl_cycle(PoolView P, const int32_t* count, int count_cycle,
+                            cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0) return;
+  volatile int32_t* ctl = P.ctl;
+  int cycles = ctl[CTL_CYCLES] + (count_cycle ? 1 : 0);
+  ctl[CTL_CYCLES] = cycles;
+  bool more = *((volatile const int32_t*)count) > 0;
+  if (more && cycles >= ctl[CTL_MAXCYCLES]) {
+    ctl[CTL_ERR] = 2;
+    more = false;
+  }
+  __threadfence();
+  if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
-k_bfs_round(PoolView P, int first, int rnd) {
+k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
   __shared__ int32_t tr[WARPS_PER_CTA][32 * 33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int in = rnd & 1, out = in ^ 1;
+  const int in = frontier_round_number(P, first) & 1, out = in ^ 1;
   int32_t* const markin = P.mark[in];
   int32_t* const markout = P.mark[out];
-  frontier_round_begin(P, in);
   int32_t* T = tr[warp];
   int done = 0;
   for (int t = blockIdx.x * WARPS_PER_CTA + warp; t < P.nt; t += gridDim.x * WARPS_PER_CTA) {
@@ -567,6 +621,7 @@ k_bfs_round(PoolView P, int first, int rnd) {
     atomicAdd(&P.rcnt[in], done);
     if (P.ktiles) atomicAdd(&P.ktiles[first ? K_BFS_FIRST : K_BFS], (unsigned long long)done);
   }
+  frontier_round_end(P, first, in, CTL_BFS_TOTAL, h);
 }
 
 // ------------------------------------------------------------------------------------
@@ -574,12 +629,11 @@ k_bfs_round(PoolView P, int first, int rnd) {
 // Round 1 also sums max(excess, 0) per image for the flow value.
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
-k_flood_round(PoolView P, int first, int rnd, ImageAcc* acc) {
+k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int in = rnd & 1, out = in ^ 1;
+  const int in = frontier_round_number(P, first) & 1, out = in ^ 1;
   int32_t* const markin = P.mark[in];
   int32_t* const markout = P.mark[out];
-  frontier_round_begin(P, in);
   int done = 0;
   for (int t = blockIdx.x * WARPS_PER_CTA + warp; t < P.nt; t += gridDim.x * WARPS_PER_CTA) {
     if (!first) {
@@ -638,6 +692,7 @@ k_flood_round(PoolView P, int first, int rnd, ImageAcc* acc) {
     atomicAdd(&P.rcnt[in], done);
     if (P.ktiles) atomicAdd(&P.ktiles[first ? K_FLOOD_FIRST : K_FLOOD], (unsigned long long)done);
   }
+  frontier_round_end(P, first, in, CTL_FLOOD_TOTAL, h);
 }
 
 // Labels of one image, row-major, padding excluded.
@@ -734,14 +789,36 @@ int launch_edge_relabel_build(const PoolView& P, int32_t* list, int32_t* count,
   return ok();
 }
 
-int launch_bfs_round(const PoolView& P, int first, int rnd, int grid, cudaStream_t s) {
-  k_bfs_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, first, rnd);
+int launch_bfs_round(const PoolView& P, int first, cudaGraphConditionalHandle h, int grid,
+                     cudaStream_t s) {
+  k_bfs_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, first, h);
   return ok();
 }
 
-int launch_flood_round(const PoolView& P, int first, int rnd, ImageAcc* acc, int grid,
-                       cudaStream_t s) {
-  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, first, rnd, acc);
+int launch_flood_round(const PoolView& P, int first, cudaGraphConditionalHandle h, ImageAcc* acc,
+                       int grid, cudaStream_t s) {
+  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, first, h, acc);
+  return ok();
+}
+
+__global__ void k_acc_reset(ImageAcc* acc, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) acc[i].sumpos_e = 0;
+}
+
+int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s) {
+  k_acc_reset<<<(n + 255) / 256, 256, 0, s>>>(acc, n);
+  return ok();
+}
+
+int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, cudaStream_t s) {
+  k_ctl_begin<<<1, 32, 0, s>>>(P, max_rounds, max_cycles);
+  return ok();
+}
+
+int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
+                     cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_ctl_cycle<<<1, 32, 0, s>>>(P, count, count_cycle, h);
   return ok();
 }
 

@@ -58,6 +58,9 @@ typedef struct gc_opts {
                               heights 0 (sink pixels) / 1 (others) */
   int max_cycles;          /* cap on global-relabel cycles; exceeded -> GC_ERR_NOT_CONVERGED */
   int max_bfs_rounds;      /* cap on tile rounds of one BFS / flood fill */
+  int use_graph;           /* 1: the solve is one CUDA-graph launch whose loops are WHILE nodes
+                              decided on the device (one host wait per solve); 0: the host
+                              drives the loops (used when profiling is on) */
 } gc_opts;
 
 typedef struct gc_stats {

@@ -33,8 +33,9 @@ def check(g, oracle, **kw):
 
 @pytest.mark.parametrize("w,h,seed", [(512, 512, 0), (512, 512, 1), (256, 384, 2), (64, 96, 3),
                                       (32, 32, 4), (1024, 512, 5)])
-def test_synthetic_matches_oracle(cuda, oracle, w, h, seed):
-    check(synth.make_graph(w, h, seed), oracle)
+@pytest.mark.parametrize("graph", [True, False])
+def test_synthetic_matches_oracle(cuda, oracle, w, h, seed, graph):
+    check(synth.make_graph(w, h, seed), oracle, use_graph=graph)
 
 
 @pytest.mark.parametrize("w,h", [(1, 1), (1, 7), (7, 1), (33, 31), (100, 37), (300, 211)])
@@ -44,10 +45,11 @@ def test_ragged_sizes(cuda, oracle, w, h):
 
 @pytest.mark.parametrize("seed,sym,sparsity", [(0, True, 0.0), (1, False, 0.0), (2, True, 0.4),
                                                (3, False, 0.6), (4, True, 0.9)])
-def test_random_graphs(cuda, oracle, seed, sym, sparsity):
+@pytest.mark.parametrize("graph", [True, False])
+def test_random_graphs(cuda, oracle, seed, sym, sparsity, graph):
     g = synth.random_graph(256, 192, seed, cap_max=100, tlink_max=150, sparsity=sparsity,
                            symmetric=sym)
-    check(g, oracle)
+    check(g, oracle, use_graph=graph)
 
 
 @pytest.mark.parametrize("iters,pulses,init", [(1, 1, 0), (4, 1, 1), (64, 5, 0), (32, 1, 1)])
@@ -181,14 +183,39 @@ def test_negative_capacity_rejected(cuda):
         assert ei.value.code == _gcut.GC_ERR_INVALID
 
 
-def test_cycle_cap_reports_not_converged(cuda):
+@pytest.mark.parametrize("graph", [True, False])
+def test_cycle_cap_reports_not_converged(cuda, graph):
     import _gcut
     g = synth.random_graph(256, 256, 3, cap_max=100, tlink_max=100)
-    with GraphCut(256, 256, max_cycles=1, bfs=1, discharge_iters=1) as gc:
+    with GraphCut(256, 256, max_cycles=1, bfs=1, discharge_iters=1, use_graph=graph) as gc:
         gc.upload_capacities(*g.planes())
         with pytest.raises(_gcut.GCError) as ei:
             gc.cut()
         assert ei.value.code == _gcut.GC_ERR_NOT_CONVERGED
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_round_cap_reports_not_converged(cuda, graph):
+    import _gcut
+    g = synth.random_graph(512, 512, 4, cap_max=100, tlink_max=100)
+    with GraphCut(512, 512, max_bfs_rounds=1, use_graph=graph) as gc:
+        gc.upload_capacities(*g.planes())
+        with pytest.raises(_gcut.GCError) as ei:
+            gc.cut()
+        assert ei.value.code == _gcut.GC_ERR_NOT_CONVERGED
+
+
+def test_repeated_solves_reuse_graph(cuda, oracle):
+    g = synth.make_graph(384, 256, 8)
+    f_ref, l_ref = oracle.maxflow_bk(*g.planes())
+    with GraphCut(g.width, g.height) as gc:
+        for _ in range(4):
+            gc.upload_capacities(*g.planes())
+            gc.cut()
+            assert gc.flow == f_ref
+            assert np.array_equal(gc.labels().cpu().numpy(), l_ref)
+        gc.cut()  # solving a solved state again is a no-op
+        assert gc.flow == f_ref
 
 
 def test_invalid_options_rejected(cuda):
