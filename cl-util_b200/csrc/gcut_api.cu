@@ -153,9 +153,9 @@ struct Pool {
   ~Pool() { release(); }
 
   void release() {
-    int32_t* bufs[] = {P.exc, P.hgt, P.cap[0], P.cap[1], P.cap[2], P.cap[3], tl, list, counts,
+    int32_t* bufs[] = {P.exc, P.hgt, P.cap[0], P.cap[1], P.cap[2], P.cap[3], tl,
                        P.touched, P.act_int, P.mark[0], P.mark[1], P.rcnt, P.ctl, P.tact,
-                       P.img_of, stage, pts};
+                       P.img_of, P.queue[0], P.queue[1], P.qcount, P.inq[0], P.inq[1], stage, pts};
     for (auto* b : bufs) if (b) cudaFree(b);
     if (P.nbr) cudaFree(P.nbr);
     if (P.mcan) cudaFree(P.mcan);
@@ -205,14 +205,17 @@ struct Pool {
     if (!e) e = dalloc(&P.msink, (size_t)nt * 32);
     if (!e) e = dalloc(&P.mexc, (size_t)nt * 32);
     if (!e) e = dalloc(&P.mreach, (size_t)nt * 32);
-    int32_t** small[] = {&P.touched, &P.act_int, &P.mark[0], &P.mark[1], &P.tact, &P.img_of, &list};
+    int32_t** small[] = {&P.touched, &P.act_int, &P.mark[0], &P.mark[1], &P.tact, &P.img_of,
+                         &P.queue[0], &P.queue[1], &P.inq[0], &P.inq[1]};
     for (auto** p : small) if (!e) e = dalloc(p, nt);
+    if (!e) e = dalloc(&P.qcount, 2);
+    list = P.queue[0];
+    counts = P.qcount;
     if (!e) e = dalloc(&P.rcnt, 2);
-    if (!e) e = dalloc(&counts, 4);
     if (!e) e = dalloc(&acc, imgs.size());
     if (!e) e = dalloc(&ktiles, GC_NKERN);
-    // look-back slots: the scan uses one per 4096 items, the list rebuild one per 8 tiles
-    if (!e) e = scan.alloc(scan_chunks(nt) > nt / 8 + 1 ? scan_chunks(nt) : nt / 8 + 1);
+    // look-back slots: the scan uses one per 4096 items, the list rebuild one per 64 tiles
+    if (!e) e = scan.alloc(scan_chunks(nt) > nt / 64 + 1 ? scan_chunks(nt) : nt / 64 + 1);
     if (!e) e = cudaMallocHost((void**)&h_count, 4 * sizeof(int32_t));
     if (!e) e = cudaMallocHost((void**)&h_ctl, CTL_N * sizeof(int32_t));
     if (!e) e = dalloc(&P.ctl, CTL_N);
@@ -233,6 +236,9 @@ struct Pool {
     CK(cudaMemset(P.mark[1], 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.rcnt, 0, sizeof(int32_t) * 2));
     CK(cudaMemset(P.ctl, 0, sizeof(int32_t) * CTL_N));
+    CK(cudaMemset(P.qcount, 0, sizeof(int32_t) * 2));
+    CK(cudaMemset(P.inq[0], 0, sizeof(int32_t) * nt));
+    CK(cudaMemset(P.inq[1], 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.act_int, 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.tact, 0, sizeof(int32_t) * nt));
     CK(cudaMemset(acc, 0, sizeof(ImageAcc) * imgs.size()));
@@ -330,6 +336,7 @@ struct Pool {
     int n = 0;
     if (relabel_first) RK(global_relabel(s));
     RK(compact(P.tact, nullptr, s));
+    RK(launch_ctl_cycle(P, counts, 0, 0, s));
     bool go = true;
     if (relabel_first) {
       RK(read_count(s, &n));
@@ -339,13 +346,17 @@ struct Pool {
       if (cycle >= opts.max_cycles) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
       stats.cycles++;
       for (int p = 0; p < opts.pulses_per_relabel; ++p) {
-        RK(timed(K_DISCHARGE, s, [&] { return launch_discharge(P, list, counts, opts.discharge_iters, grid_dis, s); }));
-        RK(timed(K_EDGE_BUILD, s, [&] { return launch_edge_relabel_build(P, list, counts, scan.st, s); }));
+        if (collect) {
+          RK(read_ctl(s));
+          CK(cudaMemcpy(h_count, P.qcount, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost));
+          stats.tiles_discharged += h_count[h_ctl[CTL_PULSE] & 1];
+        }
+        RK(timed(K_DISCHARGE, s, [&] { return launch_discharge(P, opts.discharge_iters, grid_dis, s); }));
         stats.pulses++;
-        if (collect) { int m; RK(read_count(s, &m)); stats.tiles_discharged += m; }
       }
       RK(global_relabel(s));
       RK(compact(P.tact, nullptr, s));
+      RK(launch_ctl_cycle(P, counts, 0, 0, s));
       RK(read_count(s, &n));
       go = n > 0;
     }
@@ -428,10 +439,8 @@ struct Pool {
       cudaGraphConditionalHandle hb;
       CK(cudaGraphConditionalHandleCreate(&hb, bm, 0, 0));
       RK(capture(bm, Lm, [&](cudaStream_t cs) {
-        for (int p = 0; p < opts.pulses_per_relabel; ++p) {
-          RK(launch_discharge(P, list, counts, opts.discharge_iters, grid_dis, cs));
-          RK(launch_edge_relabel_build(P, list, counts, scan.st, cs));
-        }
+        for (int p = 0; p < opts.pulses_per_relabel; ++p)
+          RK(launch_discharge(P, opts.discharge_iters, grid_dis, cs));
         return launch_bfs_round(P, 1, hb, grid_warps, cs);
       }));
       cudaGraph_t bb;
@@ -514,24 +523,27 @@ struct Pool {
     if (!uploaded) return fail(GC_ERR_STATE, "push before upload");
     if (!list_valid) {
       RK(compact(P.tact, nullptr, s));
+      RK(launch_ctl_cycle(P, counts, 0, 0, s));
       list_valid = true;
     }
     solved = false;
     bfs_fresh = false;
-    return launch_discharge(P, list, counts, opts.discharge_iters, grid_dis, s);
+    return launch_discharge(P, opts.discharge_iters, grid_dis, s);
   }
   int step_relabel(cudaStream_t s) {
     if (!uploaded) return fail(GC_ERR_STATE, "relabel before upload");
     solved = false;
     bfs_fresh = false;
     list_valid = true;
-    return launch_edge_relabel_build(P, list, counts, scan.st, s);
+    RK(launch_edge_relabel_build(P, list, counts, scan.st, s));
+    return launch_ctl_cycle(P, counts, 0, 0, s);
   }
   int step_start_bfs(cudaStream_t s) {
     if (!uploaded) return fail(GC_ERR_STATE, "startBfs before upload");
     RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, s));
     RK(global_relabel(s));
     RK(compact(P.tact, nullptr, s));
+    RK(launch_ctl_cycle(P, counts, 0, 0, s));
     list_valid = true;
     bfs_fresh = true;
     return GC_OK;
@@ -606,8 +618,8 @@ const char* gc_last_error(void) { return g_err.c_str(); }
 int gc_opts_default(gc_opts* o) {
   if (!o) return fail(GC_ERR_INVALID, "null opts");
   o->device = 0;
-  o->discharge_iters = 2;     // autotuned on 2048^2 and 4096^2 synthetic grids
-  o->pulses_per_relabel = 4;
+  o->discharge_iters = 3;     // autotuned on a 2048^2 synthetic grid (cl-util_b200/autotune.py)
+  o->pulses_per_relabel = 2;
   o->initial_relabel = 0;
   o->max_cycles = 100000;
   o->max_bfs_rounds = 1 << 20;

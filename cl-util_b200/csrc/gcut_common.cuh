@@ -40,6 +40,9 @@ struct PoolView {
   int32_t* mark[2];       // [nt] BFS / flood-fill frontier marks, alternating by round
   int32_t* rcnt;          // [2] tiles processed by the current / next frontier round
   int32_t* ctl;           // [CTL_N] device-side loop control (see CtlSlot)
+  int32_t* queue[2];      // [nt] active-tile worklists, alternating by pulse
+  int32_t* qcount;        // [2] worklist lengths
+  int32_t* inq[2];        // [nt] tile is in queue[k] (deduplication)
   int32_t* tact;          // [nt] tile has an active pixel (excess > 0, height < HINF)
   int32_t* img_of;        // [nt] image index of the tile
   unsigned long long* ktiles;  // [K_COUNT] tiles processed per kernel kind (profiling)
@@ -59,6 +62,8 @@ enum CtlSlot {
   CTL_ERR = 7,        // 1: round cap reached, 2: cycle cap reached
   CTL_MAXROUNDS = 8,
   CTL_MAXCYCLES = 9,
+  CTL_PULSE = 10,     // discharge launches since the last list rebuild (parity = worklist)
+  CTL_DDONE = 11,     // CTAs finished in the current discharge launch
   CTL_N = 16
 };
 

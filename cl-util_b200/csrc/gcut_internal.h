@@ -51,8 +51,8 @@ struct Launch {
 int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t* up,
                   const int32_t* down, const int32_t* left, const int32_t* right,
                   const int32_t* excess, int32_t* tl, ImageAcc* acc, cudaStream_t s);
-int launch_discharge(const PoolView& P, const int32_t* list, const int32_t* count, int iters,
-                     int grid, cudaStream_t s);
+// reads the worklist queue[ctl[CTL_PULSE] & 1], builds the other one
+int launch_discharge(const PoolView& P, int iters, int grid, cudaStream_t s);
 int launch_edge_relabel_build(const PoolView& P, int32_t* list, int32_t* count,
                               const ScanState& st, cudaStream_t s);
 // h: condition of the enclosing WHILE node of a CUDA graph (0 outside graphs)

@@ -90,12 +90,26 @@ k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
     P.act_int[t] = 0;
     P.mark[0][t] = 0;
     P.mark[1][t] = 0;
+    P.inq[0][t] = 0;
+    P.inq[1][t] = 0;
     P.img_of[t] = img;
   }
 }
 
 // ------------------------------------------------------------------------------------
 // Discharge.  Thread (r, q) owns pixels (r, 4q .. 4q+3) of the tile.
+//
+// Every pixel pushes along all admissible edges and relabels, tile-edge pixels included,
+// but a tile-edge pixel rises by at most 2 above its height at the start of the launch.
+// A neighbouring CTA that pushes into an edge pixel v saw either v's start height or its
+// final height; with h_final(v) <= h_start(v) + 2 every such push leaves a valid labelling
+// (h(v) <= h(u) + 1 on the new residual edge v -> u), and pushes out of the tile read the
+// neighbour's height under the same bound.  Flow leaving the tile is added to the
+// neighbour's excess and reverse residual with atomics at the end of the tile.
+//
+// Active tiles form a worklist: the launch reads queue[c] (c = pulse parity, device-side)
+// and appends, deduplicated by inq[c ^ 1], every tile that is still active or received flow
+// to queue[c ^ 1]; the last CTA advances the parity.  One launch per pulse, no compaction.
 // ------------------------------------------------------------------------------------
 struct DisSmem {
   int32_t hs[GC_TILE_PX];   // heights
@@ -106,15 +120,33 @@ struct DisSmem {
   int32_t hu[GC_TILE], hd[GC_TILE], hl[GC_TILE], hr[GC_TILE];  // halo heights
 };
 
-__global__ void __launch_bounds__(DIS_THREADS)
-k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restrict__ count,
-            int iters) {
+__device__ __forceinline__ void worklist_add(const PoolView& P, int nxt, int t) {
+  if (atomicExch(&P.inq[nxt][t], 1) == 0) {
+    const int pos = atomicAdd(&P.qcount[nxt], 1);
+    P.queue[nxt][pos] = t;
+  }
+}
+
+__device__ __forceinline__ int4 lds4(const int32_t* p) { return *reinterpret_cast<const int4*>(p); }
+__device__ __forceinline__ void sts4(int32_t* p, int a, int b, int c, int d) {
+  *reinterpret_cast<int4*>(p) = make_int4(a, b, c, d);
+}
+
+__global__ void __launch_bounds__(DIS_THREADS, 3)
+k_discharge(PoolView P, int iters) {
   __shared__ DisSmem S;
+  __shared__ int s_cur, s_n;
   const int tid = threadIdx.x;
   const int r = tid >> 3, q = tid & 7, c0 = q * 4;
-  const int n = *count;
+  if (tid == 0) {
+    s_cur = *((volatile int32_t*)&P.ctl[CTL_PULSE]) & 1;
+    s_n = *((volatile int32_t*)&P.qcount[s_cur]);
+  }
+  __syncthreads();
+  const int cur = s_cur, nxt = cur ^ 1, n = s_n;
+  const bool erow = (r == 0) || (r == 31);
   for (int li = blockIdx.x; li < n; li += gridDim.x) {
-    const int t = list[li];
+    const int t = P.queue[cur][li];
     const int4 nb = P.nbr[t];
     const long long off = (long long)t * GC_TILE_PX + r * GC_TILE + c0;
     int e[4], h[4], cu[4], cd[4], cl[4], cr[4];
@@ -126,28 +158,35 @@ k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
       v = *(const int4*)(P.cap[DLEFT] + off); cl[0] = v.x; cl[1] = v.y; cl[2] = v.z; cl[3] = v.w;
       v = *(const int4*)(P.cap[DRIGHT] + off); cr[0] = v.x; cr[1] = v.y; cr[2] = v.z; cr[3] = v.w;
     }
+    // height cap of tile-edge pixels for this launch (interior: none)
+    int hcap[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + j;
+      const bool edge = erow || c == 0 || c == 31;
+      hcap[j] = edge ? (h[j] >= GC_HINF - 2 ? GC_HINF : h[j] + 2) : GC_HINF;
+    }
     int e0[4], cu0[4], cd0[4], cl0, cr0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) { e0[j] = e[j]; cu0[j] = cu[j]; cd0[j] = cd[j]; }
     cl0 = cl[0];
     cr0 = cr[3];
-    *(int4*)(S.hs + r * GC_TILE + c0) = make_int4(h[0], h[1], h[2], h[3]);
+    sts4(S.hs + r * GC_TILE + c0, h[0], h[1], h[2], h[3]);
     if (tid < 32) S.hu[tid] = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + tid] : GC_HINF;
     else if (tid < 64) S.hd[tid - 32] = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + (tid - 32)] : GC_HINF;
     else if (tid < 96) S.hl[tid - 64] = nb.z >= 0 ? P.hgt[(long long)nb.z * GC_TILE_PX + (tid - 64) * GC_TILE + 31] : GC_HINF;
     else if (tid < 128) S.hr[tid - 96] = nb.w >= 0 ? P.hgt[(long long)nb.w * GC_TILE_PX + (tid - 96) * GC_TILE] : GC_HINF;
+    if (tid == 0) P.inq[cur][t] = 0;
     int xu[4] = {0, 0, 0, 0}, xd[4] = {0, 0, 0, 0}, xl = 0, xr = 0;  // cross-tile flow
     __syncthreads();
 
     for (int it = 0; it < iters; ++it) {
       // neighbour heights (fixed during the push phase)
       int hnu[4], hnd[4], hnl[4], hnr[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int c = c0 + j;
-        hnu[j] = r > 0 ? S.hs[(r - 1) * GC_TILE + c] : S.hu[c];
-        hnd[j] = r < 31 ? S.hs[(r + 1) * GC_TILE + c] : S.hd[c];
-      }
+      if (r > 0) { const int4 v = lds4(S.hs + (r - 1) * GC_TILE + c0); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
+      else { const int4 v = lds4(S.hu + c0); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
+      if (r < 31) { const int4 v = lds4(S.hs + (r + 1) * GC_TILE + c0); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
+      else { const int4 v = lds4(S.hd + c0); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
       hnl[0] = c0 > 0 ? S.hs[r * GC_TILE + c0 - 1] : S.hl[r];
       hnl[1] = h[0]; hnl[2] = h[1]; hnl[3] = h[2];
       hnr[0] = h[1]; hnr[1] = h[2]; hnr[2] = h[3];
@@ -169,7 +208,7 @@ k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
           e[j] = ej;
         }
       }
-      // flow leaving the tile is delivered at the end of the launch
+      // flow leaving the tile is delivered at the end of the tile
       if (r == 0) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) { xu[j] += ou[j]; ou[j] = 0; }
@@ -180,16 +219,16 @@ k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
       }
       if (q == 0) { xl += ol[0]; ol[0] = 0; }
       if (q == 7) { xr += orr[3]; orr[3] = 0; }
-      *(int4*)(S.fu + r * GC_TILE + c0) = make_int4(ou[0], ou[1], ou[2], ou[3]);
-      *(int4*)(S.fd + r * GC_TILE + c0) = make_int4(od[0], od[1], od[2], od[3]);
+      sts4(S.fu + r * GC_TILE + c0, ou[0], ou[1], ou[2], ou[3]);
+      sts4(S.fd + r * GC_TILE + c0, od[0], od[1], od[2], od[3]);
       S.fl[r * 8 + q] = ol[0];
       S.fr[r * 8 + q] = orr[3];
       __syncthreads();
       // gather inflow; a pixel receiving flow gains the reverse residual
       {
-        int4 a = r < 31 ? *(const int4*)(S.fu + (r + 1) * GC_TILE + c0) : make_int4(0, 0, 0, 0);
-        int4 b = r > 0 ? *(const int4*)(S.fd + (r - 1) * GC_TILE + c0) : make_int4(0, 0, 0, 0);
-        int fb[4] = {a.x, a.y, a.z, a.w}, fa[4] = {b.x, b.y, b.z, b.w};
+        const int4 a = r < 31 ? lds4(S.fu + (r + 1) * GC_TILE + c0) : make_int4(0, 0, 0, 0);
+        const int4 b = r > 0 ? lds4(S.fd + (r - 1) * GC_TILE + c0) : make_int4(0, 0, 0, 0);
+        const int fb[4] = {a.x, a.y, a.z, a.w}, fa[4] = {b.x, b.y, b.z, b.w};
         int fromleft[4], fromright[4];
         fromleft[0] = q > 0 ? S.fr[r * 8 + q - 1] : 0;
         fromleft[1] = orr[0]; fromleft[2] = orr[1]; fromleft[3] = orr[2];
@@ -204,14 +243,12 @@ k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
           cr[j] += fromright[j];
         }
       }
-      // relabel phase (interior pixels; tile-edge pixels keep their height in this launch)
+      // relabel phase (Jacobi; tile-edge pixels are capped at hcap)
       int nh[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         nh[j] = h[j];
-        const int c = c0 + j;
-        const bool interior = r > 0 && r < 31 && c > 0 && c < 31;
-        if (interior && e[j] > 0 && h[j] < GC_HINF) {
+        if (e[j] > 0 && h[j] < hcap[j]) {
           const bool adm = (cd[j] > 0 && h[j] == hnd[j] + 1) || (cu[j] > 0 && h[j] == hnu[j] + 1) ||
                            (cr[j] > 0 && h[j] == hnr[j] + 1) || (cl[j] > 0 && h[j] == hnl[j] + 1);
           if (!adm) {
@@ -220,7 +257,7 @@ k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
             if (cu[j] > 0) m = imin(m, hnu[j] + 1);
             if (cr[j] > 0) m = imin(m, hnr[j] + 1);
             if (cl[j] > 0) m = imin(m, hnl[j] + 1);
-            nh[j] = imin(m, GC_HINF);
+            nh[j] = imin(imin(m, GC_HINF), hcap[j]);
             changed |= nh[j] != h[j];
           }
         }
@@ -228,21 +265,20 @@ k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
       __syncthreads();  // all reads of S.hs / flow buffers of this round are done
 #pragma unroll
       for (int j = 0; j < 4; ++j) h[j] = nh[j];
-      *(int4*)(S.hs + r * GC_TILE + c0) = make_int4(h[0], h[1], h[2], h[3]);
+      sts4(S.hs + r * GC_TILE + c0, h[0], h[1], h[2], h[3]);
       if (!__syncthreads_or(changed)) break;
     }
 
     // write back: interior values are owned by this CTA; tile-edge excess and the
     // outward residual of edge pixels also receive atomics from neighbouring tiles, so
     // they are written as deltas.
-    const bool edge_row = (r == 0) || (r == 31);
-    if (!edge_row && q > 0 && q < 7) {
+    if (!erow && q > 0 && q < 7) {
       *(int4*)(P.exc + off) = make_int4(e[0], e[1], e[2], e[3]);
     } else {
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int c = c0 + j;
-        if (edge_row || c == 0 || c == 31) {
+        if (erow || c == 0 || c == 31) {
           if (e[j] != e0[j]) atomicAdd(P.exc + off + j, e[j] - e0[j]);
         } else {
           P.exc[off + j] = e[j];
@@ -279,51 +315,68 @@ k_discharge(PoolView P, const int32_t* __restrict__ list, const int32_t* __restr
     if (r == 0 && nb.x >= 0) {
 #pragma unroll
       for (int j = 0; j < 4; ++j) if (xu[j]) {
-        long long o = (long long)nb.x * GC_TILE_PX + 31 * GC_TILE + c0 + j;
+        const long long o = (long long)nb.x * GC_TILE_PX + 31 * GC_TILE + c0 + j;
         atomicAdd(P.exc + o, xu[j]); atomicAdd(P.cap[DDOWN] + o, xu[j]); sent_u = 1;
       }
     }
     if (r == 31 && nb.y >= 0) {
 #pragma unroll
       for (int j = 0; j < 4; ++j) if (xd[j]) {
-        long long o = (long long)nb.y * GC_TILE_PX + c0 + j;
+        const long long o = (long long)nb.y * GC_TILE_PX + c0 + j;
         atomicAdd(P.exc + o, xd[j]); atomicAdd(P.cap[DUP] + o, xd[j]); sent_d = 1;
       }
     }
     if (q == 0 && xl && nb.z >= 0) {
-      long long o = (long long)nb.z * GC_TILE_PX + r * GC_TILE + 31;
+      const long long o = (long long)nb.z * GC_TILE_PX + r * GC_TILE + 31;
       atomicAdd(P.exc + o, xl); atomicAdd(P.cap[DRIGHT] + o, xl); sent_l = 1;
     }
     if (q == 7 && xr && nb.w >= 0) {
-      long long o = (long long)nb.w * GC_TILE_PX + r * GC_TILE;
+      const long long o = (long long)nb.w * GC_TILE_PX + r * GC_TILE;
       atomicAdd(P.exc + o, xr); atomicAdd(P.cap[DLEFT] + o, xr); sent_r = 1;
     }
-    if (sent_u) P.touched[nb.x] = 1;
-    if (sent_d) P.touched[nb.y] = 1;
-    if (sent_l) P.touched[nb.z] = 1;
-    if (sent_r) P.touched[nb.w] = 1;
-    int act = 0;
+    int act = 0, act_int = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int c = c0 + j;
-      act |= (r > 0 && r < 31 && c > 0 && c < 31 && e[j] > 0 && h[j] < GC_HINF);
+      const int a = e[j] > 0 && h[j] < GC_HINF;
+      act |= a;
+      act_int |= a && !erow && c > 0 && c < 31;
     }
-    act = __syncthreads_or(act);
+    const int any_act = __syncthreads_or(act);
+    act_int = __syncthreads_or(act_int);
+    const int sent = __syncthreads_or(sent_u | (sent_d << 1) | (sent_l << 2) | (sent_r << 3));
+    (void)sent;
+    if (sent_u) { P.touched[nb.x] = 1; worklist_add(P, nxt, nb.x); }
+    if (sent_d) { P.touched[nb.y] = 1; worklist_add(P, nxt, nb.y); }
+    if (sent_l) { P.touched[nb.z] = 1; worklist_add(P, nxt, nb.z); }
+    if (sent_r) { P.touched[nb.w] = 1; worklist_add(P, nxt, nb.w); }
     if (tid == 0) {
       P.touched[t] = 1;
-      P.act_int[t] = act;
+      P.act_int[t] = act_int;
+      if (any_act) worklist_add(P, nxt, t);
       if (P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
+    }
+  }
+  // last CTA: the queue just read is consumed; the next launch reads the other one
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    const int d = atomicAdd(&P.ctl[CTL_DDONE], 1);
+    if (d == (int)gridDim.x - 1) {
+      P.qcount[cur] = 0;
+      P.ctl[CTL_PULSE] = P.ctl[CTL_PULSE] + 1;
+      P.ctl[CTL_DDONE] = 0;
+      __threadfence();
     }
   }
 }
 
 // ------------------------------------------------------------------------------------
-// Edge relabel + active-tile list (one launch).  CTA = 256 tiles by arrival ticket; warp w
-// walks 32 of them.  A tile is active when an interior pixel was active after its
-// discharge or a tile-edge pixel is active after this relabel.
+// Edge relabel + active-tile list.
 // ------------------------------------------------------------------------------------
-constexpr int EB_THREADS = 256;
-constexpr int EB_TILES = EB_THREADS / 32;   // one warp per tile
+constexpr int EB_THREADS = 512;
+constexpr int EB_WARPS = EB_THREADS / 32;
+constexpr int EB_TILES = 64;                 // tiles per CTA (4 per warp)
 
 // Relabels up to four tile-edge pixels of one lane (Jacobi: neighbour heights are read
 // as they are, a concurrent update only makes them larger, which keeps the labelling
@@ -367,10 +420,11 @@ __device__ __forceinline__ int edge_relabel_lane(const PoolView& P, int t, int4 
   return act;
 }
 
-// Edge relabel + active-tile list (one launch).  A CTA owns EB_TILES consecutive tiles (one
-// warp each) by arrival ticket; a tile is active when an interior pixel was active after its
-// discharge or a tile-edge pixel is active after this relabel.  The active tiles are
-// compacted in tile order with a warp-parallel decoupled look-back.
+// Edge relabel + active-tile list (one launch).  A CTA owns EB_TILES consecutive tiles by
+// arrival ticket; each warp takes 4 of them and relabels only the touched ones (one warp
+// per tile, 4 edge pixels per lane).  A tile is active when an interior pixel was active
+// after its discharge or a tile-edge pixel is active after this relabel.  The active tiles
+// are compacted in tile order with a warp-parallel decoupled look-back.
 __global__ void __launch_bounds__(EB_THREADS)
 k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
   __shared__ int32_t flag[EB_TILES];
@@ -384,21 +438,34 @@ k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
   const int chunk = s_chunk;
   const int nchunks = (P.nt + EB_TILES - 1) / EB_TILES;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int t = chunk * EB_TILES + warp;
-  int active = 0;
-  if (t < P.nt && P.touched[t]) {
+  constexpr int PER_WARP = EB_TILES / EB_WARPS;
+  const int t0 = chunk * EB_TILES + warp * PER_WARP;
+  int touched = 0;
+  if (lane < PER_WARP && t0 + lane < P.nt) {
+    touched = P.touched[t0 + lane];
+    P.inq[0][t0 + lane] = 0;  // the worklists are replaced by the rebuilt list
+    P.inq[1][t0 + lane] = 0;
+  }
+  unsigned todo = __ballot_sync(0xffffffffu, touched != 0);
+  if (lane < PER_WARP) flag[warp * PER_WARP + lane] = 0;
+  __syncwarp();
+  while (todo) {
+    const int k = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const int t = t0 + k;
     const int4 nb = P.nbr[t];
     const int a = edge_relabel_lane(P, t, nb, lane);
-    active = __any_sync(0xffffffffu, a) | P.act_int[t];
+    const int active = __any_sync(0xffffffffu, a) | P.act_int[t];
     if (lane == 0) {
+      flag[warp * PER_WARP + k] = active;
       P.touched[t] = 0;
       if (P.ktiles) atomicAdd(&P.ktiles[K_EDGE_BUILD], 1ull);
     }
   }
-  if (lane == 0) flag[warp] = active;
   __syncthreads();
   if (warp == 0) {
-    const int v = lane < EB_TILES ? flag[lane] : 0;
+    const int v0 = flag[2 * lane], v1 = flag[2 * lane + 1];   // two flags per lane
+    const int v = v0 + v1;
     int x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -407,7 +474,10 @@ k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
     }
     const int agg = __shfl_sync(0xffffffffu, x, 31);
     const int excl = lookback_exclusive_warp(st, s_tag, chunk, agg);
-    if (v) list[excl + x - v] = chunk * EB_TILES + lane;
+    int pos = excl + x - v;
+    const int tb = chunk * EB_TILES + 2 * lane;
+    if (v0) list[pos++] = tb;
+    if (v1) list[pos] = tb + 1;
     if (chunk == nchunks - 1 && lane == 0) *count = excl + agg;
     if (lane == 0) scan_finish(st, nchunks);
   }
@@ -517,6 +587,9 @@ __global__ void k_ctl_cycle(PoolView P, const int32_t* count, int count_cycle,
                             cudaGraphConditionalHandle h) {
   if (threadIdx.x != 0) return;
   volatile int32_t* ctl = P.ctl;
+  ctl[CTL_PULSE] = 0;   // the compacted list sits in queue[0]
+  ctl[CTL_DDONE] = 0;
+  P.qcount[1] = 0;
   int cycles = ctl[CTL_CYCLES] + (count_cycle ? 1 : 0);
   ctl[CTL_CYCLES] = cycles;
   bool more = *((volatile const int32_t*)count) > 0;
@@ -541,6 +614,9 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
     if (!first) {
       if (!markin[t]) continue;
       if (lane == 0) markin[t] = 0;
+    } else if (lane == 0) {
+      P.inq[0][t] = 0;  // the worklists are rebuilt from the relabelled state
+      P.inq[1][t] = 0;
     }
     ++done;
     const int4 nb = P.nbr[t];
@@ -775,9 +851,8 @@ int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t
   return ok();
 }
 
-int launch_discharge(const PoolView& P, const int32_t* list, const int32_t* count, int iters,
-                     int grid, cudaStream_t s) {
-  k_discharge<<<grid, DIS_THREADS, 0, s>>>(P, list, count, iters);
+int launch_discharge(const PoolView& P, int iters, int grid, cudaStream_t s) {
+  k_discharge<<<grid, DIS_THREADS, 0, s>>>(P, iters);
   return ok();
 }
 
