@@ -50,6 +50,7 @@ class GcKernelProf(ctypes.Structure):
 
 
 GC_NKERN = 9
+GC_COMPACT_NOALLOC_MAX_N = 4194304
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -82,6 +83,7 @@ SIGNATURES = {
     "gc_last_error": [],
     "gc_scan_exclusive": [_P, _P, _P, _I, _P],
     "gc_compact": [_P, _P, _P, _I, _P],
+    "gc_compact_noalloc": [_P, _P, _P, _I, _P],
     "gc_tiles_build": [_P, _I, _I32, _P, _P, _I, _P],
     "gc_tiles_build_logical": [_P, _P, _I, _I32, _I, _I32, _I, _P, _P, _I, _P],
     "gc_tiles_incorporate": [_P, _P, _I, _I32, _I, _I32, _I, _I32, _I, _P],

@@ -611,6 +611,11 @@ int device_scan_state(ScanState* out) {
 }
 }  // namespace
 
+int gcut::set_last_error(int code, const char* msg) {
+  g_err = msg;
+  return code;
+}
+
 extern "C" {
 
 const char* gc_last_error(void) { return g_err.c_str(); }

@@ -18,6 +18,8 @@ enum ScanMode {
 };
 
 int scan_chunks(int n);
+// Records the message returned by gc_last_error() for the calling thread; returns code.
+int set_last_error(int code, const char* msg);
 int launch_scan(int mode, const int32_t* in, const int32_t* in2, int32_t* clear,
                 int32_t* scan_out, int32_t* list_out, int32_t* total_out, int n, int op1,
                 int32_t a1, int op2, int32_t a2, int logical, const ScanState& st,

@@ -168,6 +168,23 @@ int gc_compact(const int32_t* flags, int32_t* list, int32_t* length, int n, void
    incremental_tile_list.cl:40-64 + compaction). */
 int gc_tiles_build(const int32_t* tiles, int op, int32_t operand, int32_t* list,
                    int32_t* length, int n, void* stream);
+/* Same compaction as gc_compact for callers that cannot allocate device memory.  No
+   counterpart in the reference.  gc_compact obtains its look-back scratch with cudaMalloc
+   on its first call on a device; code that must keep a fixed device-memory footprint (for
+   example a serving process with a pre-divided budget on a shared GPU) or that cannot risk
+   the implicit synchronisation of cudaMalloc/cudaFree while other work runs, calls this
+   variant instead.  Its scratch is a fixed 8208-byte array compiled into the library,
+   present on every GPU that loads the library until the process exits; it calls no
+   cudaMalloc, cudaFree or allocating library routine.
+   - n must not exceed GC_COMPACT_NOALLOC_MAX_N (4194304 items); larger n returns
+     GC_ERR_INVALID.
+   - The first call on each device looks up the array's device address (with that device
+     current); make that first call before any stream capture.
+   - All calls share the one array and each call clears the part it uses, so calls whose
+     work overlaps on the GPU (different streams, or different host threads) race and must
+     be serialised by the caller. */
+#define GC_COMPACT_NOALLOC_MAX_N 4194304
+int gc_compact_noalloc(const int32_t* flags, int32_t* list, int32_t* length, int n, void* stream);
 /* IncrementalTileList.buildLogical (IncrementalTileList.pyx:157-176,
    incremental_tile_list.cl:66-108 + compaction). */
 int gc_tiles_build_logical(const int32_t* tiles, const int32_t* tiles2, int op1, int32_t a1,
