@@ -18,6 +18,11 @@ import _gcut
 from _gcut import check, lib, ptr, stream_handle
 
 
+# schedule tuned by autotune.py on the 64-grid mixed batch (sides 256..1536)
+BATCH_DISCHARGE_ITERS = 3
+BATCH_PULSES = 4
+
+
 class GraphCutBatch:
     def __init__(self, shapes, device: int = 0, bfs=None, discharge_iters=None,
                  initial_relabel=None, max_cycles=None, max_bfs_rounds=None,
@@ -25,6 +30,8 @@ class GraphCutBatch:
         import torch
         self.shapes = [(int(w), int(h)) for (w, h) in shapes]
         self.device = torch.device("cuda", device)
+        if discharge_iters is None and bfs is None:
+            discharge_iters, bfs = BATCH_DISCHARGE_ITERS, BATCH_PULSES
         opts = _gcut.default_opts(device=device, discharge_iters=discharge_iters,
                                   pulses_per_relabel=bfs,
                                   initial_relabel=None if initial_relabel is None else int(initial_relabel),

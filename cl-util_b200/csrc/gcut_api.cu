@@ -155,7 +155,8 @@ struct Pool {
   void release() {
     int32_t* bufs[] = {P.exc, P.hgt, P.cap[0], P.cap[1], P.cap[2], P.cap[3], tl,
                        P.touched, P.act_int, P.mark[0], P.mark[1], P.rcnt, P.ctl, P.tact,
-                       P.img_of, P.queue[0], P.queue[1], P.qcount, P.inq[0], P.inq[1], stage, pts};
+                       P.img_of, P.queue[0], P.queue[1], P.qcount, P.inq[0], P.inq[1],
+                       P.img_live, stage, pts};
     for (auto* b : bufs) if (b) cudaFree(b);
     if (P.nbr) cudaFree(P.nbr);
     if (P.mcan) cudaFree(P.mcan);
@@ -209,6 +210,8 @@ struct Pool {
                          &P.queue[0], &P.queue[1], &P.inq[0], &P.inq[1]};
     for (auto** p : small) if (!e) e = dalloc(p, nt);
     if (!e) e = dalloc(&P.qcount, 2);
+    if (!e) e = dalloc(&P.img_live, imgs.size());
+    P.nimg = (int)imgs.size();
     list = P.queue[0];
     counts = P.qcount;
     if (!e) e = dalloc(&P.rcnt, 2);
@@ -237,6 +240,7 @@ struct Pool {
     CK(cudaMemset(P.rcnt, 0, sizeof(int32_t) * 2));
     CK(cudaMemset(P.ctl, 0, sizeof(int32_t) * CTL_N));
     CK(cudaMemset(P.qcount, 0, sizeof(int32_t) * 2));
+    CK(cudaMemset(P.img_live, 0, sizeof(int32_t) * imgs.size()));
     CK(cudaMemset(P.inq[0], 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.inq[1], 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.act_int, 0, sizeof(int32_t) * nt));
@@ -265,8 +269,8 @@ struct Pool {
 
   // exact BFS distances to the sink pixels (global relabel); sets tact.  h: condition
   // handle when captured into a graph (0: host-driven rounds)
-  int global_relabel(cudaStream_t s) {
-    RK(timed(K_BFS_FIRST, s, [&] { return launch_bfs_round(P, 1, 0, grid_warps, s); }));
+  int global_relabel(cudaStream_t s, int first = 1) {
+    RK(timed(K_BFS_FIRST, s, [&] { return launch_bfs_round(P, first, 0, grid_warps, s); }));
     return frontier_rounds(s, /*flood=*/false);
   }
 
@@ -336,6 +340,7 @@ struct Pool {
     int n = 0;
     if (relabel_first) RK(global_relabel(s));
     RK(compact(P.tact, nullptr, s));
+    RK(launch_mark_images(P, list, counts, 0, s));
     RK(launch_ctl_cycle(P, counts, 0, 0, s));
     bool go = true;
     if (relabel_first) {
@@ -354,9 +359,10 @@ struct Pool {
         RK(timed(K_DISCHARGE, s, [&] { return launch_discharge(P, opts.discharge_iters, grid_dis, s); }));
         stats.pulses++;
       }
-      RK(global_relabel(s));
+      RK(global_relabel(s, 2));
       RK(compact(P.tact, nullptr, s));
-      RK(launch_ctl_cycle(P, counts, 0, 0, s));
+      RK(launch_mark_images(P, list, counts, 1, s));
+      RK(launch_ctl_cycle(P, counts, 1, 0, s));
       RK(read_count(s, &n));
       go = n > 0;
     }
@@ -430,6 +436,7 @@ struct Pool {
     }
     RK(capture(g, L, [&](cudaStream_t cs) {
       RK(launch_scan(GC_SCAN_MODE_COMPACT, P.tact, nullptr, nullptr, nullptr, list, counts, nt, 0, 0, 0, 0, 0, scan.st, cs));
+      RK(launch_mark_images(P, list, counts, 0, cs));
       return launch_ctl_cycle(P, counts, 0, hmain, cs);
     }));
     cudaGraph_t bm;
@@ -441,7 +448,7 @@ struct Pool {
       RK(capture(bm, Lm, [&](cudaStream_t cs) {
         for (int p = 0; p < opts.pulses_per_relabel; ++p)
           RK(launch_discharge(P, opts.discharge_iters, grid_dis, cs));
-        return launch_bfs_round(P, 1, hb, grid_warps, cs);
+        return launch_bfs_round(P, 2, hb, grid_warps, cs);
       }));
       cudaGraph_t bb;
       RK(add_while(bm, Lm, hb, &bb));
@@ -449,6 +456,7 @@ struct Pool {
       RK(capture(bb, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, hb, grid_warps, cs); }));
       RK(capture(bm, Lm, [&](cudaStream_t cs) {
         RK(launch_scan(GC_SCAN_MODE_COMPACT, P.tact, nullptr, nullptr, nullptr, list, counts, nt, 0, 0, 0, 0, 0, scan.st, cs));
+        RK(launch_mark_images(P, list, counts, 1, cs));
         return launch_ctl_cycle(P, counts, 1, hmain, cs);
       }));
     }
@@ -510,7 +518,7 @@ struct Pool {
     if (stats.launches < 0) {  // graph solve: count the kernel nodes that ran
       stats.cycles = h_ctl[CTL_CYCLES];
       stats.pulses = stats.cycles * opts.pulses_per_relabel;
-      stats.launches = 3 + stats.cycles * (2LL * opts.pulses_per_relabel + 2) + stats.bfs_rounds +
+      stats.launches = 4 + stats.cycles * (1LL * opts.pulses_per_relabel + 3) + stats.bfs_rounds +
                        1 + stats.flood_rounds;
     }
     solved = true;

@@ -57,13 +57,17 @@ int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t
 int launch_discharge(const PoolView& P, int iters, int grid, cudaStream_t s);
 int launch_edge_relabel_build(const PoolView& P, int32_t* list, int32_t* count,
                               const ScanState& st, cudaStream_t s);
-// h: condition of the enclosing WHILE node of a CUDA graph (0 outside graphs)
+// h: condition of the enclosing WHILE node of a CUDA graph (0 outside graphs).
+// first: 0 frontier round, 1 first round over every tile, 2 first round over the tiles of
+// images that still had active tiles at the previous check.
 int launch_bfs_round(const PoolView& P, int first, cudaGraphConditionalHandle h, int grid,
                      cudaStream_t s);
 int launch_flood_round(const PoolView& P, int first, cudaGraphConditionalHandle h, ImageAcc* acc,
                        int grid, cudaStream_t s);
 int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, cudaStream_t s);
 int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s);
+int launch_mark_images(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
+                       cudaStream_t s);
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s);
 int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s);

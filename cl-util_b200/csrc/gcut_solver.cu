@@ -570,15 +570,26 @@ __device__ __forceinline__ void frontier_round_end(const PoolView& P, int first,
   if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
-// Solve prologue: reset the control words.
+// Solve prologue: reset the control words and the image stamps.
 __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles) {
   if (threadIdx.x < CTL_N) P.ctl[threadIdx.x] = 0;
+  for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) P.img_live[i] = 0;
   if (threadIdx.x == 0) {
     P.ctl[CTL_MAXROUNDS] = max_rounds;
     P.ctl[CTL_MAXCYCLES] = max_cycles;
     P.rcnt[0] = 0;
     P.rcnt[1] = 0;
   }
+}
+
+// After the active-tile compaction: stamp the images that still have active tiles, so the
+// next cycle's global relabel covers only them (stamp = cycles + 1 + bump, where bump = 1
+// when k_ctl_cycle will count this check as a finished cycle).
+__global__ void k_mark_images(PoolView P, const int32_t* list, const int32_t* count, int bump) {
+  const int n = *((volatile const int32_t*)count);
+  const int stamp = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1 + bump;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    P.img_live[P.img_of[list[i]]] = stamp;
 }
 
 // After the active-tile compaction: another cycle runs while tiles are active and the cycle
@@ -610,13 +621,19 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
   int32_t* const markout = P.mark[out];
   int32_t* T = tr[warp];
   int done = 0;
+  // first == 2: a global relabel inside the solve loop skips images whose cut was final at
+  // the previous check (no active tile); their state no longer changes
+  const int live = first == 2 ? *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1 : 0;
   for (int t = blockIdx.x * WARPS_PER_CTA + warp; t < P.nt; t += gridDim.x * WARPS_PER_CTA) {
     if (!first) {
       if (!markin[t]) continue;
       if (lane == 0) markin[t] = 0;
-    } else if (lane == 0) {
-      P.inq[0][t] = 0;  // the worklists are rebuilt from the relabelled state
-      P.inq[1][t] = 0;
+    } else {
+      if (first == 2 && P.img_live[P.img_of[t]] != live) continue;
+      if (lane == 0) {
+        P.inq[0][t] = 0;  // the worklists are rebuilt from the relabelled state
+        P.inq[1][t] = 0;
+      }
     }
     ++done;
     const int4 nb = P.nbr[t];
@@ -888,6 +905,12 @@ int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s) {
 
 int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, cudaStream_t s) {
   k_ctl_begin<<<1, 32, 0, s>>>(P, max_rounds, max_cycles);
+  return ok();
+}
+
+int launch_mark_images(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
+                       cudaStream_t s) {
+  k_mark_images<<<32, 256, 0, s>>>(P, list, count, bump);
   return ok();
 }
 

@@ -246,3 +246,21 @@ def random_graph(width: int, height: int, seed: int, cap_max=100, tlink_max=2000
         down[:-1] = draw((height - 1, width))
         right[:, :-1] = draw((height, width - 1))
     return Graph(width, height, up, down, left, right, excess)
+
+
+def _make_one(args):
+    w, h, seed = args
+    return make_graph(w, h, seed)
+
+
+def make_graphs(specs, processes=None):
+    """make_graph for each (width, height, seed), in a 'spawn' process pool (safe to call
+    after CUDA has been initialised in the parent)."""
+    import multiprocessing as mp
+    import os
+    specs = list(specs)
+    n = processes or min(len(specs), os.cpu_count() or 1)
+    if n <= 1 or len(specs) <= 1:
+        return [_make_one(s) for s in specs]
+    with mp.get_context("spawn").Pool(n) as pool:
+        return pool.map(_make_one, specs, chunksize=1)
