@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--size", type=int, default=2048)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--host-driven", action="store_true",
+                    help="solve loops decided by the host (use_graph=0); ncu does not profile "
+                         "kernels inside conditional CUDA-graph nodes, so profiling runs use this")
     return ap.parse_args()
 
 
@@ -230,7 +233,7 @@ def main():
     stream = torch.cuda.Stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     labels = torch.empty((H, W), dtype=torch.uint8, device="cuda")
-    gc = GraphCut(W, H, device=local)
+    gc = GraphCut(W, H, device=local, use_graph=not args.host_driven)
 
     def step():
         gc.upload_capacities(*dev_planes, stream=stream)
@@ -351,6 +354,7 @@ def main():
                                    "t-links x100, 50*exp(-beta*dI^2) n-links), seed 1+rank",
                        "l2": "flushed between steps (256 MiB write, outside the timed region)",
                        "parallelism": f"replicas x{world}",
+                       "loop": "host-driven" if args.host_driven else "one CUDA graph per solve",
                        "solver": {"discharge_iters": gc.opts.discharge_iters,
                                   "pulses_per_relabel": gc.opts.pulses_per_relabel,
                                   "initial_relabel": gc.opts.initial_relabel}},

@@ -156,7 +156,8 @@ struct Pool {
     int32_t* bufs[] = {P.exc, P.hgt, P.cap[0], P.cap[1], P.cap[2], P.cap[3], tl,
                        P.touched, P.act_int, P.mark[0], P.mark[1], P.rcnt, P.ctl, P.tact,
                        P.img_of, P.queue[0], P.queue[1], P.qcount, P.inq[0], P.inq[1],
-                       P.img_live, stage, pts};
+                       P.img_live, P.mdirty, stage, pts};
+    if (P.tpos) cudaFree(P.tpos);
     for (auto* b : bufs) if (b) cudaFree(b);
     if (P.nbr) cudaFree(P.nbr);
     if (P.mcan) cudaFree(P.mcan);
@@ -207,10 +208,11 @@ struct Pool {
     if (!e) e = dalloc(&P.mexc, (size_t)nt * 32);
     if (!e) e = dalloc(&P.mreach, (size_t)nt * 32);
     int32_t** small[] = {&P.touched, &P.act_int, &P.mark[0], &P.mark[1], &P.tact, &P.img_of,
-                         &P.queue[0], &P.queue[1], &P.inq[0], &P.inq[1]};
+                         &P.queue[0], &P.queue[1], &P.inq[0], &P.inq[1], &P.mdirty};
     for (auto** p : small) if (!e) e = dalloc(p, nt);
     if (!e) e = dalloc(&P.qcount, 2);
     if (!e) e = dalloc(&P.img_live, imgs.size());
+    if (!e) e = dalloc(&P.tpos, nt);
     P.nimg = (int)imgs.size();
     list = P.queue[0];
     counts = P.qcount;
@@ -241,6 +243,8 @@ struct Pool {
     CK(cudaMemset(P.ctl, 0, sizeof(int32_t) * CTL_N));
     CK(cudaMemset(P.qcount, 0, sizeof(int32_t) * 2));
     CK(cudaMemset(P.img_live, 0, sizeof(int32_t) * imgs.size()));
+    CK(cudaMemset(P.mdirty, 0, sizeof(int32_t) * nt));
+    CK(cudaMemset(P.tpos, 0, sizeof(long long) * nt));
     CK(cudaMemset(P.inq[0], 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.inq[1], 0, sizeof(int32_t) * nt));
     CK(cudaMemset(P.act_int, 0, sizeof(int32_t) * nt));
@@ -511,6 +515,7 @@ struct Pool {
     RK(check_device_error(s));
     if (h_ctl[CTL_ERR] == 1) return fail(GC_ERR_NOT_CONVERGED, "BFS round cap reached");
     if (h_ctl[CTL_ERR] == 2) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
+    if (h_ctl[CTL_ERR] == 3) return fail(GC_ERR_INTERNAL, "a bounded wait for a tile copy gave up");
     for (size_t i = 0; i < imgs.size(); ++i)
       if (h_acc[i].bad_caps) return fail(GC_ERR_INVALID, "negative capacity in the upload");
     stats.bfs_rounds = h_ctl[CTL_BFS_TOTAL];

@@ -45,6 +45,8 @@ struct PoolView {
   int32_t* inq[2];        // [nt] tile is in queue[k] (deduplication)
   int32_t* tact;          // [nt] tile has an active pixel (excess > 0, height < HINF)
   int32_t* img_of;        // [nt] image index of the tile
+  int32_t* mdirty;        // [nt] the tile's planes changed since its masks were computed
+  long long* tpos;        // [nt] sum of max(excess, 0) over the tile (with the masks)
   int nimg;               // images in the pool
   int32_t* img_live;      // [nimg] cycle stamp of images that still have active tiles
   unsigned long long* ktiles;  // [K_COUNT] tiles processed per kernel kind (profiling)

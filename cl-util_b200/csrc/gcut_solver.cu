@@ -92,6 +92,7 @@ k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
     P.mark[1][t] = 0;
     P.inq[0][t] = 0;
     P.inq[1][t] = 0;
+    P.mdirty[t] = 1;
     P.img_of[t] = img;
   }
 }
@@ -132,31 +133,102 @@ __device__ __forceinline__ void sts4(int32_t* p, int a, int b, int c, int d) {
   *reinterpret_cast<int4*>(p) = make_int4(a, b, c, d);
 }
 
+// Bulk copies global -> shared memory (cp.async.bulk, completion on an mbarrier).  The
+// copies are plain (no cluster multicast); every wait on the mbarrier is bounded.
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, unsigned count) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(mbar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mbar, unsigned bytes) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(mbar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* mbar) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const unsigned m = (unsigned)__cvta_generic_to_shared(mbar);
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(d), "l"(src), "r"(bytes), "r"(m) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, unsigned parity) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(mbar);
+  unsigned ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+               : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+  return ok != 0;
+}
+// Bounded wait: false when the copy did not complete within the limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, unsigned parity) {
+  for (int i = 0; i < GC_SPIN_LIMIT; ++i)
+    if (mbar_try_wait(mbar, parity)) return true;
+  return false;
+}
+
+constexpr int DIS_PLANES = 6;                                  // excess, height, 4 residuals
+constexpr unsigned DIS_TILE_BYTES = DIS_PLANES * GC_TILE_PX * 4;  // 24 KiB
+// dynamic shared memory: two tile buffers + the per-round exchange arrays
+constexpr size_t DIS_DYN_SMEM = 2 * (size_t)DIS_TILE_BYTES + sizeof(DisSmem);
+
+__device__ __forceinline__ const int32_t* dis_plane(const PoolView& P, int k) {
+  return k == 0 ? P.exc : k == 1 ? P.hgt : P.cap[k - 2];
+}
+
+// Thread 0: start the bulk copy of tile t's six planes into buffer `buf`.
+__device__ __forceinline__ void dis_prefetch(const PoolView& P, int t, int32_t* buf, uint64_t* mbar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // buffer was last read by threads
+  mbar_expect_tx(mbar, DIS_TILE_BYTES);
+#pragma unroll
+  for (int k = 0; k < DIS_PLANES; ++k)
+    bulk_g2s(buf + k * GC_TILE_PX, dis_plane(P, k) + (long long)t * GC_TILE_PX, GC_TILE_PX * 4, mbar);
+}
+
 __global__ void __launch_bounds__(DIS_THREADS, 3)
 k_discharge(PoolView P, int iters) {
-  __shared__ DisSmem S;
+  extern __shared__ __align__(128) int32_t dsm[];
+  int32_t* const bufs = dsm;                                   // [2][6][1024]
+  DisSmem& S = *reinterpret_cast<DisSmem*>(dsm + 2 * DIS_PLANES * GC_TILE_PX);
+  __shared__ uint64_t mbar[2];
   __shared__ int s_cur, s_n;
   const int tid = threadIdx.x;
   const int r = tid >> 3, q = tid & 7, c0 = q * 4;
   if (tid == 0) {
     s_cur = *((volatile int32_t*)&P.ctl[CTL_PULSE]) & 1;
     s_n = *((volatile int32_t*)&P.qcount[s_cur]);
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
   const int cur = s_cur, nxt = cur ^ 1, n = s_n;
   const bool erow = (r == 0) || (r == 31);
-  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+  const int pix = r * GC_TILE + c0;
+  unsigned phase[2] = {0, 0};
+  int it_local = 0;
+  bool failed = false;
+  if (tid == 0 && (int)blockIdx.x < n) dis_prefetch(P, P.queue[cur][blockIdx.x], bufs, &mbar[0]);
+  for (int li = blockIdx.x; li < n; li += gridDim.x, ++it_local) {
+    const int b = it_local & 1;
+    int32_t* const buf = bufs + b * DIS_PLANES * GC_TILE_PX;
     const int t = P.queue[cur][li];
+    // prefetch the next tile of this CTA into the other buffer (read two tiles ago)
+    if (tid == 0 && li + (int)gridDim.x < n)
+      dis_prefetch(P, P.queue[cur][li + gridDim.x], bufs + (b ^ 1) * DIS_PLANES * GC_TILE_PX, &mbar[b ^ 1]);
     const int4 nb = P.nbr[t];
-    const long long off = (long long)t * GC_TILE_PX + r * GC_TILE + c0;
+    if (tid < 32) S.hu[tid] = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + tid] : GC_HINF;
+    else if (tid < 64) S.hd[tid - 32] = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + (tid - 32)] : GC_HINF;
+    else if (tid < 96) S.hl[tid - 64] = nb.z >= 0 ? P.hgt[(long long)nb.z * GC_TILE_PX + (tid - 64) * GC_TILE + 31] : GC_HINF;
+    else if (tid < 128) S.hr[tid - 96] = nb.w >= 0 ? P.hgt[(long long)nb.w * GC_TILE_PX + (tid - 96) * GC_TILE] : GC_HINF;
+    if (tid == 0) P.inq[cur][t] = 0;
+    const bool ok = mbar_wait(&mbar[b], phase[b]);
+    if (__syncthreads_or(!ok)) { failed = true; break; }  // block-uniform decision
+    phase[b] ^= 1u;
     int e[4], h[4], cu[4], cd[4], cl[4], cr[4];
     {
-      int4 v = *(const int4*)(P.exc + off); e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w;
-      v = *(const int4*)(P.hgt + off); h[0] = v.x; h[1] = v.y; h[2] = v.z; h[3] = v.w;
-      v = *(const int4*)(P.cap[DUP] + off); cu[0] = v.x; cu[1] = v.y; cu[2] = v.z; cu[3] = v.w;
-      v = *(const int4*)(P.cap[DDOWN] + off); cd[0] = v.x; cd[1] = v.y; cd[2] = v.z; cd[3] = v.w;
-      v = *(const int4*)(P.cap[DLEFT] + off); cl[0] = v.x; cl[1] = v.y; cl[2] = v.z; cl[3] = v.w;
-      v = *(const int4*)(P.cap[DRIGHT] + off); cr[0] = v.x; cr[1] = v.y; cr[2] = v.z; cr[3] = v.w;
+      int4 v = lds4(buf + 0 * GC_TILE_PX + pix); e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w;
+      v = lds4(buf + 1 * GC_TILE_PX + pix); h[0] = v.x; h[1] = v.y; h[2] = v.z; h[3] = v.w;
+      v = lds4(buf + 2 * GC_TILE_PX + pix); cu[0] = v.x; cu[1] = v.y; cu[2] = v.z; cu[3] = v.w;
+      v = lds4(buf + 3 * GC_TILE_PX + pix); cd[0] = v.x; cd[1] = v.y; cd[2] = v.z; cd[3] = v.w;
+      v = lds4(buf + 4 * GC_TILE_PX + pix); cl[0] = v.x; cl[1] = v.y; cl[2] = v.z; cl[3] = v.w;
+      v = lds4(buf + 5 * GC_TILE_PX + pix); cr[0] = v.x; cr[1] = v.y; cr[2] = v.z; cr[3] = v.w;
     }
     // height cap of tile-edge pixels for this launch (interior: none)
     int hcap[4];
@@ -166,31 +238,21 @@ k_discharge(PoolView P, int iters) {
       const bool edge = erow || c == 0 || c == 31;
       hcap[j] = edge ? (h[j] >= GC_HINF - 2 ? GC_HINF : h[j] + 2) : GC_HINF;
     }
-    int e0[4], cu0[4], cd0[4], cl0, cr0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) { e0[j] = e[j]; cu0[j] = cu[j]; cd0[j] = cd[j]; }
-    cl0 = cl[0];
-    cr0 = cr[3];
-    sts4(S.hs + r * GC_TILE + c0, h[0], h[1], h[2], h[3]);
-    if (tid < 32) S.hu[tid] = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + tid] : GC_HINF;
-    else if (tid < 64) S.hd[tid - 32] = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + (tid - 32)] : GC_HINF;
-    else if (tid < 96) S.hl[tid - 64] = nb.z >= 0 ? P.hgt[(long long)nb.z * GC_TILE_PX + (tid - 64) * GC_TILE + 31] : GC_HINF;
-    else if (tid < 128) S.hr[tid - 96] = nb.w >= 0 ? P.hgt[(long long)nb.w * GC_TILE_PX + (tid - 96) * GC_TILE] : GC_HINF;
-    if (tid == 0) P.inq[cur][t] = 0;
+    sts4(S.hs + pix, h[0], h[1], h[2], h[3]);
     int xu[4] = {0, 0, 0, 0}, xd[4] = {0, 0, 0, 0}, xl = 0, xr = 0;  // cross-tile flow
     __syncthreads();
 
     for (int it = 0; it < iters; ++it) {
       // neighbour heights (fixed during the push phase)
       int hnu[4], hnd[4], hnl[4], hnr[4];
-      if (r > 0) { const int4 v = lds4(S.hs + (r - 1) * GC_TILE + c0); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
+      if (r > 0) { const int4 v = lds4(S.hs + pix - GC_TILE); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
       else { const int4 v = lds4(S.hu + c0); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
-      if (r < 31) { const int4 v = lds4(S.hs + (r + 1) * GC_TILE + c0); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
+      if (r < 31) { const int4 v = lds4(S.hs + pix + GC_TILE); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
       else { const int4 v = lds4(S.hd + c0); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
-      hnl[0] = c0 > 0 ? S.hs[r * GC_TILE + c0 - 1] : S.hl[r];
+      hnl[0] = c0 > 0 ? S.hs[pix - 1] : S.hl[r];
       hnl[1] = h[0]; hnl[2] = h[1]; hnl[3] = h[2];
       hnr[0] = h[1]; hnr[1] = h[2]; hnr[2] = h[3];
-      hnr[3] = c0 < 28 ? S.hs[r * GC_TILE + c0 + 4] : S.hr[r];
+      hnr[3] = c0 < 28 ? S.hs[pix + 4] : S.hr[r];
 
       // push phase
       int ou[4], od[4], ol[4], orr[4];
@@ -219,16 +281,16 @@ k_discharge(PoolView P, int iters) {
       }
       if (q == 0) { xl += ol[0]; ol[0] = 0; }
       if (q == 7) { xr += orr[3]; orr[3] = 0; }
-      sts4(S.fu + r * GC_TILE + c0, ou[0], ou[1], ou[2], ou[3]);
-      sts4(S.fd + r * GC_TILE + c0, od[0], od[1], od[2], od[3]);
+      sts4(S.fu + pix, ou[0], ou[1], ou[2], ou[3]);
+      sts4(S.fd + pix, od[0], od[1], od[2], od[3]);
       S.fl[r * 8 + q] = ol[0];
       S.fr[r * 8 + q] = orr[3];
       __syncthreads();
       // gather inflow; a pixel receiving flow gains the reverse residual
       {
-        const int4 a = r < 31 ? lds4(S.fu + (r + 1) * GC_TILE + c0) : make_int4(0, 0, 0, 0);
-        const int4 b = r > 0 ? lds4(S.fd + (r - 1) * GC_TILE + c0) : make_int4(0, 0, 0, 0);
-        const int fb[4] = {a.x, a.y, a.z, a.w}, fa[4] = {b.x, b.y, b.z, b.w};
+        const int4 a = r < 31 ? lds4(S.fu + pix + GC_TILE) : make_int4(0, 0, 0, 0);
+        const int4 bb = r > 0 ? lds4(S.fd + pix - GC_TILE) : make_int4(0, 0, 0, 0);
+        const int fb[4] = {a.x, a.y, a.z, a.w}, fa[4] = {bb.x, bb.y, bb.z, bb.w};
         int fromleft[4], fromright[4];
         fromleft[0] = q > 0 ? S.fr[r * 8 + q - 1] : 0;
         fromleft[1] = orr[0]; fromleft[2] = orr[1]; fromleft[3] = orr[2];
@@ -265,21 +327,24 @@ k_discharge(PoolView P, int iters) {
       __syncthreads();  // all reads of S.hs / flow buffers of this round are done
 #pragma unroll
       for (int j = 0; j < 4; ++j) h[j] = nh[j];
-      sts4(S.hs + r * GC_TILE + c0, h[0], h[1], h[2], h[3]);
+      sts4(S.hs + pix, h[0], h[1], h[2], h[3]);
       if (!__syncthreads_or(changed)) break;
     }
 
     // write back: interior values are owned by this CTA; tile-edge excess and the
     // outward residual of edge pixels also receive atomics from neighbouring tiles, so
-    // they are written as deltas.
+    // they are written as deltas against the values loaded (still in the tile buffer).
+    const long long off = (long long)t * GC_TILE_PX + pix;
     if (!erow && q > 0 && q < 7) {
       *(int4*)(P.exc + off) = make_int4(e[0], e[1], e[2], e[3]);
     } else {
+      const int4 e0 = lds4(buf + 0 * GC_TILE_PX + pix);
+      const int e0a[4] = {e0.x, e0.y, e0.z, e0.w};
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int c = c0 + j;
         if (erow || c == 0 || c == 31) {
-          if (e[j] != e0[j]) atomicAdd(P.exc + off + j, e[j] - e0[j]);
+          if (e[j] != e0a[j]) atomicAdd(P.exc + off + j, e[j] - e0a[j]);
         } else {
           P.exc[off + j] = e[j];
         }
@@ -287,24 +352,30 @@ k_discharge(PoolView P, int iters) {
     }
     *(int4*)(P.hgt + off) = make_int4(h[0], h[1], h[2], h[3]);
     if (r == 0) {
+      const int4 o = lds4(buf + 2 * GC_TILE_PX + pix);
+      const int oa[4] = {o.x, o.y, o.z, o.w};
 #pragma unroll
-      for (int j = 0; j < 4; ++j) if (cu[j] != cu0[j]) atomicAdd(P.cap[DUP] + off + j, cu[j] - cu0[j]);
+      for (int j = 0; j < 4; ++j) if (cu[j] != oa[j]) atomicAdd(P.cap[DUP] + off + j, cu[j] - oa[j]);
     } else {
       *(int4*)(P.cap[DUP] + off) = make_int4(cu[0], cu[1], cu[2], cu[3]);
     }
     if (r == 31) {
+      const int4 o = lds4(buf + 3 * GC_TILE_PX + pix);
+      const int oa[4] = {o.x, o.y, o.z, o.w};
 #pragma unroll
-      for (int j = 0; j < 4; ++j) if (cd[j] != cd0[j]) atomicAdd(P.cap[DDOWN] + off + j, cd[j] - cd0[j]);
+      for (int j = 0; j < 4; ++j) if (cd[j] != oa[j]) atomicAdd(P.cap[DDOWN] + off + j, cd[j] - oa[j]);
     } else {
       *(int4*)(P.cap[DDOWN] + off) = make_int4(cd[0], cd[1], cd[2], cd[3]);
     }
     if (q == 0) {
+      const int cl0 = buf[4 * GC_TILE_PX + pix];
       if (cl[0] != cl0) atomicAdd(P.cap[DLEFT] + off, cl[0] - cl0);
       P.cap[DLEFT][off + 1] = cl[1]; P.cap[DLEFT][off + 2] = cl[2]; P.cap[DLEFT][off + 3] = cl[3];
     } else {
       *(int4*)(P.cap[DLEFT] + off) = make_int4(cl[0], cl[1], cl[2], cl[3]);
     }
     if (q == 7) {
+      const int cr0 = buf[5 * GC_TILE_PX + pix + 3];
       if (cr[3] != cr0) atomicAdd(P.cap[DRIGHT] + off + 3, cr[3] - cr0);
       P.cap[DRIGHT][off] = cr[0]; P.cap[DRIGHT][off + 1] = cr[1]; P.cap[DRIGHT][off + 2] = cr[2];
     } else {
@@ -342,20 +413,29 @@ k_discharge(PoolView P, int iters) {
       act |= a;
       act_int |= a && !erow && c > 0 && c < 31;
     }
+    if (sent_u) { P.touched[nb.x] = 1; P.mdirty[nb.x] = 1; worklist_add(P, nxt, nb.x); }
+    if (sent_d) { P.touched[nb.y] = 1; P.mdirty[nb.y] = 1; worklist_add(P, nxt, nb.y); }
+    if (sent_l) { P.touched[nb.z] = 1; P.mdirty[nb.z] = 1; worklist_add(P, nxt, nb.z); }
+    if (sent_r) { P.touched[nb.w] = 1; P.mdirty[nb.w] = 1; worklist_add(P, nxt, nb.w); }
+    // the block-wide reductions also order every read of this buffer before its reuse
     const int any_act = __syncthreads_or(act);
     act_int = __syncthreads_or(act_int);
-    const int sent = __syncthreads_or(sent_u | (sent_d << 1) | (sent_l << 2) | (sent_r << 3));
-    (void)sent;
-    if (sent_u) { P.touched[nb.x] = 1; worklist_add(P, nxt, nb.x); }
-    if (sent_d) { P.touched[nb.y] = 1; worklist_add(P, nxt, nb.y); }
-    if (sent_l) { P.touched[nb.z] = 1; worklist_add(P, nxt, nb.z); }
-    if (sent_r) { P.touched[nb.w] = 1; worklist_add(P, nxt, nb.w); }
     if (tid == 0) {
       P.touched[t] = 1;
+      P.mdirty[t] = 1;
       P.act_int[t] = act_int;
       if (any_act) worklist_add(P, nxt, t);
       if (P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
     }
+  }
+  if (failed) {
+    // a bulk copy did not complete in time: record it, let our copies drain, stop
+    if (tid == 0) {
+      atomicExch(&P.ctl[CTL_ERR], 3);
+      mbar_wait(&mbar[0], phase[0]);
+      mbar_wait(&mbar[1], phase[1]);
+    }
+    __syncthreads();
   }
   // last CTA: the queue just read is consumed; the next launch reads the other one
   __syncthreads();
@@ -639,17 +719,34 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
     const int4 nb = P.nbr[t];
     const long long base = (long long)t * GC_TILE_PX;
     uint32_t canU, canD, canL, canR, sink;
-    if (first) {
+    if (first && P.mdirty[t]) {
+      // the tile changed since its masks were built: rebuild them (row masks by ballot),
+      // together with the tile's sum of positive excess
       canU = rows_ballot(P.cap[DUP] + base, lane, [](int v) { return v > 0; });
       canD = rows_ballot(P.cap[DDOWN] + base, lane, [](int v) { return v > 0; });
       canL = rows_ballot(P.cap[DLEFT] + base, lane, [](int v) { return v > 0; });
       canR = rows_ballot(P.cap[DRIGHT] + base, lane, [](int v) { return v > 0; });
-      sink = rows_ballot(P.exc + base, lane, [](int v) { return v < 0; });
-      const uint32_t pos = rows_ballot(P.exc + base, lane, [](int v) { return v > 0; });
+      uint32_t pos = 0;
+      sink = 0;
+      long long ps = 0;
+#pragma unroll 4
+      for (int rr = 0; rr < 32; ++rr) {
+        const int v = P.exc[base + rr * GC_TILE + lane];
+        const uint32_t bs = __ballot_sync(0xffffffffu, v < 0);
+        const uint32_t bp = __ballot_sync(0xffffffffu, v > 0);
+        if (lane == rr) { sink = bs; pos = bp; }
+        ps += v > 0 ? v : 0;
+      }
+#pragma unroll
+      for (int o = 16; o; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
       uint32_t* mc = P.mcan + (long long)t * 128;
       mc[lane] = canU; mc[32 + lane] = canD; mc[64 + lane] = canL; mc[96 + lane] = canR;
       P.msink[(long long)t * 32 + lane] = sink;
       P.mexc[(long long)t * 32 + lane] = pos;
+      if (lane == 0) {
+        P.tpos[t] = ps;
+        P.mdirty[t] = 0;
+      }
     } else {
       const uint32_t* mc = P.mcan + (long long)t * 128;
       canU = mc[lane]; canD = mc[32 + lane]; canL = mc[64 + lane]; canR = mc[96 + lane];
@@ -741,13 +838,10 @@ k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc
     if (first) {
       R = P.mexc[(long long)t * 32 + lane];
       R0 = 0;
-      long long s = 0;
-      const int32_t* ep = P.exc + (long long)t * GC_TILE_PX;
-#pragma unroll 4
-      for (int rr = 0; rr < 32; ++rr) { const int v = ep[rr * GC_TILE + lane]; s += v > 0 ? v : 0; }
-#pragma unroll
-      for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0 && s) atomicAdd(&acc[P.img_of[t]].sumpos_e, (unsigned long long)s);
+      // Σ max(excess, 0) of the tile was taken with its masks at the last global relabel,
+      // after which the tile did not change
+      const long long ps = P.tpos[t];
+      if (lane == 0 && ps) atomicAdd(&acc[P.img_of[t]].sumpos_e, (unsigned long long)ps);
     } else {
       R = R0 = P.mreach[(long long)t * 32 + lane];
       if (lane == 0 && nb.x >= 0)
@@ -788,13 +882,26 @@ k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc
   frontier_round_end(P, first, in, CTL_FLOOD_TOTAL, h);
 }
 
-// Labels of one image, row-major, padding excluded.
+// Labels of one image, row-major, padding excluded.  One thread writes the 32 pixels of
+// one tile row (one mask word); consecutive threads take consecutive tiles of an image row.
 __global__ void k_labels_out(PoolView P, ImageDesc im, uint8_t* __restrict__ out) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)im.W * im.H) return;
-  const int y = (int)(i / im.W), x = (int)(i % im.W);
-  const int t = im.tile0 + (y >> 5) * im.tw + (x >> 5);
-  out[i] = (uint8_t)((P.mreach[(long long)t * 32 + (y & 31)] >> (x & 31)) & 1u);
+  if (i >= (long long)im.H * im.tw) return;
+  const int y = (int)(i / im.tw), tx = (int)(i % im.tw);
+  const int t = im.tile0 + (y >> 5) * im.tw + tx;
+  const uint32_t m = P.mreach[(long long)t * 32 + (y & 31)];
+  const int x0 = tx * GC_TILE;
+  uint8_t* row = out + (long long)y * im.W + x0;
+  if (x0 + GC_TILE <= im.W && (((uintptr_t)row) & 3) == 0) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t b = (m >> (4 * k)) & 0xfu;
+      const uint32_t w = (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21);
+      reinterpret_cast<uint32_t*>(row)[k] = w;
+    }
+  } else {
+    for (int c = 0; c < GC_TILE && x0 + c < im.W; ++c) row[c] = (uint8_t)((m >> c) & 1u);
+  }
 }
 
 // One plane of one image back to row-major.
@@ -815,6 +922,7 @@ __device__ __forceinline__ void apply_tlink(const PoolView& P, const ImageDesc& 
   if (old == v) return;
   tl[o] = v;
   atomicAdd(P.exc + o, v - old);
+  P.mdirty[t] = 1;
   const long long dpos = (long long)(v > 0 ? v : 0) - (long long)(old > 0 ? old : 0);
   if (dpos) atomicAdd(&acc[img].sumpos_t, (unsigned long long)dpos);
 }
@@ -869,7 +977,7 @@ int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t
 }
 
 int launch_discharge(const PoolView& P, int iters, int grid, cudaStream_t s) {
-  k_discharge<<<grid, DIS_THREADS, 0, s>>>(P, iters);
+  k_discharge<<<grid, DIS_THREADS, DIS_DYN_SMEM, s>>>(P, iters);
   return ok();
 }
 
@@ -922,7 +1030,9 @@ int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
 
 int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s) {
   const long long n = (long long)im.W * im.H;
-  k_labels_out<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, im, out);
+  const long long segs = (long long)im.H * im.tw;
+  (void)n;
+  k_labels_out<<<(unsigned)((segs + 255) / 256), 256, 0, s>>>(P, im, out);
   return ok();
 }
 
@@ -964,7 +1074,8 @@ int launch_stroke(const PoolView& P, const ImageDesc& im, int img, const int32_t
 
 int occupancy_discharge(int device) {
   int per_sm = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_discharge, DIS_THREADS, 0);
+  cudaFuncSetAttribute(k_discharge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DIS_DYN_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_discharge, DIS_THREADS, DIS_DYN_SMEM);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
 }
