@@ -39,6 +39,24 @@ __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 // isolated (all zero).  Heights start at 0 for sink pixels and 1 otherwise (a valid
 // labelling).  Replaces init_gc + load_tiles (graphcut.cl:63-112, 1033-1132).
 // ------------------------------------------------------------------------------------
+// Spreads bits 0..7 of x to bit positions 0, 4, ..., 28.
+__device__ __forceinline__ uint32_t spread8(uint32_t x) {
+  x &= 0xffu;
+  x = (x | (x << 12)) & 0x000F000Fu;
+  x = (x | (x << 6)) & 0x03030303u;
+  x = (x | (x << 3)) & 0x11111111u;
+  return x;
+}
+
+// Row mask of row (lane & 3) of this warp's four rows, from the ballots of the four pixels
+// each thread holds (thread (g, q) of the warp holds pixels 4q..4q+3 of row g).
+__device__ __forceinline__ uint32_t warp_row_mask(uint32_t b0, uint32_t b1, uint32_t b2, uint32_t b3,
+                                                  int ri) {
+  const int sh = 8 * ri;
+  return spread8(b0 >> sh) | (spread8(b1 >> sh) << 1) | (spread8(b2 >> sh) << 2) |
+         (spread8(b3 >> sh) << 3);
+}
+
 __global__ void __launch_bounds__(DIS_THREADS)
 k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
          const int32_t* __restrict__ down, const int32_t* __restrict__ left,
@@ -78,12 +96,41 @@ k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
   *(int4*)(P.cap[DLEFT] + off) = make_int4(cl[0], cl[1], cl[2], cl[3]);
   *(int4*)(P.cap[DRIGHT] + off) = make_int4(cr[0], cr[1], cr[2], cr[3]);
   // block reductions
+  // row masks of the residual graph (the BFS reads these instead of the planes)
+  {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned F = 0xffffffffu;
+    uint32_t m[6];
+    const int* planes4[4] = {cu, cd, cl, cr};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int* v = planes4[k];
+      m[k] = warp_row_mask(__ballot_sync(F, v[0] > 0), __ballot_sync(F, v[1] > 0),
+                           __ballot_sync(F, v[2] > 0), __ballot_sync(F, v[3] > 0), lane & 3);
+    }
+    m[4] = warp_row_mask(__ballot_sync(F, e[0] < 0), __ballot_sync(F, e[1] < 0),
+                         __ballot_sync(F, e[2] < 0), __ballot_sync(F, e[3] < 0), lane & 3);
+    m[5] = warp_row_mask(__ballot_sync(F, e[0] > 0), __ballot_sync(F, e[1] > 0),
+                         __ballot_sync(F, e[2] > 0), __ballot_sync(F, e[3] > 0), lane & 3);
+    if (lane < 4) {
+      const int row = 4 * w + lane;
+      uint32_t* mc = P.mcan + (long long)t * 128;
+      mc[row] = m[0]; mc[32 + row] = m[1]; mc[64 + row] = m[2]; mc[96 + row] = m[3];
+      P.msink[(long long)t * 32 + row] = m[4];
+      P.mexc[(long long)t * 32 + row] = m[5];
+    }
+  }
+  __shared__ long long wpos[DIS_THREADS / 32];
 #pragma unroll
   for (int o = 16; o; o >>= 1) pos += __shfl_xor_sync(0xffffffffu, pos, o);
+  if ((threadIdx.x & 31) == 0) wpos[threadIdx.x >> 5] = pos;
   bad = __syncthreads_or(bad);
   anypos = __syncthreads_or(anypos);
   if ((threadIdx.x & 31) == 0 && pos) atomicAdd(&acc[img].sumpos_t, (unsigned long long)pos);
   if (threadIdx.x == 0) {
+    long long tp = 0;
+    for (int k = 0; k < DIS_THREADS / 32; ++k) tp += wpos[k];
+    P.tpos[t] = tp;
     if (bad) atomicAdd(&acc[img].bad_caps, 1);
     P.tact[t] = anypos;
     P.touched[t] = 0;
@@ -92,7 +139,7 @@ k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
     P.mark[1][t] = 0;
     P.inq[0][t] = 0;
     P.inq[1][t] = 0;
-    P.mdirty[t] = 1;
+    P.mdirty[t] = 0;  // the masks above are current
     P.img_of[t] = img;
   }
 }
@@ -572,7 +619,7 @@ constexpr int WARPS_PER_CTA = 4;
 template <class F>
 __device__ __forceinline__ uint32_t rows_ballot(const int32_t* __restrict__ plane, int lane, F f) {
   uint32_t mine = 0;
-#pragma unroll 4
+#pragma unroll
   for (int rr = 0; rr < 32; ++rr) {
     const uint32_t b = __ballot_sync(0xffffffffu, f(plane[rr * GC_TILE + lane]));
     if (lane == rr) mine = b;
