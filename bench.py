@@ -1,7 +1,7 @@
 """Benchmark: Mpix/s to the bit-exact min cut on one (or N) B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config single|batch] [--size 2048]
+                    [--config single|batch|strokes|serving] [--size 2048]
 
 A step is one solve of one synthetic grid: capacities already resident in HBM (row-major
 int32 planes) -> tile upload -> push-relabel with global relabels -> canonical cut flood
@@ -42,7 +42,8 @@ import numpy as np  # noqa: E402
 METRIC = "Mpix/s at bit-exact min cut"
 UNIT = "Mpix/s"
 
-# Algorithmic bytes per tile (32x32 pixels, int32 planes) of each kernel kind; see DESIGN.md.
+# Algorithmic bytes per tile (32x32 pixels, int32 planes) of each kernel kind: the bytes a
+# kernel must move for one tile, counting each plane it reads or writes once.
 ALGO_BYTES_PER_TILE = {
     "upload": 1024 * 4 * (5 + 7),          # read 5 row-major planes, write 7 tile planes
     "discharge": 1024 * 4 * (6 + 6) + 4 * 32 * 4,  # read+write excess/height/4 caps, halo
@@ -62,10 +63,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="single", choices=["single", "batch", "strokes"])
+    ap.add_argument("--config", default="single",
+                    choices=["single", "batch", "strokes", "serving"])
     ap.add_argument("--batch", type=int, default=64, help="grids in --config batch")
     ap.add_argument("--strokes", type=int, default=200, help="strokes in --config strokes")
     ap.add_argument("--size", type=int, default=2048)
+    ap.add_argument("--duration", type=float, default=60.0, help="seconds of --config serving trace")
+    ap.add_argument("--rate", type=float, default=200.0, help="requests/s of --config serving")
+    ap.add_argument("--slots", type=int, default=4, help="requests in flight, --config serving")
+    ap.add_argument("--verify-s", type=float, default=90.0,
+                    help="wall-time cap of the --config serving result verification")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--host-driven", action="store_true",
@@ -208,6 +215,8 @@ def main():
         return run_batch(args)
     if args.config == "strokes":
         return run_strokes(args)
+    if args.config == "serving":
+        return run_serving(args)
     import torch
     import torch.distributed as dist
 
@@ -540,6 +549,167 @@ def run_strokes(args):
         "warm_mpix_per_s": mpix / (np.mean(lat) / 1000),
         "cold_solve_ms_mean": float(np.mean(cold_ms)),
         "warm_vs_cold_mismatches": mism, "oracle_checks_ok": bool(oracle_ok and parity0),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def serving_images(n=12, seed=4):
+    """The image pool of --config serving: n grids with sides drawn uniformly from
+    [256, 4096] (width and height independent), built as the synthetic generator, seeds
+    20000+i.  New-image requests draw from this pool; each starts its own session."""
+    import synth
+    rng = np.random.default_rng(seed)
+    shapes = [(int(rng.integers(256, 4097)), int(rng.integers(256, 4097))) for _ in range(n)]
+    return synth.make_graphs([(w, h, 20_000 + i) for i, (w, h) in enumerate(shapes)])
+
+
+def run_trace(graphs, host_planes, trace, slots, budget, seed=5, solver_kw=None):
+    """Replays a (time, kind, image) trace against a GraphCutServer in real time.  A stroke
+    targets one of the 8 most recently opened sessions (random polyline, radius 8-32,
+    t-links +-10**6).  Returns (results, history, server counters, wall seconds)."""
+    import strokes
+    from serving import GraphCutServer, NewImage, Stroke
+    rng = np.random.default_rng(seed)
+    srv = GraphCutServer(slots=slots, hbm_budget=budget, solver_kw=solver_kw)
+    history = {}     # session -> (image index, [strokes in submission order])
+    sid = 0
+    t0 = time.perf_counter()
+    for t, kind, img in trace:
+        now = time.perf_counter() - t0
+        if t > now:
+            time.sleep(t - now)
+        if kind == "image" or not history:
+            history[sid] = (img, [])
+            srv.submit(NewImage(sid, host_planes[img]), arrival=t0 + t)
+            sid += 1
+        else:
+            recent = list(history)[-8:]
+            target = recent[int(rng.integers(len(recent)))]
+            g = graphs[history[target][0]]
+            s = strokes.random_stroke(rng, g.width, g.height)
+            history[target][1].append(s)
+            srv.submit(Stroke(target, s.xs, s.ys, s.radius, s.value), arrival=t0 + t)
+    srv.drain()
+    wall = time.perf_counter() - t0
+    results = sorted(srv.results, key=lambda r: r.arrival)
+    counters = {"misses": srv.misses, "evictions": srv.evictions}
+    srv.close()
+    return results, history, counters, wall
+
+
+def _latency_summary(results, wall):
+    lat = {k: [r.latency_ms for r in results if r.kind == k] for k in ("image", "stroke")}
+    big = [r.latency_ms for r in results if r.kind == "stroke" and r.pixels >= 3072 * 3072]
+    svc = [1000.0 * (r.done - r.start) for r in results]
+    pct = lambda xs, p: _percentile(xs, p) if xs else None  # noqa: E731
+    first = min(r.arrival for r in results)
+    last = max(r.done for r in results)
+    return {
+        "stroke_p50_ms": pct(lat["stroke"], 50), "stroke_p99_ms": pct(lat["stroke"], 99),
+        "stroke_p99_ms_images_ge_3072sq": pct(big, 99), "strokes_on_images_ge_3072sq": len(big),
+        "image_p50_ms": pct(lat["image"], 50), "image_p99_ms": pct(lat["image"], 99),
+        "all_p50_ms": pct(lat["image"] + lat["stroke"], 50),
+        "all_p99_ms": pct(lat["image"] + lat["stroke"], 99),
+        "service_p50_ms": pct(svc, 50), "service_p99_ms": pct(svc, 99),
+        "served_mpix_per_s": sum(r.pixels for r in results) / 1e6 / (last - first),
+        "phases_p50_ms": {k: [round(_percentile([r.phases_ms[j] for r in results
+                                                if r.kind == k], 50), 3) for j in range(3)]
+                          for k in ("image", "stroke") if lat[k]},
+        "phases": "(input upload or stroke edit, solve, labels to host) per request",
+        "results": len(results), "images": len(lat["image"]), "strokes": len(lat["stroke"]),
+        "wall_s": wall,
+    }
+
+
+def verify_results(graphs, dev_planes, results, history, cap_s):
+    """Checks results against cold solves of the same edited graph (host stroke raster,
+    fresh upload, one solve), session by session in random order, until cap_s seconds.
+    Returns (checked, mismatches, examples)."""
+    import torch
+
+    import strokes
+    from GraphCut import GraphCut
+    by_session = {}
+    for r in results:
+        by_session.setdefault(r.session, []).append(r)
+    order = list(by_session)
+    np.random.default_rng(9).shuffle(order)
+    cold = {}
+    checked, bad, examples = 0, 0, []
+    t0 = time.perf_counter()
+    for sid in order:
+        if time.perf_counter() - t0 > cap_s:
+            break
+        img, strks = history[sid]
+        g = graphs[img]
+        key = (g.width, g.height)
+        if key not in cold:
+            cold[key] = GraphCut(g.width, g.height)
+        gc = cold[key]
+        t = g.excess.copy()
+        for k, r in enumerate(by_session[sid]):   # the k-th result follows the first k strokes
+            if k:
+                t = strokes.apply(t, strks[k - 1])
+            pl = list(dev_planes[img][:4]) + [torch.from_numpy(t).cuda()]
+            gc.upload_capacities(*pl)
+            gc.cut()
+            f, lab = gc.flow, gc.labels_host()
+            checked += 1
+            if f != r.flow or not np.array_equal(lab, r.labels):
+                bad += 1
+                if len(examples) < 5:
+                    examples.append({"session": sid, "kind": r.kind, "k": k, "flow": r.flow,
+                                     "cold": f, "size": list(key)})
+    for gc in cold.values():
+        gc.close()
+    return checked, bad, examples
+
+
+def run_serving(args):
+    """Config 4: a Poisson request stream (`--rate` 200 req/s for `--duration` 60 s), 30 %
+    new images (sides uniform in [256, 4096]) and 70 % brush strokes on resident sessions,
+    served by GraphCutServer with `--slots` requests in flight under a 64 GiB HBM budget,
+    then the same trace served one request at a time (slots=1).  Latency = result on the
+    host - arrival; every request's inputs come from pinned host memory and its labels go
+    back to host memory.  A time-capped sample of the results (whole sessions) is checked
+    bit-exactly against cold solves."""
+    import torch
+
+    from serving import poisson_trace
+    graphs = serving_images()
+    torch.cuda.set_device(0)
+    pinned = [[torch.from_numpy(p).pin_memory() for p in g.planes()] for g in graphs]
+    host_planes = [tuple(t.numpy() for t in pl) for pl in pinned]   # views; pinned keeps them
+    dev_planes = [[t.cuda() for t in pl] for pl in pinned]
+    trace = poisson_trace(np.random.default_rng(6), args.rate, args.duration, len(graphs))
+    budget = 64 << 30
+    # warm-up: an untimed trace of another seed (up to 15 s): the driver's first few hundred
+    # CUDA-graph instantiations in a process are slow, which is start-up, not serving
+    warm = poisson_trace(np.random.default_rng(7), args.rate, min(args.duration, 15.0),
+                         len(graphs))
+    run_trace(graphs, host_planes, warm, args.slots, budget, seed=8)
+    clocks = ClockSampler(0)
+    with clocks:
+        res, hist, cnt, wall = run_trace(graphs, host_planes, trace, args.slots, budget)
+    main_sum = _latency_summary(res, wall)
+    res1, hist1, cnt1, wall1 = run_trace(graphs, host_planes, trace, 1, budget)
+    one_sum = _latency_summary(res1, wall1)
+    checked, bad, examples = verify_results(graphs, dev_planes, res, hist, args.verify_s)
+    line = {
+        "metric": "p99 stroke re-solve latency, mixed-size load", "value": main_sum["stroke_p99_ms"],
+        "unit": "ms", "n_gpus": 1, "steps": len(trace), "warmup": len(warm),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic",
+        "config": {"workload": f"Poisson {args.rate:g} req/s for {args.duration:g} s: 30% new "
+                               "image (pool of 12 synthetic grids, sides uniform in [256, 4096], "
+                               "seeds 20000+i; each request opens its own session), 70% stroke "
+                               "(radius 8-32, t-links +-10^6) on one of the 8 newest sessions",
+                   "slots": args.slots, "hbm_budget_gib": budget >> 30,
+                   "latency": "arrival to labels in host memory (queueing included)"},
+        **main_sum, **cnt,
+        "one_at_a_time": {**one_sum, **cnt1},
+        "verified_results": checked, "mismatches": bad, "mismatch_examples": examples,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)

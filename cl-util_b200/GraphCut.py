@@ -37,13 +37,26 @@ def _as_i32_device(a, device):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.int32)).to(device)
 
 
+def _on(stream):
+    """Makes `stream` torch's current stream (no-op for None), so that torch copies made for
+    a call are ordered before the library's kernels on that stream."""
+    import contextlib
+    import torch
+    return contextlib.nullcontext() if stream is None else torch.cuda.stream(stream)
+
+
+def unpack_labels(bits: np.ndarray, width: int) -> np.ndarray:
+    """uint8 [H, W] labels from the packed rows of GraphCut.labels_packed*."""
+    return np.unpackbits(np.asarray(bits), axis=1, count=width, bitorder="little")
+
+
 class GraphCut:
     """Tiled push-relabel graph cut on one width x height 4-connected grid."""
 
     def __init__(self, width: int, height: int, device: int = 0, bfs: int | None = None,
                  discharge_iters: int | None = None, initial_relabel: bool | None = None,
                  max_cycles: int | None = None, max_bfs_rounds: int | None = None,
-                 use_graph: bool | None = None):
+                 use_graph: bool | None = None, arena=None):
         import torch
         self.width, self.height = int(width), int(height)
         self.device = torch.device("cuda", device)
@@ -55,9 +68,24 @@ class GraphCut:
         self.opts = opts
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            check(lib().gc_create(self.width, self.height, ctypes.byref(opts), ctypes.byref(h)))
+            if arena is None:
+                check(lib().gc_create(self.width, self.height, ctypes.byref(opts),
+                                      ctypes.byref(h)))
+            else:   # (device address, bytes) of caller-owned memory, or a CUDA tensor
+                addr, nbytes = ((arena.data_ptr(), arena.numel() * arena.element_size())
+                                if hasattr(arena, "data_ptr") else arena)
+                check(lib().gc_create_in(self.width, self.height, ctypes.byref(opts),
+                                         ctypes.c_void_p(addr), int(nbytes), ctypes.byref(h)))
+        self._arena = arena   # the memory must outlive the handle
         self._h = h
         self._solved = False
+
+    @staticmethod
+    def arena_bytes(width: int, height: int) -> int:
+        """Device bytes of a width x height handle (what `arena=` must provide)."""
+        out = ctypes.c_int64()
+        check(lib().gc_arena_bytes(int(width), int(height), ctypes.byref(out)))
+        return out.value
 
     def close(self):
         if getattr(self, "_h", None):
@@ -86,7 +114,8 @@ class GraphCut:
             if tuple(p.shape) != (self.height, self.width):
                 raise ValueError(f"plane shape {tuple(p.shape)} != {(self.height, self.width)}")
         if all(isinstance(p, torch.Tensor) and p.is_cuda for p in planes):
-            dev = [_as_i32_device(p, self.device) for p in planes]
+            with _on(stream):   # conversions are ordered before the upload kernel
+                dev = [_as_i32_device(p, self.device) for p in planes]
             check(lib().gc_upload(self._h, *[ptr(d) for d in dev], stream_handle(stream)))
             self._keep = dev  # the upload kernel reads them asynchronously
         else:
@@ -135,6 +164,23 @@ class GraphCut:
         check(lib().gc_labels(self._h, ptr(out), stream_handle(stream)))
         return out
 
+    def labels_packed(self, out=None, stream=None):
+        """Bit-packed canonical labels as a torch uint8 CUDA tensor [H, (W + 7) // 8]:
+        pixel x of a row is bit x % 8 of byte x // 8 (``unpack_labels`` inverts it)."""
+        import torch
+        if out is None:
+            out = torch.empty((self.height, (self.width + 7) // 8), dtype=torch.uint8,
+                              device=self.device)
+        check(lib().gc_labels_packed(self._h, ptr(out), stream_handle(stream)))
+        return out
+
+    def labels_packed_host(self, out=None, stream=None) -> np.ndarray:
+        """labels_packed into host memory (numpy; `out` may be a pinned buffer)."""
+        if out is None:
+            out = np.empty((self.height, (self.width + 7) // 8), np.uint8)
+        check(lib().gc_labels_packed_host(self._h, ptr(out), stream_handle(stream)))
+        return out
+
     def labels_host(self, stream=None) -> np.ndarray:
         out = np.empty((self.height, self.width), np.uint8)
         check(lib().gc_labels_host(self._h, ptr(out), stream_handle(stream)))
@@ -159,10 +205,11 @@ class GraphCut:
     def edit_tlinks(self, idx, values, stream=None):
         """Sets t-links of pixels idx (flat y*W+x, distinct) to values; warm-starts cut()."""
         import torch
-        idx = torch.as_tensor(np.asarray(idx.cpu() if isinstance(idx, torch.Tensor) else idx),
-                              dtype=torch.int32).to(self.device).contiguous()
-        vals = torch.as_tensor(np.asarray(values.cpu() if isinstance(values, torch.Tensor) else values),
-                               dtype=torch.int32).to(self.device).contiguous()
+        with _on(stream):   # the copies are ordered before the edit kernel
+            idx = torch.as_tensor(np.asarray(idx.cpu() if isinstance(idx, torch.Tensor) else idx),
+                                  dtype=torch.int32).to(self.device).contiguous()
+            vals = torch.as_tensor(np.asarray(values.cpu() if isinstance(values, torch.Tensor) else values),
+                                   dtype=torch.int32).to(self.device).contiguous()
         if idx.numel() != vals.numel():
             raise ValueError("idx and values differ in length")
         check(lib().gc_edit_tlinks(self._h, ptr(idx), ptr(vals), int(idx.numel()),

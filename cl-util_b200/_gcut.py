@@ -61,6 +61,8 @@ SIGNATURES = {
     "gc_opts_default": [_P],
     "gc_create": [_I, _I, _P, _P],
     "gc_destroy": [_P],
+    "gc_arena_bytes": [_I, _I, _P],
+    "gc_create_in": [_I, _I, _P, _P, ctypes.c_int64, _P],
     "gc_size": [_P, _P, _P],
     "gc_upload": [_P] * 6 + [_P],
     "gc_upload_host": [_P] * 6 + [_P],
@@ -72,6 +74,8 @@ SIGNATURES = {
     "gc_flow": [_P, _P],
     "gc_labels": [_P, _P, _P],
     "gc_labels_host": [_P, _P, _P],
+    "gc_labels_packed": [_P, _P, _P],
+    "gc_labels_packed_host": [_P, _P, _P],
     "gc_edit_tlinks": [_P, _P, _P, _I, _P],
     "gc_edit_stroke": [_P, _P, _P, _I, _I, _I32, _P],
     "gc_download_state": [_P] * 7 + [_P],

@@ -63,7 +63,10 @@ struct ScanBuffers {
     if ((e = cudaMemset(st.status, 0, sizeof(unsigned long long) * max_chunks))) return e;
     if ((e = cudaMemset(st.ticket, 0, 4 * sizeof(int32_t)))) return e;
     uint32_t one = 1;
-    return cudaMemcpy(st.seq, &one, sizeof(one), cudaMemcpyHostToDevice);
+    if ((e = cudaMemcpy(st.seq, &one, sizeof(one), cudaMemcpyHostToDevice))) return e;
+    // The clears above run on the legacy default stream, which does not order itself
+    // with non-blocking streams: finish them before any caller stream uses the state.
+    return cudaStreamSynchronize(cudaStreamLegacy);
   }
   void release() {
     if (st.status) cudaFree(st.status);
@@ -75,7 +78,58 @@ struct ScanBuffers {
 }  // namespace
 
 // ------------------------------------------------------------------------------------
-// Tile pool: one or more images, all solved together.
+// Small pinned host blocks (control words and accumulators copied back after a solve).
+// Page-locking host memory costs milliseconds per call, so blocks come from a
+// process-wide slab, allocated 64 at a time and recycled; larger requests (batch pools
+// with many images) get their own allocation.  Portable: usable from every device.
+// ------------------------------------------------------------------------------------
+namespace {
+constexpr size_t kPinBlock = 1024;
+constexpr int kPinPerChunk = 64;
+std::mutex g_pin_mu;
+std::vector<char*> g_pin_free;
+
+void* pinned_take(size_t bytes) {
+  void* p = nullptr;
+  if (bytes > kPinBlock) return cudaHostAlloc(&p, bytes, cudaHostAllocPortable) ? nullptr : p;
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  if (g_pin_free.empty()) {
+    char* c = nullptr;
+    if (cudaHostAlloc((void**)&c, kPinBlock * kPinPerChunk, cudaHostAllocPortable)) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    for (int i = kPinPerChunk - 1; i >= 0; --i) g_pin_free.push_back(c + (size_t)i * kPinBlock);
+  }
+  p = g_pin_free.back();
+  g_pin_free.pop_back();
+  return p;
+}
+
+void pinned_give(void* p, size_t bytes) {
+  if (!p) return;
+  if (bytes > kPinBlock) { cudaFreeHost(p); return; }
+  std::lock_guard<std::mutex> lock(g_pin_mu);
+  g_pin_free.push_back(static_cast<char*>(p));
+}
+
+// Sub-buffers of one device allocation, each 256-byte aligned.  Run once with base ==
+// nullptr to size the arena, then with the allocation to place the buffers.
+struct Carve {
+  char* base = nullptr;
+  size_t off = 0;
+  template <class T>
+  void take(T** out, size_t n) {
+    off = (off + 255) & ~(size_t)255;
+    *out = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += n * sizeof(T);
+  }
+};
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// Tile pool: one or more images, all solved together.  Every device buffer of the pool
+// lives in one allocation (the arena), cleared once at creation.
 // ------------------------------------------------------------------------------------
 struct Pool {
   int device = 0;
@@ -87,7 +141,13 @@ struct Pool {
   int32_t* list = nullptr;     // active / frontier tile list
   int32_t* counts = nullptr;   // [0] list length
   ImageAcc* acc = nullptr;     // per image
-  ScanBuffers scan;
+  ScanBuffers scan;            // look-back state (inside the arena)
+  char* arena = nullptr;       // every device buffer of the pool
+  size_t arena_bytes = 0;
+  bool own_arena = true;       // false: caller-owned memory (gc_create_in)
+  cudaEvent_t done_ev = nullptr;   // recorded after every call's work (see track)
+  void* pin = nullptr;         // pinned block holding h_count, h_ctl, h_acc
+  size_t pin_bytes = 0;
   int32_t* h_count = nullptr;  // pinned
   int32_t* h_ctl = nullptr;    // pinned copy of the control words
   bool use_graph = true;
@@ -145,48 +205,75 @@ struct Pool {
     ev_used.clear();
     return GC_OK;
   }
-  // staging for host uploads / label reads (single-image handles)
+  // staging for host uploads (allocated on first use) and label reads (in the arena,
+  // single-image handles)
   int32_t* stage = nullptr;
   uint8_t* lstage = nullptr;
-  int32_t* pts = nullptr;      // stroke points (device)
+  int32_t* pts = nullptr;      // stroke points (device, in the arena)
 
   ~Pool() { release(); }
 
-  void release() {
-    int32_t* bufs[] = {P.exc, P.hgt, P.cap[0], P.cap[1], P.cap[2], P.cap[3], tl,
-                       P.touched, P.act_int, P.mark[0], P.mark[1], P.rcnt, P.ctl, P.tact,
-                       P.img_of, P.queue[0], P.queue[1], P.qcount, P.inq[0], P.inq[1],
-                       P.img_live, P.mdirty, stage, pts};
-    if (P.tpos) cudaFree(P.tpos);
-    for (auto* b : bufs) if (b) cudaFree(b);
-    if (P.nbr) cudaFree(P.nbr);
-    if (P.mcan) cudaFree(P.mcan);
-    if (P.msink) cudaFree(P.msink);
-    if (P.mexc) cudaFree(P.mexc);
-    if (P.mreach) cudaFree(P.mreach);
-    if (acc) cudaFree(acc);
-    if (lstage) cudaFree(lstage);
-    release_graphs();
-    if (h_count) cudaFreeHost(h_count);
-    if (h_ctl) cudaFreeHost(h_ctl);
-    h_ctl = nullptr;
-    if (h_acc) cudaFreeHost(h_acc);
-    if (ktiles) cudaFree(ktiles);
-    for (auto e : ev_pool) cudaEventDestroy(e);
-    ev_pool.clear();
-    ktiles = nullptr;
-    scan.release();
-    P = PoolView{};
-    tl = list = counts = stage = pts = nullptr;
-    acc = nullptr; lstage = nullptr; h_count = nullptr; h_acc = nullptr;
+  // marks the end of the work a call enqueued on s; gc_destroy of a handle in caller-owned
+  // memory waits for it before the caller may reuse that memory
+  void track(cudaStream_t s) {
+    if (done_ev) cudaEventRecord(done_ev, s);
   }
 
-  int create(int n, const int* W, const int* H, const gc_opts* o) {
+  void release() {
+    if (done_ev) {
+      if (!own_arena) cudaEventSynchronize(done_ev);
+      cudaEventDestroy(done_ev);
+      done_ev = nullptr;
+    }
+    release_graphs();
+    if (stage) cudaFree(stage);   // host-upload staging, allocated on first use
+    if (arena && own_arena) cudaFree(arena);
+    pinned_give(pin, pin_bytes);
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    ev_pool.clear();
+    arena = nullptr;
+    pin = nullptr;
+    ktiles = nullptr;
+    scan.st = ScanState{};
+    P = PoolView{};
+    tl = list = counts = stage = pts = nullptr;
+    acc = nullptr; lstage = nullptr; h_count = nullptr; h_ctl = nullptr; h_acc = nullptr;
+  }
+
+  // places every device buffer of the pool (see Carve)
+  void layout(Carve& c) {
+    const size_t px = (size_t)nt * GC_TILE_PX;
+    int32_t** planes[] = {&P.exc, &P.hgt, &P.cap[0], &P.cap[1], &P.cap[2], &P.cap[3], &tl};
+    for (auto** p : planes) c.take(p, px);
+    c.take(&P.nbr, nt);
+    c.take(&P.mcan, (size_t)nt * 128);
+    c.take(&P.msink, (size_t)nt * 32);
+    c.take(&P.mexc, (size_t)nt * 32);
+    c.take(&P.mreach, (size_t)nt * 32);
+    int32_t** small[] = {&P.touched, &P.act_int, &P.mark[0], &P.mark[1], &P.tact, &P.img_of,
+                         &P.queue[0], &P.queue[1], &P.inq[0], &P.inq[1], &P.mdirty};
+    for (auto** p : small) c.take(p, nt);
+    c.take(&P.qcount, 2);
+    c.take(&P.img_live, imgs.size());
+    c.take(&P.tpos, nt);
+    c.take(&P.rcnt, 2);
+    c.take(&P.ctl, CTL_N);
+    c.take(&acc, imgs.size());
+    c.take(&ktiles, GC_NKERN);
+    // look-back slots: the scan uses one per 4096 items, the list rebuild one per 64 tiles
+    const int chunks = scan_chunks(nt) > nt / 64 + 1 ? scan_chunks(nt) : nt / 64 + 1;
+    c.take(&scan.st.status, chunks);
+    c.take(&scan.st.ticket, 4);
+    scan.st.max_chunks = chunks;
+    c.take(&pts, 2 * 1024);
+    if (imgs.size() == 1) c.take(&lstage, (size_t)imgs[0].W * imgs[0].H);
+  }
+
+  // image descriptors and the arena size (host only, no CUDA calls)
+  int describe(int n, const int* W, const int* H) {
     if (n <= 0 || !W || !H) return fail(GC_ERR_INVALID, "no images");
-    opts = *o;
-    device = opts.device;
-    use_graph = opts.use_graph != 0;
     nt = 0;
+    imgs.clear();
     for (int i = 0; i < n; ++i) {
       if (W[i] <= 0 || H[i] <= 0 || W[i] > (1 << 16) || H[i] > (1 << 16))
         return fail(GC_ERR_INVALID, "image size out of range");
@@ -196,37 +283,50 @@ struct Pool {
       nt += (int)tiles;
       imgs.push_back(d);
     }
-    CK(cudaSetDevice(device));
-    const size_t px = (size_t)nt * GC_TILE_PX;
     P.nt = nt;
-    cudaError_t e = cudaSuccess;
-    int32_t** planes[] = {&P.exc, &P.hgt, &P.cap[0], &P.cap[1], &P.cap[2], &P.cap[3], &tl};
-    for (auto** p : planes) if (!e) e = dalloc(p, px);
-    if (!e) e = dalloc(&P.nbr, nt);
-    if (!e) e = dalloc(&P.mcan, (size_t)nt * 128);
-    if (!e) e = dalloc(&P.msink, (size_t)nt * 32);
-    if (!e) e = dalloc(&P.mexc, (size_t)nt * 32);
-    if (!e) e = dalloc(&P.mreach, (size_t)nt * 32);
-    int32_t** small[] = {&P.touched, &P.act_int, &P.mark[0], &P.mark[1], &P.tact, &P.img_of,
-                         &P.queue[0], &P.queue[1], &P.inq[0], &P.inq[1], &P.mdirty};
-    for (auto** p : small) if (!e) e = dalloc(p, nt);
-    if (!e) e = dalloc(&P.qcount, 2);
-    if (!e) e = dalloc(&P.img_live, imgs.size());
-    if (!e) e = dalloc(&P.tpos, nt);
     P.nimg = (int)imgs.size();
+    Carve sizing;
+    layout(sizing);
+    arena_bytes = sizing.off + 256;   // slack after the last buffer
+    return GC_OK;
+  }
+
+  // ext: caller-owned device memory of ext_bytes (256-byte aligned), or null to allocate
+  int create(int n, const int* W, const int* H, const gc_opts* o, void* ext = nullptr,
+             size_t ext_bytes = 0) {
+    opts = *o;
+    device = opts.device;
+    use_graph = opts.use_graph != 0;
+    RK(describe(n, W, H));
+    if (ext) {
+      if ((reinterpret_cast<uintptr_t>(ext) & 255) != 0) return fail(GC_ERR_INVALID, "arena not 256-byte aligned");
+      if (ext_bytes < arena_bytes) return fail(GC_ERR_INVALID, "arena smaller than gc_arena_bytes");
+    }
+    CK(cudaSetDevice(device));
+    cudaError_t e = cudaSuccess;
+    if (ext) {
+      arena = static_cast<char*>(ext);
+      own_arena = false;
+    } else {
+      e = cudaMalloc((void**)&arena, arena_bytes);
+      if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); arena = nullptr; release(); return fail(GC_ERR_OOM, "device allocation failed"); }
+      if (e) { arena = nullptr; release(); return cuda_fail(e, "pool allocation"); }
+    }
+    e = cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming);
+    if (e) { done_ev = nullptr; release(); return cuda_fail(e, "event"); }
+    Carve place{arena, 0};
+    layout(place);
     list = P.queue[0];
     counts = P.qcount;
-    if (!e) e = dalloc(&P.rcnt, 2);
-    if (!e) e = dalloc(&acc, imgs.size());
-    if (!e) e = dalloc(&ktiles, GC_NKERN);
-    // look-back slots: the scan uses one per 4096 items, the list rebuild one per 64 tiles
-    if (!e) e = scan.alloc(scan_chunks(nt) > nt / 64 + 1 ? scan_chunks(nt) : nt / 64 + 1);
-    if (!e) e = cudaMallocHost((void**)&h_count, 4 * sizeof(int32_t));
-    if (!e) e = cudaMallocHost((void**)&h_ctl, CTL_N * sizeof(int32_t));
-    if (!e) e = dalloc(&P.ctl, CTL_N);
-    if (!e) e = cudaMallocHost((void**)&h_acc, imgs.size() * sizeof(ImageAcc));
-    if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); release(); return fail(GC_ERR_OOM, "device allocation failed"); }
-    if (e) { release(); return cuda_fail(e, "pool allocation"); }
+    scan.st.done = scan.st.ticket + 1;
+    scan.st.err = scan.st.ticket + 2;
+    scan.st.seq = (uint32_t*)(scan.st.ticket + 3);
+    pin_bytes = 32 + 64 + imgs.size() * sizeof(ImageAcc);
+    pin = pinned_take(pin_bytes);
+    if (!pin) { release(); return fail(GC_ERR_OOM, "pinned host allocation failed"); }
+    h_count = static_cast<int32_t*>(pin);
+    h_ctl = reinterpret_cast<int32_t*>(static_cast<char*>(pin) + 32);
+    h_acc = reinterpret_cast<ImageAcc*>(static_cast<char*>(pin) + 96);
     std::vector<int4> nb(nt);
     for (const auto& d : imgs)
       for (int ty = 0; ty < d.th; ++ty)
@@ -235,21 +335,15 @@ struct Pool {
           nb[t] = make_int4(ty > 0 ? t - d.tw : -1, ty < d.th - 1 ? t + d.tw : -1,
                             tx > 0 ? t - 1 : -1, tx < d.tw - 1 ? t + 1 : -1);
         }
+    // every buffer starts at zero; the look-back tag starts at 1
+    CK(cudaMemset(arena, 0, arena_bytes));
     CK(cudaMemcpy(P.nbr, nb.data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
-    CK(cudaMemset(P.touched, 0, sizeof(int32_t) * nt));
-    CK(cudaMemset(P.mark[0], 0, sizeof(int32_t) * nt));
-    CK(cudaMemset(P.mark[1], 0, sizeof(int32_t) * nt));
-    CK(cudaMemset(P.rcnt, 0, sizeof(int32_t) * 2));
-    CK(cudaMemset(P.ctl, 0, sizeof(int32_t) * CTL_N));
-    CK(cudaMemset(P.qcount, 0, sizeof(int32_t) * 2));
-    CK(cudaMemset(P.img_live, 0, sizeof(int32_t) * imgs.size()));
-    CK(cudaMemset(P.mdirty, 0, sizeof(int32_t) * nt));
-    CK(cudaMemset(P.tpos, 0, sizeof(long long) * nt));
-    CK(cudaMemset(P.inq[0], 0, sizeof(int32_t) * nt));
-    CK(cudaMemset(P.inq[1], 0, sizeof(int32_t) * nt));
-    CK(cudaMemset(P.act_int, 0, sizeof(int32_t) * nt));
-    CK(cudaMemset(P.tact, 0, sizeof(int32_t) * nt));
-    CK(cudaMemset(acc, 0, sizeof(ImageAcc) * imgs.size()));
+    const uint32_t one = 1;
+    CK(cudaMemcpy(scan.st.seq, &one, sizeof(one), cudaMemcpyHostToDevice));
+    // These clears were issued on the legacy default stream, which non-blocking streams
+    // (torch's, for one) do not wait for: an upload on such a stream could otherwise run
+    // first and have its masks, tile sums and flow accumulator zeroed afterwards.
+    CK(cudaStreamSynchronize(cudaStreamLegacy));
     grid_dis = occupancy_discharge(device);
     grid_warps = occupancy_warps(device);
     return GC_OK;
@@ -516,6 +610,12 @@ struct Pool {
     if (h_ctl[CTL_ERR] == 1) return fail(GC_ERR_NOT_CONVERGED, "BFS round cap reached");
     if (h_ctl[CTL_ERR] == 2) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
     if (h_ctl[CTL_ERR] == 3) return fail(GC_ERR_INTERNAL, "a bounded wait for a tile copy gave up");
+    if (h_ctl[CTL_ERR] == 4) {
+      char msg[96];
+      snprintf(msg, sizeof(msg), "self-check: worklist value %d out of range (site %d)",
+               h_ctl[CTL_BAD], h_ctl[CTL_BADWHERE]);
+      return fail(GC_ERR_INTERNAL, msg);
+    }
     for (size_t i = 0; i < imgs.size(); ++i)
       if (h_acc[i].bad_caps) return fail(GC_ERR_INVALID, "negative capacity in the upload");
     stats.bfs_rounds = h_ctl[CTL_BFS_TOTAL];
@@ -589,6 +689,13 @@ struct Pool {
     if (i < 0 || i >= (int)imgs.size() || !out) return fail(GC_ERR_INVALID, "bad argument");
     CK(cudaSetDevice(device));
     return timed(K_LABELS, s, [&] { return launch_labels_out(P, imgs[i], out, s); });
+  }
+
+  int labels_packed(int i, uint8_t* out, cudaStream_t s) {
+    if (!solved) return fail(GC_ERR_STATE, "labels before solve");
+    if (i < 0 || i >= (int)imgs.size() || !out) return fail(GC_ERR_INVALID, "bad argument");
+    CK(cudaSetDevice(device));
+    return timed(K_LABELS, s, [&] { return launch_labels_packed(P, imgs[i], out, s); });
   }
 };
 
@@ -667,6 +774,34 @@ int gc_create(int width, int height, const gc_opts* opts, gc_handle** out) {
   return GC_OK;
 }
 
+int gc_arena_bytes(int width, int height, int64_t* bytes) {
+  g_err.clear();
+  if (!bytes) return fail(GC_ERR_INVALID, "null out");
+  Pool p;
+  int w[1] = {width}, hh[1] = {height};
+  RK(p.describe(1, w, hh));
+  *bytes = (int64_t)p.arena_bytes;
+  return GC_OK;
+}
+
+int gc_create_in(int width, int height, const gc_opts* opts, void* arena, int64_t bytes,
+                 gc_handle** out) {
+  g_err.clear();
+  if (!out) return fail(GC_ERR_INVALID, "null out");
+  *out = nullptr;
+  if (!arena || bytes <= 0) return fail(GC_ERR_INVALID, "null arena");
+  gc_opts o;
+  if (opts) o = *opts; else gc_opts_default(&o);
+  RK(check_opts(&o));
+  gc_handle* h = new (std::nothrow) gc_handle();
+  if (!h) return fail(GC_ERR_OOM, "host allocation");
+  int w[1] = {width}, hh[1] = {height};
+  int r = h->pool.create(1, w, hh, &o, arena, (size_t)bytes);
+  if (r) { delete h; return r; }
+  *out = h;
+  return GC_OK;
+}
+
 int gc_destroy(gc_handle* h) {
   if (!h) return GC_OK;
   cudaSetDevice(h->pool.device);
@@ -685,7 +820,9 @@ int gc_upload(gc_handle* h, const int32_t* up, const int32_t* down, const int32_
               const int32_t* right, const int32_t* excess, void* stream) {
   g_err.clear();
   if (!h) return fail(GC_ERR_INVALID, "null handle");
-  return h->pool.upload(0, up, down, left, right, excess, (cudaStream_t)stream);
+  const int r = h->pool.upload(0, up, down, left, right, excess, (cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
 }
 
 int gc_upload_host(gc_handle* h, const int32_t* up, const int32_t* down, const int32_t* left,
@@ -704,6 +841,7 @@ int gc_upload_host(gc_handle* h, const int32_t* up, const int32_t* down, const i
   for (int k = 0; k < 5; ++k)
     CK(cudaMemcpyAsync(p.stage + k * n, src[k], n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   int r = p.upload(0, p.stage, p.stage + n, p.stage + 2 * n, p.stage + 3 * n, p.stage + 4 * n, s);
+  p.track(s);
   if (r) return r;
   CK(cudaStreamSynchronize(s));
   return GC_OK;
@@ -712,7 +850,9 @@ int gc_upload_host(gc_handle* h, const int32_t* up, const int32_t* down, const i
 int gc_solve(gc_handle* h, void* stream) {
   g_err.clear();
   if (!h) return fail(GC_ERR_INVALID, "null handle");
-  return h->pool.solve((cudaStream_t)stream);
+  const int r = h->pool.solve((cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
 }
 
 int gc_flow(gc_handle* h, int64_t* flow) {
@@ -724,7 +864,9 @@ int gc_flow(gc_handle* h, int64_t* flow) {
 int gc_labels(gc_handle* h, uint8_t* labels, void* stream) {
   g_err.clear();
   if (!h) return fail(GC_ERR_INVALID, "null handle");
-  return h->pool.labels(0, labels, (cudaStream_t)stream);
+  const int r = h->pool.labels(0, labels, (cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
 }
 
 int gc_labels_host(gc_handle* h, uint8_t* labels, void* stream) {
@@ -733,13 +875,32 @@ int gc_labels_host(gc_handle* h, uint8_t* labels, void* stream) {
   Pool& p = h->pool;
   CK(cudaSetDevice(p.device));
   const size_t n = (size_t)p.imgs[0].W * p.imgs[0].H;
-  if (!p.lstage) {
-    cudaError_t e = cudaMalloc((void**)&p.lstage, n);
-    if (e) { p.lstage = nullptr; cudaGetLastError(); return fail(GC_ERR_OOM, "label staging"); }
-  }
   cudaStream_t s = (cudaStream_t)stream;
   RK(p.labels(0, p.lstage, s));
   CK(cudaMemcpyAsync(labels, p.lstage, n, cudaMemcpyDeviceToHost, s));
+  p.track(s);
+  CK(cudaStreamSynchronize(s));
+  return GC_OK;
+}
+
+int gc_labels_packed(gc_handle* h, uint8_t* bits, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  const int r = h->pool.labels_packed(0, bits, (cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
+}
+
+int gc_labels_packed_host(gc_handle* h, uint8_t* bits, void* stream) {
+  g_err.clear();
+  if (!h || !bits) return fail(GC_ERR_INVALID, "null argument");
+  Pool& p = h->pool;
+  CK(cudaSetDevice(p.device));
+  const size_t n = (size_t)p.imgs[0].H * ((p.imgs[0].W + 7) / 8);   // fits the label staging
+  cudaStream_t s = (cudaStream_t)stream;
+  RK(p.labels_packed(0, p.lstage, s));
+  CK(cudaMemcpyAsync(bits, p.lstage, n, cudaMemcpyDeviceToHost, s));
+  p.track(s);
   CK(cudaStreamSynchronize(s));
   return GC_OK;
 }
@@ -751,6 +912,7 @@ int gc_edit_tlinks(gc_handle* h, const int32_t* idx, const int32_t* value, int n
   if (!p.uploaded) return fail(GC_ERR_STATE, "edit before upload");
   CK(cudaSetDevice(p.device));
   RK(launch_edit(p.P, p.imgs[0], 0, idx, value, n, p.tl, p.acc, (cudaStream_t)stream));
+  p.track((cudaStream_t)stream);
   p.edited = true;
   p.bfs_fresh = false;
   return GC_OK;
@@ -764,15 +926,12 @@ int gc_edit_stroke(gc_handle* h, const int32_t* xs, const int32_t* ys, int npts,
   Pool& p = h->pool;
   if (!p.uploaded) return fail(GC_ERR_STATE, "edit before upload");
   CK(cudaSetDevice(p.device));
-  if (!p.pts) {
-    cudaError_t e = cudaMalloc((void**)&p.pts, 2 * 1024 * sizeof(int32_t));
-    if (e) { p.pts = nullptr; cudaGetLastError(); return fail(GC_ERR_OOM, "stroke buffer"); }
-  }
   std::vector<int32_t> pts(2 * npts);
   for (int k = 0; k < npts; ++k) { pts[2 * k] = xs[k]; pts[2 * k + 1] = ys[k]; }
   cudaStream_t s = (cudaStream_t)stream;
   CK(cudaMemcpyAsync(p.pts, pts.data(), pts.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   RK(launch_stroke(p.P, p.imgs[0], 0, p.pts, pts.data(), npts, radius, value, p.tl, p.acc, s));
+  p.track(s);
   CK(cudaStreamSynchronize(s));  // pts (host vector) must outlive the copy
   p.edited = true;
   p.bfs_fresh = false;
@@ -790,31 +949,40 @@ int gc_download_state(gc_handle* h, int32_t* excess, int32_t* height, int32_t* u
   int32_t* outs[6] = {excess, height, up, down, left, right};
   for (int k = 0; k < 6; ++k)
     if (outs[k]) RK(launch_state_out(p.P, p.imgs[0], planes[k], outs[k], s));
+  p.track(s);
   return GC_OK;
 }
 
 int gc_push(gc_handle* h, void* stream) {
   g_err.clear();
   if (!h) return fail(GC_ERR_INVALID, "null handle");
-  return h->pool.step_push((cudaStream_t)stream);
+  const int r = h->pool.step_push((cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
 }
 
 int gc_relabel(gc_handle* h, void* stream) {
   g_err.clear();
   if (!h) return fail(GC_ERR_INVALID, "null handle");
-  return h->pool.step_relabel((cudaStream_t)stream);
+  const int r = h->pool.step_relabel((cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
 }
 
 int gc_start_bfs(gc_handle* h, void* stream) {
   g_err.clear();
   if (!h) return fail(GC_ERR_INVALID, "null handle");
-  return h->pool.step_start_bfs((cudaStream_t)stream);
+  const int r = h->pool.step_start_bfs((cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
 }
 
 int gc_is_completed(gc_handle* h, int* completed, void* stream) {
   g_err.clear();
   if (!h || !completed) return fail(GC_ERR_INVALID, "null argument");
-  return h->pool.step_is_completed(completed, (cudaStream_t)stream);
+  const int r = h->pool.step_is_completed(completed, (cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
 }
 
 int gc_get_stats(const gc_handle* h, gc_stats* st) {

@@ -63,13 +63,22 @@ enum CtlSlot {
   CTL_BFS_TOTAL = 4,  // BFS rounds of the solve
   CTL_FLOOD_TOTAL = 5,
   CTL_CYCLES = 6,     // global-relabel cycles of the solve
-  CTL_ERR = 7,        // 1: round cap reached, 2: cycle cap reached
+  CTL_ERR = 7,        // 1: round cap, 2: cycle cap, 3: copy wait gave up, 4: self-check
   CTL_MAXROUNDS = 8,
   CTL_MAXCYCLES = 9,
   CTL_PULSE = 10,     // discharge launches since the last list rebuild (parity = worklist)
   CTL_DDONE = 11,     // CTAs finished in the current discharge launch
+  CTL_BAD = 12,       // first out-of-range worklist value seen by a self-check
+  CTL_BADWHERE = 13,  // 1: worklist append, 2: worklist length, 3: list length, 4: image id
   CTL_N = 16
 };
+
+// A self-check found a worklist value outside the pool: keep the first one, flag the solve
+// (the loops stop at the next check and the host returns GC_ERR_INTERNAL).
+__device__ __forceinline__ void record_bad(const PoolView& P, int where, int value) {
+  if (atomicCAS(&P.ctl[CTL_BADWHERE], 0, where) == 0) P.ctl[CTL_BAD] = value;
+  atomicCAS(&P.ctl[CTL_ERR], 0, 4);
+}
 
 // Kernel kinds for profiling (launch counts, event time, tiles processed).
 enum KernelKind { K_UPLOAD = 0, K_DISCHARGE, K_EDGE_BUILD, K_BFS_FIRST, K_BFS, K_FLOOD_FIRST,

@@ -71,6 +71,7 @@ int launch_mark_images(const PoolView& P, const int32_t* list, const int32_t* co
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s);
 int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s);
+int launch_labels_packed(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s);
 int launch_state_out(const PoolView& P, const ImageDesc& im, const int32_t* plane,
                      int32_t* out, cudaStream_t s);
 int launch_edit(const PoolView& P, const ImageDesc& im, int img, const int32_t* idx,

@@ -111,7 +111,10 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(ScanArgs a, ScanState st)
     long long i = base + k;
     if (i < a.n) {
       if (a.mode == GC_SCAN_MODE_SCAN) a.scan_out[i] = run;
-      else if (v[k]) a.list_out[run] = (int32_t)i;
+      else if (v[k]) {
+        if ((unsigned)run < (unsigned)a.n) a.list_out[run] = (int32_t)i;
+        else atomicExch(st.err, 2);   // only after a look-back that gave up
+      }
     }
     run += v[k];
   }

@@ -24,6 +24,8 @@
 //  * k_flood_round canonical cut: the same tile rounds flood the set reachable from excess
 //                  pixels over residual edges (the minimal source set).
 #include <cstdio>
+#include <mutex>
+#include <unordered_map>
 
 #include "gcut_common.cuh"
 #include "gcut_internal.h"
@@ -171,7 +173,8 @@ struct DisSmem {
 __device__ __forceinline__ void worklist_add(const PoolView& P, int nxt, int t) {
   if (atomicExch(&P.inq[nxt][t], 1) == 0) {
     const int pos = atomicAdd(&P.qcount[nxt], 1);
-    P.queue[nxt][pos] = t;
+    if (pos < P.nt) P.queue[nxt][pos] = t;   // inq deduplicates, so pos < nt always holds
+    else record_bad(P, 1, pos);
   }
 }
 
@@ -203,10 +206,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, unsigned parity) {
                : "=r"(ok) : "r"(a), "r"(parity) : "memory");
   return ok != 0;
 }
-// Bounded wait: false when the copy did not complete within the limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, unsigned parity) {
-  for (int i = 0; i < GC_SPIN_LIMIT; ++i)
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// A tile copy normally lands in microseconds; a wait gives up after this long.  The bound
+// is on time, not on polls: try_wait may return at once, and a poll count then would allow
+// only milliseconds under load (a CTA that gave up early would leave while its copy is
+// still landing in shared memory).
+constexpr unsigned long long GC_COPY_WAIT_NS = 2000000000ull;
+// Bounded wait: false when the copy did not complete within limit_ns.  The iteration cap
+// only guards against a timer that does not advance.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, unsigned parity,
+                                          unsigned long long limit_ns = GC_COPY_WAIT_NS) {
+  if (mbar_try_wait(mbar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned i = 1; i < (1u << 31); ++i) {
     if (mbar_try_wait(mbar, parity)) return true;
+    if ((i & 255u) == 0 && global_ns() - t0 > limit_ns) return false;
+  }
   return false;
 }
 
@@ -245,20 +264,28 @@ k_discharge(PoolView P, int iters) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const int cur = s_cur, nxt = cur ^ 1, n = s_n;
+  const int cur = s_cur, nxt = cur ^ 1;
+  int n = s_n;
+  if (n < 0 || n > P.nt) {   // self-check: a list never holds more than every tile once
+    if (tid == 0 && blockIdx.x == 0) record_bad(P, 2, n);
+    n = 0;
+  }
+  // list entry li: every position below the checked count was written with a tile id of
+  // the pool (by worklist_add or the compaction) before this launch
+  auto entry = [&](int li) { return P.queue[cur][li]; };
   const bool erow = (r == 0) || (r == 31);
   const int pix = r * GC_TILE + c0;
   unsigned phase[2] = {0, 0};
   int it_local = 0;
   bool failed = false;
-  if (tid == 0 && (int)blockIdx.x < n) dis_prefetch(P, P.queue[cur][blockIdx.x], bufs, &mbar[0]);
+  if (tid == 0 && (int)blockIdx.x < n) dis_prefetch(P, entry(blockIdx.x), bufs, &mbar[0]);
   for (int li = blockIdx.x; li < n; li += gridDim.x, ++it_local) {
     const int b = it_local & 1;
     int32_t* const buf = bufs + b * DIS_PLANES * GC_TILE_PX;
-    const int t = P.queue[cur][li];
+    const int t = entry(li);
     // prefetch the next tile of this CTA into the other buffer (read two tiles ago)
     if (tid == 0 && li + (int)gridDim.x < n)
-      dis_prefetch(P, P.queue[cur][li + gridDim.x], bufs + (b ^ 1) * DIS_PLANES * GC_TILE_PX, &mbar[b ^ 1]);
+      dis_prefetch(P, entry(li + gridDim.x), bufs + (b ^ 1) * DIS_PLANES * GC_TILE_PX, &mbar[b ^ 1]);
     const int4 nb = P.nbr[t];
     if (tid < 32) S.hu[tid] = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + tid] : GC_HINF;
     else if (tid < 64) S.hd[tid - 32] = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + (tid - 32)] : GC_HINF;
@@ -479,8 +506,8 @@ k_discharge(PoolView P, int iters) {
     // a bulk copy did not complete in time: record it, let our copies drain, stop
     if (tid == 0) {
       atomicExch(&P.ctl[CTL_ERR], 3);
-      mbar_wait(&mbar[0], phase[0]);
-      mbar_wait(&mbar[1], phase[1]);
+      mbar_wait(&mbar[0], phase[0], 5 * GC_COPY_WAIT_NS);
+      mbar_wait(&mbar[1], phase[1], 5 * GC_COPY_WAIT_NS);
     }
     __syncthreads();
   }
@@ -603,8 +630,12 @@ k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
     const int excl = lookback_exclusive_warp(st, s_tag, chunk, agg);
     int pos = excl + x - v;
     const int tb = chunk * EB_TILES + 2 * lane;
-    if (v0) list[pos++] = tb;
-    if (v1) list[pos] = tb + 1;
+    if ((unsigned)pos + (unsigned)(v0 + v1) <= (unsigned)P.nt) {
+      if (v0) list[pos++] = tb;
+      if (v1) list[pos] = tb + 1;
+    } else if (v) {
+      atomicExch(st.err, 2);   // only after a look-back that gave up
+    }
     if (chunk == nchunks - 1 && lane == 0) *count = excl + agg;
     if (lane == 0) scan_finish(st, nchunks);
   }
@@ -688,7 +719,7 @@ __device__ __forceinline__ void frontier_round_end(const PoolView& P, int first,
   ctl[CTL_ROUNDS] = rounds;
   ctl[total_slot] = ctl[total_slot] + 1;
   ctl[CTL_DONE] = 0;
-  bool more = cnt > 0;
+  bool more = cnt > 0 && ctl[CTL_ERR] < 3;   // a copy or self-check error ends the loop
   if (more && rounds >= ctl[CTL_MAXROUNDS]) {
     ctl[CTL_ERR] = 1;
     more = false;
@@ -713,10 +744,17 @@ __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles) {
 // next cycle's global relabel covers only them (stamp = cycles + 1 + bump, where bump = 1
 // when k_ctl_cycle will count this check as a finished cycle).
 __global__ void k_mark_images(PoolView P, const int32_t* list, const int32_t* count, int bump) {
-  const int n = *((volatile const int32_t*)count);
+  int n = *((volatile const int32_t*)count);
+  if (n < 0 || n > P.nt) {   // self-check: a list holds each tile at most once
+    if (blockIdx.x == 0 && threadIdx.x == 0) record_bad(P, 3, n);
+    n = 0;
+  }
   const int stamp = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1 + bump;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    P.img_live[P.img_of[list[i]]] = stamp;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int img = P.img_of[list[i]];
+    if ((unsigned)img < (unsigned)P.nimg) P.img_live[img] = stamp;
+    else record_bad(P, 4, img);
+  }
 }
 
 // After the active-tile compaction: another cycle runs while tiles are active and the cycle
@@ -730,7 +768,7 @@ __global__ void k_ctl_cycle(PoolView P, const int32_t* count, int count_cycle,
   P.qcount[1] = 0;
   int cycles = ctl[CTL_CYCLES] + (count_cycle ? 1 : 0);
   ctl[CTL_CYCLES] = cycles;
-  bool more = *((volatile const int32_t*)count) > 0;
+  bool more = *((volatile const int32_t*)count) > 0 && ctl[CTL_ERR] < 3;
   if (more && cycles >= ctl[CTL_MAXCYCLES]) {
     ctl[CTL_ERR] = 2;
     more = false;
@@ -756,7 +794,14 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
       if (!markin[t]) continue;
       if (lane == 0) markin[t] = 0;
     } else {
-      if (first == 2 && P.img_live[P.img_of[t]] != live) continue;
+      if (first == 2) {
+        const int img = P.img_of[t];
+        if ((unsigned)img >= (unsigned)P.nimg) {   // self-check
+          if (lane == 0) record_bad(P, 4, img);
+          continue;
+        }
+        if (P.img_live[img] != live) continue;
+      }
       if (lane == 0) {
         P.inq[0][t] = 0;  // the worklists are rebuilt from the relabelled state
         P.inq[1][t] = 0;
@@ -888,7 +933,11 @@ k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc
       // Σ max(excess, 0) of the tile was taken with its masks at the last global relabel,
       // after which the tile did not change
       const long long ps = P.tpos[t];
-      if (lane == 0 && ps) atomicAdd(&acc[P.img_of[t]].sumpos_e, (unsigned long long)ps);
+      const int img = P.img_of[t];
+      if (lane == 0 && ps) {
+        if ((unsigned)img < (unsigned)P.nimg) atomicAdd(&acc[img].sumpos_e, (unsigned long long)ps);
+        else record_bad(P, 4, img);   // self-check
+      }
     } else {
       R = R0 = P.mreach[(long long)t * 32 + lane];
       if (lane == 0 && nb.x >= 0)
@@ -948,6 +997,25 @@ __global__ void k_labels_out(PoolView P, ImageDesc im, uint8_t* __restrict__ out
     }
   } else {
     for (int c = 0; c < GC_TILE && x0 + c < im.W; ++c) row[c] = (uint8_t)((m >> c) & 1u);
+  }
+}
+
+// Bit-packed labels: thread (y, tx) writes the up to four bytes of tile column tx in row y
+// (row stride (W + 7) / 8 bytes, little bit order).  Pixels of a ragged tile beyond the
+// image have no capacities and no excess, so their reach bits are 0.
+__global__ void k_labels_packed(PoolView P, ImageDesc im, uint8_t* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)im.H * im.tw) return;
+  const int y = (int)(i / im.tw), tx = (int)(i % im.tw);
+  const int t = im.tile0 + (y >> 5) * im.tw + tx;
+  const uint32_t m = P.mreach[(long long)t * 32 + (y & 31)];
+  const int stride = (im.W + 7) >> 3;
+  uint8_t* row = out + (long long)y * stride + 4 * tx;
+  const int nb = stride - 4 * tx < 4 ? stride - 4 * tx : 4;
+  if (nb == 4 && (((uintptr_t)row) & 3) == 0) {
+    *reinterpret_cast<uint32_t*>(row) = m;
+  } else {
+    for (int k = 0; k < nb; ++k) row[k] = (uint8_t)(m >> (8 * k));
   }
 }
 
@@ -1083,6 +1151,12 @@ int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cuda
   return ok();
 }
 
+int launch_labels_packed(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s) {
+  const long long segs = (long long)im.H * im.tw;
+  k_labels_packed<<<(unsigned)((segs + 255) / 256), 256, 0, s>>>(P, im, out);
+  return ok();
+}
+
 int launch_state_out(const PoolView& P, const ImageDesc& im, const int32_t* plane,
                      int32_t* out, cudaStream_t s) {
   (void)P;
@@ -1119,19 +1193,31 @@ int launch_stroke(const PoolView& P, const ImageDesc& im, int img, const int32_t
   return ok();
 }
 
-int occupancy_discharge(int device) {
-  int per_sm = 0, sms = 0;
-  cudaFuncSetAttribute(k_discharge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DIS_DYN_SMEM);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_discharge, DIS_THREADS, DIS_DYN_SMEM);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
-}
+namespace {
+// Launch geometry per device, set up once: the dynamic shared memory opt-in of k_discharge
+// changes the function's state, so it is not repeated while other threads launch or
+// instantiate graphs that contain the kernel.
+struct Geometry { int dis = 0, warps = 0; };
+std::mutex g_geom_mu;
+std::unordered_map<int, Geometry> g_geom;
 
-int occupancy_warps(int device) {
-  int per_sm = 0, sms = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bfs_round, WARPS_PER_CTA * 32, 0);
+Geometry device_geometry(int device) {
+  std::lock_guard<std::mutex> lock(g_geom_mu);
+  auto it = g_geom.find(device);
+  if (it != g_geom.end()) return it->second;
+  int per_dis = 0, per_bfs = 0, sms = 0;
+  cudaFuncSetAttribute(k_discharge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DIS_DYN_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_dis, k_discharge, DIS_THREADS, DIS_DYN_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_bfs, k_bfs_round, WARPS_PER_CTA * 32, 0);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  sms = sms > 0 ? sms : 1;
+  Geometry g{(per_dis > 0 ? per_dis : 1) * sms, (per_bfs > 0 ? per_bfs : 1) * sms};
+  g_geom.emplace(device, g);
+  return g;
 }
+}  // namespace
+
+int occupancy_discharge(int device) { return device_geometry(device).dis; }
+int occupancy_warps(int device) { return device_geometry(device).warps; }
 
 }  // namespace gcut

@@ -1,0 +1,455 @@
+"""Serving loop: image sessions and brush-stroke edits arriving over time.
+
+The reference is an interactive tool: one image, strokes from the GUI, ``GraphCut.cut`` run
+on a button press (test_GraphCut.py:78-99).  Here many sessions share one GPU:
+
+* a request is either a NEW image (capacity planes in host memory) or a STROKE on a
+  resident session; every request returns the flow value and the canonical labels of its
+  session after the solve, read back bit-packed (one bit per pixel; ``Result.labels``
+  unpacks them);
+* each session keeps its residual graph, heights and t-links resident on the device
+  (one ``GraphCut`` handle), so a stroke re-solves warm from the previous flow;
+* admission is gated by HBM: the server owns one device region of ``hbm_budget`` bytes
+  (the slab) and places every session's state in a range of it (best fit, freed ranges
+  coalesce; ``GraphCut(arena=...)``).  A new image takes a free range, else the handle
+  of the least-recently-used idle session of its size, else evicts least-recently-used
+  idle sessions until a range fits.  Creating and evicting sessions therefore never calls
+  cudaMalloc / cudaFree, which synchronise the device, on the request path;
+* continuous batching: up to ``slots`` requests are on the GPU at once, each on its own
+  worker thread and stream; a request starts as soon as a slot is free and its session is
+  idle (a stroke waits only for its own session), so solves of different sizes overlap on
+  the device.  The solver calls release the Python GIL;
+* scheduling is earliest-arrival-first over the head new image and the sessions with a
+  queued stroke, with one slot kept for strokes (at most ``slots - 1`` new images in
+  flight), so an edit never waits behind a wall of image uploads.  Strokes of one session
+  run in submission order.  A stroke for a session that was evicted is a miss.
+
+Host planes in pinned memory are copied to the device asynchronously (into per-worker
+staging); pageable planes work too, with synchronous copies.
+
+Results do not depend on the mix: the flow value and the canonical cut of a session are
+unique for its graph, which the tests check request by request.
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import heapq
+import itertools
+import threading
+import time
+
+import numpy as np
+
+import _gcut
+from GraphCut import GraphCut, unpack_labels
+
+ALIGN = 256   # arena alignment the solver requires
+
+
+def session_bytes(width: int, height: int) -> int:
+    """Device bytes of one resident session of this size: its solver arena (tile planes,
+    masks, flags, label staging), rounded to the slab's alignment."""
+    n = GraphCut.arena_bytes(width, height)
+    return -(-n // ALIGN) * ALIGN
+
+
+class Slab:
+    """Best-fit range allocator over [0, size): offsets and lengths in ALIGN units; a
+    released range merges with free neighbours.  Host bookkeeping only."""
+
+    def __init__(self, size: int):
+        self.size = size - size % ALIGN
+        self.free = {0: self.size} if self.size else {}   # offset -> length
+        self.used = 0
+
+    def alloc(self, n: int):
+        """Offset of a free range of n bytes (rounded up), or None."""
+        n = -(-n // ALIGN) * ALIGN
+        best = None
+        for off, ln in self.free.items():
+            if ln >= n and (best is None or ln < self.free[best]):
+                best = off
+        if best is None:
+            return None
+        ln = self.free.pop(best)
+        if ln > n:
+            self.free[best + n] = ln - n
+        self.used += n
+        return best
+
+    def release(self, off: int, n: int):
+        n = -(-n // ALIGN) * ALIGN
+        self.used -= n
+        end = off + n
+        if end in self.free:
+            n += self.free.pop(end)
+        prev = next((o for o, ln in self.free.items() if o + ln == off), None)
+        if prev is not None:
+            self.free[prev] += n
+        else:
+            self.free[off] = n
+
+
+@dataclasses.dataclass
+class NewImage:
+    session: int
+    planes: tuple            # (up, down, left, right, excess) host int32 [H, W]
+
+
+@dataclasses.dataclass
+class Stroke:
+    session: int
+    xs: np.ndarray
+    ys: np.ndarray
+    radius: int
+    value: int
+
+
+@dataclasses.dataclass
+class Result:
+    session: int
+    kind: str
+    flow: int
+    bits: np.ndarray         # canonical labels, bit-packed rows (GraphCut.labels_packed)
+    width: int
+    arrival: float
+    start: float
+    done: float
+    pixels: int
+    phases_ms: tuple = ()    # (input, solve, labels) host-side durations
+
+    @property
+    def labels(self) -> np.ndarray:
+        """uint8 [H, W] canonical labels (1 = source side), unpacked on access."""
+        return unpack_labels(self.bits, self.width)
+
+    @property
+    def latency_ms(self) -> float:
+        return 1000.0 * (self.done - self.arrival)
+
+
+class _Session:
+    def __init__(self, sid, gc, width, height, off, nbytes):
+        self.sid, self.gc, self.width, self.height = sid, gc, width, height
+        self.off, self.nbytes = off, nbytes      # its range of the slab
+        self.busy = False
+        self.last_use = time.perf_counter()
+
+
+class GraphCutServer:
+    """Serves NewImage / Stroke requests on one GPU (see the module docstring)."""
+
+    def __init__(self, slots: int = 4, hbm_budget: int = 16 << 30, device: int = 0,
+                 solver_kw=None, max_pixels: int = 4096 * 4096):
+        import torch
+        self.torch = torch
+        self.device = device
+        self.slots = slots
+        self.budget = hbm_budget
+        self.solver_kw = dict(solver_kw or {})
+        self.max_pixels = max_pixels   # staging of each worker is sized for this at start
+        self.lock = threading.Condition()
+        self.images = collections.deque()              # (NewImage, arrival) in arrival order
+        self.strokes = collections.defaultdict(collections.deque)  # session -> (Stroke, arrival)
+        self.ready = []          # heap of (head stroke arrival, seq, session): idle + queued
+        self._seq = itertools.count()
+        self.sessions: dict[int, _Session] = {}
+        self.lru = collections.OrderedDict()           # idle resident sessions, oldest first
+        self.slab = Slab(hbm_budget)
+        self._slab_mem, self._base = self._device_slab(self.slab.size)
+        self.queued_images = set()    # sessions whose NewImage is queued or being solved
+        self.results: list[Result] = []
+        self.misses = 0
+        self.evictions = 0
+        self.errors = []
+        self.stop = False
+        self.inflight = 0
+        self.images_inflight = 0
+        self._ready = 0
+        self.workers = [threading.Thread(target=self._worker, args=(k,), daemon=True)
+                        for k in range(slots)]
+        for w in self.workers:
+            w.start()
+        # start-up (streams, staging) is not request latency: wait until every worker is set
+        with self.lock:
+            while self._ready < slots:
+                self.lock.wait(0.05)
+        if self.errors:
+            raise self.errors[0]
+
+    # ---- client side ------------------------------------------------------------
+    def submit(self, request, arrival=None):
+        arrival = time.perf_counter() if arrival is None else arrival
+        with self.lock:
+            sid = request.session
+            if isinstance(request, Stroke):
+                s = self.sessions.get(sid)
+                if s is None and sid not in self.queued_images:
+                    self.misses += 1      # the session was evicted (or never existed)
+                    return
+                q = self.strokes[sid]
+                q.append((request, arrival))
+                if s is not None and not s.busy and len(q) == 1:
+                    self._make_ready(s)
+            else:
+                self.queued_images.add(sid)
+                self.images.append((request, arrival))
+            self.lock.notify()
+
+    def drain(self, timeout=600.0):
+        t0 = time.perf_counter()
+        with self.lock:
+            while (self.images or self.ready or self.inflight) and time.perf_counter() - t0 < timeout:
+                self.lock.wait(0.05)
+        if self.errors:
+            raise self.errors[0]
+
+    def close(self):
+        with self.lock:
+            self.stop = True
+            self.lock.notify_all()
+        for w in self.workers:
+            w.join()
+        for s in list(self.sessions.values()):
+            self._destroy(s.gc)
+            self.slab.release(s.off, s.nbytes)
+        self.sessions.clear()
+        self.lru.clear()
+        self._slab_mem = None
+
+    @property
+    def used(self) -> int:
+        """Bytes of the slab held by resident and in-flight sessions."""
+        return self.slab.used
+
+    # ---- scheduling (all under self.lock) ------------------------------------------
+    def _make_ready(self, s):
+        """s is resident, idle and has a queued stroke: it may be picked."""
+        self.lru.pop(s.sid, None)
+        heapq.heappush(self.ready, (self.strokes[s.sid][0][1], next(self._seq), s.sid))
+
+    def _release(self, s):
+        """s finished a request: it is ready again, or idle (evictable)."""
+        s.busy = False
+        s.last_use = time.perf_counter()
+        if self.strokes.get(s.sid):
+            self._make_ready(s)
+        else:
+            self.strokes.pop(s.sid, None)
+            self.lru[s.sid] = s
+
+    def _pick(self):
+        """Next request that can start now, or None."""
+        stroke_arr = self.ready[0][0] if self.ready else float("inf")
+        image_ok = self.images and self.images_inflight < max(1, self.slots - 1)
+        if image_ok and self.images[0][1] <= stroke_arr:
+            job = self._pick_image()
+            if job is not None:
+                return job
+        if self.ready:
+            _, _, sid = heapq.heappop(self.ready)
+            s = self.sessions[sid]
+            req, arr = self.strokes[sid].popleft()
+            s.busy = True
+            return req, arr, s
+        return self._pick_image() if image_ok else None
+
+    def _pick_image(self):
+        if not self.images:
+            return None
+        req, arr = self.images[0]
+        h, w = req.planes[4].shape
+        if session_bytes(w, h) > self.slab.size:   # can never fit: refuse it
+            self.images.popleft()
+            self.queued_images.discard(req.session)
+            self.strokes.pop(req.session, None)
+            self.errors.append(MemoryError(f"session {req.session}: {w}x{h} needs more than "
+                                           f"the HBM budget of {self.slab.size} bytes"))
+            return None
+        place = self._admit(w, h)
+        if place is None:
+            return None
+        self.images.popleft()
+        self.images_inflight += 1
+        return req, arr, place
+
+    def _evict(self, s):
+        del self.sessions[s.sid]
+        self.lru.pop(s.sid, None)
+        self.evictions += 1
+
+    def _admit(self, w, h):
+        """Room for a (w, h) session: (handle to reuse or None, offset, bytes), or None when
+        nothing fits until a session goes idle."""
+        need = session_bytes(w, h)
+        off = self.slab.alloc(need)
+        if off is not None:
+            return None, off, need
+        # full: the least-recently-used idle session of this size hands over its handle
+        for s in self.lru.values():
+            if (s.width, s.height) == (w, h):
+                self._evict(s)
+                return s.gc, s.off, s.nbytes
+        # else evict least-recently-used idle sessions until a range fits
+        while self.lru:
+            victim = next(iter(self.lru.values()))
+            self._evict(victim)
+            self._destroy(victim.gc)
+            self.slab.release(victim.off, victim.nbytes)
+            off = self.slab.alloc(need)
+            if off is not None:
+                return None, off, need
+        return None
+
+    # ---- workers ----------------------------------------------------------------------
+    def _context(self):
+        """Per-worker device context (a stream and staging buffers); called on the worker."""
+        return _DeviceContext(self.torch, self.device, self.max_pixels)
+
+    def _device_slab(self, nbytes):
+        """(owner, device address) of the slab's memory: one allocation for the server's
+        lifetime."""
+        t = self.torch.empty(max(nbytes, 1), dtype=self.torch.uint8,
+                             device=self.torch.device("cuda", self.device))
+        assert t.data_ptr() % ALIGN == 0
+        return t, t.data_ptr()
+
+    def _new_handle(self, w, h, off, nbytes):
+        return GraphCut(w, h, device=self.device, arena=(self._base + off, nbytes),
+                        **self.solver_kw)
+
+    def _destroy(self, gc):
+        gc.close()   # idle: returns at once; the range may be reused afterwards
+
+    def _worker(self, k):
+        try:
+            ctx = self._context()
+        except Exception as exc:   # surfaced by the constructor
+            with self.lock:
+                self.errors.append(exc)
+                self._ready += 1
+                self.lock.notify_all()
+            return
+        with self.lock:
+            self._ready += 1
+            self.lock.notify_all()
+        while True:
+            with self.lock:
+                job = None
+                while not self.stop:
+                    job = self._pick()
+                    if job is not None:
+                        break
+                    self.lock.wait(0.05)
+                if job is None:
+                    return
+                req, arrival, sess = job
+                self.inflight += 1
+                gc = None
+                if isinstance(req, NewImage):
+                    (gc, off, nbytes), sess = sess, None
+            try:
+                start = time.perf_counter()
+                if sess is None:
+                    h, w = req.planes[4].shape
+                    if gc is None:
+                        gc = self._new_handle(w, h, off, nbytes)
+                    flow, bits, phases = ctx.run_image(gc, req.planes, w, h)
+                    res = Result(req.session, "image", flow, bits, w, arrival, start,
+                                 time.perf_counter(), w * h, phases)
+                else:
+                    flow, bits, phases = ctx.run_stroke(sess.gc, req, sess.width, sess.height)
+                    res = Result(req.session, "stroke", flow, bits, sess.width, arrival, start,
+                                 time.perf_counter(), sess.width * sess.height, phases)
+                with self.lock:
+                    self.results.append(res)
+                    if sess is None:
+                        sess = _Session(req.session, gc, w, h, off, nbytes)
+                        self.sessions[req.session] = sess
+                        self.queued_images.discard(req.session)
+                        self.images_inflight -= 1
+                    self._release(sess)
+            except Exception as exc:  # surfaced by drain()
+                with self.lock:
+                    self.errors.append(exc)
+                    if sess is not None:
+                        self._release(sess)
+                    else:   # the session never opened: its handle and range are released
+                        self.queued_images.discard(req.session)
+                        self.images_inflight -= 1
+                        self.strokes.pop(req.session, None)
+                        if gc is not None:
+                            self._destroy(gc)
+                        self.slab.release(off, nbytes)
+            finally:
+                with self.lock:
+                    self.inflight -= 1
+                    self.lock.notify_all()
+
+
+class _DeviceContext:
+    """One worker's stream, device staging for the input planes and pinned staging for the
+    packed labels, reused across requests in stream order.  Both are sized for `max_pixels`
+    when the worker starts (allocation on the request path would stall the device) and grow
+    only for a larger image."""
+
+    def __init__(self, torch, device, max_pixels):
+        self.torch = torch
+        torch.cuda.set_device(device)
+        self.device = device
+        self.stream = torch.cuda.Stream()
+        self.dstage = torch.empty(5 * max_pixels, dtype=torch.int32, device=device)
+        self.lstage = torch.empty(max_pixels // 8 + 65536, dtype=torch.uint8, pin_memory=True)
+
+    def _upload(self, gc, planes, w, h):
+        torch, n = self.torch, w * h
+        if self.dstage.numel() < 5 * n:
+            self.dstage = torch.empty(5 * n, dtype=torch.int32, device=self.device)
+        dev = []
+        for j, p in enumerate(planes):
+            d = self.dstage[j * n:(j + 1) * n].view(h, w)
+            d.copy_(torch.from_numpy(np.ascontiguousarray(p, dtype=np.int32)), non_blocking=True)
+            dev.append(d)
+        gc.upload_capacities(*dev, stream=self.stream)
+
+    def _labels(self, gc, w, h):
+        n = h * ((w + 7) // 8)
+        if self.lstage.numel() < n:
+            self.lstage = self.torch.empty(n, dtype=self.torch.uint8, pin_memory=True)
+        buf = self.lstage[:n].numpy().reshape(h, (w + 7) // 8)
+        gc.labels_packed_host(out=buf, stream=self.stream)
+        return buf.copy()
+
+    def run_image(self, gc, planes, w, h):
+        t0 = time.perf_counter()
+        with self.torch.cuda.stream(self.stream):
+            self._upload(gc, planes, w, h)
+            t1 = time.perf_counter()
+            gc.cut(stream=self.stream)
+            t2 = time.perf_counter()
+            labels = self._labels(gc, w, h)
+        t3 = time.perf_counter()
+        return gc.flow, labels, (1e3 * (t1 - t0), 1e3 * (t2 - t1), 1e3 * (t3 - t2))
+
+    def run_stroke(self, gc, req, w, h):
+        t0 = time.perf_counter()
+        with self.torch.cuda.stream(self.stream):
+            gc.edit_stroke(req.xs, req.ys, req.radius, req.value, stream=self.stream)
+            t1 = time.perf_counter()
+            gc.cut(stream=self.stream)
+            t2 = time.perf_counter()
+            labels = self._labels(gc, w, h)
+        t3 = time.perf_counter()
+        return gc.flow, labels, (1e3 * (t1 - t0), 1e3 * (t2 - t1), 1e3 * (t3 - t2))
+
+
+def poisson_trace(rng, rate_hz, duration_s, n_images, p_new=0.3):
+    """(time, kind, image index) tuples of a Poisson stream: a new image with probability
+    p_new, else a stroke on a resident session."""
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate_hz)
+        if t >= duration_s:
+            return out
+        out.append((t, "image" if rng.random() < p_new else "stroke", int(rng.integers(n_images))))

@@ -82,6 +82,20 @@ int gc_opts_default(gc_opts* opts);
    Replaces GraphCut.__init__ (GraphCut.pyx:80-154). */
 int gc_create(int width, int height, const gc_opts* opts, gc_handle** out);
 int gc_destroy(gc_handle* h);
+
+/* Bytes of device memory a width x height handle keeps (its arena: tile planes, masks,
+   flags, label staging).  Host-only computation, no device needed. */
+int gc_arena_bytes(int width, int height, int64_t* bytes);
+/* gc_create inside caller-owned device memory: `arena` (256-byte aligned, at least
+   gc_arena_bytes bytes, on opts->device) holds every device buffer of the handle, so
+   creating and destroying handles allocates and frees no device memory (gc_upload_host
+   alone allocates its staging on first use).  A server that sub-allocates one HBM region
+   between sessions uses this to keep cudaMalloc / cudaFree, which synchronise the device,
+   off its request path.  gc_destroy waits for the work of the handle's last call (on that
+   call's stream), after which the caller may reuse the memory.  No counterpart in the
+   reference (GraphCut.__init__ allocates its buffers, GraphCut.pyx:117-154). */
+int gc_create_in(int width, int height, const gc_opts* opts, void* arena, int64_t bytes,
+                 gc_handle** out);
 int gc_size(const gc_handle* h, int* width, int* height);
 
 /* Capacity upload from DEVICE buffers (row-major, see above).  Replaces init_gc +
@@ -119,6 +133,14 @@ int gc_flow(gc_handle* h, int64_t* flow);
 int gc_labels(gc_handle* h, uint8_t* labels, void* stream);
 /* Same into a HOST buffer (synchronous). */
 int gc_labels_host(gc_handle* h, uint8_t* labels, void* stream);
+/* Canonical labels bit-packed, one row of (width + 7) / 8 bytes per image row, pixel x in
+   bit x % 8 of byte x / 8 (numpy.packbits(labels, axis=1, bitorder="little")); unused
+   bits of a row's last byte are 0.  The serving loop returns these: 8x fewer bytes to
+   read back than gc_labels.  No counterpart in the reference (its cut stays on the
+   device as a float mask).  DEVICE buffer of height * ((width + 7) / 8) bytes. */
+int gc_labels_packed(gc_handle* h, uint8_t* bits, void* stream);
+/* Same into a HOST buffer (synchronous). */
+int gc_labels_packed_host(gc_handle* h, uint8_t* bits, void* stream);
 
 /* Sets the signed t-link of n pixels (flat indices y*width+x, DEVICE arrays) to value[i];
    the excess changes by value - previous t-link, which warm-starts the next gc_solve from

@@ -18,8 +18,12 @@
 //                        kernel below cites the reference lines it follows.  It is the CPU
 //                        baseline (OpenMP over tiles) and a second independent solver.
 //
-// Parity of the graph cut against the reference kernels themselves is pinned separately by
-// the emulation harness in oracle/clref (the reference's graphcut.cl compiled for the CPU).
+// Parity status: the flow value of a graph is unique, and so is its canonical cut (the
+// minimal source set), so orc_maxflow_bk pins both for any correct solver.  The reference's
+// own kernels were not run here (they need an OpenCL runtime; the image has none), and its
+// graph-cut test asserts no outputs, so parity with the reference's kernels themselves is
+// unpinned; the primitives (scan, compaction, tile lists) are pinned against the
+// reference's own test vectors.
 //
 // Plane layout: row-major int32 [H][W]; up/down/left/right hold the residual capacity of
 // the edge from the pixel to that neighbour; excess is the signed t-link (positive:

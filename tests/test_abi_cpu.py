@@ -10,7 +10,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def header_functions():
-    src = open(os.path.join(ROOT, "include", "gcut.h")).read()
+    with open(os.path.join(ROOT, "include", "gcut.h")) as f:
+        src = f.read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(gcb?_[a-z_]+)\s*\(", src)))
 
@@ -56,3 +57,19 @@ def test_calls_without_gpu_fail_cleanly(libgcut):
     assert L.gc_solve(None, None) == _gcut.GC_ERR_INVALID
     o = _gcut.GcOpts()
     assert L.gc_opts_default(ctypes.byref(o)) == 0 and o.discharge_iters > 0
+
+
+def test_arena_bytes_host_only():
+    """gc_arena_bytes needs no device: it sizes the arena of a handle from its grid."""
+    import _gcut
+    lib = _gcut.lib()
+    out = ctypes.c_int64()
+    sizes = {}
+    for w, h in [(1, 1), (32, 32), (33, 32), (512, 512), (4096, 4096)]:
+        assert lib.gc_arena_bytes(w, h, ctypes.byref(out)) == 0
+        sizes[(w, h)] = out.value
+    assert 0 < sizes[(1, 1)] <= sizes[(32, 32)]            # one tile; label staging W*H
+    assert sizes[(33, 32)] > sizes[(32, 32)]
+    assert sizes[(4096, 4096)] > 28 * 4096 * 4096            # 7 int32 planes at least
+    assert sizes[(4096, 4096)] < 32 * 4096 * 4096
+    assert lib.gc_arena_bytes(0, 5, ctypes.byref(out)) == 1   # GC_ERR_INVALID

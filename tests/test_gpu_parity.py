@@ -52,6 +52,49 @@ def test_random_graphs(cuda, oracle, seed, sym, sparsity, graph):
     check(g, oracle, use_graph=graph)
 
 
+@pytest.mark.parametrize("w,h", [(1, 1), (7, 3), (33, 31), (100, 37), (257, 130), (1000, 3),
+                                 (64, 64)])
+def test_packed_labels_match_oracle(cuda, oracle, w, h):
+    """Bit-packed labels (device and host forms) unpack to the oracle's canonical cut, and
+    the padding bits of each row's last byte are 0."""
+    from GraphCut import unpack_labels
+    g = synth.random_graph(w, h, 7 * w + h, cap_max=30, tlink_max=60)
+    _, l_ref = oracle.maxflow_bk(*g.planes())
+    with GraphCut(w, h) as gc:
+        gc.upload_capacities(*g.planes())
+        gc.cut()
+        dev = gc.labels_packed().cpu().numpy()
+        host = gc.labels_packed_host()
+    assert host.shape == (h, (w + 7) // 8)
+    assert np.array_equal(dev, host)
+    assert np.array_equal(host, np.packbits(l_ref, axis=1, bitorder="little"))
+    assert np.array_equal(unpack_labels(host, w), l_ref)
+
+
+def test_handles_in_caller_memory(cuda, oracle):
+    """gc_create_in: handles placed in one caller-owned buffer solve like gc_create, and
+    the memory is reused for a handle of another size after gc_destroy."""
+    import torch
+    from _gcut import GCError
+    sizes = [(300, 211), (64, 500), (513, 97)]
+    need = max(GraphCut.arena_bytes(w, h) for w, h in sizes)
+    buf = torch.empty(need + 4096, dtype=torch.uint8, device="cuda")
+    base = buf.data_ptr()
+    for k, (w, h) in enumerate(sizes):
+        g = synth.random_graph(w, h, 40 + k, cap_max=40, tlink_max=80)
+        f_ref, l_ref = oracle.maxflow_bk(*g.planes())
+        buf.fill_(0xAB)   # garbage left by an earlier tenant must not matter
+        with GraphCut(w, h, arena=(base, GraphCut.arena_bytes(w, h))) as gc:
+            gc.upload_capacities(*g.planes())
+            gc.cut()
+            assert gc.flow == f_ref
+            assert np.array_equal(gc.labels_host(), l_ref)
+    with pytest.raises(GCError):   # too small
+        GraphCut(300, 211, arena=(base, GraphCut.arena_bytes(300, 211) - 256))
+    with pytest.raises(GCError):   # not 256-byte aligned
+        GraphCut(64, 64, arena=(base + 16, need))
+
+
 @pytest.mark.parametrize("iters,pulses,init", [(1, 1, 0), (4, 1, 1), (64, 5, 0), (32, 1, 1)])
 def test_schedules_agree(cuda, oracle, iters, pulses, init):
     g = synth.random_graph(160, 128, 11, cap_max=80, tlink_max=120, symmetric=False)

@@ -1,0 +1,84 @@
+"""Serving loop: results are the same alone and in the mix (bit-exact), with several
+solves in flight on separate streams and HBM admission evicting idle sessions."""
+import numpy as np
+import pytest
+
+import strokes
+import synth
+from GraphCut import GraphCut
+from serving import GraphCutServer, NewImage, Stroke, session_bytes
+
+pytestmark = pytest.mark.gpu
+
+
+def _alone(g, strks):
+    t = g.excess.copy()
+    for s in strks:
+        t = strokes.apply(t, s)
+    with GraphCut(g.width, g.height) as gc:
+        gc.upload_capacities(g.up, g.down, g.left, g.right, t)
+        gc.cut()
+        return gc.flow, gc.labels_host()
+
+
+@pytest.mark.parametrize("slots,budget_images", [(3, 100), (3, 2), (1, 100), (6, 3)])
+def test_results_same_alone_and_in_mix(cuda, slots, budget_images):
+    rng = np.random.default_rng(slots * 10 + budget_images)
+    shapes = [(int(rng.integers(64, 400)), int(rng.integers(64, 400))) for _ in range(4)]
+    graphs = [synth.make_graph(w, h, 300 + i) for i, (w, h) in enumerate(shapes)]
+    budget = budget_images * max(session_bytes(w, h) for w, h in shapes)
+    srv = GraphCutServer(slots=slots, hbm_budget=budget)
+    history = {}
+    sid = 0
+    for step in range(40):
+        if step % 4 == 0 or not history:
+            img = step // 4 % len(graphs)
+            history[sid] = (img, [])
+            srv.submit(NewImage(sid, graphs[img].planes()))
+            sid += 1
+        else:
+            target = max(history) - int(rng.integers(0, min(2, len(history))))
+            g = graphs[history[target][0]]
+            s = strokes.random_stroke(rng, g.width, g.height, rmin=4, rmax=12)
+            history[target][1].append(s)
+            srv.submit(Stroke(target, s.xs, s.ys, s.radius, s.value))
+    srv.drain()
+    results = sorted(srv.results, key=lambda r: r.arrival)
+    srv.close()
+    assert results
+    if budget_images <= 3:
+        assert srv.evictions > 0
+    seen = {}
+    for r in results:
+        k = seen.get(r.session, 0)
+        seen[r.session] = k + 1
+        img, strks = history[r.session]
+        f, lab = _alone(graphs[img], strks[:k])
+        assert r.flow == f, (r.session, k)
+        assert np.array_equal(r.labels, lab), (r.session, k)
+    # every request either has a result or was a stroke on an evicted session
+    assert len(results) + srv.misses == 40
+
+
+def test_fresh_handles_on_nonblocking_streams(cuda):
+    """A handle created while other streams are busy and used at once on a non-blocking
+    stream sees its initial state (create's clears finish before it returns)."""
+    import torch
+    g = synth.make_graph(700, 500, 77)
+    with GraphCut(g.width, g.height) as gc:
+        gc.upload_capacities(*g.planes())
+        gc.cut()
+        want = gc.flow, gc.labels_host()
+    busy = torch.cuda.Stream()
+    x = torch.zeros(1 << 26, device="cuda")
+    for _ in range(8):
+        with torch.cuda.stream(busy):      # keep the device busy on another stream
+            for _ in range(20):
+                x.add_(1.0)
+        s = torch.cuda.Stream()
+        with GraphCut(g.width, g.height) as gc, torch.cuda.stream(s):
+            gc.upload_capacities(*g.planes(), stream=s)
+            gc.cut(stream=s)
+            assert (gc.flow, ) == (want[0], )
+            assert np.array_equal(gc.labels_host(stream=s), want[1])
+    torch.cuda.synchronize()
