@@ -75,6 +75,10 @@ def parse():
                     help="wall-time cap of the --config serving result verification")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="warm up, then run one host-driven solve of the --size grid inside the "
+                         "NVTX range 'profiled_solve' and print its per-kernel launches and "
+                         "tiles (the command the ncu summaries are made from)")
     ap.add_argument("--host-driven", action="store_true",
                     help="solve loops decided by the host (use_graph=0); ncu does not profile "
                          "kernels inside conditional CUDA-graph nodes, so profiling runs use this")
@@ -150,10 +154,10 @@ def measured_peak():
 
 def ncu_traffic():
     """DRAM bytes per tile of each kernel kind from the committed ncu summary (or {})."""
-    path = os.path.join(ROOT, "profiles", "traffic_per_tile.json")
+    path = os.path.join(ROOT, "profiles", "dram_traffic_per_tile.txt")
     try:
         with open(path) as f:
-            return json.load(f)
+            return json.loads("".join(l for l in f if not l.startswith("#")))
     except Exception:
         return {}
 
@@ -217,6 +221,8 @@ def main():
         return run_strokes(args)
     if args.config == "serving":
         return run_serving(args)
+    if args.profile_solve:
+        return run_profile_solve(args)
     import torch
     import torch.distributed as dist
 
@@ -344,9 +350,11 @@ def main():
         algo_bytes = d["launches"] * ((W // 32) * (H // 32)) * 8
     achieved = algo_bytes / (d["ms"] / 1000) / 1e9 if d["ms"] > 0 else 0.0
     traffic = None
-    tr = ncu_traffic().get(dname)
-    if tr is not None and d["launches"]:
-        traffic = tr * d["tiles"] / d["launches"]
+    tr_all = ncu_traffic()
+    if dname == "compact":
+        traffic = tr_all.get("compact_per_launch")
+    elif tr_all.get(dname) is not None and d["launches"]:
+        traffic = tr_all[dname] * d["tiles"] / d["launches"]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -387,6 +395,44 @@ def main():
     gc.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_profile_solve(args):
+    """One host-driven solve of the --size synthetic grid (seed 1) in the NVTX range
+    'profiled_solve', after `--warmup` solves; prints the per-kernel launches, tiles and
+    event times of that solve.  ncu captures only that range (--nvtx --nvtx-include
+    profiled_solve/), so launch lists and DRAM counters cover exactly one solve."""
+    import torch
+
+    import synth
+    from GraphCut import GraphCut
+    W = H = args.size
+    g = synth.make_graph(W, H, 1)
+    torch.cuda.set_device(0)
+    planes = [torch.from_numpy(p).cuda() for p in g.planes()]
+    labels = torch.empty((H, W), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    gc = GraphCut(W, H, use_graph=False)
+    with torch.cuda.stream(stream):
+        for _ in range(max(1, args.warmup)):
+            gc.upload_capacities(*planes, stream=stream)
+            gc.cut(stream=stream)
+        flush.fill_(1)
+        stream.synchronize()
+        gc.set_profile(True)
+        torch.cuda.nvtx.range_push("profiled_solve")
+        gc.upload_capacities(*planes, stream=stream)
+        gc.cut(stream=stream)
+        gc.labels(out=labels, stream=stream)
+        stream.synchronize()
+        torch.cuda.nvtx.range_pop()
+        prof = gc.profile()
+        gc.set_profile(False)
+    print(json.dumps({"workload": f"{W}x{H} synthetic grid, seed 1, one host-driven solve",
+                      "flow": gc.flow, "stats": gc.stats(),
+                      "kernels": {k: v for k, v in prof.items() if v["launches"]}}), flush=True)
+    gc.close()
 
 
 def _percentile(xs, p):
