@@ -70,7 +70,9 @@ def parse():
     ap.add_argument("--size", type=int, default=2048)
     ap.add_argument("--duration", type=float, default=60.0, help="seconds of --config serving trace")
     ap.add_argument("--rate", type=float, default=200.0, help="requests/s of --config serving")
-    ap.add_argument("--slots", type=int, default=4, help="requests in flight, --config serving")
+    ap.add_argument("--slots", type=int, default=1,
+                    help="requests in flight, --config serving (more than 1 raised an "
+                         "intermittent device fault whose cause is not yet found)")
     ap.add_argument("--verify-s", type=float, default=90.0,
                     help="wall-time cap of the --config serving result verification")
     ap.add_argument("--no-cpu-baseline", action="store_true")
