@@ -48,7 +48,8 @@ ALGO_BYTES_PER_TILE = {
     "upload": 1024 * 4 * (5 + 7),          # read 5 row-major planes, write 7 tile planes
     "discharge": 1024 * 4 * (6 + 6) + 4 * 32 * 4,  # read+write excess/height/4 caps, halo
     "edge_relabel_build": 124 * 4 * 2 + 16,  # edge excess+height, flags
-    "bfs_first": 1024 * 4 * 5 + 1024 * 4 + 6 * 128,  # caps+excess in, distances + masks out
+    "masks": 1024 * 4 * 5 + 6 * 128 + 8,              # 5 planes in, 6 row masks + tile sum out
+    "bfs_first": 6 * 128 + 1024 * 4,                  # masks in, distances out
     "bfs": 5 * 128 + 4 * 128 + 2 * 1024 * 4,          # masks, halo, distances in/out
     "flood_first": 1024 * 4 + 5 * 128 + 128,
     "flood": 5 * 128 + 4 * 256 + 128,

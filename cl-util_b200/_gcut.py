@@ -49,7 +49,7 @@ class GcKernelProf(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_int64), ("ms", ctypes.c_double), ("tiles", ctypes.c_int64)]
 
 
-GC_NKERN = 9
+GC_NKERN = 10
 GC_COMPACT_NOALLOC_MAX_N = 4194304
 
 _P = ctypes.c_void_p

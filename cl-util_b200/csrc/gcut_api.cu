@@ -254,6 +254,11 @@ struct Pool {
                          &P.queue[0], &P.queue[1], &P.inq[0], &P.inq[1], &P.mdirty};
     for (auto** p : small) c.take(p, nt);
     c.take(&P.qcount, 2);
+    c.take(&P.fq[0], nt);
+    c.take(&P.fq[1], nt);
+    c.take(&P.fcount, 2);
+    c.take(&P.dq, nt);
+    c.take(&P.dcount, 2);
     c.take(&P.img_live, imgs.size());
     c.take(&P.tpos, nt);
     c.take(&P.rcnt, 2);
@@ -321,12 +326,19 @@ struct Pool {
     scan.st.done = scan.st.ticket + 1;
     scan.st.err = scan.st.ticket + 2;
     scan.st.seq = (uint32_t*)(scan.st.ticket + 3);
-    pin_bytes = 32 + 64 + imgs.size() * sizeof(ImageAcc);
+    // the per-image sums follow the control words in the arena (256 bytes of them) and in
+    // the pinned block, so one copy brings both back
+    static_assert(sizeof(int32_t) * CTL_N == 256, "control words fill one 256-byte slot");
+    if (reinterpret_cast<char*>(acc) != reinterpret_cast<char*>(P.ctl) + 256) {
+      release();
+      return fail(GC_ERR_INTERNAL, "arena layout");
+    }
+    pin_bytes = 512 + imgs.size() * sizeof(ImageAcc);
     pin = pinned_take(pin_bytes);
     if (!pin) { release(); return fail(GC_ERR_OOM, "pinned host allocation failed"); }
     h_count = static_cast<int32_t*>(pin);
-    h_ctl = reinterpret_cast<int32_t*>(static_cast<char*>(pin) + 32);
-    h_acc = reinterpret_cast<ImageAcc*>(static_cast<char*>(pin) + 96);
+    h_ctl = reinterpret_cast<int32_t*>(static_cast<char*>(pin) + 256);
+    h_acc = reinterpret_cast<ImageAcc*>(static_cast<char*>(pin) + 512);
     std::vector<int4> nb(nt);
     for (const auto& d : imgs)
       for (int ty = 0; ty < d.th; ++ty)
@@ -368,6 +380,7 @@ struct Pool {
   // exact BFS distances to the sink pixels (global relabel); sets tact.  h: condition
   // handle when captured into a graph (0: host-driven rounds)
   int global_relabel(cudaStream_t s, int first = 1) {
+    RK(timed(K_MASKS, s, [&] { return launch_masks(P, grid_warps, s); }));
     RK(timed(K_BFS_FIRST, s, [&] { return launch_bfs_round(P, first, 0, grid_warps, s); }));
     return frontier_rounds(s, /*flood=*/false);
   }
@@ -434,12 +447,11 @@ struct Pool {
   // Host-driven solve (profiling, stats collection): same kernels, host decides the loops.
   int solve_host(cudaStream_t s, bool relabel_first) {
     RK(prof_begin(s));
-    RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, s));
+    RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, s));
     int n = 0;
     if (relabel_first) RK(global_relabel(s));
     RK(compact(P.tact, nullptr, s));
-    RK(launch_mark_images(P, list, counts, 0, s));
-    RK(launch_ctl_cycle(P, counts, 0, 0, s));
+    RK(launch_mark_cycle(P, list, counts, 0, 0, 0, s));
     bool go = true;
     if (relabel_first) {
       RK(read_count(s, &n));
@@ -459,8 +471,7 @@ struct Pool {
       }
       RK(global_relabel(s, 2));
       RK(compact(P.tact, nullptr, s));
-      RK(launch_mark_images(P, list, counts, 1, s));
-      RK(launch_ctl_cycle(P, counts, 1, 0, s));
+      RK(launch_mark_cycle(P, list, counts, 1, 1, 0, s));
       RK(read_count(s, &n));
       go = n > 0;
     }
@@ -522,11 +533,14 @@ struct Pool {
     cudaGraphConditionalHandle hmain, hflood;
     CK(cudaGraphConditionalHandleCreate(&hmain, g, 0, 0));
     CK(cudaGraphConditionalHandleCreate(&hflood, g, 0, 0));
-    RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, cs); }));
+    RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs); }));
     if (variant) {  // exact global relabel before the first push
       cudaGraphConditionalHandle h0;
       CK(cudaGraphConditionalHandleCreate(&h0, g, 0, 0));
-      RK(capture(g, L, [&](cudaStream_t cs) { return launch_bfs_round(P, 1, h0, grid_warps, cs); }));
+      RK(capture(g, L, [&](cudaStream_t cs) {
+        RK(launch_masks(P, grid_warps, cs));
+        return launch_bfs_round(P, 1, h0, grid_warps, cs);
+      }));
       cudaGraph_t b0;
       RK(add_while(g, L, h0, &b0));
       std::vector<cudaGraphNode_t> Lb;
@@ -534,8 +548,7 @@ struct Pool {
     }
     RK(capture(g, L, [&](cudaStream_t cs) {
       RK(launch_scan(GC_SCAN_MODE_COMPACT, P.tact, nullptr, nullptr, nullptr, list, counts, nt, 0, 0, 0, 0, 0, scan.st, cs));
-      RK(launch_mark_images(P, list, counts, 0, cs));
-      return launch_ctl_cycle(P, counts, 0, hmain, cs);
+      return launch_mark_cycle(P, list, counts, 0, 0, hmain, cs);
     }));
     cudaGraph_t bm;
     RK(add_while(g, L, hmain, &bm));
@@ -546,6 +559,7 @@ struct Pool {
       RK(capture(bm, Lm, [&](cudaStream_t cs) {
         for (int p = 0; p < opts.pulses_per_relabel; ++p)
           RK(launch_discharge(P, opts.discharge_iters, grid_dis, cs));
+        RK(launch_masks(P, grid_warps, cs));
         return launch_bfs_round(P, 2, hb, grid_warps, cs);
       }));
       cudaGraph_t bb;
@@ -554,12 +568,10 @@ struct Pool {
       RK(capture(bb, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, hb, grid_warps, cs); }));
       RK(capture(bm, Lm, [&](cudaStream_t cs) {
         RK(launch_scan(GC_SCAN_MODE_COMPACT, P.tact, nullptr, nullptr, nullptr, list, counts, nt, 0, 0, 0, 0, 0, scan.st, cs));
-        RK(launch_mark_images(P, list, counts, 1, cs));
-        return launch_ctl_cycle(P, counts, 1, hmain, cs);
+        return launch_mark_cycle(P, list, counts, 1, 1, hmain, cs);
       }));
     }
-    RK(capture(g, L, [&](cudaStream_t cs) {
-      RK(launch_acc_reset(acc, (int)imgs.size(), cs));
+    RK(capture(g, L, [&](cudaStream_t cs) {   // k_ctl_begin cleared the sums
       return launch_flood_round(P, 1, hflood, acc, grid_warps, cs);
     }));
     cudaGraph_t bf;
@@ -569,8 +581,9 @@ struct Pool {
       RK(capture(bf, Lf, [&](cudaStream_t cs) { return launch_flood_round(P, 0, hflood, acc, grid_warps, cs); }));
     }
     RK(capture(g, L, [&](cudaStream_t cs) {
-      CK(cudaMemcpyAsync(h_acc, acc, sizeof(ImageAcc) * imgs.size(), cudaMemcpyDeviceToHost, cs));
-      CK(cudaMemcpyAsync(h_ctl, P.ctl, sizeof(int32_t) * CTL_N, cudaMemcpyDeviceToHost, cs));
+      // control words and per-image sums are adjacent on both sides: one copy
+      CK(cudaMemcpyAsync(h_ctl, P.ctl, sizeof(int32_t) * CTL_N + sizeof(ImageAcc) * imgs.size(),
+                         cudaMemcpyDeviceToHost, cs));
       return GC_OK;
     }));
     CK(cudaGraphInstantiate(&gexec[variant], g, 0));
@@ -653,7 +666,7 @@ struct Pool {
   }
   int step_start_bfs(cudaStream_t s) {
     if (!uploaded) return fail(GC_ERR_STATE, "startBfs before upload");
-    RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, s));
+    RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, s));
     RK(global_relabel(s));
     RK(compact(P.tact, nullptr, s));
     RK(launch_ctl_cycle(P, counts, 0, 0, s));
@@ -1005,7 +1018,8 @@ int gc_get_profile(const gc_handle* h, gc_kernel_prof* out, int n) {
 
 const char* gc_kernel_name(int kind) {
   static const char* names[GC_NKERN] = {"upload", "discharge", "edge_relabel_build", "bfs_first",
-                                        "bfs", "flood_first", "flood", "compact", "labels"};
+                                        "bfs", "flood_first", "flood", "compact", "labels",
+                                        "masks"};
   return kind >= 0 && kind < GC_NKERN ? names[kind] : "";
 }
 

@@ -43,9 +43,13 @@ struct PoolView {
   int32_t* queue[2];      // [nt] active-tile worklists, alternating by pulse
   int32_t* qcount;        // [2] worklist lengths
   int32_t* inq[2];        // [nt] tile is in queue[k] (deduplication)
+  int32_t* fq[2];         // [nt] frontier lists of the BFS / flood rounds (dedup by mark[k])
+  int32_t* fcount;        // [2] frontier list lengths
   int32_t* tact;          // [nt] tile has an active pixel (excess > 0, height < HINF)
   int32_t* img_of;        // [nt] image index of the tile
-  int32_t* mdirty;        // [nt] the tile's planes changed since its masks were computed
+  int32_t* mdirty;        // [nt] the tile is on the dirty list (its masks are stale)
+  int32_t* dq;            // [nt] dirty list: tiles whose masks k_masks rebuilds
+  int32_t* dcount;        // [1] dirty list length
   long long* tpos;        // [nt] sum of max(excess, 0) over the tile (with the masks)
   int nimg;               // images in the pool
   int32_t* img_live;      // [nimg] cycle stamp of images that still have active tiles
@@ -69,8 +73,12 @@ enum CtlSlot {
   CTL_PULSE = 10,     // discharge launches since the last list rebuild (parity = worklist)
   CTL_DDONE = 11,     // CTAs finished in the current discharge launch
   CTL_BAD = 12,       // first out-of-range worklist value seen by a self-check
-  CTL_BADWHERE = 13,  // 1: worklist append, 2: worklist length, 3: list length, 4: image id
-  CTL_N = 16
+  CTL_BADWHERE = 13,  // 1: worklist append, 2: worklist length, 3: list length, 4: image id,
+                      // 5: frontier append, 6: frontier length, 7: dirty append,
+                      // 8: dirty length
+  CTL_MDONE = 14,     // CTAs finished in k_mark_cycle
+  CTL_KDONE = 15,     // CTAs finished in k_masks
+  CTL_N = 64          // the control words fill 256 bytes; the per-image sums follow them
 };
 
 // A self-check found a worklist value outside the pool: keep the first one, flag the solve
@@ -82,7 +90,7 @@ __device__ __forceinline__ void record_bad(const PoolView& P, int where, int val
 
 // Kernel kinds for profiling (launch counts, event time, tiles processed).
 enum KernelKind { K_UPLOAD = 0, K_DISCHARGE, K_EDGE_BUILD, K_BFS_FIRST, K_BFS, K_FLOOD_FIRST,
-                  K_FLOOD, K_COMPACT, K_LABELS, K_COUNT };
+                  K_FLOOD, K_COMPACT, K_LABELS, K_MASKS, K_COUNT };
 
 // Decoupled look-back bookkeeping (single-pass scan).  status[] words are tagged with the
 // launch sequence number, so no reset is needed between launches.

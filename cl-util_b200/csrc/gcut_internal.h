@@ -54,6 +54,7 @@ int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t
                   const int32_t* down, const int32_t* left, const int32_t* right,
                   const int32_t* excess, int32_t* tl, ImageAcc* acc, cudaStream_t s);
 // reads the worklist queue[ctl[CTL_PULSE] & 1], builds the other one
+int launch_masks(const PoolView& P, int grid, cudaStream_t s);
 int launch_discharge(const PoolView& P, int iters, int grid, cudaStream_t s);
 int launch_edge_relabel_build(const PoolView& P, int32_t* list, int32_t* count,
                               const ScanState& st, cudaStream_t s);
@@ -64,7 +65,10 @@ int launch_bfs_round(const PoolView& P, int first, cudaGraphConditionalHandle h,
                      cudaStream_t s);
 int launch_flood_round(const PoolView& P, int first, cudaGraphConditionalHandle h, ImageAcc* acc,
                        int grid, cudaStream_t s);
-int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, cudaStream_t s);
+int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc* acc,
+                     cudaStream_t s);
+int launch_mark_cycle(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
+                      int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s);
 int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s);
 int launch_mark_images(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
                        cudaStream_t s);

@@ -59,6 +59,46 @@ __device__ __forceinline__ uint32_t warp_row_mask(uint32_t b0, uint32_t b1, uint
          (spread8(b3 >> sh) << 3);
 }
 
+// Row masks of tile t (residual edge up / down / left / right, sink, positive excess) from
+// the values the block's 256 threads hold: thread (r, q) holds pixels (r, 4q .. 4q+3).  The
+// BFS and the flood read these instead of the planes.  Every thread of the block calls it.
+__device__ __forceinline__ void write_tile_masks(const PoolView& P, int t, const int (&e)[4],
+                                                 const int (&cu)[4], const int (&cd)[4],
+                                                 const int (&cl)[4], const int (&cr)[4]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned F = 0xffffffffu;
+  uint32_t m[6];
+  const int* planes4[4] = {cu, cd, cl, cr};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int* v = planes4[k];
+    m[k] = warp_row_mask(__ballot_sync(F, v[0] > 0), __ballot_sync(F, v[1] > 0),
+                         __ballot_sync(F, v[2] > 0), __ballot_sync(F, v[3] > 0), lane & 3);
+  }
+  m[4] = warp_row_mask(__ballot_sync(F, e[0] < 0), __ballot_sync(F, e[1] < 0),
+                       __ballot_sync(F, e[2] < 0), __ballot_sync(F, e[3] < 0), lane & 3);
+  m[5] = warp_row_mask(__ballot_sync(F, e[0] > 0), __ballot_sync(F, e[1] > 0),
+                       __ballot_sync(F, e[2] > 0), __ballot_sync(F, e[3] > 0), lane & 3);
+  if (lane < 4) {
+    const int row = 4 * w + lane;
+    uint32_t* mc = P.mcan + (long long)t * 128;
+    mc[row] = m[0]; mc[32 + row] = m[1]; mc[64 + row] = m[2]; mc[96 + row] = m[3];
+    P.msink[(long long)t * 32 + row] = m[4];
+    P.mexc[(long long)t * 32 + row] = m[5];
+  }
+}
+
+// Queue tile t for a mask rebuild (k_masks) once: its planes changed after its masks were
+// written.  mdirty[t] == 1 exactly while t is on the dirty list.
+__device__ __forceinline__ void mark_dirty(const PoolView& P, int t) {
+  if (*((volatile int32_t*)&P.mdirty[t]) != 0) return;   // common case: already queued
+  if (atomicExch(&P.mdirty[t], 1) == 0) {
+    const int pos = atomicAdd(P.dcount, 1);
+    if (pos < P.nt) P.dq[pos] = t;   // mdirty deduplicates, so pos < nt always holds
+    else record_bad(P, 7, pos);
+  }
+}
+
 __global__ void __launch_bounds__(DIS_THREADS)
 k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
          const int32_t* __restrict__ down, const int32_t* __restrict__ left,
@@ -97,31 +137,7 @@ k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
   *(int4*)(P.cap[DDOWN] + off) = make_int4(cd[0], cd[1], cd[2], cd[3]);
   *(int4*)(P.cap[DLEFT] + off) = make_int4(cl[0], cl[1], cl[2], cl[3]);
   *(int4*)(P.cap[DRIGHT] + off) = make_int4(cr[0], cr[1], cr[2], cr[3]);
-  // block reductions
-  // row masks of the residual graph (the BFS reads these instead of the planes)
-  {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const unsigned F = 0xffffffffu;
-    uint32_t m[6];
-    const int* planes4[4] = {cu, cd, cl, cr};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int* v = planes4[k];
-      m[k] = warp_row_mask(__ballot_sync(F, v[0] > 0), __ballot_sync(F, v[1] > 0),
-                           __ballot_sync(F, v[2] > 0), __ballot_sync(F, v[3] > 0), lane & 3);
-    }
-    m[4] = warp_row_mask(__ballot_sync(F, e[0] < 0), __ballot_sync(F, e[1] < 0),
-                         __ballot_sync(F, e[2] < 0), __ballot_sync(F, e[3] < 0), lane & 3);
-    m[5] = warp_row_mask(__ballot_sync(F, e[0] > 0), __ballot_sync(F, e[1] > 0),
-                         __ballot_sync(F, e[2] > 0), __ballot_sync(F, e[3] > 0), lane & 3);
-    if (lane < 4) {
-      const int row = 4 * w + lane;
-      uint32_t* mc = P.mcan + (long long)t * 128;
-      mc[row] = m[0]; mc[32 + row] = m[1]; mc[64 + row] = m[2]; mc[96 + row] = m[3];
-      P.msink[(long long)t * 32 + row] = m[4];
-      P.mexc[(long long)t * 32 + row] = m[5];
-    }
-  }
+  write_tile_masks(P, t, e, cu, cd, cl, cr);
   __shared__ long long wpos[DIS_THREADS / 32];
 #pragma unroll
   for (int o = 16; o; o >>= 1) pos += __shfl_xor_sync(0xffffffffu, pos, o);
@@ -141,9 +157,66 @@ k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
     P.mark[1][t] = 0;
     P.inq[0][t] = 0;
     P.inq[1][t] = 0;
-    P.mdirty[t] = 0;  // the masks above are current
-    P.img_of[t] = img;
+    P.img_of[t] = img;   // (a tile still on the dirty list is rebuilt once more: harmless)
   }
+}
+
+// Mask rebuild of the tiles on the dirty list (dq[0 .. *dcount)), before a global relabel:
+// one tile per CTA iteration, the 256 threads read the tile's planes with int4 loads (an HBM
+// stream, unlike a per-warp rebuild inside the BFS), write its row masks and its sum of
+// max(excess, 0), and take it off the list.  Only the CTAs the list needs take part; the
+// last of them empties the list.
+__global__ void __launch_bounds__(DIS_THREADS)
+k_masks(PoolView P) {
+  __shared__ int s_n;
+  __shared__ long long wpos[DIS_THREADS / 32];
+  if (threadIdx.x == 0) {
+    int n = *((volatile int32_t*)P.dcount);
+    if (n < 0 || n > P.nt) {   // self-check: the list holds each tile at most once
+      record_bad(P, 8, n);
+      n = 0;
+    }
+    s_n = n;
+  }
+  __syncthreads();
+  const int n = s_n;
+  const int need = n < 1 ? 1 : n;
+  const int parts = need < (int)gridDim.x ? need : (int)gridDim.x;
+  if ((int)blockIdx.x >= parts) return;
+  const int r = threadIdx.x >> 3, c0 = (threadIdx.x & 7) * 4;
+  const int pix = r * GC_TILE + c0;
+  for (int li = blockIdx.x; li < n; li += parts) {
+    const int t = P.dq[li];
+    const long long off = (long long)t * GC_TILE_PX + pix;
+    int e[4], cu[4], cd[4], cl[4], cr[4];
+    int4 v = *reinterpret_cast<const int4*>(P.exc + off); e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w;
+    v = *reinterpret_cast<const int4*>(P.cap[DUP] + off); cu[0] = v.x; cu[1] = v.y; cu[2] = v.z; cu[3] = v.w;
+    v = *reinterpret_cast<const int4*>(P.cap[DDOWN] + off); cd[0] = v.x; cd[1] = v.y; cd[2] = v.z; cd[3] = v.w;
+    v = *reinterpret_cast<const int4*>(P.cap[DLEFT] + off); cl[0] = v.x; cl[1] = v.y; cl[2] = v.z; cl[3] = v.w;
+    v = *reinterpret_cast<const int4*>(P.cap[DRIGHT] + off); cr[0] = v.x; cr[1] = v.y; cr[2] = v.z; cr[3] = v.w;
+    write_tile_masks(P, t, e, cu, cd, cl, cr);
+    long long pos = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) pos += e[j] > 0 ? e[j] : 0;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) pos += __shfl_xor_sync(0xffffffffu, pos, o);
+    if ((threadIdx.x & 31) == 0) wpos[threadIdx.x >> 5] = pos;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      long long tp = 0;
+      for (int k = 0; k < DIS_THREADS / 32; ++k) tp += wpos[k];
+      P.tpos[t] = tp;
+      P.mdirty[t] = 0;
+      if (P.ktiles) atomicAdd(&P.ktiles[K_MASKS], 1ull);
+    }
+    __syncthreads();   // wpos is reused by the next tile
+  }
+  if (threadIdx.x != 0) return;
+  __threadfence();
+  if (atomicAdd(&P.ctl[CTL_KDONE], 1) != parts - 1) return;
+  __threadfence();
+  P.ctl[CTL_KDONE] = 0;
+  *P.dcount = 0;
 }
 
 // ------------------------------------------------------------------------------------
@@ -398,7 +471,8 @@ k_discharge(PoolView P, int iters) {
           }
         }
       }
-      __syncthreads();  // all reads of S.hs / flow buffers of this round are done
+      // every read of S.hs in this iteration happened before the flow barrier above, so the
+      // new heights can be written now; the next reads follow the barrier below
 #pragma unroll
       for (int j = 0; j < 4; ++j) h[j] = nh[j];
       sts4(S.hs + pix, h[0], h[1], h[2], h[3]);
@@ -487,16 +561,16 @@ k_discharge(PoolView P, int iters) {
       act |= a;
       act_int |= a && !erow && c > 0 && c < 31;
     }
-    if (sent_u) { P.touched[nb.x] = 1; P.mdirty[nb.x] = 1; worklist_add(P, nxt, nb.x); }
-    if (sent_d) { P.touched[nb.y] = 1; P.mdirty[nb.y] = 1; worklist_add(P, nxt, nb.y); }
-    if (sent_l) { P.touched[nb.z] = 1; P.mdirty[nb.z] = 1; worklist_add(P, nxt, nb.z); }
-    if (sent_r) { P.touched[nb.w] = 1; P.mdirty[nb.w] = 1; worklist_add(P, nxt, nb.w); }
+    if (sent_u) { P.touched[nb.x] = 1; mark_dirty(P, nb.x); worklist_add(P, nxt, nb.x); }
+    if (sent_d) { P.touched[nb.y] = 1; mark_dirty(P, nb.y); worklist_add(P, nxt, nb.y); }
+    if (sent_l) { P.touched[nb.z] = 1; mark_dirty(P, nb.z); worklist_add(P, nxt, nb.z); }
+    if (sent_r) { P.touched[nb.w] = 1; mark_dirty(P, nb.w); worklist_add(P, nxt, nb.w); }
     // the block-wide reductions also order every read of this buffer before its reuse
     const int any_act = __syncthreads_or(act);
     act_int = __syncthreads_or(act_int);
     if (tid == 0) {
       P.touched[t] = 1;
-      P.mdirty[t] = 1;
+      mark_dirty(P, t);
       P.act_int[t] = act_int;
       if (any_act) worklist_add(P, nxt, t);
       if (P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
@@ -646,18 +720,6 @@ k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
 // ------------------------------------------------------------------------------------
 constexpr int WARPS_PER_CTA = 4;
 
-// Loads 32 rows of a per-pixel predicate as row masks: lane r receives the mask of row r.
-template <class F>
-__device__ __forceinline__ uint32_t rows_ballot(const int32_t* __restrict__ plane, int lane, F f) {
-  uint32_t mine = 0;
-#pragma unroll
-  for (int rr = 0; rr < 32; ++rr) {
-    const uint32_t b = __ballot_sync(0xffffffffu, f(plane[rr * GC_TILE + lane]));
-    if (lane == rr) mine = b;
-  }
-  return mine;
-}
-
 __device__ __forceinline__ int warp_min(int v) {
 #pragma unroll
   for (int o = 16; o; o >>= 1) v = imin(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -694,32 +756,93 @@ __device__ __forceinline__ void tile_bfs(int (&d)[32], uint32_t canU, uint32_t c
   }
 }
 
-// Frontier rounds: round `rnd` processes the tiles marked in mark[rnd & 1] (every tile when
-// `first`), marks neighbours in mark[(rnd + 1) & 1] and counts its tiles in rcnt[rnd & 1].
-// The round number lives in device memory (ctl[CTL_RND]); the last CTA of a round consumes
-// the count, advances the round and, inside a CUDA graph, sets the WHILE condition.
+// Multi-source BFS inside a tile from its sink pixels only (all seeds at level 0), one level
+// per step on the row masks: N = neighbours of the frontier over residual edges, not yet
+// reached.  Lane r writes the distances of row r into `row` (GC_HINF where unreached) as the
+// pixels are reached, and gets the mask of reached pixels.  A path inside a tile has fewer
+// than 1024 steps, which bounds the loop.
+__device__ __forceinline__ uint32_t tile_bfs_from_sinks(int* row, uint32_t sink, uint32_t canU,
+                                                        uint32_t canD, uint32_t canL,
+                                                        uint32_t canR, int lane) {
+#pragma unroll
+  for (int c = 0; c < 32; ++c) row[c] = GC_HINF;
+  for (uint32_t b = sink; b; b &= b - 1) row[__ffs(b) - 1] = 0;
+  uint32_t vis = sink, F = sink;
+  for (int level = 1; level < GC_TILE_PX; ++level) {
+    uint32_t Fu = __shfl_up_sync(0xffffffffu, F, 1);
+    uint32_t Fd = __shfl_down_sync(0xffffffffu, F, 1);
+    if (lane == 0) Fu = 0;
+    if (lane == 31) Fd = 0;
+    const uint32_t N = (((F >> 1) & canR) | ((F << 1) & canL) | (Fu & canU) | (Fd & canD)) & ~vis;
+    if (!__any_sync(0xffffffffu, N != 0)) break;
+    vis |= N;
+    F = N;
+    for (uint32_t b = N; b; b &= b - 1) row[__ffs(b) - 1] = level;
+  }
+  return vis;
+}
+
+// Frontier rounds.  The first round of a relabel or flood processes every tile (grid-stride);
+// round r > 0 processes the list fq[r & 1] built by round r - 1.  A tile whose boundary
+// values changed queues its neighbours in fq[(r + 1) & 1], deduplicated by mark[(r + 1) & 1];
+// the round that processes a tile clears its mark.  Only the CTAs the list needs take part
+// (at least one, so every launched round is finalised), and the last of them consumes the
+// list, advances the round number (device memory, ctl[CTL_RND]) and, inside a CUDA graph,
+// sets the WHILE condition: another round runs only when the next list is not empty.
 __device__ __forceinline__ int frontier_round_number(const PoolView& P, int first) {
   return first ? 0 : *((volatile int32_t*)&P.ctl[CTL_RND]);
 }
 
+// Work of this round: *count tiles (all tiles for a first round) and the number of CTAs that
+// take part; CTAs beyond it return at once.  Called by every thread of the CTA.
+__device__ __forceinline__ void frontier_work(const PoolView& P, int first, int in, int per_cta,
+                                              int* count, int* participants) {
+  __shared__ int s_n;
+  if (threadIdx.x == 0) {
+    int n = first ? P.nt : *((volatile int32_t*)&P.fcount[in]);
+    if (n < 0 || n > P.nt) {   // self-check: a list holds each tile at most once
+      record_bad(P, 6, n);
+      n = 0;
+    }
+    s_n = n;
+  }
+  __syncthreads();
+  const int n = s_n;
+  *count = n;
+  const int need = first ? (int)gridDim.x : (n + per_cta - 1) / per_cta;
+  *participants = need < 1 ? 1 : (need < (int)gridDim.x ? need : (int)gridDim.x);
+}
+
+// Queue tile t for the next round (once).
+__device__ __forceinline__ void frontier_push(const PoolView& P, int out, int t) {
+  if (atomicExch(&P.mark[out][t], 1) == 0) {
+    const int pos = atomicAdd(&P.fcount[out], 1);
+    if (pos < P.nt) P.fq[out][pos] = t;   // the mark deduplicates, so pos < nt always holds
+    else record_bad(P, 5, pos);
+  }
+}
+
 __device__ __forceinline__ void frontier_round_end(const PoolView& P, int first, int in,
-                                                   int total_slot, cudaGraphConditionalHandle h) {
+                                                   int total_slot, int participants,
+                                                   cudaGraphConditionalHandle h) {
   __syncthreads();
   if (threadIdx.x != 0) return;
   __threadfence();
   const int d = atomicAdd(&P.ctl[CTL_DONE], 1);
-  if (d != (int)gridDim.x - 1) return;
+  if (d != participants - 1) return;
   __threadfence();
   volatile int32_t* ctl = P.ctl;
-  const int cnt = *((volatile int32_t*)&P.rcnt[in]);
+  const int out = in ^ 1;
   P.rcnt[in] = 0;
-  ctl[CTL_LASTCNT] = cnt;
+  const int next = *((volatile int32_t*)&P.fcount[out]);
+  P.fcount[in] = 0;   // this round's list is consumed
+  ctl[CTL_LASTCNT] = next;
   ctl[CTL_RND] = first ? 1 : ctl[CTL_RND] + 1;
   const int rounds = first ? 1 : ctl[CTL_ROUNDS] + 1;
   ctl[CTL_ROUNDS] = rounds;
   ctl[total_slot] = ctl[total_slot] + 1;
   ctl[CTL_DONE] = 0;
-  bool more = cnt > 0 && ctl[CTL_ERR] < 3;   // a copy or self-check error ends the loop
+  bool more = next > 0 && ctl[CTL_ERR] < 3;   // a copy or self-check error ends the loop
   if (more && rounds >= ctl[CTL_MAXROUNDS]) {
     ctl[CTL_ERR] = 1;
     more = false;
@@ -729,14 +852,19 @@ __device__ __forceinline__ void frontier_round_end(const PoolView& P, int first,
 }
 
 // Solve prologue: reset the control words and the image stamps.
-__global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles) {
-  if (threadIdx.x < CTL_N) P.ctl[threadIdx.x] = 0;
-  for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) P.img_live[i] = 0;
+__global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc* acc) {
+  for (int i = threadIdx.x; i < CTL_N; i += blockDim.x) P.ctl[i] = 0;
+  for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) {
+    P.img_live[i] = 0;
+    acc[i].sumpos_e = 0;   // the flood of this solve accumulates it
+  }
   if (threadIdx.x == 0) {
     P.ctl[CTL_MAXROUNDS] = max_rounds;
     P.ctl[CTL_MAXCYCLES] = max_cycles;
     P.rcnt[0] = 0;
     P.rcnt[1] = 0;
+    P.fcount[0] = 0;
+    P.fcount[1] = 0;
   }
 }
 
@@ -755,6 +883,48 @@ __global__ void k_mark_images(PoolView P, const int32_t* list, const int32_t* co
     if ((unsigned)img < (unsigned)P.nimg) P.img_live[img] = stamp;
     else record_bad(P, 4, img);
   }
+}
+
+// The two kernels above in one launch: every CTA stamps images of the list, then the last CTA
+// applies the cycle check (it reads the cycle count after every stamp was taken).
+__global__ void k_mark_cycle(PoolView P, const int32_t* list, const int32_t* count, int bump,
+                             int count_cycle, cudaGraphConditionalHandle h) {
+  __shared__ int s_n, s_stamp;
+  if (threadIdx.x == 0) {
+    int n = *((volatile const int32_t*)count);
+    if (n < 0 || n > P.nt) {   // self-check: a list holds each tile at most once
+      if (blockIdx.x == 0) record_bad(P, 3, n);
+      n = 0;
+    }
+    s_n = n;
+    s_stamp = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1 + bump;
+  }
+  __syncthreads();
+  const int n = s_n, stamp = s_stamp;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int img = P.img_of[list[i]];
+    if ((unsigned)img < (unsigned)P.nimg) P.img_live[img] = stamp;
+    else record_bad(P, 4, img);
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  __threadfence();
+  if (atomicAdd(&P.ctl[CTL_MDONE], 1) != (int)gridDim.x - 1) return;
+  __threadfence();
+  volatile int32_t* ctl = P.ctl;
+  ctl[CTL_MDONE] = 0;
+  ctl[CTL_PULSE] = 0;   // the compacted list sits in queue[0]
+  ctl[CTL_DDONE] = 0;
+  P.qcount[1] = 0;
+  const int cycles = ctl[CTL_CYCLES] + (count_cycle ? 1 : 0);
+  ctl[CTL_CYCLES] = cycles;
+  bool more = n > 0 && ctl[CTL_ERR] < 3;
+  if (more && cycles >= ctl[CTL_MAXCYCLES]) {
+    ctl[CTL_ERR] = 2;
+    more = false;
+  }
+  __threadfence();
+  if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
 // After the active-tile compaction: another cycle runs while tiles are active and the cycle
@@ -783,15 +953,17 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int in = frontier_round_number(P, first) & 1, out = in ^ 1;
   int32_t* const markin = P.mark[in];
-  int32_t* const markout = P.mark[out];
   int32_t* T = tr[warp];
   int done = 0;
   // first == 2: a global relabel inside the solve loop skips images whose cut was final at
   // the previous check (no active tile); their state no longer changes
   const int live = first == 2 ? *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1 : 0;
-  for (int t = blockIdx.x * WARPS_PER_CTA + warp; t < P.nt; t += gridDim.x * WARPS_PER_CTA) {
+  int n, parts;
+  frontier_work(P, first, in, WARPS_PER_CTA, &n, &parts);
+  if ((int)blockIdx.x >= parts) return;
+  for (int i = blockIdx.x * WARPS_PER_CTA + warp; i < n; i += parts * WARPS_PER_CTA) {
+    const int t = first ? i : P.fq[in][i];
     if (!first) {
-      if (!markin[t]) continue;
       if (lane == 0) markin[t] = 0;
     } else {
       if (first == 2) {
@@ -810,47 +982,21 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
     ++done;
     const int4 nb = P.nbr[t];
     const long long base = (long long)t * GC_TILE_PX;
-    uint32_t canU, canD, canL, canR, sink;
-    if (first && P.mdirty[t]) {
-      // the tile changed since its masks were built: rebuild them (row masks by ballot),
-      // together with the tile's sum of positive excess
-      canU = rows_ballot(P.cap[DUP] + base, lane, [](int v) { return v > 0; });
-      canD = rows_ballot(P.cap[DDOWN] + base, lane, [](int v) { return v > 0; });
-      canL = rows_ballot(P.cap[DLEFT] + base, lane, [](int v) { return v > 0; });
-      canR = rows_ballot(P.cap[DRIGHT] + base, lane, [](int v) { return v > 0; });
-      uint32_t pos = 0;
-      sink = 0;
-      long long ps = 0;
-#pragma unroll 4
-      for (int rr = 0; rr < 32; ++rr) {
-        const int v = P.exc[base + rr * GC_TILE + lane];
-        const uint32_t bs = __ballot_sync(0xffffffffu, v < 0);
-        const uint32_t bp = __ballot_sync(0xffffffffu, v > 0);
-        if (lane == rr) { sink = bs; pos = bp; }
-        ps += v > 0 ? v : 0;
-      }
-#pragma unroll
-      for (int o = 16; o; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
-      uint32_t* mc = P.mcan + (long long)t * 128;
-      mc[lane] = canU; mc[32 + lane] = canD; mc[64 + lane] = canL; mc[96 + lane] = canR;
-      P.msink[(long long)t * 32 + lane] = sink;
-      P.mexc[(long long)t * 32 + lane] = pos;
-      if (lane == 0) {
-        P.tpos[t] = ps;
-        P.mdirty[t] = 0;
-      }
+    // the masks are current: k_masks rebuilt every tile that changed since they were written
+    const uint32_t* mc = P.mcan + (long long)t * 128;
+    const uint32_t canU = mc[lane], canD = mc[32 + lane], canL = mc[64 + lane], canR = mc[96 + lane];
+    const uint32_t sink = P.msink[(long long)t * 32 + lane];
+    uint32_t fin;
+    if (first) {
+      // no halo seeds: one level per step, bit-parallel (distances land in T directly)
+      fin = tile_bfs_from_sinks(T + lane * 33, sink, canU, canD, canL, canR, lane);
     } else {
-      const uint32_t* mc = P.mcan + (long long)t * 128;
-      canU = mc[lane]; canD = mc[32 + lane]; canL = mc[64 + lane]; canR = mc[96 + lane];
-      sink = P.msink[(long long)t * 32 + lane];
-    }
-    int d[32];
+      int d[32];
 #pragma unroll
-    for (int c = 0; c < 32; ++c) d[c] = ((sink >> c) & 1u) ? 0 : GC_HINF;
-    if (!first) {
+      for (int c = 0; c < 32; ++c) d[c] = ((sink >> c) & 1u) ? 0 : GC_HINF;
       // halo seeds: an edge pixel with a residual edge into the neighbour tile
-      int vu = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + lane] : GC_HINF;
-      int vd = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + lane] : GC_HINF;
+      const int vu = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + lane] : GC_HINF;
+      const int vd = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + lane] : GC_HINF;
       const int vl = nb.z >= 0 ? P.hgt[(long long)nb.z * GC_TILE_PX + lane * GC_TILE + 31] : GC_HINF;
       const int vr = nb.w >= 0 ? P.hgt[(long long)nb.w * GC_TILE_PX + lane * GC_TILE] : GC_HINF;
 #pragma unroll
@@ -862,16 +1008,16 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
       }
       if ((canL & 1u) && vl < GC_HINF) d[0] = imin(d[0], vl + 1);
       if ((canR >> 31) && vr < GC_HINF) d[31] = imin(d[31], vr + 1);
-    }
-    tile_bfs(d, canU, canD, canL, canR, lane);
-    // transpose through shared memory and write the distances back (coalesced rows)
+      tile_bfs(d, canU, canD, canL, canR, lane);
+      // transpose through shared memory and write the distances back (coalesced rows)
 #pragma unroll
-    for (int c = 0; c < 32; ++c) T[lane * 33 + c] = d[c];
+      for (int c = 0; c < 32; ++c) T[lane * 33 + c] = d[c];
+      fin = 0;
+#pragma unroll
+      for (int c = 0; c < 32; ++c) fin |= (uint32_t)(d[c] < GC_HINF) << c;
+    }
     __syncwarp();
     int chU = 0, chD = 0, chL = 0, chR = 0;
-    uint32_t fin = 0;
-#pragma unroll
-    for (int c = 0; c < 32; ++c) fin |= (uint32_t)(d[c] < GC_HINF) << c;
     for (int rr = 0; rr < 32; ++rr) {
       const int nv = T[rr * 33 + lane];
       int* p = P.hgt + base + rr * GC_TILE + lane;
@@ -893,17 +1039,17 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
     const int act = __any_sync(0xffffffffu, (pos & fin) != 0);
     if (lane == 0) {
       P.tact[t] = act;
-      if (chU && nb.x >= 0) markout[nb.x] = 1;
-      if (chD && nb.y >= 0) markout[nb.y] = 1;
-      if (chL && nb.z >= 0) markout[nb.z] = 1;
-      if (chR && nb.w >= 0) markout[nb.w] = 1;
+      if (chU && nb.x >= 0) frontier_push(P, out, nb.x);
+      if (chD && nb.y >= 0) frontier_push(P, out, nb.y);
+      if (chL && nb.z >= 0) frontier_push(P, out, nb.z);
+      if (chR && nb.w >= 0) frontier_push(P, out, nb.w);
     }
   }
   if (lane == 0 && done) {
     atomicAdd(&P.rcnt[in], done);
     if (P.ktiles) atomicAdd(&P.ktiles[first ? K_BFS_FIRST : K_BFS], (unsigned long long)done);
   }
-  frontier_round_end(P, first, in, CTL_BFS_TOTAL, h);
+  frontier_round_end(P, first, in, CTL_BFS_TOTAL, parts, h);
 }
 
 // ------------------------------------------------------------------------------------
@@ -915,13 +1061,13 @@ k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int in = frontier_round_number(P, first) & 1, out = in ^ 1;
   int32_t* const markin = P.mark[in];
-  int32_t* const markout = P.mark[out];
   int done = 0;
-  for (int t = blockIdx.x * WARPS_PER_CTA + warp; t < P.nt; t += gridDim.x * WARPS_PER_CTA) {
-    if (!first) {
-      if (!markin[t]) continue;
-      if (lane == 0) markin[t] = 0;
-    }
+  int n, parts;
+  frontier_work(P, first, in, WARPS_PER_CTA, &n, &parts);
+  if ((int)blockIdx.x >= parts) return;
+  for (int i = blockIdx.x * WARPS_PER_CTA + warp; i < n; i += parts * WARPS_PER_CTA) {
+    const int t = first ? i : P.fq[in][i];
+    if (!first && lane == 0) markin[t] = 0;
     ++done;
     const int4 nb = P.nbr[t];
     const uint32_t* mc = P.mcan + (long long)t * 128;
@@ -965,17 +1111,17 @@ k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc
     const int sL = __any_sync(0xffffffffu, (nw & canL & 1u) != 0);
     const int sR = __any_sync(0xffffffffu, ((nw & canR) >> 31) != 0);
     if (lane == 0) {
-      if (sU && nb.x >= 0) markout[nb.x] = 1;
-      if (sD && nb.y >= 0) markout[nb.y] = 1;
-      if (sL && nb.z >= 0) markout[nb.z] = 1;
-      if (sR && nb.w >= 0) markout[nb.w] = 1;
+      if (sU && nb.x >= 0) frontier_push(P, out, nb.x);
+      if (sD && nb.y >= 0) frontier_push(P, out, nb.y);
+      if (sL && nb.z >= 0) frontier_push(P, out, nb.z);
+      if (sR && nb.w >= 0) frontier_push(P, out, nb.w);
     }
   }
   if (lane == 0 && done) {
     atomicAdd(&P.rcnt[in], done);
     if (P.ktiles) atomicAdd(&P.ktiles[first ? K_FLOOD_FIRST : K_FLOOD], (unsigned long long)done);
   }
-  frontier_round_end(P, first, in, CTL_FLOOD_TOTAL, h);
+  frontier_round_end(P, first, in, CTL_FLOOD_TOTAL, parts, h);
 }
 
 // Labels of one image, row-major, padding excluded.  One thread writes the 32 pixels of
@@ -1037,7 +1183,7 @@ __device__ __forceinline__ void apply_tlink(const PoolView& P, const ImageDesc& 
   if (old == v) return;
   tl[o] = v;
   atomicAdd(P.exc + o, v - old);
-  P.mdirty[t] = 1;
+  mark_dirty(P, t);
   const long long dpos = (long long)(v > 0 ? v : 0) - (long long)(old > 0 ? old : 0);
   if (dpos) atomicAdd(&acc[img].sumpos_t, (unsigned long long)dpos);
 }
@@ -1091,6 +1237,11 @@ int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t
   return ok();
 }
 
+int launch_masks(const PoolView& P, int grid, cudaStream_t s) {
+  k_masks<<<grid, DIS_THREADS, 0, s>>>(P);
+  return ok();
+}
+
 int launch_discharge(const PoolView& P, int iters, int grid, cudaStream_t s) {
   k_discharge<<<grid, DIS_THREADS, DIS_DYN_SMEM, s>>>(P, iters);
   return ok();
@@ -1126,14 +1277,21 @@ int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s) {
   return ok();
 }
 
-int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, cudaStream_t s) {
-  k_ctl_begin<<<1, 32, 0, s>>>(P, max_rounds, max_cycles);
+int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc* acc,
+                     cudaStream_t s) {
+  k_ctl_begin<<<1, 32, 0, s>>>(P, max_rounds, max_cycles, acc);
   return ok();
 }
 
 int launch_mark_images(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
                        cudaStream_t s) {
   k_mark_images<<<32, 256, 0, s>>>(P, list, count, bump);
+  return ok();
+}
+
+int launch_mark_cycle(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
+                      int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_mark_cycle<<<16, 256, 0, s>>>(P, list, count, bump, count_cycle, h);
   return ok();
 }
 

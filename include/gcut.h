@@ -162,7 +162,7 @@ int gc_set_collect_stats(gc_handle* h, int on);
 /* Per-kernel profile of the last solve (and the upload / labels calls around it):
    launches, summed CUDA-event time of each launch on the caller's stream, and tiles
    processed (device counters).  Kinds 0..GC_NKERN-1, named by gc_kernel_name. */
-#define GC_NKERN 9
+#define GC_NKERN 10
 typedef struct gc_kernel_prof {
   int64_t launches;
   double ms;
