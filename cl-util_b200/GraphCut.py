@@ -45,6 +45,27 @@ def _on(stream):
     return contextlib.nullcontext() if stream is None else torch.cuda.stream(stream)
 
 
+def _as_rgba32(img):
+    """uint32 [H, W] view of an RGB(A) image (R in the low byte); torch or numpy."""
+    import torch
+    if isinstance(img, torch.Tensor):
+        if img.dtype == torch.uint8 and img.dim() == 3:
+            if img.shape[2] == 3:
+                img = torch.cat([img, torch.full_like(img[..., :1], 255)], dim=2)
+            return img.contiguous().view(torch.int32).squeeze(-1)
+        if img.dtype not in (torch.int32,):
+            raise TypeError("rgba must be uint8 [H, W, 3|4] or 32-bit [H, W]")
+        return img
+    a = np.asarray(img)
+    if a.dtype == np.uint8 and a.ndim == 3:
+        if a.shape[2] == 3:
+            a = np.concatenate([a, np.full(a.shape[:2] + (1,), 255, np.uint8)], axis=2)
+        return np.ascontiguousarray(a).view(np.uint32)[..., 0]
+    if a.dtype not in (np.uint32, np.int32):
+        raise TypeError("rgba must be uint8 [H, W, 3|4] or 32-bit [H, W]")
+    return a
+
+
 def unpack_labels(bits: np.ndarray, width: int) -> np.ndarray:
     """uint8 [H, W] labels from the packed rows of GraphCut.labels_packed*."""
     return np.unpackbits(np.asarray(bits), axis=1, count=width, bitorder="little")
@@ -123,6 +144,29 @@ class GraphCut:
                                          dtype=np.int32) for p in planes]
             with torch.cuda.device(self.device):
                 check(lib().gc_upload_host(self._h, *[ptr(a) for a in host], stream_handle(stream)))
+        self._solved = False
+
+    def upload_image(self, rgba, excess, stream=None):
+        """Builds the capacities on the device from an image and the t-links (gc_upload_rgba):
+        n-link = floor(50 * exp(-beta * |dI|^2) + 0.5), beta = 1 / (2 * mean |dI|^2).  `rgba`
+        is uint32 [H, W] (RGBA bytes viewed as uint32) or uint8 [H, W, 3|4]; `excess` int32
+        [H, W].  Torch CUDA tensors are read in place; numpy arrays are copied."""
+        import torch
+        rgba = _as_rgba32(rgba)
+        if tuple(rgba.shape) != (self.height, self.width) or tuple(excess.shape) != (self.height, self.width):
+            raise ValueError("image / excess shape differs from the graph")
+        if isinstance(rgba, torch.Tensor) and rgba.is_cuda and isinstance(excess, torch.Tensor) and excess.is_cuda:
+            with _on(stream):
+                ex = _as_i32_device(excess, self.device)
+                img = rgba.contiguous()
+            check(lib().gc_upload_rgba(self._h, ptr(img), ptr(ex), stream_handle(stream)))
+            self._keep = (img, ex)
+        else:
+            img = np.ascontiguousarray(rgba.cpu().numpy() if isinstance(rgba, torch.Tensor) else rgba)
+            ex = np.ascontiguousarray(excess.cpu().numpy() if isinstance(excess, torch.Tensor) else excess,
+                                      dtype=np.int32)
+            with torch.cuda.device(self.device):
+                check(lib().gc_upload_rgba_host(self._h, ptr(img), ptr(ex), stream_handle(stream)))
         self._solved = False
 
     # ---- solve ------------------------------------------------------------------

@@ -66,6 +66,8 @@ SIGNATURES = {
     "gc_size": [_P, _P, _P],
     "gc_upload": [_P] * 6 + [_P],
     "gc_upload_host": [_P] * 6 + [_P],
+    "gc_upload_rgba": [_P, _P, _P, _P],
+    "gc_upload_rgba_host": [_P, _P, _P, _P],
     "gc_solve": [_P, _P],
     "gc_push": [_P, _P],
     "gc_relabel": [_P, _P],

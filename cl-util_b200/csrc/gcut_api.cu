@@ -5,6 +5,7 @@
 // a cycle here is `pulses_per_relabel` x {discharge, edge-relabel + list rebuild} and one
 // exact global relabel, all enqueued without a host wait; the host reads one int (the
 // active-tile count) per cycle and one per few BFS rounds.
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -152,7 +153,9 @@ struct Pool {
   int32_t* h_ctl = nullptr;    // pinned copy of the control words
   bool use_graph = true;
   ImageAcc* h_acc = nullptr;   // pinned
-  int grid_dis = 0, grid_warps = 0;
+  int grid_dis = 0, grid_warps = 0, sms = 1;
+  unsigned long long* dsum = nullptr;     // device: sum of |dI|^2 (gc_upload_rgba)
+  unsigned long long* h_dsum = nullptr;   // pinned copy
   bool uploaded = false, solved = false, edited = false, collect = false;
   bool list_valid = false, bfs_fresh = false;
   gc_stats stats{};
@@ -238,6 +241,7 @@ struct Pool {
     P = PoolView{};
     tl = list = counts = stage = pts = nullptr;
     acc = nullptr; lstage = nullptr; h_count = nullptr; h_ctl = nullptr; h_acc = nullptr;
+    dsum = nullptr; h_dsum = nullptr;
   }
 
   // places every device buffer of the pool (see Carve)
@@ -271,6 +275,7 @@ struct Pool {
     c.take(&scan.st.ticket, 4);
     scan.st.max_chunks = chunks;
     c.take(&pts, 2 * 1024);
+    c.take(&dsum, 1);
     if (imgs.size() == 1) c.take(&lstage, (size_t)imgs[0].W * imgs[0].H);
   }
 
@@ -337,6 +342,7 @@ struct Pool {
     pin = pinned_take(pin_bytes);
     if (!pin) { release(); return fail(GC_ERR_OOM, "pinned host allocation failed"); }
     h_count = static_cast<int32_t*>(pin);
+    h_dsum = reinterpret_cast<unsigned long long*>(static_cast<char*>(pin) + 64);
     h_ctl = reinterpret_cast<int32_t*>(static_cast<char*>(pin) + 256);
     h_acc = reinterpret_cast<ImageAcc*>(static_cast<char*>(pin) + 512);
     std::vector<int4> nb(nt);
@@ -358,6 +364,7 @@ struct Pool {
     CK(cudaStreamSynchronize(cudaStreamLegacy));
     grid_dis = occupancy_discharge(device);
     grid_warps = occupancy_warps(device);
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     return GC_OK;
   }
 
@@ -375,6 +382,55 @@ struct Pool {
     list_valid = false;
     bfs_fresh = false;
     return GC_OK;
+  }
+
+  // Capacities from an RGBA image (n-links) and int32 t-links: the sum of |dI|^2 over all
+  // 4-neighbour pairs is taken on the device (exact), the host turns it into beta and the
+  // n-link table, and the upload kernel builds the tile planes from the image.
+  int upload_rgba(int i, const uint32_t* rgba, const int32_t* excess, cudaStream_t s) {
+    if (i < 0 || i >= (int)imgs.size()) return fail(GC_ERR_INVALID, "image index");
+    if (!rgba || !excess) return fail(GC_ERR_INVALID, "null plane");
+    CK(cudaSetDevice(device));
+    const ImageDesc& im = imgs[i];
+    CK(cudaMemsetAsync(dsum, 0, sizeof(unsigned long long), s));
+    RK(launch_dsum(rgba, im.W, im.H, dsum, sms, s));
+    CK(cudaMemcpyAsync(h_dsum, dsum, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const long long npairs = (long long)(im.H - 1) * im.W + (long long)im.H * (im.W - 1);
+    NlinkTable tab;
+    nlink_table(*h_dsum, npairs, &tab);
+    CK(cudaMemsetAsync(acc + i, 0, sizeof(ImageAcc), s));
+    P.ktiles = nullptr;
+    RK(timed(K_UPLOAD, s, [&] { return launch_upload_rgba(P, im, i, rgba, excess, tab, tl, acc, s); }));
+    uploaded = true;
+    solved = false;
+    edited = false;
+    list_valid = false;
+    bfs_fresh = false;
+    return GC_OK;
+  }
+
+  // weight(d) = floor(50 * exp(-beta * d) + 0.5), beta = 1 / (2 * mean |dI|^2) (0 when the
+  // mean is 0), for d = |dI|^2 in [0, 3 * 255^2]; the weight does not increase with d, so it
+  // is stored as t[k - 1] = the largest d with weight >= k.  Each entry is located from the
+  // real root and then settled by evaluating the formula itself at the integers around it.
+  static void nlink_table(unsigned long long sum, long long npairs, NlinkTable* tab) {
+    const long kMax = 3L * 255 * 255;
+    const double mean = (double)sum / (double)(npairs > 1 ? npairs : 1);
+    const double beta = mean > 0 ? 1.0 / (2.0 * mean) : 0.0;
+    auto w = [&](long d) {
+      const double x = std::exp(-beta * (double)d);
+      const double y = 50.0 * x;
+      return (int)std::floor(y + 0.5);
+    };
+    for (int k = 1; k <= GC_NLINK_LEVELS; ++k) {
+      if (beta <= 0) { tab->t[k - 1] = (int32_t)kMax; continue; }
+      const double root = std::log(50.0 / (k - 0.5)) / beta;   // w(d) >= k  <=>  d <= root
+      long d = root >= (double)kMax ? kMax : (root < 0 ? 0 : (long)std::floor(root));
+      while (d < kMax && w(d + 1) >= k) ++d;
+      while (d >= 0 && w(d) < k) --d;
+      tab->t[k - 1] = (int32_t)d;
+    }
   }
 
   // exact BFS distances to the sink pixels (global relabel); sets tact.  h: condition
@@ -854,6 +910,35 @@ int gc_upload_host(gc_handle* h, const int32_t* up, const int32_t* down, const i
   for (int k = 0; k < 5; ++k)
     CK(cudaMemcpyAsync(p.stage + k * n, src[k], n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   int r = p.upload(0, p.stage, p.stage + n, p.stage + 2 * n, p.stage + 3 * n, p.stage + 4 * n, s);
+  p.track(s);
+  if (r) return r;
+  CK(cudaStreamSynchronize(s));
+  return GC_OK;
+}
+
+int gc_upload_rgba(gc_handle* h, const uint32_t* rgba, const int32_t* excess, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  const int r = h->pool.upload_rgba(0, rgba, excess, (cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
+}
+
+int gc_upload_rgba_host(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
+                        void* stream) {
+  g_err.clear();
+  if (!h || !rgba || !excess) return fail(GC_ERR_INVALID, "null argument");
+  Pool& p = h->pool;
+  CK(cudaSetDevice(p.device));
+  const size_t n = (size_t)p.imgs[0].W * p.imgs[0].H;
+  if (!p.stage) {
+    cudaError_t e = cudaMalloc((void**)&p.stage, 5 * n * sizeof(int32_t));
+    if (e) { p.stage = nullptr; cudaGetLastError(); return fail(GC_ERR_OOM, "staging buffer"); }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(p.stage, rgba, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(p.stage + n, excess, n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  int r = p.upload_rgba(0, reinterpret_cast<const uint32_t*>(p.stage), p.stage + n, s);
   p.track(s);
   if (r) return r;
   CK(cudaStreamSynchronize(s));

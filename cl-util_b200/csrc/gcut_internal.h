@@ -55,6 +55,18 @@ int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t
                   const int32_t* excess, int32_t* tl, ImageAcc* acc, cudaStream_t s);
 // reads the worklist queue[ctl[CTL_PULSE] & 1], builds the other one
 int launch_masks(const PoolView& P, int grid, cudaStream_t s);
+
+// n-link table of gc_upload_rgba: weight(d) = floor(50 * exp(-beta * d) + 0.5) for d = |dI|^2
+// equals the number of entries t[k] >= d (t[k] = largest d with weight >= k + 1).
+constexpr int GC_NLINK_LEVELS = 50;
+struct NlinkTable {
+  int32_t t[GC_NLINK_LEVELS];
+};
+int launch_upload_rgba(const PoolView& P, const ImageDesc& im, int img, const uint32_t* rgba,
+                       const int32_t* excess, const NlinkTable& tab, int32_t* tl, ImageAcc* acc,
+                       cudaStream_t s);
+int launch_dsum(const uint32_t* rgba, int W, int H, unsigned long long* sum, int sms,
+                cudaStream_t s);
 int launch_discharge(const PoolView& P, int iters, int grid, cudaStream_t s);
 int launch_edge_relabel_build(const PoolView& P, int32_t* list, int32_t* count,
                               const ScanState& st, cudaStream_t s);

@@ -99,11 +99,63 @@ __device__ __forceinline__ void mark_dirty(const PoolView& P, int t) {
   }
 }
 
+// Capacity sources of the upload.  PlaneSource: row-major capacity planes (gc_upload).
+// RgbaSource: n-links built from an RGBA image and the n-link table (gc_upload_rgba).
+struct PlaneSource {
+  const int32_t *up, *down, *left, *right, *excess;
+  __device__ __forceinline__ void prepare(int32_t*) const {}
+  __device__ __forceinline__ void pixel(const ImageDesc& im, const int32_t*, int x, int y, int& e,
+                                        int& cu, int& cd, int& cl, int& cr) const {
+    const long long i = (long long)y * im.W + x;
+    e = excess[i];
+    cu = y > 0 ? up[i] : 0;
+    cd = y < im.H - 1 ? down[i] : 0;
+    cl = x > 0 ? left[i] : 0;
+    cr = x < im.W - 1 ? right[i] : 0;
+  }
+};
+
+__device__ __forceinline__ int rgb_dist2(uint32_t a, uint32_t b) {
+  const int dr = (int)(a & 255u) - (int)(b & 255u);
+  const int dg = (int)((a >> 8) & 255u) - (int)((b >> 8) & 255u);
+  const int db = (int)((a >> 16) & 255u) - (int)((b >> 16) & 255u);
+  return dr * dr + dg * dg + db * db;
+}
+
+struct RgbaSource {
+  const uint32_t* rgba;
+  const int32_t* excess;
+  NlinkTable tab;
+  __device__ __forceinline__ void prepare(int32_t* s_tab) const {
+    if (threadIdx.x < GC_NLINK_LEVELS) s_tab[threadIdx.x] = tab.t[threadIdx.x];
+  }
+  // weight of |dI|^2 = d: the number of table entries >= d (the entries do not increase)
+  __device__ __forceinline__ static int weight(const int32_t* s_tab, int d) {
+    int lo = 0, hi = GC_NLINK_LEVELS;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (s_tab[mid] >= d) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ void pixel(const ImageDesc& im, const int32_t* s_tab, int x, int y,
+                                        int& e, int& cu, int& cd, int& cl, int& cr) const {
+    const long long i = (long long)y * im.W + x;
+    const uint32_t c = rgba[i];
+    e = excess[i];
+    cu = y > 0 ? weight(s_tab, rgb_dist2(c, rgba[i - im.W])) : 0;
+    cd = y < im.H - 1 ? weight(s_tab, rgb_dist2(c, rgba[i + im.W])) : 0;
+    cl = x > 0 ? weight(s_tab, rgb_dist2(c, rgba[i - 1])) : 0;
+    cr = x < im.W - 1 ? weight(s_tab, rgb_dist2(c, rgba[i + 1])) : 0;
+  }
+};
+
+template <class Source>
 __global__ void __launch_bounds__(DIS_THREADS)
-k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
-         const int32_t* __restrict__ down, const int32_t* __restrict__ left,
-         const int32_t* __restrict__ right, const int32_t* __restrict__ excess,
-         int32_t* __restrict__ tl, ImageAcc* acc) {
+k_upload(PoolView P, ImageDesc im, int img, Source src, int32_t* __restrict__ tl, ImageAcc* acc) {
+  __shared__ int32_t s_tab[GC_NLINK_LEVELS];
+  src.prepare(s_tab);
+  __syncthreads();
   const int bt = blockIdx.x;
   const int tx = bt % im.tw, ty = bt / im.tw;
   const int t = im.tile0 + bt;
@@ -117,12 +169,7 @@ k_upload(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ up,
     const int x = tx * GC_TILE + c0 + j;
     e[j] = cu[j] = cd[j] = cl[j] = cr[j] = 0;
     if (x < im.W && y < im.H) {
-      const long long i = (long long)y * im.W + x;
-      e[j] = excess[i];
-      cu[j] = y > 0 ? up[i] : 0;
-      cd[j] = y < im.H - 1 ? down[i] : 0;
-      cl[j] = x > 0 ? left[i] : 0;
-      cr[j] = x < im.W - 1 ? right[i] : 0;
+      src.pixel(im, s_tab, x, y, e[j], cu[j], cd[j], cl[j], cr[j]);
       bad |= (cu[j] | cd[j] | cl[j] | cr[j]) < 0;
     }
     h[j] = e[j] < 0 ? 0 : 1;
@@ -1233,7 +1280,50 @@ static inline int ok() { return cudaGetLastError() == cudaSuccess ? GC_OK : GC_E
 int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t* up,
                   const int32_t* down, const int32_t* left, const int32_t* right,
                   const int32_t* excess, int32_t* tl, ImageAcc* acc, cudaStream_t s) {
-  k_upload<<<im.tw * im.th, DIS_THREADS, 0, s>>>(P, im, img, up, down, left, right, excess, tl, acc);
+  const PlaneSource src{up, down, left, right, excess};
+  k_upload<<<im.tw * im.th, DIS_THREADS, 0, s>>>(P, im, img, src, tl, acc);
+  return ok();
+}
+
+int launch_upload_rgba(const PoolView& P, const ImageDesc& im, int img, const uint32_t* rgba,
+                       const int32_t* excess, const NlinkTable& tab, int32_t* tl, ImageAcc* acc,
+                       cudaStream_t s) {
+  const RgbaSource src{rgba, excess, tab};
+  k_upload<<<im.tw * im.th, DIS_THREADS, 0, s>>>(P, im, img, src, tl, acc);
+  return ok();
+}
+
+// Sum over all 4-neighbour pairs of |I_i - I_j|^2 (R, G, B), exact in 64 bits: the mean the
+// n-link scale beta comes from.
+__global__ void __launch_bounds__(256) k_dsum(const uint32_t* __restrict__ rgba, int W, int H,
+                                              unsigned long long* sum) {
+  __shared__ unsigned long long part[8];
+  unsigned long long acc = 0;
+  const long long n = (long long)W * H;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % W);
+    const uint32_t c = rgba[i];
+    if (i >= W) acc += (unsigned)rgb_dist2(c, rgba[i - W]);
+    if (x > 0) acc += (unsigned)rgb_dist2(c, rgba[i - 1]);
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long tsum = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) tsum += part[k];
+    if (tsum) atomicAdd(sum, tsum);
+  }
+}
+
+int launch_dsum(const uint32_t* rgba, int W, int H, unsigned long long* sum, int sms,
+                cudaStream_t s) {
+  const long long n = (long long)W * H;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 8LL * sms) blocks = 8LL * sms;
+  k_dsum<<<(unsigned)(blocks > 0 ? blocks : 1), 256, 0, s>>>(rgba, W, H, sum);
   return ok();
 }
 

@@ -35,7 +35,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
             and os.path.getmtime(OUT) >= max(os.path.getmtime(d) for d in deps)):
         return OUT
     cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-O3", "-I", os.path.join(ROOT, "include"), "-o", OUT + ".tmp", *srcs]
+           "-Xcompiler", "-O3", "-Xcompiler", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"), "-o", OUT + ".tmp", *srcs]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)

@@ -108,6 +108,19 @@ int gc_upload(gc_handle* h, const int32_t* up, const int32_t* down, const int32_
 int gc_upload_host(gc_handle* h, const int32_t* up, const int32_t* down, const int32_t* left,
                    const int32_t* right, const int32_t* excess, void* stream);
 
+/* Capacities built on the device from an image, as the reference builds its n-links in
+   load_tiles from the RGBA image it was given (graphcut.cl:1033-1132, GraphCut.pyx:80-116):
+   the n-link between 4-neighbours i, j is floor(50 * exp(-beta * |I_i - I_j|^2) + 0.5) with
+   |.|^2 over R, G, B and beta = 1 / (2 * mean |dI|^2) over all 4-neighbour pairs (0 for a
+   uniform image); t-links are the int32 excess plane (positive: source).  rgba: DEVICE
+   uint32 [height][width], R in bits 0-7, G 8-15, B 16-23 (alpha ignored), i.e. RGBA bytes
+   viewed as uint32 (test_GraphCut.py:21); excess: DEVICE int32 [height][width].  Replaces
+   the 20 bytes per pixel of gc_upload with 8. */
+int gc_upload_rgba(gc_handle* h, const uint32_t* rgba, const int32_t* excess, void* stream);
+/* Same with HOST arrays (copied through a device staging buffer; synchronous). */
+int gc_upload_rgba_host(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
+                        void* stream);
+
 /* Max-flow to the final cut.  Replaces GraphCut.cut (GraphCut.pyx:348-418); warm-starts
    from the current residual graph when called again after gc_edit_tlinks.  Blocks the
    calling host thread until the solve is done (it polls the active-tile count). */

@@ -95,6 +95,39 @@ def test_handles_in_caller_memory(cuda, oracle):
         GraphCut(64, 64, arena=(base + 16, need))
 
 
+@pytest.mark.parametrize("w,h,seed,kind", [(1, 1, 0, "random"), (1, 9, 1, "random"),
+                                            (9, 1, 2, "random"), (33, 31, 3, "random"),
+                                            (300, 211, 4, "synthetic"), (512, 512, 5, "synthetic"),
+                                            (70, 40, 6, "uniform")])
+def test_upload_image_builds_the_generator_planes(cuda, oracle, w, h, seed, kind):
+    """gc_upload_rgba(_host): capacities built on the device from the image equal the
+    generator's planes bit for bit, and the solve matches the oracle."""
+    import torch
+    rng = np.random.default_rng(seed)
+    if kind == "synthetic":
+        g = synth.make_graph(w, h, seed, keep_image=True)
+        img, excess = g.image, g.excess
+    else:
+        img = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+        if kind == "uniform":
+            img[:] = img[0, 0]
+        excess = rng.integers(-300, 300, (h, w)).astype(np.int32)
+    wv, wh = synth.nlinks(img)
+    planes = synth.planes_from_weights(wv, wh, excess) + (excess,)
+    f_ref, l_ref = oracle.maxflow_bk(*planes)
+    for host in (False, True):
+        with GraphCut(w, h) as gc:
+            if host:
+                gc.upload_image(img, excess)
+            else:
+                gc.upload_image(torch.from_numpy(img).cuda(), torch.from_numpy(excess).cuda())
+            for name, ref in zip(("dUp", "dDown", "dLeft", "dRight", "dExcess"), planes):
+                assert np.array_equal(getattr(gc, name).cpu().numpy(), ref), (name, host)
+            gc.cut()
+            assert gc.flow == f_ref
+            assert np.array_equal(gc.labels_host(), l_ref)
+
+
 @pytest.mark.parametrize("iters,pulses,init", [(1, 1, 0), (4, 1, 1), (64, 5, 0), (32, 1, 1)])
 def test_schedules_agree(cuda, oracle, iters, pulses, init):
     g = synth.random_graph(160, 128, 11, cap_max=80, tlink_max=120, symmetric=False)
