@@ -773,58 +773,49 @@ __device__ __forceinline__ int warp_min(int v) {
   return v;
 }
 
-// Multi-source BFS inside a tile: d[] holds the seeds (GC_HINF elsewhere); on return d[]
-// holds the exact distances given the seeds, where an edge u -> v of the residual graph
-// lets u take d(v) + 1.
-__device__ __forceinline__ void tile_bfs(int (&d)[32], uint32_t canU, uint32_t canD,
-                                         uint32_t canL, uint32_t canR, int lane) {
-  uint32_t vis = 0;
-  for (int guard = 0; guard < 2 * GC_TILE_PX + 2; ++guard) {
-    int m = GC_HINF;
-#pragma unroll
-    for (int c = 0; c < 32; ++c) if (!((vis >> c) & 1u)) m = imin(m, d[c]);
-    m = warp_min(m);
-    if (m >= GC_HINF) break;
-    uint32_t F = 0;
-#pragma unroll
-    for (int c = 0; c < 32; ++c) F |= (uint32_t)(d[c] == m) << c;
-    F &= ~vis;
-    vis |= F;
-    uint32_t Fu = __shfl_up_sync(0xffffffffu, F, 1);
-    uint32_t Fd = __shfl_down_sync(0xffffffffu, F, 1);
-    if (lane == 0) Fu = 0;
-    if (lane == 31) Fd = 0;
-    uint32_t N = ((F >> 1) & canR) | ((F << 1) & canL) | (Fu & canU) | (Fd & canD);
-    N &= ~vis;
-    if (N) {
-#pragma unroll
-      for (int c = 0; c < 32; ++c) if ((N >> c) & 1u) d[c] = imin(d[c], m + 1);
-    }
-  }
-}
-
-// Multi-source BFS inside a tile from its sink pixels only (all seeds at level 0), one level
-// per step on the row masks: N = neighbours of the frontier over residual edges, not yet
-// reached.  Lane r writes the distances of row r into `row` (GC_HINF where unreached) as the
-// pixels are reached, and gets the mask of reached pixels.  A path inside a tile has fewer
-// than 1024 steps, which bounds the loop.
-__device__ __forceinline__ uint32_t tile_bfs_from_sinks(int* row, uint32_t sink, uint32_t canU,
-                                                        uint32_t canD, uint32_t canL,
-                                                        uint32_t canR, int lane) {
+// Multi-source BFS inside a tile on the row masks, level by level (a bucketed BFS with unit
+// steps): level 0 holds the sink pixels; a tile-edge pixel with a residual edge into the
+// neighbour tile is also seeded at (neighbour height + 1).  Lane c holds the seeds of column c
+// in the top row (`top`) and the bottom row (`bot`); lane r holds the seeds of row r at column
+// 0 (`sl`) and 31 (`sr`); GC_HINF where there is none.  Level L visits the unvisited pixels
+// that are seeds of value L or neighbours, over residual edges, of level L - 1; an empty level
+// jumps to the smallest unvisited seed.  Lane r writes the distances of row r into `row`
+// (GC_HINF where unreached) and gets the mask of reached pixels.
+__device__ __forceinline__ uint32_t tile_bfs_seeded(int* row, uint32_t sink, uint32_t canU,
+                                                    uint32_t canD, uint32_t canL, uint32_t canR,
+                                                    int lane, int top, int bot, int sl, int sr) {
+  const unsigned FULL = 0xffffffffu;
 #pragma unroll
   for (int c = 0; c < 32; ++c) row[c] = GC_HINF;
-  for (uint32_t b = sink; b; b &= b - 1) row[__ffs(b) - 1] = 0;
-  uint32_t vis = sink, F = sink;
-  for (int level = 1; level < GC_TILE_PX; ++level) {
-    uint32_t Fu = __shfl_up_sync(0xffffffffu, F, 1);
-    uint32_t Fd = __shfl_down_sync(0xffffffffu, F, 1);
+  uint32_t vis = 0, F = 0;
+  int L = __any_sync(FULL, sink != 0) ? 0 : warp_min(imin(imin(top, bot), imin(sl, sr)));
+  // every step visits a pixel or jumps to an unvisited seed: at most 1024 + 128 steps
+  for (int step = 0; step < 2 * GC_TILE_PX && L < GC_HINF; ++step) {
+    uint32_t Fu = __shfl_up_sync(FULL, F, 1);
+    uint32_t Fd = __shfl_down_sync(FULL, F, 1);
     if (lane == 0) Fu = 0;
     if (lane == 31) Fd = 0;
-    const uint32_t N = (((F >> 1) & canR) | ((F << 1) & canL) | (Fu & canU) | (Fd & canD)) & ~vis;
-    if (!__any_sync(0xffffffffu, N != 0)) break;
+    const uint32_t bt = __ballot_sync(FULL, top == L);
+    const uint32_t bb = __ballot_sync(FULL, bot == L);
+    uint32_t S = (L == 0 ? sink : 0u) | (sl == L ? 1u : 0u) | (sr == L ? 0x80000000u : 0u);
+    if (lane == 0) S |= bt;
+    if (lane == 31) S |= bb;
+    const uint32_t N = (((F >> 1) & canR) | ((F << 1) & canL) | (Fu & canU) | (Fd & canD) | S) & ~vis;
     vis |= N;
     F = N;
-    for (uint32_t b = N; b; b &= b - 1) row[__ffs(b) - 1] = level;
+    for (uint32_t b = N; b; b &= b - 1) row[__ffs(b) - 1] = L;
+    if (__any_sync(FULL, F != 0)) {
+      ++L;
+      continue;
+    }
+    // the frontier is empty: the next level that still has an unvisited seed
+    const uint32_t v0 = __shfl_sync(FULL, vis, 0), v31 = __shfl_sync(FULL, vis, 31);
+    int cand = GC_HINF;
+    if (top > L && !((v0 >> lane) & 1u)) cand = imin(cand, top);
+    if (bot > L && !((v31 >> lane) & 1u)) cand = imin(cand, bot);
+    if (sl > L && !(vis & 1u)) cand = imin(cand, sl);
+    if (sr > L && !(vis >> 31)) cand = imin(cand, sr);
+    L = warp_min(cand);
   }
   return vis;
 }
@@ -1033,36 +1024,23 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
     const uint32_t* mc = P.mcan + (long long)t * 128;
     const uint32_t canU = mc[lane], canD = mc[32 + lane], canL = mc[64 + lane], canR = mc[96 + lane];
     const uint32_t sink = P.msink[(long long)t * 32 + lane];
-    uint32_t fin;
-    if (first) {
-      // no halo seeds: one level per step, bit-parallel (distances land in T directly)
-      fin = tile_bfs_from_sinks(T + lane * 33, sink, canU, canD, canL, canR, lane);
-    } else {
-      int d[32];
-#pragma unroll
-      for (int c = 0; c < 32; ++c) d[c] = ((sink >> c) & 1u) ? 0 : GC_HINF;
-      // halo seeds: an edge pixel with a residual edge into the neighbour tile
+    // seeds from the neighbour tiles' heights (frontier rounds only): an edge pixel with a
+    // residual edge into the neighbour starts at the neighbour's height + 1
+    int top = GC_HINF, bot = GC_HINF, sl = GC_HINF, sr = GC_HINF;
+    if (!first) {
+      const uint32_t cu0 = __shfl_sync(0xffffffffu, canU, 0);
+      const uint32_t cd31 = __shfl_sync(0xffffffffu, canD, 31);
       const int vu = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + lane] : GC_HINF;
       const int vd = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + lane] : GC_HINF;
       const int vl = nb.z >= 0 ? P.hgt[(long long)nb.z * GC_TILE_PX + lane * GC_TILE + 31] : GC_HINF;
       const int vr = nb.w >= 0 ? P.hgt[(long long)nb.w * GC_TILE_PX + lane * GC_TILE] : GC_HINF;
-#pragma unroll
-      for (int c = 0; c < 32; ++c) {
-        const int a = __shfl_sync(0xffffffffu, vu, c);
-        const int b = __shfl_sync(0xffffffffu, vd, c);
-        if (lane == 0 && ((canU >> c) & 1u) && a < GC_HINF) d[c] = imin(d[c], a + 1);
-        if (lane == 31 && ((canD >> c) & 1u) && b < GC_HINF) d[c] = imin(d[c], b + 1);
-      }
-      if ((canL & 1u) && vl < GC_HINF) d[0] = imin(d[0], vl + 1);
-      if ((canR >> 31) && vr < GC_HINF) d[31] = imin(d[31], vr + 1);
-      tile_bfs(d, canU, canD, canL, canR, lane);
-      // transpose through shared memory and write the distances back (coalesced rows)
-#pragma unroll
-      for (int c = 0; c < 32; ++c) T[lane * 33 + c] = d[c];
-      fin = 0;
-#pragma unroll
-      for (int c = 0; c < 32; ++c) fin |= (uint32_t)(d[c] < GC_HINF) << c;
+      if (((cu0 >> lane) & 1u) && vu < GC_HINF) top = vu + 1;
+      if (((cd31 >> lane) & 1u) && vd < GC_HINF) bot = vd + 1;
+      if ((canL & 1u) && vl < GC_HINF) sl = vl + 1;
+      if ((canR >> 31) && vr < GC_HINF) sr = vr + 1;
     }
+    const uint32_t fin = tile_bfs_seeded(T + lane * 33, sink, canU, canD, canL, canR, lane, top,
+                                         bot, sl, sr);
     __syncwarp();
     int chU = 0, chD = 0, chL = 0, chR = 0;
     for (int rr = 0; rr < 32; ++rr) {
