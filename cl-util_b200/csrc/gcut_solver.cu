@@ -288,6 +288,12 @@ struct DisSmem {
   int32_t fl[GC_TILE * 8];  // flow pushed left by the first pixel of each 4-pixel strip
   int32_t fr[GC_TILE * 8];  // flow pushed right by the last pixel of each strip
   int32_t hu[GC_TILE], hd[GC_TILE], hl[GC_TILE], hr[GC_TILE];  // halo heights
+  // launch-start values of the tile-edge pixels that also receive atomics from the
+  // neighbouring tiles (written back as deltas against these)
+  int32_t eo_top[GC_TILE], eo_bot[GC_TILE], eo_left[GC_TILE], eo_right[GC_TILE];
+  int32_t cu_top[GC_TILE], cd_bot[GC_TILE], cl_left[GC_TILE], cr_right[GC_TILE];
+  // flow leaving the tile, per edge pixel, delivered at the end of the tile
+  int32_t xu[GC_TILE], xd[GC_TILE], xl[GC_TILE], xr[GC_TILE];
 };
 
 __device__ __forceinline__ void worklist_add(const PoolView& P, int nxt, int t) {
@@ -351,8 +357,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, unsigned parity,
 
 constexpr int DIS_PLANES = 6;                                  // excess, height, 4 residuals
 constexpr unsigned DIS_TILE_BYTES = DIS_PLANES * GC_TILE_PX * 4;  // 24 KiB
-// dynamic shared memory: two tile buffers + the per-round exchange arrays
-constexpr size_t DIS_DYN_SMEM = 2 * (size_t)DIS_TILE_BYTES + sizeof(DisSmem);
+// dynamic shared memory: the tile staging buffer + the per-round exchange arrays
+constexpr size_t DIS_DYN_SMEM = (size_t)DIS_TILE_BYTES + sizeof(DisSmem);
 
 __device__ __forceinline__ const int32_t* dis_plane(const PoolView& P, int k) {
   return k == 0 ? P.exc : k == 1 ? P.hgt : P.cap[k - 2];
@@ -367,20 +373,19 @@ __device__ __forceinline__ void dis_prefetch(const PoolView& P, int t, int32_t* 
     bulk_g2s(buf + k * GC_TILE_PX, dis_plane(P, k) + (long long)t * GC_TILE_PX, GC_TILE_PX * 4, mbar);
 }
 
-__global__ void __launch_bounds__(DIS_THREADS, 3)
+__global__ void __launch_bounds__(DIS_THREADS, 4)
 k_discharge(PoolView P, int iters) {
   extern __shared__ __align__(128) int32_t dsm[];
-  int32_t* const bufs = dsm;                                   // [2][6][1024]
-  DisSmem& S = *reinterpret_cast<DisSmem*>(dsm + 2 * DIS_PLANES * GC_TILE_PX);
-  __shared__ uint64_t mbar[2];
+  int32_t* const buf = dsm;                                    // [6][1024] staging
+  DisSmem& S = *reinterpret_cast<DisSmem*>(dsm + DIS_PLANES * GC_TILE_PX);
+  __shared__ uint64_t mbar;
   __shared__ int s_cur, s_n;
   const int tid = threadIdx.x;
   const int r = tid >> 3, q = tid & 7, c0 = q * 4;
   if (tid == 0) {
     s_cur = *((volatile int32_t*)&P.ctl[CTL_PULSE]) & 1;
     s_n = *((volatile int32_t*)&P.qcount[s_cur]);
-    mbar_init(&mbar[0], 1);
-    mbar_init(&mbar[1], 1);
+    mbar_init(&mbar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -395,26 +400,24 @@ k_discharge(PoolView P, int iters) {
   auto entry = [&](int li) { return P.queue[cur][li]; };
   const bool erow = (r == 0) || (r == 31);
   const int pix = r * GC_TILE + c0;
-  unsigned phase[2] = {0, 0};
-  int it_local = 0;
-  bool failed = false;
-  if (tid == 0 && (int)blockIdx.x < n) dis_prefetch(P, entry(blockIdx.x), bufs, &mbar[0]);
-  for (int li = blockIdx.x; li < n; li += gridDim.x, ++it_local) {
-    const int b = it_local & 1;
-    int32_t* const buf = bufs + b * DIS_PLANES * GC_TILE_PX;
+  unsigned phase = 0;
+  bool failed = false, pending = false;
+  if (tid == 0 && (int)blockIdx.x < n) dis_prefetch(P, entry(blockIdx.x), buf, &mbar);
+  for (int li = blockIdx.x; li < n; li += gridDim.x) {
     const int t = entry(li);
-    // prefetch the next tile of this CTA into the other buffer (read two tiles ago)
-    if (tid == 0 && li + (int)gridDim.x < n)
-      dis_prefetch(P, entry(li + gridDim.x), bufs + (b ^ 1) * DIS_PLANES * GC_TILE_PX, &mbar[b ^ 1]);
     const int4 nb = P.nbr[t];
     if (tid < 32) S.hu[tid] = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + tid] : GC_HINF;
     else if (tid < 64) S.hd[tid - 32] = nb.y >= 0 ? P.hgt[(long long)nb.y * GC_TILE_PX + (tid - 32)] : GC_HINF;
     else if (tid < 96) S.hl[tid - 64] = nb.z >= 0 ? P.hgt[(long long)nb.z * GC_TILE_PX + (tid - 64) * GC_TILE + 31] : GC_HINF;
     else if (tid < 128) S.hr[tid - 96] = nb.w >= 0 ? P.hgt[(long long)nb.w * GC_TILE_PX + (tid - 96) * GC_TILE] : GC_HINF;
+    else if (tid < 160) S.xu[tid - 128] = 0;
+    else if (tid < 192) S.xd[tid - 160] = 0;
+    else if (tid < 224) S.xl[tid - 192] = 0;
+    else S.xr[tid - 224] = 0;
     if (tid == 0) P.inq[cur][t] = 0;
-    const bool ok = mbar_wait(&mbar[b], phase[b]);
-    if (__syncthreads_or(!ok)) { failed = true; break; }  // block-uniform decision
-    phase[b] ^= 1u;
+    const bool ok = mbar_wait(&mbar, phase);
+    if (__syncthreads_or(!ok)) { failed = true; pending = true; break; }  // block-uniform
+    phase ^= 1u;
     int e[4], h[4], cu[4], cd[4], cl[4], cr[4];
     {
       int4 v = lds4(buf + 0 * GC_TILE_PX + pix); e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w;
@@ -424,6 +427,17 @@ k_discharge(PoolView P, int iters) {
       v = lds4(buf + 4 * GC_TILE_PX + pix); cl[0] = v.x; cl[1] = v.y; cl[2] = v.z; cl[3] = v.w;
       v = lds4(buf + 5 * GC_TILE_PX + pix); cr[0] = v.x; cr[1] = v.y; cr[2] = v.z; cr[3] = v.w;
     }
+    // keep the launch-start values the write-back needs (tile-edge pixels only)
+    if (r == 0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) { S.eo_top[c0 + j] = e[j]; S.cu_top[c0 + j] = cu[j]; }
+    }
+    if (r == 31) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) { S.eo_bot[c0 + j] = e[j]; S.cd_bot[c0 + j] = cd[j]; }
+    }
+    if (q == 0) { S.eo_left[r] = e[0]; S.cl_left[r] = cl[0]; }
+    if (q == 7) { S.eo_right[r] = e[3]; S.cr_right[r] = cr[3]; }
     // height cap of tile-edge pixels for this launch (interior: none)
     int hcap[4];
 #pragma unroll
@@ -433,8 +447,9 @@ k_discharge(PoolView P, int iters) {
       hcap[j] = edge ? (h[j] >= GC_HINF - 2 ? GC_HINF : h[j] + 2) : GC_HINF;
     }
     sts4(S.hs + pix, h[0], h[1], h[2], h[3]);
-    int xu[4] = {0, 0, 0, 0}, xd[4] = {0, 0, 0, 0}, xl = 0, xr = 0;  // cross-tile flow
-    __syncthreads();
+    __syncthreads();   // every thread has its values in registers: the buffer is free
+    // prefetch this CTA's next tile into the buffer while this one is worked on
+    if (tid == 0 && li + (int)gridDim.x < n) dis_prefetch(P, entry(li + gridDim.x), buf, &mbar);
 
     for (int it = 0; it < iters; ++it) {
       // neighbour heights (fixed during the push phase)
@@ -448,33 +463,43 @@ k_discharge(PoolView P, int iters) {
       hnr[0] = h[1]; hnr[1] = h[2]; hnr[2] = h[3];
       hnr[3] = c0 < 28 ? S.hs[pix + 4] : S.hr[r];
 
-      // push phase
+      // push phase.  `rem` marks pixels that still hold excess after pushing: every
+      // admissible edge of theirs is then saturated, and inflow only adds residual towards
+      // higher neighbours, so they relabel without another admissibility test.
       int ou[4], od[4], ol[4], orr[4];
       int changed = 0;
+      unsigned rem = 0;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        ou[j] = od[j] = ol[j] = orr[j] = 0;
-        int ej = e[j];
-        if (ej > 0 && h[j] < GC_HINF) {
-          if (cd[j] > 0 && h[j] == hnd[j] + 1) { int f = imin(ej, cd[j]); ej -= f; cd[j] -= f; od[j] = f; }
-          if (ej > 0 && cu[j] > 0 && h[j] == hnu[j] + 1) { int f = imin(ej, cu[j]); ej -= f; cu[j] -= f; ou[j] = f; }
-          if (ej > 0 && cr[j] > 0 && h[j] == hnr[j] + 1) { int f = imin(ej, cr[j]); ej -= f; cr[j] -= f; orr[j] = f; }
-          if (ej > 0 && cl[j] > 0 && h[j] == hnl[j] + 1) { int f = imin(ej, cl[j]); ej -= f; cl[j] -= f; ol[j] = f; }
-          changed |= ej != e[j];
-          e[j] = ej;
+      for (int j = 0; j < 4; ++j) ou[j] = od[j] = ol[j] = orr[j] = 0;
+      const bool any_act = (e[0] > 0 && h[0] < GC_HINF) || (e[1] > 0 && h[1] < GC_HINF) ||
+                           (e[2] > 0 && h[2] < GC_HINF) || (e[3] > 0 && h[3] < GC_HINF);
+      if (__any_sync(0xffffffffu, any_act)) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          int ej = e[j];
+          if (ej > 0 && h[j] < GC_HINF) {
+            const int hm1 = h[j] - 1;
+            if (cd[j] > 0 && hnd[j] == hm1) { const int f = imin(ej, cd[j]); ej -= f; cd[j] -= f; od[j] = f; }
+            if (ej > 0 && cu[j] > 0 && hnu[j] == hm1) { const int f = imin(ej, cu[j]); ej -= f; cu[j] -= f; ou[j] = f; }
+            if (ej > 0 && cr[j] > 0 && hnr[j] == hm1) { const int f = imin(ej, cr[j]); ej -= f; cr[j] -= f; orr[j] = f; }
+            if (ej > 0 && cl[j] > 0 && hnl[j] == hm1) { const int f = imin(ej, cl[j]); ej -= f; cl[j] -= f; ol[j] = f; }
+            changed |= ej != e[j];
+            rem |= (ej > 0 ? 1u : 0u) << j;
+            e[j] = ej;
+          }
         }
       }
       // flow leaving the tile is delivered at the end of the tile
       if (r == 0) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) { xu[j] += ou[j]; ou[j] = 0; }
+        for (int j = 0; j < 4; ++j) { S.xu[c0 + j] += ou[j]; ou[j] = 0; }
       }
       if (r == 31) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) { xd[j] += od[j]; od[j] = 0; }
+        for (int j = 0; j < 4; ++j) { S.xd[c0 + j] += od[j]; od[j] = 0; }
       }
-      if (q == 0) { xl += ol[0]; ol[0] = 0; }
-      if (q == 7) { xr += orr[3]; orr[3] = 0; }
+      if (q == 0) { S.xl[r] += ol[0]; ol[0] = 0; }
+      if (q == 7) { S.xr[r] += orr[3]; orr[3] = 0; }
       sts4(S.fu + pix, ou[0], ou[1], ou[2], ou[3]);
       sts4(S.fd + pix, od[0], od[1], od[2], od[3]);
       S.fl[r * 8 + q] = ol[0];
@@ -500,21 +525,26 @@ k_discharge(PoolView P, int iters) {
         }
       }
       // relabel phase (Jacobi; tile-edge pixels are capped at hcap)
-      int nh[4];
+      int nh[4] = {h[0], h[1], h[2], h[3]};
+      const bool any_need = (e[0] > 0 && h[0] < hcap[0]) || (e[1] > 0 && h[1] < hcap[1]) ||
+                            (e[2] > 0 && h[2] < hcap[2]) || (e[3] > 0 && h[3] < hcap[3]);
+      if (__any_sync(0xffffffffu, any_need)) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        nh[j] = h[j];
-        if (e[j] > 0 && h[j] < hcap[j]) {
-          const bool adm = (cd[j] > 0 && h[j] == hnd[j] + 1) || (cu[j] > 0 && h[j] == hnu[j] + 1) ||
-                           (cr[j] > 0 && h[j] == hnr[j] + 1) || (cl[j] > 0 && h[j] == hnl[j] + 1);
-          if (!adm) {
-            int m = GC_HINF;
-            if (cd[j] > 0) m = imin(m, hnd[j] + 1);
-            if (cu[j] > 0) m = imin(m, hnu[j] + 1);
-            if (cr[j] > 0) m = imin(m, hnr[j] + 1);
-            if (cl[j] > 0) m = imin(m, hnl[j] + 1);
-            nh[j] = imin(imin(m, GC_HINF), hcap[j]);
-            changed |= nh[j] != h[j];
+        for (int j = 0; j < 4; ++j) {
+          if (e[j] > 0 && h[j] < hcap[j]) {
+            const int hm1 = h[j] - 1;
+            const bool adm = !((rem >> j) & 1u) &&
+                             ((cd[j] > 0 && hnd[j] == hm1) || (cu[j] > 0 && hnu[j] == hm1) ||
+                              (cr[j] > 0 && hnr[j] == hm1) || (cl[j] > 0 && hnl[j] == hm1));
+            if (!adm) {
+              int m = GC_HINF;
+              if (cd[j] > 0) m = imin(m, hnd[j] + 1);
+              if (cu[j] > 0) m = imin(m, hnu[j] + 1);
+              if (cr[j] > 0) m = imin(m, hnr[j] + 1);
+              if (cl[j] > 0) m = imin(m, hnl[j] + 1);
+              nh[j] = imin(imin(m, GC_HINF), hcap[j]);
+              changed |= nh[j] != h[j];
+            }
           }
         }
       }
@@ -528,18 +558,17 @@ k_discharge(PoolView P, int iters) {
 
     // write back: interior values are owned by this CTA; tile-edge excess and the
     // outward residual of edge pixels also receive atomics from neighbouring tiles, so
-    // they are written as deltas against the values loaded (still in the tile buffer).
+    // they are written as deltas against their launch-start values.
     const long long off = (long long)t * GC_TILE_PX + pix;
     if (!erow && q > 0 && q < 7) {
       *(int4*)(P.exc + off) = make_int4(e[0], e[1], e[2], e[3]);
     } else {
-      const int4 e0 = lds4(buf + 0 * GC_TILE_PX + pix);
-      const int e0a[4] = {e0.x, e0.y, e0.z, e0.w};
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const int c = c0 + j;
         if (erow || c == 0 || c == 31) {
-          if (e[j] != e0a[j]) atomicAdd(P.exc + off + j, e[j] - e0a[j]);
+          const int e0 = r == 0 ? S.eo_top[c] : r == 31 ? S.eo_bot[c] : c == 0 ? S.eo_left[r] : S.eo_right[r];
+          if (e[j] != e0) atomicAdd(P.exc + off + j, e[j] - e0);
         } else {
           P.exc[off + j] = e[j];
         }
@@ -547,30 +576,32 @@ k_discharge(PoolView P, int iters) {
     }
     *(int4*)(P.hgt + off) = make_int4(h[0], h[1], h[2], h[3]);
     if (r == 0) {
-      const int4 o = lds4(buf + 2 * GC_TILE_PX + pix);
-      const int oa[4] = {o.x, o.y, o.z, o.w};
 #pragma unroll
-      for (int j = 0; j < 4; ++j) if (cu[j] != oa[j]) atomicAdd(P.cap[DUP] + off + j, cu[j] - oa[j]);
+      for (int j = 0; j < 4; ++j) {
+        const int o0 = S.cu_top[c0 + j];
+        if (cu[j] != o0) atomicAdd(P.cap[DUP] + off + j, cu[j] - o0);
+      }
     } else {
       *(int4*)(P.cap[DUP] + off) = make_int4(cu[0], cu[1], cu[2], cu[3]);
     }
     if (r == 31) {
-      const int4 o = lds4(buf + 3 * GC_TILE_PX + pix);
-      const int oa[4] = {o.x, o.y, o.z, o.w};
 #pragma unroll
-      for (int j = 0; j < 4; ++j) if (cd[j] != oa[j]) atomicAdd(P.cap[DDOWN] + off + j, cd[j] - oa[j]);
+      for (int j = 0; j < 4; ++j) {
+        const int o0 = S.cd_bot[c0 + j];
+        if (cd[j] != o0) atomicAdd(P.cap[DDOWN] + off + j, cd[j] - o0);
+      }
     } else {
       *(int4*)(P.cap[DDOWN] + off) = make_int4(cd[0], cd[1], cd[2], cd[3]);
     }
     if (q == 0) {
-      const int cl0 = buf[4 * GC_TILE_PX + pix];
+      const int cl0 = S.cl_left[r];
       if (cl[0] != cl0) atomicAdd(P.cap[DLEFT] + off, cl[0] - cl0);
       P.cap[DLEFT][off + 1] = cl[1]; P.cap[DLEFT][off + 2] = cl[2]; P.cap[DLEFT][off + 3] = cl[3];
     } else {
       *(int4*)(P.cap[DLEFT] + off) = make_int4(cl[0], cl[1], cl[2], cl[3]);
     }
     if (q == 7) {
-      const int cr0 = buf[5 * GC_TILE_PX + pix + 3];
+      const int cr0 = S.cr_right[r];
       if (cr[3] != cr0) atomicAdd(P.cap[DRIGHT] + off + 3, cr[3] - cr0);
       P.cap[DRIGHT][off] = cr[0]; P.cap[DRIGHT][off + 1] = cr[1]; P.cap[DRIGHT][off + 2] = cr[2];
     } else {
@@ -580,25 +611,37 @@ k_discharge(PoolView P, int iters) {
     int sent_u = 0, sent_d = 0, sent_l = 0, sent_r = 0;
     if (r == 0 && nb.x >= 0) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) if (xu[j]) {
-        const long long o = (long long)nb.x * GC_TILE_PX + 31 * GC_TILE + c0 + j;
-        atomicAdd(P.exc + o, xu[j]); atomicAdd(P.cap[DDOWN] + o, xu[j]); sent_u = 1;
+      for (int j = 0; j < 4; ++j) {
+        const int x = S.xu[c0 + j];
+        if (x) {
+          const long long o = (long long)nb.x * GC_TILE_PX + 31 * GC_TILE + c0 + j;
+          atomicAdd(P.exc + o, x); atomicAdd(P.cap[DDOWN] + o, x); sent_u = 1;
+        }
       }
     }
     if (r == 31 && nb.y >= 0) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) if (xd[j]) {
-        const long long o = (long long)nb.y * GC_TILE_PX + c0 + j;
-        atomicAdd(P.exc + o, xd[j]); atomicAdd(P.cap[DUP] + o, xd[j]); sent_d = 1;
+      for (int j = 0; j < 4; ++j) {
+        const int x = S.xd[c0 + j];
+        if (x) {
+          const long long o = (long long)nb.y * GC_TILE_PX + c0 + j;
+          atomicAdd(P.exc + o, x); atomicAdd(P.cap[DUP] + o, x); sent_d = 1;
+        }
       }
     }
-    if (q == 0 && xl && nb.z >= 0) {
-      const long long o = (long long)nb.z * GC_TILE_PX + r * GC_TILE + 31;
-      atomicAdd(P.exc + o, xl); atomicAdd(P.cap[DRIGHT] + o, xl); sent_l = 1;
+    if (q == 0 && nb.z >= 0) {
+      const int x = S.xl[r];
+      if (x) {
+        const long long o = (long long)nb.z * GC_TILE_PX + r * GC_TILE + 31;
+        atomicAdd(P.exc + o, x); atomicAdd(P.cap[DRIGHT] + o, x); sent_l = 1;
+      }
     }
-    if (q == 7 && xr && nb.w >= 0) {
-      const long long o = (long long)nb.w * GC_TILE_PX + r * GC_TILE;
-      atomicAdd(P.exc + o, xr); atomicAdd(P.cap[DLEFT] + o, xr); sent_r = 1;
+    if (q == 7 && nb.w >= 0) {
+      const int x = S.xr[r];
+      if (x) {
+        const long long o = (long long)nb.w * GC_TILE_PX + r * GC_TILE;
+        atomicAdd(P.exc + o, x); atomicAdd(P.cap[DLEFT] + o, x); sent_r = 1;
+      }
     }
     int act = 0, act_int = 0;
 #pragma unroll
@@ -624,11 +667,10 @@ k_discharge(PoolView P, int iters) {
     }
   }
   if (failed) {
-    // a bulk copy did not complete in time: record it, let our copies drain, stop
+    // a bulk copy did not complete in time: record it, let our copy drain, stop
     if (tid == 0) {
       atomicExch(&P.ctl[CTL_ERR], 3);
-      mbar_wait(&mbar[0], phase[0], 5 * GC_COPY_WAIT_NS);
-      mbar_wait(&mbar[1], phase[1], 5 * GC_COPY_WAIT_NS);
+      if (pending) mbar_wait(&mbar, phase, 5 * GC_COPY_WAIT_NS);
     }
     __syncthreads();
   }
