@@ -231,6 +231,7 @@ def main():
 
     import synth
     from GraphCut import GraphCut
+    from sharding import reduce_max
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -288,11 +289,7 @@ def main():
                 launches += gc.stats()["launches"] + 2  # + upload + labels
         torch.cuda.synchronize()
         barrier()
-        total_ms = sum(step_ms)
-        if world > 1:
-            t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
+        total_ms = reduce_max(sum(step_ms), torch.device("cuda", local))
         mpix_all = world * args.steps * W * H / 1e6
         value = mpix_all / (total_ms / 1000)
 
@@ -341,11 +338,7 @@ def main():
                 out_host[:] = gc.labels_host(stream=stream)
                 _ = gc.flow
                 e_ms.append(1000 * (time.perf_counter() - t0))
-            e_tot = sum(e_ms)
-            if world > 1:
-                t = torch.tensor([e_tot], dtype=torch.float64, device="cuda")
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                e_tot = float(t.item())
+            e_tot = reduce_max(sum(e_ms), torch.device("cuda", local))
             e2e = {"value": mpix_all / (e_tot / 1000), "unit": UNIT,
                    "h2d_bytes_per_step": 2 * 4 * W * H, "d2h_bytes_per_step": W * H + 8,
                    "ms_per_step": e_tot / args.steps, "parity": e2e_parity,
@@ -453,22 +446,35 @@ def _percentile(xs, p):
 def run_batch(args):
     """Config 2: `--batch` (64) independent grids, sides drawn from {256, 384, ..., 1536},
     solved together in one tile pool (one CUDA-graph launch per solve over a shared tile
-    worklist), against the same grids solved one at a time by the single-grid solver."""
+    worklist), against the same grids solved one at a time by the single-grid solver.
+    Under torchrun each rank takes its LPT share of the grids (by pixel count); the job's
+    time is the slowest rank's."""
     import torch
+    import torch.distributed as dist
 
     import synth
     from GraphCut import GraphCut
     from GraphCutBatch import GraphCutBatch
     from oracle import oracle as O
-    shapes = synth.batch_shapes(args.batch, seed=2)
-    graphs = synth.make_graphs([(w, h, 10_000 + i) for i, (w, h) in enumerate(shapes)])
-    torch.cuda.set_device(0)
+    from sharding import lpt_assign, reduce_max, reduce_min
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    all_shapes = synth.batch_shapes(args.batch, seed=2)
+    mine = lpt_assign([w * h for w, h in all_shapes], world)[rank]
+    shapes = [all_shapes[i] for i in mine]
+    graphs = synth.make_graphs([(all_shapes[i][0], all_shapes[i][1], 10_000 + i) for i in mine])
     planes = [[torch.from_numpy(p).cuda() for p in g.planes()] for g in graphs]
-    mpix = sum(w * h for w, h in shapes) / 1e6
+    mpix = sum(w * h for w, h in all_shapes) / 1e6
     stream = torch.cuda.Stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     labels = [torch.empty((h, w), dtype=torch.uint8, device="cuda") for w, h in shapes]
-    b = GraphCutBatch(shapes)
+    b = GraphCutBatch(shapes, device=local)
 
     def step_batch():
         for i, pl in enumerate(planes):
@@ -477,7 +483,7 @@ def run_batch(args):
         for i in range(len(shapes)):
             b.labels(i, out=labels[i], stream=stream)
 
-    singles = [GraphCut(w, h) for w, h in shapes]
+    singles = [GraphCut(w, h, device=local) for w, h in shapes]
 
     def step_single():
         for i, (gc, pl) in enumerate(zip(singles, planes)):
@@ -511,26 +517,37 @@ def run_batch(args):
         for i, g in enumerate(graphs):
             f_ref, l_ref = O.maxflow_bk(*g.planes())
             parity &= bl[i][0] == f_ref and np.array_equal(bl[i][1], l_ref)
-        clocks = ClockSampler(0)
+        if world > 1:
+            dist.barrier()
+        clocks = ClockSampler(local)
         with clocks:
             ms_batch = timed(step_batch)
         ms_single = timed(step_single)
         st = b.stats()
+    dev = torch.device("cuda", local)
+    ms_batch = reduce_max(ms_batch, dev)     # the job takes as long as its slowest rank
+    ms_single = reduce_max(ms_single, dev)
+    parity = reduce_min(1.0 if parity else 0.0, dev) > 0
     line = {
         "metric": METRIC + " (batched)", "value": mpix / (ms_batch / 1000), "unit": UNIT,
-        "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_batch,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_batch,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic",
-        "config": {"workload": f"{len(shapes)} independent grids, sides uniform in "
+        "config": {"workload": f"{len(all_shapes)} independent grids, sides uniform in "
                                "{256,384,...,1536}, built as the synthetic generator, seeds "
-                               "10000+i; one tile pool, one CUDA-graph solve",
-                   "total_mpix": mpix, "l2": "flushed between steps"},
+                               "10000+i; one tile pool per rank, one CUDA-graph solve",
+                   "total_mpix": mpix, "l2": "flushed between steps",
+                   "parallelism": f"LPT split of the grids over {world} rank(s)"},
         "single_solver_one_at_a_time": {"value": mpix / (ms_single / 1000), "unit": UNIT,
                                          "ms_per_step": ms_single},
         "batch_over_single": ms_single / ms_batch,
         "parity": bool(parity), "solve_stats": st, "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    b.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def run_strokes(args):
