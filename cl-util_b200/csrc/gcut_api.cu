@@ -787,6 +787,7 @@ int device_scan_state(ScanState* out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e) return cuda_fail(e, "cudaGetDevice");
+  preload_kernels();
   std::lock_guard<std::mutex> lock(g_scan_mu);
   auto it = g_scan.find(dev);
   if (it == g_scan.end()) {

@@ -96,6 +96,10 @@ int launch_edit(const PoolView& P, const ImageDesc& im, int img, const int32_t* 
 int launch_stroke(const PoolView& P, const ImageDesc& im, int img, const int32_t* pts_dev,
                   const int32_t* pts_host, int npts, int radius, int32_t value, int32_t* tl,
                   ImageAcc* acc, cudaStream_t s);
+// Loads every kernel of the library on the current device (once per device; called by the
+// first handle creation and the first stand-alone primitive on a device).
+void preload_kernels();
+void preload_scan_kernels();
 int occupancy_discharge(int device);
 int occupancy_warps(int device);
 

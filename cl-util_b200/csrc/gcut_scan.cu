@@ -138,6 +138,13 @@ __global__ void k_fill(int32_t* p, int n, int32_t v) {
   if (i < n) p[i] = v;
 }
 
+void preload_scan_kernels() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, (const void*)k_scan);
+  cudaFuncGetAttributes(&a, (const void*)k_increment_logical);
+  cudaFuncGetAttributes(&a, (const void*)k_fill);
+}
+
 int scan_chunks(int n) { return n <= 0 ? 1 : (n + SCAN_CHUNK - 1) / SCAN_CHUNK; }
 
 int launch_scan(int mode, const int32_t* in, const int32_t* in2, int32_t* clear,

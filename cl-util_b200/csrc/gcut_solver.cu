@@ -1461,6 +1461,31 @@ int launch_stroke(const PoolView& P, const ImageDesc& im, int img, const int32_t
   return ok();
 }
 
+// Loads every kernel of the library on the current device.  With lazy module loading (the
+// CUDA default) a kernel is loaded at its first launch or graph instantiation; doing it
+// here, once per device under a lock, keeps that loading away from threads that solve on
+// several streams at once.
+void preload_kernels() {
+  static std::mutex mu;
+  static std::unordered_map<int, bool> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return;
+  cudaFuncAttributes a;
+  const void* kernels[] = {
+      (const void*)k_upload<PlaneSource>, (const void*)k_upload<RgbaSource>, (const void*)k_dsum,
+      (const void*)k_masks, (const void*)k_discharge, (const void*)k_edge_relabel_build,
+      (const void*)k_bfs_round, (const void*)k_flood_round, (const void*)k_ctl_begin,
+      (const void*)k_mark_images, (const void*)k_mark_cycle, (const void*)k_ctl_cycle,
+      (const void*)k_acc_reset, (const void*)k_labels_out, (const void*)k_labels_packed,
+      (const void*)k_state_out, (const void*)k_edit, (const void*)k_stroke};
+  for (const void* k : kernels) cudaFuncGetAttributes(&a, k);
+  preload_scan_kernels();
+  cudaGetLastError();
+  done[dev] = true;
+}
+
 namespace {
 // Launch geometry per device, set up once: the dynamic shared memory opt-in of k_discharge
 // changes the function's state, so it is not repeated while other threads launch or
@@ -1473,6 +1498,7 @@ Geometry device_geometry(int device) {
   std::lock_guard<std::mutex> lock(g_geom_mu);
   auto it = g_geom.find(device);
   if (it != g_geom.end()) return it->second;
+  preload_kernels();
   int per_dis = 0, per_bfs = 0, sms = 0;
   cudaFuncSetAttribute(k_discharge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DIS_DYN_SMEM);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_dis, k_discharge, DIS_THREADS, DIS_DYN_SMEM);
