@@ -82,8 +82,6 @@ int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc
 int launch_mark_cycle(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
                       int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s);
 int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s);
-int launch_mark_images(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
-                       cudaStream_t s);
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s);
 int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s);

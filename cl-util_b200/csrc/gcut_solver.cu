@@ -948,25 +948,10 @@ __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc
   }
 }
 
-// After the active-tile compaction: stamp the images that still have active tiles, so the
-// next cycle's global relabel covers only them (stamp = cycles + 1 + bump, where bump = 1
-// when k_ctl_cycle will count this check as a finished cycle).
-__global__ void k_mark_images(PoolView P, const int32_t* list, const int32_t* count, int bump) {
-  int n = *((volatile const int32_t*)count);
-  if (n < 0 || n > P.nt) {   // self-check: a list holds each tile at most once
-    if (blockIdx.x == 0 && threadIdx.x == 0) record_bad(P, 3, n);
-    n = 0;
-  }
-  const int stamp = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1 + bump;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int img = P.img_of[list[i]];
-    if ((unsigned)img < (unsigned)P.nimg) P.img_live[img] = stamp;
-    else record_bad(P, 4, img);
-  }
-}
-
-// The two kernels above in one launch: every CTA stamps images of the list, then the last CTA
-// applies the cycle check (it reads the cycle count after every stamp was taken).
+// After the active-tile compaction: every CTA stamps the images of the list entries it reads,
+// so the next cycle's global relabel covers only images that still have active tiles (stamp =
+// cycles + 1 + bump, where bump = 1 when this check counts as a finished cycle); then the last
+// CTA applies the cycle check (it reads the cycle count after every stamp was taken).
 __global__ void k_mark_cycle(PoolView P, const int32_t* list, const int32_t* count, int bump,
                              int count_cycle, cudaGraphConditionalHandle h) {
   __shared__ int s_n, s_stamp;
@@ -1393,12 +1378,6 @@ int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc
   return ok();
 }
 
-int launch_mark_images(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
-                       cudaStream_t s) {
-  k_mark_images<<<32, 256, 0, s>>>(P, list, count, bump);
-  return ok();
-}
-
 int launch_mark_cycle(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
                       int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s) {
   k_mark_cycle<<<16, 256, 0, s>>>(P, list, count, bump, count_cycle, h);
@@ -1477,7 +1456,7 @@ void preload_kernels() {
       (const void*)k_upload<PlaneSource>, (const void*)k_upload<RgbaSource>, (const void*)k_dsum,
       (const void*)k_masks, (const void*)k_discharge, (const void*)k_edge_relabel_build,
       (const void*)k_bfs_round, (const void*)k_flood_round, (const void*)k_ctl_begin,
-      (const void*)k_mark_images, (const void*)k_mark_cycle, (const void*)k_ctl_cycle,
+      (const void*)k_mark_cycle, (const void*)k_ctl_cycle,
       (const void*)k_acc_reset, (const void*)k_labels_out, (const void*)k_labels_packed,
       (const void*)k_state_out, (const void*)k_edit, (const void*)k_stroke};
   for (const void* k : kernels) cudaFuncGetAttributes(&a, k);
