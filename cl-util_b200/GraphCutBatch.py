@@ -19,8 +19,8 @@ from _gcut import check, lib, ptr, stream_handle
 
 
 # schedule tuned by autotune.py on the 64-grid mixed batch (sides 256..1536)
-BATCH_DISCHARGE_ITERS = 3
-BATCH_PULSES = 4
+BATCH_DISCHARGE_ITERS = 4
+BATCH_PULSES = 2
 
 
 class GraphCutBatch:
