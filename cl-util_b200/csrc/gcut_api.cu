@@ -506,8 +506,7 @@ struct Pool {
     RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, s));
     int n = 0;
     if (relabel_first) RK(global_relabel(s));
-    RK(compact(P.tact, nullptr, s));
-    RK(launch_mark_cycle(P, list, counts, 0, 0, 0, s));
+    RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 0, 0, 0, s); }));
     bool go = true;
     if (relabel_first) {
       RK(read_count(s, &n));
@@ -526,8 +525,7 @@ struct Pool {
         stats.pulses++;
       }
       RK(global_relabel(s, 2));
-      RK(compact(P.tact, nullptr, s));
-      RK(launch_mark_cycle(P, list, counts, 1, 1, 0, s));
+      RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 1, 1, 0, s); }));
       RK(read_count(s, &n));
       go = n > 0;
     }
@@ -603,8 +601,7 @@ struct Pool {
       RK(capture(b0, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, h0, grid_warps, cs); }));
     }
     RK(capture(g, L, [&](cudaStream_t cs) {
-      RK(launch_scan(GC_SCAN_MODE_COMPACT, P.tact, nullptr, nullptr, nullptr, list, counts, nt, 0, 0, 0, 0, 0, scan.st, cs));
-      return launch_mark_cycle(P, list, counts, 0, 0, hmain, cs);
+      return launch_active_list(P, scan.st, list, counts, 0, 0, hmain, cs);
     }));
     cudaGraph_t bm;
     RK(add_while(g, L, hmain, &bm));
@@ -623,8 +620,7 @@ struct Pool {
       std::vector<cudaGraphNode_t> Lb;
       RK(capture(bb, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, hb, grid_warps, cs); }));
       RK(capture(bm, Lm, [&](cudaStream_t cs) {
-        RK(launch_scan(GC_SCAN_MODE_COMPACT, P.tact, nullptr, nullptr, nullptr, list, counts, nt, 0, 0, 0, 0, 0, scan.st, cs));
-        return launch_mark_cycle(P, list, counts, 1, 1, hmain, cs);
+        return launch_active_list(P, scan.st, list, counts, 1, 1, hmain, cs);
       }));
     }
     RK(capture(g, L, [&](cudaStream_t cs) {   // k_ctl_begin cleared the sums

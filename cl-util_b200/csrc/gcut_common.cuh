@@ -76,8 +76,7 @@ enum CtlSlot {
   CTL_BADWHERE = 13,  // 1: worklist append, 2: worklist length, 3: list length, 4: image id,
                       // 5: frontier append, 6: frontier length, 7: dirty append,
                       // 8: dirty length
-  CTL_MDONE = 14,     // CTAs finished in k_mark_cycle
-  CTL_KDONE = 15,     // CTAs finished in k_masks
+  CTL_KDONE = 14,     // CTAs finished in k_masks
   CTL_N = 64          // the control words fill 256 bytes; the per-image sums follow them
 };
 

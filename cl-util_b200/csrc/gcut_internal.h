@@ -79,8 +79,8 @@ int launch_flood_round(const PoolView& P, int first, cudaGraphConditionalHandle 
                        int grid, cudaStream_t s);
 int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc* acc,
                      cudaStream_t s);
-int launch_mark_cycle(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
-                      int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s);
+int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, int32_t* count,
+                       int bump, int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s);
 int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s);
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s);

@@ -948,37 +948,80 @@ __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc
   }
 }
 
-// After the active-tile compaction: every CTA stamps the images of the list entries it reads,
-// so the next cycle's global relabel covers only images that still have active tiles (stamp =
-// cycles + 1 + bump, where bump = 1 when this check counts as a finished cycle); then the last
-// CTA applies the cycle check (it reads the cycle count after every stamp was taken).
-__global__ void k_mark_cycle(PoolView P, const int32_t* list, const int32_t* count, int bump,
-                             int count_cycle, cudaGraphConditionalHandle h) {
-  __shared__ int s_n, s_stamp;
+// The active-tile list after a global relabel, in one launch: a single-pass scan (chunks by
+// arrival ticket, decoupled look-back) of the tiles' activity flags writes the ids of the
+// active tiles in order and stamps their images live for the next cycle (stamp = cycles + 1
+// + bump); the last CTA to finish closes the scan and applies the cycle check: another cycle
+// runs while tiles are active and the cycle cap is not reached (`count_cycle` counts this
+// check as a finished cycle).  Replaces a compaction and a separate stamping launch.
+constexpr int ACT_THREADS = 256;
+constexpr int ACT_ITEMS = 16;
+constexpr int ACT_CHUNK = ACT_THREADS * ACT_ITEMS;
+
+__global__ void __launch_bounds__(ACT_THREADS)
+k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
+              int count_cycle, cudaGraphConditionalHandle h) {
+  __shared__ int32_t sm[32];
+  __shared__ int32_t s_chunk, s_excl, s_stamp;
+  __shared__ uint32_t s_tag;
   if (threadIdx.x == 0) {
-    int n = *((volatile const int32_t*)count);
-    if (n < 0 || n > P.nt) {   // self-check: a list holds each tile at most once
-      if (blockIdx.x == 0) record_bad(P, 3, n);
-      n = 0;
-    }
-    s_n = n;
+    s_chunk = atomicAdd(st.ticket, 1);
+    s_tag = *((volatile uint32_t*)st.seq);
     s_stamp = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1 + bump;
   }
   __syncthreads();
-  const int n = s_n, stamp = s_stamp;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int img = P.img_of[list[i]];
-    if ((unsigned)img < (unsigned)P.nimg) P.img_live[img] = stamp;
-    else record_bad(P, 4, img);
+  const int chunk = s_chunk, stamp = s_stamp;
+  const int nt = P.nt;
+  const int nchunks = (nt + ACT_CHUNK - 1) / ACT_CHUNK;
+  const int base = chunk * ACT_CHUNK + threadIdx.x * ACT_ITEMS;
+  int32_t v[ACT_ITEMS];
+  if (base + ACT_ITEMS <= nt) {
+#pragma unroll
+    for (int k = 0; k < ACT_ITEMS; k += 4) {
+      const int4 q = *reinterpret_cast<const int4*>(P.tact + base + k);
+      v[k] = q.x != 0; v[k + 1] = q.y != 0; v[k + 2] = q.z != 0; v[k + 3] = q.w != 0;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < ACT_ITEMS; ++k) v[k] = (base + k < nt) ? (P.tact[base + k] != 0) : 0;
+  }
+  int32_t tsum = 0;
+#pragma unroll
+  for (int k = 0; k < ACT_ITEMS; ++k) tsum += v[k];
+  int32_t agg;
+  const int32_t tex = block_exclusive_scan(tsum, sm, &agg);
+  if (threadIdx.x < 32) {
+    const int32_t ex = lookback_exclusive_warp(st, s_tag, chunk, agg);
+    if (threadIdx.x == 0) s_excl = ex;
   }
   __syncthreads();
+  int32_t run = s_excl + tex;
+#pragma unroll
+  for (int k = 0; k < ACT_ITEMS; ++k) {
+    if (v[k]) {
+      const int t = base + k;
+      if ((unsigned)run < (unsigned)nt) list[run] = t;
+      else atomicExch(st.err, 2);   // only after a look-back that gave up
+      const int img = P.img_of[t];
+      if ((unsigned)img < (unsigned)P.nimg) P.img_live[img] = stamp;
+      else record_bad(P, 4, img);
+      ++run;
+    }
+  }
+  if (chunk == nchunks - 1 && threadIdx.x == 0) *count = s_excl + agg;
   if (threadIdx.x != 0) return;
   __threadfence();
-  if (atomicAdd(&P.ctl[CTL_MDONE], 1) != (int)gridDim.x - 1) return;
+  if (atomicAdd(st.done, 1) != nchunks - 1) return;
+  // last CTA: close the scan (tickets, tag) and apply the cycle check
   __threadfence();
+  *st.ticket = 0;
+  *st.done = 0;
+  uint32_t sq = *st.seq + 1;
+  if ((sq & 0x3fffffffu) == 0) sq = 1;
+  *st.seq = sq;
   volatile int32_t* ctl = P.ctl;
-  ctl[CTL_MDONE] = 0;
-  ctl[CTL_PULSE] = 0;   // the compacted list sits in queue[0]
+  const int n = *((volatile int32_t*)count);
+  ctl[CTL_PULSE] = 0;   // the list sits in queue[0]
   ctl[CTL_DDONE] = 0;
   P.qcount[1] = 0;
   const int cycles = ctl[CTL_CYCLES] + (count_cycle ? 1 : 0);
@@ -1378,9 +1421,11 @@ int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc
   return ok();
 }
 
-int launch_mark_cycle(const PoolView& P, const int32_t* list, const int32_t* count, int bump,
-                      int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s) {
-  k_mark_cycle<<<16, 256, 0, s>>>(P, list, count, bump, count_cycle, h);
+int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, int32_t* count,
+                       int bump, int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s) {
+  const int nch = (P.nt + ACT_CHUNK - 1) / ACT_CHUNK;
+  if (nch > st.max_chunks) return GC_ERR_INVALID;
+  k_active_list<<<nch > 0 ? nch : 1, ACT_THREADS, 0, s>>>(P, st, list, count, bump, count_cycle, h);
   return ok();
 }
 
@@ -1456,7 +1501,7 @@ void preload_kernels() {
       (const void*)k_upload<PlaneSource>, (const void*)k_upload<RgbaSource>, (const void*)k_dsum,
       (const void*)k_masks, (const void*)k_discharge, (const void*)k_edge_relabel_build,
       (const void*)k_bfs_round, (const void*)k_flood_round, (const void*)k_ctl_begin,
-      (const void*)k_mark_cycle, (const void*)k_ctl_cycle,
+      (const void*)k_active_list, (const void*)k_ctl_cycle,
       (const void*)k_acc_reset, (const void*)k_labels_out, (const void*)k_labels_packed,
       (const void*)k_state_out, (const void*)k_edit, (const void*)k_stroke};
   for (const void* k : kernels) cudaFuncGetAttributes(&a, k);

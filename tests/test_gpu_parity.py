@@ -166,6 +166,26 @@ def test_flow_equals_cut_capacity(cuda, oracle):
     assert oracle.cut_capacity(*g.planes(), lab) == f
 
 
+@pytest.mark.parametrize("w,h,seed", [(4096, 4096, 3), (3000, 4096, 21)])
+def test_full_size_certificates(cuda, oracle, w, h, seed):
+    """Sizes of the stroke and serving workloads, checked without an exact max-flow run:
+    (1) the flow equals the capacity of the returned cut, which by weak duality proves both
+    optimal; (2) the labels equal the canonical cut recomputed by the oracle from the final
+    residual graph the device holds; (3) the flow the oracle derives from that residual
+    state equals the reported one."""
+    g = synth.make_graph(w, h, seed)
+    with GraphCut(w, h) as gc:
+        gc.upload_capacities(*g.planes())
+        gc.cut()
+        f = gc.flow
+        lab = gc.labels_host()
+        state = [getattr(gc, n).cpu().numpy() for n in ("dUp", "dDown", "dLeft", "dRight", "dExcess")]
+    assert oracle.cut_capacity(*g.planes(), lab) == f
+    f_state, l_state = oracle.canonical(*state, g.excess)
+    assert f_state == f
+    assert np.array_equal(l_state, lab)
+
+
 def test_manual_stepping_matches(cuda, oracle):
     g = synth.random_graph(128, 96, 5, cap_max=60, tlink_max=90)
     f_ref, l_ref = oracle.maxflow_bk(*g.planes())
