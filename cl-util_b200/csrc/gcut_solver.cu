@@ -103,7 +103,25 @@ __device__ __forceinline__ void mark_dirty(const PoolView& P, int t) {
 // RgbaSource: n-links built from an RGBA image and the n-link table (gc_upload_rgba).
 struct PlaneSource {
   const int32_t *up, *down, *left, *right, *excess;
+  bool vec;   // all planes 16-byte aligned and the width a multiple of 4: int4 row loads
   __device__ __forceinline__ void prepare(int32_t*) const {}
+  // the four pixels (x0 .. x0+3, y) at once, all inside the image (x0 + 3 < W)
+  __device__ __forceinline__ void pixel4(const ImageDesc& im, int x0, int y, int (&e)[4],
+                                         int (&cu)[4], int (&cd)[4], int (&cl)[4],
+                                         int (&cr)[4]) const {
+    const long long i = (long long)y * im.W + x0;
+    const int4 a = *reinterpret_cast<const int4*>(excess + i);
+    const int4 b = *reinterpret_cast<const int4*>(up + i);
+    const int4 c = *reinterpret_cast<const int4*>(down + i);
+    const int4 d = *reinterpret_cast<const int4*>(left + i);
+    const int4 f = *reinterpret_cast<const int4*>(right + i);
+    e[0] = a.x; e[1] = a.y; e[2] = a.z; e[3] = a.w;
+    const bool top = y == 0, bottom = y == im.H - 1;
+    cu[0] = top ? 0 : b.x; cu[1] = top ? 0 : b.y; cu[2] = top ? 0 : b.z; cu[3] = top ? 0 : b.w;
+    cd[0] = bottom ? 0 : c.x; cd[1] = bottom ? 0 : c.y; cd[2] = bottom ? 0 : c.z; cd[3] = bottom ? 0 : c.w;
+    cl[0] = x0 == 0 ? 0 : d.x; cl[1] = d.y; cl[2] = d.z; cl[3] = d.w;
+    cr[0] = f.x; cr[1] = f.y; cr[2] = f.z; cr[3] = x0 + 3 == im.W - 1 ? 0 : f.w;
+  }
   __device__ __forceinline__ void pixel(const ImageDesc& im, const int32_t*, int x, int y, int& e,
                                         int& cu, int& cd, int& cl, int& cr) const {
     const long long i = (long long)y * im.W + x;
@@ -126,6 +144,9 @@ struct RgbaSource {
   const uint32_t* rgba;
   const int32_t* excess;
   NlinkTable tab;
+  static constexpr bool vec = false;
+  __device__ __forceinline__ void pixel4(const ImageDesc&, int, int, int (&)[4], int (&)[4],
+                                         int (&)[4], int (&)[4], int (&)[4]) const {}
   __device__ __forceinline__ void prepare(int32_t* s_tab) const {
     if (threadIdx.x < GC_NLINK_LEVELS) s_tab[threadIdx.x] = tab.t[threadIdx.x];
   }
@@ -164,14 +185,20 @@ k_upload(PoolView P, ImageDesc im, int img, Source src, int32_t* __restrict__ tl
   int e[4], h[4], cu[4], cd[4], cl[4], cr[4];
   long long pos = 0;
   int bad = 0, anypos = 0;
+  const int xb = tx * GC_TILE + c0;
+  if (src.vec && y < im.H && xb + 3 < im.W) {
+    src.pixel4(im, xb, y, e, cu, cd, cl, cr);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int x = xb + j;
+      e[j] = cu[j] = cd[j] = cl[j] = cr[j] = 0;
+      if (x < im.W && y < im.H) src.pixel(im, s_tab, x, y, e[j], cu[j], cd[j], cl[j], cr[j]);
+    }
+  }
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    const int x = tx * GC_TILE + c0 + j;
-    e[j] = cu[j] = cd[j] = cl[j] = cr[j] = 0;
-    if (x < im.W && y < im.H) {
-      src.pixel(im, s_tab, x, y, e[j], cu[j], cd[j], cl[j], cr[j]);
-      bad |= (cu[j] | cd[j] | cl[j] | cr[j]) < 0;
-    }
+    bad |= (cu[j] | cd[j] | cl[j] | cr[j]) < 0;
     h[j] = e[j] < 0 ? 0 : 1;
     pos += e[j] > 0 ? e[j] : 0;
     anypos |= e[j] > 0;
@@ -1328,7 +1355,9 @@ static inline int ok() { return cudaGetLastError() == cudaSuccess ? GC_OK : GC_E
 int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t* up,
                   const int32_t* down, const int32_t* left, const int32_t* right,
                   const int32_t* excess, int32_t* tl, ImageAcc* acc, cudaStream_t s) {
-  const PlaneSource src{up, down, left, right, excess};
+  auto a16 = [](const int32_t* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  const bool vec = im.W % 4 == 0 && a16(up) && a16(down) && a16(left) && a16(right) && a16(excess);
+  const PlaneSource src{up, down, left, right, excess, vec};
   k_upload<<<im.tw * im.th, DIS_THREADS, 0, s>>>(P, im, img, src, tl, acc);
   return ok();
 }
