@@ -225,8 +225,13 @@ class GraphCut:
         check(lib().gc_labels_packed_host(self._h, ptr(out), stream_handle(stream)))
         return out
 
-    def labels_host(self, stream=None) -> np.ndarray:
-        out = np.empty((self.height, self.width), np.uint8)
+    def labels_host(self, out=None, stream=None) -> np.ndarray:
+        """Canonical labels in host memory, uint8 [H, W]; `out` may be a (pinned) buffer of
+        that shape, written in place."""
+        if out is None:
+            out = np.empty((self.height, self.width), np.uint8)
+        elif out.shape != (self.height, self.width) or out.dtype != np.uint8 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous uint8 array of shape (height, width)")
         check(lib().gc_labels_host(self._h, ptr(out), stream_handle(stream)))
         return out
 

@@ -147,6 +147,7 @@ struct Pool {
   size_t arena_bytes = 0;
   bool own_arena = true;       // false: caller-owned memory (gc_create_in)
   cudaEvent_t done_ev = nullptr;   // recorded after every call's work (see track)
+  cudaEvent_t dsum_ev = nullptr;   // the |dI|^2 sum of gc_upload_rgba reached the host
   void* pin = nullptr;         // pinned block holding h_count, h_ctl, h_acc
   size_t pin_bytes = 0;
   int32_t* h_count = nullptr;  // pinned
@@ -223,6 +224,10 @@ struct Pool {
   }
 
   void release() {
+    if (dsum_ev) {
+      cudaEventDestroy(dsum_ev);
+      dsum_ev = nullptr;
+    }
     if (done_ev) {
       if (!own_arena) cudaEventSynchronize(done_ev);
       cudaEventDestroy(done_ev);
@@ -324,6 +329,8 @@ struct Pool {
     }
     e = cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming);
     if (e) { done_ev = nullptr; release(); return cuda_fail(e, "event"); }
+    e = cudaEventCreateWithFlags(&dsum_ev, cudaEventDisableTiming);
+    if (e) { dsum_ev = nullptr; release(); return cuda_fail(e, "event"); }
     Carve place{arena, 0};
     layout(place);
     list = P.queue[0];
@@ -388,14 +395,29 @@ struct Pool {
   // 4-neighbour pairs is taken on the device (exact), the host turns it into beta and the
   // n-link table, and the upload kernel builds the tile planes from the image.
   int upload_rgba(int i, const uint32_t* rgba, const int32_t* excess, cudaStream_t s) {
+    RK(rgba_sum_begin(i, rgba, s));
+    return upload_rgba_finish(i, rgba, excess, s);
+  }
+
+  // first half of upload_rgba: the sum of |dI|^2 on the device and its copy to the host,
+  // marked by dsum_ev (work queued after it, such as another input copy, overlaps the wait)
+  int rgba_sum_begin(int i, const uint32_t* rgba, cudaStream_t s) {
     if (i < 0 || i >= (int)imgs.size()) return fail(GC_ERR_INVALID, "image index");
-    if (!rgba || !excess) return fail(GC_ERR_INVALID, "null plane");
+    if (!rgba) return fail(GC_ERR_INVALID, "null plane");
     CK(cudaSetDevice(device));
     const ImageDesc& im = imgs[i];
     CK(cudaMemsetAsync(dsum, 0, sizeof(unsigned long long), s));
     RK(launch_dsum(rgba, im.W, im.H, dsum, sms, s));
     CK(cudaMemcpyAsync(h_dsum, dsum, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    CK(cudaEventRecord(dsum_ev, s));
+    return GC_OK;
+  }
+
+  // second half: wait for the sum, build the n-link table, launch the upload
+  int upload_rgba_finish(int i, const uint32_t* rgba, const int32_t* excess, cudaStream_t s) {
+    if (!excess) return fail(GC_ERR_INVALID, "null plane");
+    const ImageDesc& im = imgs[i];
+    CK(cudaEventSynchronize(dsum_ev));
     const long long npairs = (long long)(im.H - 1) * im.W + (long long)im.H * (im.W - 1);
     NlinkTable tab;
     nlink_table(*h_dsum, npairs, &tab);
@@ -936,9 +958,12 @@ int gc_upload_rgba_host(gc_handle* h, const uint32_t* rgba, const int32_t* exces
     if (e) { p.stage = nullptr; cudaGetLastError(); return fail(GC_ERR_OOM, "staging buffer"); }
   }
   cudaStream_t s = (cudaStream_t)stream;
+  const uint32_t* img = reinterpret_cast<const uint32_t*>(p.stage);
+  // the image first: its |dI|^2 sum travels to the host while the t-links are copied
   CK(cudaMemcpyAsync(p.stage, rgba, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  RK(p.rgba_sum_begin(0, img, s));
   CK(cudaMemcpyAsync(p.stage + n, excess, n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-  int r = p.upload_rgba(0, reinterpret_cast<const uint32_t*>(p.stage), p.stage + n, s);
+  int r = p.upload_rgba_finish(0, img, p.stage + n, s);
   p.track(s);
   if (r) return r;
   CK(cudaStreamSynchronize(s));
