@@ -631,11 +631,13 @@ def run_strokes(args):
 def serving_images(n=12, seed=4):
     """The image pool of --config serving: n grids with sides drawn uniformly from
     [256, 4096] (width and height independent), built as the synthetic generator, seeds
-    20000+i.  New-image requests draw from this pool; each starts its own session."""
+    20000+i, with their images.  New-image requests draw from this pool; each starts its own
+    session."""
     import synth
     rng = np.random.default_rng(seed)
     shapes = [(int(rng.integers(256, 4097)), int(rng.integers(256, 4097))) for _ in range(n)]
-    return synth.make_graphs([(w, h, 20_000 + i) for i, (w, h) in enumerate(shapes)])
+    return synth.make_graphs([(w, h, 20_000 + i) for i, (w, h) in enumerate(shapes)],
+                             keep_image=True)
 
 
 def run_trace(graphs, host_planes, trace, slots, budget, seed=5, solver_kw=None):
@@ -751,11 +753,15 @@ def run_serving(args):
     import torch
 
     from serving import poisson_trace
+    from GraphCut import _as_rgba32
     graphs = serving_images()
     torch.cuda.set_device(0)
-    pinned = [[torch.from_numpy(p).pin_memory() for p in g.planes()] for g in graphs]
-    host_planes = [tuple(t.numpy() for t in pl) for pl in pinned]   # views; pinned keeps them
-    dev_planes = [[t.cuda() for t in pl] for pl in pinned]
+    # requests carry the reference's inputs: the image and the t-links (8 B/px); the device
+    # builds the n-links, which equal the generator's planes the results are checked against
+    pinned = [[torch.from_numpy(np.ascontiguousarray(_as_rgba32(g.image)).view(np.int32)).pin_memory(),
+               torch.from_numpy(g.excess).pin_memory()] for g in graphs]
+    host_planes = [(pl[0].numpy().view(np.uint32), pl[1].numpy()) for pl in pinned]
+    dev_planes = [[torch.from_numpy(p).cuda() for p in g.planes()] for g in graphs]
     trace = poisson_trace(np.random.default_rng(6), args.rate, args.duration, len(graphs))
     budget = 64 << 30
     # warm-up: an untimed trace of another seed (up to 15 s): the driver's first few hundred

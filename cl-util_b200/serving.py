@@ -93,8 +93,16 @@ class Slab:
 
 @dataclasses.dataclass
 class NewImage:
+    """A new session.  `planes` = (up, down, left, right, excess) host int32 [H, W], or
+    `planes` = (rgba, excess): the image (uint32 [H, W], RGBA bytes viewed as uint32) and the
+    t-links, the reference's own inputs, from which the n-links are built on the device
+    (8 bytes per pixel to upload instead of 20)."""
     session: int
-    planes: tuple            # (up, down, left, right, excess) host int32 [H, W]
+    planes: tuple
+
+    @property
+    def shape(self):
+        return self.planes[-1].shape   # (H, W) of the excess plane
 
 
 @dataclasses.dataclass
@@ -259,7 +267,7 @@ class GraphCutServer:
         if not self.images:
             return None
         req, arr = self.images[0]
-        h, w = req.planes[4].shape
+        h, w = req.shape
         if session_bytes(w, h) > self.slab.size:   # can never fit: refuse it
             self.images.popleft()
             self.queued_images.discard(req.session)
@@ -352,7 +360,7 @@ class GraphCutServer:
             try:
                 start = time.perf_counter()
                 if sess is None:
-                    h, w = req.planes[4].shape
+                    h, w = req.shape
                     if gc is None:
                         gc = self._new_handle(w, h, off, nbytes)
                     flow, bits, phases = ctx.run_image(gc, req.planes, w, h)
@@ -409,9 +417,15 @@ class _DeviceContext:
         dev = []
         for j, p in enumerate(planes):
             d = self.dstage[j * n:(j + 1) * n].view(h, w)
-            d.copy_(torch.from_numpy(np.ascontiguousarray(p, dtype=np.int32)), non_blocking=True)
+            src = np.ascontiguousarray(p)
+            if src.dtype == np.uint32:
+                src = src.view(np.int32)   # the image: same bits, a dtype torch copies
+            d.copy_(torch.from_numpy(np.ascontiguousarray(src, dtype=np.int32)), non_blocking=True)
             dev.append(d)
-        gc.upload_capacities(*dev, stream=self.stream)
+        if len(dev) == 2:   # (rgba, excess): n-links built on the device
+            gc.upload_image(dev[0], dev[1], stream=self.stream)
+        else:
+            gc.upload_capacities(*dev, stream=self.stream)
 
     def _labels(self, gc, w, h):
         n = h * ((w + 7) // 8)

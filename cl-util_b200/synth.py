@@ -249,16 +249,16 @@ def random_graph(width: int, height: int, seed: int, cap_max=100, tlink_max=2000
 
 
 def _make_one(args):
-    w, h, seed = args
-    return make_graph(w, h, seed)
+    w, h, seed, keep = args
+    return make_graph(w, h, seed, keep_image=keep)
 
 
-def make_graphs(specs, processes=None):
+def make_graphs(specs, processes=None, keep_image=False):
     """make_graph for each (width, height, seed), in a 'spawn' process pool (safe to call
     after CUDA has been initialised in the parent)."""
     import multiprocessing as mp
     import os
-    specs = list(specs)
+    specs = [(w, h, seed, keep_image) for w, h, seed in specs]
     n = processes or min(len(specs), os.cpu_count() or 1)
     if n <= 1 or len(specs) <= 1:
         return [_make_one(s) for s in specs]

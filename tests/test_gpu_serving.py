@@ -64,6 +64,36 @@ def test_results_same_alone_and_in_mix(cuda, slots, budget_images):
     assert len(results) + srv.misses == 40
 
 
+def test_image_requests_from_rgba(cuda):
+    """New sessions that carry the image and t-links (n-links built on the device) give the
+    same results as solves of the generator's planes."""
+    from GraphCut import _as_rgba32
+    graphs = [synth.make_graph(w, h, 500 + i, keep_image=True)
+              for i, (w, h) in enumerate([(200, 150), (96, 300), (257, 131)])]
+    srv = GraphCutServer(slots=1, hbm_budget=2 * max(session_bytes(g.width, g.height) for g in graphs))
+    rng = np.random.default_rng(3)
+    hist = {}
+    for sid in range(9):
+        g = graphs[sid % 3]
+        hist[sid] = (g, [])
+        srv.submit(NewImage(sid, (_as_rgba32(g.image), g.excess)))
+        s = strokes.random_stroke(rng, g.width, g.height, rmin=4, rmax=10)
+        hist[sid][1].append(s)
+        srv.submit(Stroke(sid, s.xs, s.ys, s.radius, s.value))
+    srv.drain()
+    results = sorted(srv.results, key=lambda r: r.arrival)
+    srv.close()
+    assert srv.evictions > 0
+    seen = {}
+    for r in results:
+        k = seen.get(r.session, 0)
+        seen[r.session] = k + 1
+        g, strks = hist[r.session]
+        f, lab = _alone(g, strks[:k])
+        assert r.flow == f and np.array_equal(r.labels, lab), (r.session, k)
+    assert len(results) + srv.misses == 18
+
+
 def test_fresh_handles_on_nonblocking_streams(cuda):
     """A handle created while other streams are busy and used at once on a non-blocking
     stream sees its initial state (create's clears finish before it returns)."""
