@@ -8,8 +8,10 @@ int32 planes) -> tile upload -> push-relabel with global relabels -> canonical c
 -> labels in a device buffer + the flow value on the host.  `value` is the whole-job
 throughput (pixels solved by all ranks / max-over-ranks device time), timed with CUDA
 events on the solver's stream; L2 is flushed (256 MiB write) between steps, outside the
-timed region.  `e2e` is the same metric through the public API with host buffers: pinned
-host planes -> GraphCut.upload_capacities -> cut -> labels_host + flow, copies included.
+timed region.  `e2e` is the same metric through the public API with host buffers: the
+pinned RGBA image and t-link plane -> GraphCut.upload_image (n-links built on the device)
+-> cut -> labels_host + flow, copies included.  `e2e_image_and_models` starts one step
+earlier, from the image and the two colour models (t-links from gmm_tlinks.tlinks).
 
 Workload (`--config single`, the default): one 2048x2048 grid per rank built as in the
 synthetic generator (12 blurred ellipses + noise, 2-component GMM t-links, exp n-links),
@@ -313,7 +315,7 @@ def main():
         gc.set_profile(False)
 
         # e2e through the public API with host buffers
-        e2e = None
+        e2e = e2e_models = None
         if not args.no_e2e:
             # the reference's own inputs: the RGBA image (n-links are built on the device)
             # and the t-link plane, from pinned host memory; labels back to host memory
@@ -344,6 +346,56 @@ def main():
                    "ms_per_step": e_tot / args.steps, "parity": e2e_parity,
                    "api": "GraphCut.upload_image (RGBA + int32 t-links, host) -> cut -> "
                           "labels_host + flow"}
+
+            # one step further back in the reference's pipeline: the image and the two colour
+            # models only (t-links from gc_tlinks_gmm, n-links from gc_upload_rgba; 4 B/px up)
+            from gmm_tlinks import Mixture, tlinks
+            models = tuple(Mixture.from_components(c) for c in g.models)
+            rgba_pin32 = torch.from_numpy(
+                np.ascontiguousarray(_as_rgba32(g.image)).view(np.int32)).pin_memory()
+            rgba_dev = torch.empty((H, W), dtype=torch.int32, device="cuda")
+            ex_dev = torch.empty((H, W), dtype=torch.int32, device="cuda")
+
+            def model_step():
+                rgba_dev.copy_(rgba_pin32, non_blocking=True)
+                tlinks(rgba_dev, *models, out=ex_dev, stream=stream)
+                gc.upload_image(rgba_dev, ex_dev, stream=stream)
+                gc.cut(stream=stream)
+                gc.labels_host(out=out_host, stream=stream)
+                return gc.flow
+
+            for _ in range(2):
+                fm = model_step()
+            m_parity = bool(fm == f_ref and np.array_equal(out_host, l_ref))
+            m_ms = []
+            barrier()
+            for _ in range(args.steps):
+                flush.fill_(1)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                model_step()
+                m_ms.append(1000 * (time.perf_counter() - t0))
+            m_tot = reduce_max(sum(m_ms), torch.device("cuda", local))
+            # the t-link kernel alone (CUDA events on its stream, L2 flushed before each)
+            tl_ms = []
+            for _ in range(max(3, args.steps // 5)):
+                flush.fill_(1)
+                ev0 = torch.cuda.Event(enable_timing=True)
+                ev1 = torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                tlinks(rgba_dev, *models, out=ex_dev, stream=stream)
+                ev1.record(stream)
+                ev1.synchronize()
+                tl_ms.append(ev0.elapsed_time(ev1))
+            tl_avg = sum(tl_ms) / len(tl_ms)
+            e2e_models = {"value": mpix_all / (m_tot / 1000), "unit": UNIT,
+                          "h2d_bytes_per_step": 4 * W * H, "d2h_bytes_per_step": W * H + 8,
+                          "ms_per_step": m_tot / args.steps, "parity": m_parity,
+                          "tlinks_gmm_ms": tl_avg,
+                          "tlinks_gmm_gbs": 8 * W * H / (tl_avg / 1000) / 1e9,
+                          "api": "RGBA (host, pinned) -> gmm_tlinks.tlinks (2x2-component "
+                                 "full-covariance models) -> GraphCut.upload_image -> cut -> "
+                                 "labels_host + flow"}
 
     # roofline of the dominant kernel (largest summed event time)
     peak, peak_kind = measured_peak()
@@ -382,6 +434,7 @@ def main():
             "parity": parity,
             "flow": flow,
             "e2e": e2e,
+            "e2e_image_and_models": e2e_models,
             "gpu_launches": launches,
             "ms_per_step_host_driven": sum(prof_ms) / len(prof_ms),
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,

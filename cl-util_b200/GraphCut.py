@@ -150,9 +150,22 @@ class GraphCut:
         """Builds the capacities on the device from an image and the t-links (gc_upload_rgba):
         n-link = floor(50 * exp(-beta * |dI|^2) + 0.5), beta = 1 / (2 * mean |dI|^2).  `rgba`
         is uint32 [H, W] (RGBA bytes viewed as uint32) or uint8 [H, W, 3|4]; `excess` int32
-        [H, W].  Torch CUDA tensors are read in place; numpy arrays are copied."""
+        [H, W], or a pair (fg, bg) of colour models (gmm_tlinks.Mixture) from which the t-links
+        are computed on the device (gc_tlinks_gmm, 100 * (score_bg - score_fg) rounded).
+        Torch CUDA tensors are read in place; numpy arrays are copied."""
         import torch
         rgba = _as_rgba32(rgba)
+        if isinstance(excess, tuple):
+            import gmm_tlinks
+            fg, bg = excess
+            with _on(stream), torch.cuda.device(self.device):
+                if not (isinstance(rgba, torch.Tensor) and rgba.is_cuda):
+                    host = rgba.cpu().numpy() if isinstance(rgba, torch.Tensor) else rgba
+                    rgba = torch.from_numpy(np.ascontiguousarray(host).view(np.int32)).to(self.device)
+                rgba = rgba.contiguous()
+                if tuple(rgba.shape) != (self.height, self.width):
+                    raise ValueError("image shape differs from the graph")
+                excess = gmm_tlinks.tlinks(rgba, fg, bg, stream=stream)
         if tuple(rgba.shape) != (self.height, self.width) or tuple(excess.shape) != (self.height, self.width):
             raise ValueError("image / excess shape differs from the graph")
         if isinstance(rgba, torch.Tensor) and rgba.is_cuda and isinstance(excess, torch.Tensor) and excess.is_cuda:

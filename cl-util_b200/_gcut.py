@@ -49,8 +49,15 @@ class GcKernelProf(ctypes.Structure):
     _fields_ = [("launches", ctypes.c_int64), ("ms", ctypes.c_double), ("tiles", ctypes.c_int64)]
 
 
+class GcGauss(ctypes.Structure):
+    """One colour-model component: log(w N(x | mean, S)) = c - 0.5 |Li (x - mean)|^2."""
+    _fields_ = [("c", ctypes.c_double), ("mean", ctypes.c_double * 3),
+                ("li", ctypes.c_double * 6)]
+
+
 GC_NKERN = 10
 GC_COMPACT_NOALLOC_MAX_N = 4194304
+GC_GMM_MAX_COMPONENTS = 8
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -68,6 +75,7 @@ SIGNATURES = {
     "gc_upload_host": [_P] * 6 + [_P],
     "gc_upload_rgba": [_P, _P, _P, _P],
     "gc_upload_rgba_host": [_P, _P, _P, _P],
+    "gc_tlinks_gmm": [_P, _I, _I, _I, _P, _I, _P, _I, ctypes.c_double, _I32, _P, _P],
     "gc_solve": [_P, _P],
     "gc_push": [_P, _P],
     "gc_relabel": [_P, _P],

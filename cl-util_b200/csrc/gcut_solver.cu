@@ -1176,7 +1176,7 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
 
 // ------------------------------------------------------------------------------------
 // Canonical cut: flood from excess pixels over residual edges (forward direction).
-// Round 1 also sums max(excess, 0) per image for the flow value.
+// The first flood round also sums max(excess, 0) per image for the flow value.
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
 k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc) {

@@ -93,15 +93,19 @@ class Slab:
 
 @dataclasses.dataclass
 class NewImage:
-    """A new session.  `planes` = (up, down, left, right, excess) host int32 [H, W], or
-    `planes` = (rgba, excess): the image (uint32 [H, W], RGBA bytes viewed as uint32) and the
-    t-links, the reference's own inputs, from which the n-links are built on the device
-    (8 bytes per pixel to upload instead of 20)."""
+    """A new session.  `planes` is one of
+    - (up, down, left, right, excess): host int32 [H, W] capacity planes (20 B/px);
+    - (rgba, excess): the image (uint32 [H, W], RGBA bytes viewed as uint32) and the t-links,
+      the reference's own inputs; the n-links are built on the device (8 B/px);
+    - (rgba, (fg, bg)): the image and two colour models (gmm_tlinks.Mixture or components
+      arrays); n-links and t-links are both built on the device (4 B/px)."""
     session: int
     planes: tuple
 
     @property
     def shape(self):
+        if isinstance(self.planes[-1], tuple):
+            return tuple(self.planes[0].shape[:2])
         return self.planes[-1].shape   # (H, W) of the excess plane
 
 
@@ -414,6 +418,16 @@ class _DeviceContext:
         torch, n = self.torch, w * h
         if self.dstage.numel() < 5 * n:
             self.dstage = torch.empty(5 * n, dtype=torch.int32, device=self.device)
+        if isinstance(planes[-1], tuple):   # (rgba, (fg, bg)): t-links from the models
+            import gmm_tlinks
+            from GraphCut import _as_rgba32
+            img = self.dstage[:n].view(h, w)
+            img.copy_(torch.from_numpy(np.ascontiguousarray(_as_rgba32(planes[0])).view(np.int32)),
+                      non_blocking=True)
+            ex = gmm_tlinks.tlinks(img, *planes[1], out=self.dstage[n:2 * n].view(h, w),
+                                   stream=self.stream)
+            gc.upload_image(img, ex, stream=self.stream)
+            return
         dev = []
         for j, p in enumerate(planes):
             d = self.dstage[j * n:(j + 1) * n].view(h, w)

@@ -29,6 +29,8 @@ import dataclasses
 import numpy as np
 from scipy import ndimage
 
+from gmm_tlinks import components
+
 N_ELLIPSES = 12
 BLUR_SIGMA = 3.0
 NOISE_SIGMA = 8.0
@@ -50,13 +52,15 @@ class Graph:
     right: np.ndarray
     excess: np.ndarray
     image: np.ndarray | None = None
+    models: tuple | None = None   # (fg, bg) components (gmm_tlinks.components), with image
 
     def planes(self):
         return self.up, self.down, self.left, self.right, self.excess
 
     def copy(self) -> "Graph":
         return Graph(self.width, self.height, self.up.copy(), self.down.copy(),
-                     self.left.copy(), self.right.copy(), self.excess.copy(), self.image)
+                     self.left.copy(), self.right.copy(), self.excess.copy(), self.image,
+                     self.models)
 
 
 def _ellipse_masks(width, height, rng, n):
@@ -136,21 +140,19 @@ def _fit_gmm2(x: np.ndarray):
 
 
 def _component_logpdf(x: np.ndarray, params):
-    """log(w_k N(x | mu_k, S_k)) for k = 0, 1, elementwise (no BLAS reductions)."""
-    weights, means, covs = params
+    """log(w_k N(x | mu_k, S_k)) for k = 0, 1, elementwise (no BLAS reductions), in the
+    evaluation form and operation order of gc_tlinks_gmm."""
+    comps = components(*params)
     out = np.empty((x.shape[0], 2))
     for k in range(2):
-        L = np.linalg.cholesky(covs[k])
-        Li = np.linalg.inv(L)
-        d0 = x[:, 0] - means[k, 0]
-        d1 = x[:, 1] - means[k, 1]
-        d2 = x[:, 2] - means[k, 2]
-        y0 = Li[0, 0] * d0
-        y1 = Li[1, 0] * d0 + Li[1, 1] * d1
-        y2 = Li[2, 0] * d0 + Li[2, 1] * d1 + Li[2, 2] * d2
-        logdet = 2.0 * np.log(np.diag(L)).sum()
-        out[:, k] = (np.log(weights[k]) - 0.5 * (3 * np.log(2 * np.pi) + logdet)
-                     - 0.5 * (y0 * y0 + y1 * y1 + y2 * y2))
+        c, mu, li = comps[k, 0], comps[k, 1:4], comps[k, 4:10]
+        d0 = x[:, 0] - mu[0]
+        d1 = x[:, 1] - mu[1]
+        d2 = x[:, 2] - mu[2]
+        y0 = li[0] * d0
+        y1 = li[1] * d0 + li[2] * d1
+        y2 = li[3] * d0 + li[4] * d1 + li[5] * d2
+        out[:, k] = c - 0.5 * (y0 * y0 + y1 * y1 + y2 * y2)
     return out
 
 
@@ -213,8 +215,9 @@ def make_graph(width: int, height: int, seed: int, keep_image=False) -> Graph:
     excess = np.clip(t, -TLINK_CLAMP, TLINK_CLAMP).astype(np.int32)
     wv, wh = nlinks(img)
     up, down, left, right = planes_from_weights(wv, wh, excess)
+    models = (components(*gmm_fg), components(*gmm_bg)) if keep_image else None
     return Graph(width, height, up, down, left, right, np.ascontiguousarray(excess),
-                 img if keep_image else None)
+                 img if keep_image else None, models)
 
 
 def batch_shapes(n: int, seed: int, lo: int = 256, hi: int = 1536, step: int = 128):

@@ -121,6 +121,42 @@ int gc_upload_rgba(gc_handle* h, const uint32_t* rgba, const int32_t* excess, vo
 int gc_upload_rgba_host(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
                         void* stream);
 
+/* One Gaussian component of a colour model, in the form its log-density is evaluated in:
+   log(w N(x | mean, S)) = c - 0.5 * |Li (x - mean)|^2 for the pixel colour x = (R, G, B),
+   with Li the inverse of the lower Cholesky factor of S (lower triangle, row-major: Li00,
+   Li10, Li11, Li20, Li21, Li22) and c = log w - 0.5 * (3 log 2pi + log det S).  A diagonal
+   model (the reference's, GMM.calcA_cpu GMM.pyx:375-395) has Li = diag(1 / sqrt(S_ii)). */
+typedef struct gc_gauss {
+  double c;
+  double mean[3];
+  double li[6];
+} gc_gauss;
+#define GC_GMM_MAX_COMPONENTS 8 /* MAX_NCOMPONENT of gmm.cl:4-5 */
+
+/* T-links from a foreground and a background colour model, on the device.  The reference
+   scores every pixel under each mixture (GMM.score, GMM.pyx:130-163; score_buf and
+   score_img2d, gmm.cl:373-491: s = -log sum_k exp(e_k)) and gives the solver
+   excess = scoreBg - scoreFg (test_GraphCut.py:44-47).  Here both scores, the difference
+   and the int32 rounding are one pass:
+     excess = clamp(floor(scale * (s_bg - s_fg) + 0.5), -clamp, clamp)
+   with s = -(m + log(sum_k exp(e_k - m))), m = max_k e_k, the sum over k = 0, 1, ... in
+   turn, and for each component d_j = x_j - mean_j, y0 = Li00 d0, y1 = Li10 d0 + Li11 d1,
+   y2 = (Li20 d0 + Li21 d1) + Li22 d2, e = c - 0.5 * ((y0 y0 + y1 y1) + y2 y2): float64,
+   every add and multiply rounded on its own (no fused multiply-add), in that order.
+   - rgba: DEVICE uint32, row y at rgba + y * pitch (pitch >= width, in pixels), R in bits
+     0-7, G 8-15, B 16-23; excess: DEVICE int32 [height][width] (row-major, dense).
+   - 1 <= n_fg, n_bg <= GC_GMM_MAX_COMPONENTS; every parameter finite with |c| <= 2^64,
+     |mean| <= 2^32, |li| <= 2^32; |scale| <= 2^32; 0 <= clamp <= 2^30.  Otherwise
+     GC_ERR_INVALID.  width or height 0 is a no-op.
+   - The result equals a float64 host evaluation of the same expression except where the
+     host's and the device's exp / log differ in the last bit and that moves
+     scale * (s_bg - s_fg) + 0.5 across an integer (then the two differ by 1).
+   - Pass excess to gc_upload_rgba with the same image to build the whole graph on the
+     device from 4 bytes per pixel. */
+int gc_tlinks_gmm(const uint32_t* rgba, int width, int height, int pitch, const gc_gauss* fg,
+                  int n_fg, const gc_gauss* bg, int n_bg, double scale, int32_t clamp,
+                  int32_t* excess, void* stream);
+
 /* Max-flow to the final cut.  Replaces GraphCut.cut (GraphCut.pyx:348-418); warm-starts
    from the current residual graph when called again after gc_edit_tlinks.  Blocks the
    calling host thread until the solve is done (it polls the active-tile count). */

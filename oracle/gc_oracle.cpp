@@ -1,5 +1,5 @@
 // CPU oracle for the tiled push-relabel graph cut.  TEST INFRASTRUCTURE ONLY: the parity
-// tests, the smoke check and the CPU-baseline leg of the benchmark call it as the checker;
+// tests, the smoke check and the CPU-baseline leg of the benchmark use it to check results;
 // nothing in the product links or loads it.
 //
 // Three parts, all int32/int64 arithmetic:

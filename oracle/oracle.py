@@ -1,7 +1,7 @@
 """CPU oracle wrapper.  TEST INFRASTRUCTURE ONLY.
 
 The parity tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use
-this module as the checker; the product never imports it.
+this module to check results; the product never imports it.
 
 * ``maxflow_bk``      exact max-flow (Boykov-Kolmogorov, TPAMI 2004), canonical labels.
 * ``ref_tiled``       int32 restatement of the reference schedule (GraphCut.pyx:348-418 +
@@ -14,6 +14,8 @@ this module as the checker; the product never imports it.
   incremental_tile_list.cl:40-154 (stamp predicates).  Pinned by the reference's own
   known-answer checks (test_PrefixSum.py:35, test_StreamCompact.py:40-41,
   test_IncrementalTileList.py:38-40) in tests/test_oracle.py.
+* ``tlinks_gmm``      t-links from a foreground and a background colour model (GMM.score,
+                      gmm.cl:373-491, and scoreBg - scoreFg, test_GraphCut.py:44-47).
 """
 from __future__ import annotations
 
@@ -146,3 +148,41 @@ def increment_logical(t1, t2, op1, op2, a1, a2, logical, iteration):
     out = np.array(t1, dtype=np.int32, copy=True)
     out[flag_logical(t1, t2, op1, op2, a1, a2, logical) != 0] = iteration
     return out
+
+
+# --- t-links from colour models (GMM.score + scoreBg - scoreFg) --------------------------
+
+def mixture_score(x, comps):
+    """-log sum_k w_k N(x | mean_k, S_k) per row of x (float64 [n, 3] colours), restating
+    score_buf / score_img2d (gmm.cl:373-491: e_k per component, eMax, -(eMax + log(sum
+    exp(e_k - eMax)))) with full covariances.  ``comps`` [K, 10] rows (c, mean[3], li[6]):
+    e_k = c - 0.5 * ((y0 y0 + y1 y1) + y2 y2), y = Li (x - mean), evaluated left to right
+    with one rounding per operation (numpy applies no fused multiply-add)."""
+    comps = np.asarray(comps, np.float64).reshape(-1, 10)
+    e = np.empty((x.shape[0], comps.shape[0]))
+    for k, row in enumerate(comps):
+        c, mu, li = row[0], row[1:4], row[4:10]
+        d0, d1, d2 = x[:, 0] - mu[0], x[:, 1] - mu[1], x[:, 2] - mu[2]
+        y0 = li[0] * d0
+        y1 = li[1] * d0 + li[2] * d1
+        y2 = (li[3] * d0 + li[4] * d1) + li[5] * d2
+        e[:, k] = c - 0.5 * ((y0 * y0 + y1 * y1) + y2 * y2)
+    m = e.max(1)
+    s = np.exp(e[:, 0] - m)
+    for k in range(1, e.shape[1]):
+        s = s + np.exp(e[:, k] - m)
+    return -(m + np.log(s))
+
+
+def tlinks_gmm(rgba, fg, bg, scale=100.0, clamp=10 ** 6):
+    """int32 excess = clamp(floor(scale * (s_bg - s_fg) + 0.5), -clamp, clamp), the
+    reference's ``hSink - hSrc`` (test_GraphCut.py:44-47) in the solver's integer units, for
+    a uint32 [H, W] image (R in bits 0-7, G 8-15, B 16-23).  Also returns the unrounded
+    ``scale * (s_bg - s_fg) + 0.5`` (float64 [H, W]) so that a test can tell rounding ties."""
+    img = np.asarray(rgba).view(np.uint32)
+    h, w = img.shape
+    p = img.reshape(-1)
+    x = np.stack([(p & 0xFF), (p >> 8) & 0xFF, (p >> 16) & 0xFF], 1).astype(np.float64)
+    v = scale * (mixture_score(x, bg) - mixture_score(x, fg)) + 0.5
+    t = np.clip(np.floor(v), -clamp, clamp).astype(np.int32)
+    return t.reshape(h, w), v.reshape(h, w)

@@ -116,3 +116,31 @@ def test_fresh_handles_on_nonblocking_streams(cuda):
             assert (gc.flow, ) == (want[0], )
             assert np.array_equal(gc.labels_host(stream=s), want[1])
     torch.cuda.synchronize()
+
+
+def test_image_requests_from_colour_models(cuda):
+    """New sessions that carry only the image and two colour models (n-links and t-links
+    built on the device, 4 B/px) give the generator's results."""
+    graphs = [synth.make_graph(w, h, 600 + i, keep_image=True)
+              for i, (w, h) in enumerate([(180, 140), (300, 96)])]
+    srv = GraphCutServer(slots=1, hbm_budget=4 * max(session_bytes(g.width, g.height) for g in graphs))
+    rng = np.random.default_rng(4)
+    hist = {}
+    for sid in range(6):
+        g = graphs[sid % 2]
+        hist[sid] = (g, [])
+        srv.submit(NewImage(sid, (g.image, g.models)))
+        s = strokes.random_stroke(rng, g.width, g.height, rmin=4, rmax=10)
+        hist[sid][1].append(s)
+        srv.submit(Stroke(sid, s.xs, s.ys, s.radius, s.value))
+    srv.drain()
+    results = sorted(srv.results, key=lambda r: r.arrival)
+    srv.close()
+    assert len(results) == 12
+    seen = {}
+    for r in results:
+        k = seen.get(r.session, 0)
+        seen[r.session] = k + 1
+        g, strks = hist[r.session]
+        f, lab = _alone(g, strks[:k])
+        assert r.flow == f and np.array_equal(r.labels, lab), (r.session, k)
