@@ -163,6 +163,22 @@ class IncrementalTileList:
                                            self.n_tiles, stream_handle(stream)))
         self.is_dirty = True
 
+    def execute(self, out=None, stream=None):
+        """The display layer of the list (IncrementalTileList.execute,
+        IncrementalTileList.pyx:191-208): 32-bit RGBA words [H, W] on the device, opaque red
+        (0xFF0000FF) on the tiles stamped with the current iteration, opaque black elsewhere.
+        Written into `out` (a contiguous 32-bit [H, W] tensor) when given."""
+        import torch
+        w, h = self.global_dim
+        if out is None:
+            out = torch.empty((h, w), dtype=torch.int32, device=self.device)
+        elif tuple(out.shape) != (h, w) or out.element_size() != 4 or not out.is_contiguous():
+            raise ValueError("out must be a contiguous 32-bit [H, W] tensor")
+        check(lib().gc_tiles_view(ptr(self.d_tiles), self.dim[0], self.dim[1],
+                                  self.tiles_dim[0], self.tiles_dim[1], int(self.iteration),
+                                  w, h, ptr(out), stream_handle(stream)))
+        return out
+
     def reset(self, stream=None):
         self.iteration = self.init_iteration + 1
         check(lib().gc_tiles_fill(ptr(self.d_tiles), int(self.init_iteration), self.n_tiles,

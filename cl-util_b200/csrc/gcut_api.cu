@@ -1199,6 +1199,18 @@ int gc_tiles_fill(int32_t* tiles, int32_t value, int n, void* stream) {
   return launch_fill(tiles, n, value, (cudaStream_t)stream);
 }
 
+int gc_tiles_view(const int32_t* tiles, int tiles_w, int tiles_h, int tile_w, int tile_h,
+                  int32_t iteration, int width, int height, uint32_t* out, void* stream) {
+  g_err.clear();
+  if (tiles_w < 0 || tiles_h < 0 || tile_w < 1 || tile_h < 1 || width < 0 || height < 0)
+    return fail(GC_ERR_INVALID, "gc_tiles_view: bad size");
+  if ((long long)width * height > 0 && (!out || ((long long)tiles_w * tiles_h > 0 && !tiles)))
+    return fail(GC_ERR_INVALID, "gc_tiles_view: null pointer");
+  const int r = launch_tiles_view(tiles, tiles_w, tiles_h, tile_w, tile_h, iteration, width,
+                                  height, out, (cudaStream_t)stream);
+  return r == GC_OK ? GC_OK : fail(r, "gc_tiles_view: launch failed");
+}
+
 // ---- batch ------------------------------------------------------------------------
 int gcb_create(int n, const int* widths, const int* heights, const gc_opts* opts,
                gcb_handle** out) {

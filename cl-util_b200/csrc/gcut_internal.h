@@ -28,6 +28,8 @@ int launch_increment_logical(const int32_t* in1, const int32_t* in2, int32_t* ou
                              int op1, int op2, int32_t a1, int32_t a2, int logical,
                              int32_t iteration, cudaStream_t s);
 int launch_fill(int32_t* p, int n, int32_t v, cudaStream_t s);
+int launch_tiles_view(const int32_t* tiles, int tiles_w, int tiles_h, int tile_w, int tile_h,
+                      int32_t iteration, int width, int height, uint32_t* out, cudaStream_t s);
 
 // One image inside a tile pool.
 struct ImageDesc {

@@ -138,11 +138,31 @@ __global__ void k_fill(int32_t* p, int n, int32_t v) {
   if (i < n) p[i] = v;
 }
 
+// IncrementalTileList.execute (IncrementalTileList.pyx:191-208; filter,
+// incremental_tile_list.cl:156-175): one RGBA word per pixel, opaque red where the pixel's
+// tile carries `iteration`, opaque black elsewhere.  Pixels outside the tile grid (an image
+// side that is not a multiple of the tile side) are black; the reference has no bounds check
+// there and reads past its tile array.
+__global__ void k_tiles_view(const int32_t* __restrict__ tiles, int tiles_w, int tiles_h,
+                             int tile_w, int tile_h, int32_t iteration, int width, long long n,
+                             uint32_t* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i / width);
+    const int x = (int)(i - (long long)y * width);
+    const int tx = x / tile_w, ty = y / tile_h;
+    bool on = false;
+    if (tx < tiles_w && ty < tiles_h) on = tiles[(long long)ty * tiles_w + tx] == iteration;
+    out[i] = on ? 0xFF0000FFu : 0xFF000000u;
+  }
+}
+
 void preload_scan_kernels() {
   cudaFuncAttributes a;
   cudaFuncGetAttributes(&a, (const void*)k_scan);
   cudaFuncGetAttributes(&a, (const void*)k_increment_logical);
   cudaFuncGetAttributes(&a, (const void*)k_fill);
+  cudaFuncGetAttributes(&a, (const void*)k_tiles_view);
 }
 
 int scan_chunks(int n) { return n <= 0 ? 1 : (n + SCAN_CHUNK - 1) / SCAN_CHUNK; }
@@ -170,6 +190,17 @@ int launch_increment_logical(const int32_t* in1, const int32_t* in2, int32_t* ou
 int launch_fill(int32_t* p, int n, int32_t v, cudaStream_t s) {
   if (n <= 0) return GC_OK;
   k_fill<<<(n + 255) / 256, 256, 0, s>>>(p, n, v);
+  return cudaGetLastError() == cudaSuccess ? GC_OK : GC_ERR_CUDA;
+}
+
+int launch_tiles_view(const int32_t* tiles, int tiles_w, int tiles_h, int tile_w, int tile_h,
+                      int32_t iteration, int width, int height, uint32_t* out, cudaStream_t s) {
+  const long long n = (long long)width * height;
+  if (n <= 0) return GC_OK;
+  const long long blocks = (n + 255) / 256;
+  const unsigned grid = (unsigned)(blocks < (1LL << 30) ? blocks : (1LL << 30));
+  k_tiles_view<<<grid, 256, 0, s>>>(tiles, tiles_w, tiles_h, tile_w, tile_h, iteration, width,
+                                    n, out);
   return cudaGetLastError() == cudaSuccess ? GC_OK : GC_ERR_CUDA;
 }
 

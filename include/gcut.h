@@ -268,6 +268,14 @@ int gc_tiles_incorporate(int32_t* tiles, const int32_t* tiles2, int op1, int32_t
 /* IncrementalTileList.reset (IncrementalTileList.pyx:178-189, init_incremental
    incremental_tile_list.cl:26-38): tiles[i] = value. */
 int gc_tiles_fill(int32_t* tiles, int32_t value, int n, void* stream);
+/* IncrementalTileList.execute (IncrementalTileList.pyx:191-208; filter,
+   incremental_tile_list.cl:156-175), the tile-list display layer without a graphics stack:
+   out[y * width + x] = 0xFF0000FF (opaque red, R in the low byte) where
+   tiles[(y / tile_h) * tiles_w + x / tile_w] == iteration, else 0xFF000000.  tiles: DEVICE
+   int32 [tiles_h][tiles_w]; out: DEVICE uint32 [height][width].  Pixels outside the
+   tiles_w x tiles_h tile grid are black (the reference reads past its tile array there). */
+int gc_tiles_view(const int32_t* tiles, int tiles_w, int tiles_h, int tile_w, int tile_h,
+                  int32_t iteration, int width, int height, uint32_t* out, void* stream);
 
 /* ---- batched solver: many independent grids in one tile pool ------------------------ */
 typedef struct gcb_handle gcb_handle;

@@ -186,3 +186,19 @@ def tlinks_gmm(rgba, fg, bg, scale=100.0, clamp=10 ** 6):
     v = scale * (mixture_score(x, bg) - mixture_score(x, fg)) + 0.5
     t = np.clip(np.floor(v), -clamp, clamp).astype(np.int32)
     return t.reshape(h, w), v.reshape(h, w)
+
+
+def tiles_view(tiles, tile_w, tile_h, iteration, width, height):
+    """incremental_tile_list.cl:156-175 (filter): uint32 [height, width], 0xFF0000FF where the
+    pixel's tile stamp equals ``iteration``, else 0xFF000000; pixels outside the tile grid are
+    black."""
+    tiles = np.asarray(tiles, np.int32)
+    th, tw = tiles.shape
+    ty = np.arange(height)[:, None] // tile_h
+    tx = np.arange(width)[None, :] // tile_w
+    inside = (ty < th) & (tx < tw)
+    on = np.zeros((height, width), bool)
+    if th and tw:
+        stamp = tiles[np.minimum(ty, th - 1), np.minimum(tx, tw - 1)]
+        on = inside & (stamp == iteration)
+    return np.where(on, np.uint32(0xFF0000FF), np.uint32(0xFF000000)).astype(np.uint32)

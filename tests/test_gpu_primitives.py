@@ -123,3 +123,23 @@ def test_repeated_calls_reuse_lookback_state(cuda, oracle):
         m = int(dN.item())
         assert m == int(f.sum())
         assert np.array_equal(np.flatnonzero(f), dL[:m].cpu().numpy())
+
+
+@pytest.mark.parametrize("global_dim,tiles_dim", [((4096, 4096), (16, 16)), ((800, 608), (32, 32)),
+                                                  ((100, 37), (16, 16)), ((1, 1), (16, 16))])
+def test_tile_list_execute_view(cuda, oracle, global_dim, tiles_dim):
+    """IncrementalTileList.execute (IncrementalTileList.pyx:191-208): the display layer of the
+    tiles stamped with the current iteration equals the oracle's, bit for bit."""
+    torch = cuda
+    tl = IncrementalTileList(global_dim, tiles_dim)
+    dim = tl.dim
+    h = np.random.default_rng(3).integers(0, 4, (dim[1], dim[0])).astype(np.int32)
+    if h.size:
+        tl.d_tiles.copy_(_dev(h, torch))
+    for it in (tl.iteration, 2):
+        tl.iteration = it
+        got = tl.execute().cpu().numpy().view(np.uint32)
+        want = oracle.tiles_view(h, tiles_dim[0], tiles_dim[1], it, *global_dim)
+        assert np.array_equal(got, want)
+    out = torch.zeros((global_dim[1], global_dim[0]), dtype=torch.int32, device="cuda")
+    assert tl.execute(out=out) is out

@@ -151,3 +151,16 @@ def test_generator_is_deterministic():
     assert (a.up[0] == 0).all() and (a.down[-1] == 0).all()
     assert (a.left[:, 0] == 0).all() and (a.right[:, -1] == 0).all()
     assert np.array_equal(a.down[:-1], a.up[1:]) and np.array_equal(a.right[:, :-1], a.left[:, 1:])
+
+
+def test_tiles_view_oracle_small_case(oracle):
+    """incremental_tile_list.cl:156-175 by hand: 2x2 tiles of 4x3 pixels, image 9x7 (one
+    column and one row past the tile grid stay black)."""
+    tiles = np.array([[5, 2], [2, 5]], np.int32)
+    v = oracle.tiles_view(tiles, 4, 3, 5, 9, 7)
+    red, black = 0xFF0000FF, 0xFF000000
+    want = np.full((7, 9), black, np.uint32)
+    want[0:3, 0:4] = red
+    want[3:6, 4:8] = red
+    assert np.array_equal(v, want)
+    assert np.all(oracle.tiles_view(np.zeros((0, 0), np.int32), 4, 4, 0, 5, 5) == black)
