@@ -167,6 +167,52 @@ def ncu_traffic():
         return {}
 
 
+def time_gmm_fit(g, stream, with_cpu):
+    """The colour-model fit of the reference's own fit test (test_GMM.py:58-67: 20x500 = 10000
+    samples, 4 components, 65 iterations, likelihood test 0.01), here on the pixels of the
+    largest ellipse of the bench image: gc_gmm_fit's device time (CUDA events on its stream,
+    one launch) and, as its CPU baseline, the float64 numpy restatement of the same EM."""
+    import ctypes
+
+    import torch
+
+    import _gcut
+    from GraphCut import _as_rgba32
+    img = g.image
+    h, w = img.shape[:2]
+    rgba = _as_rgba32(img)
+    # samples: a 20x500 window around the image centre (the reference test's rectangle shape)
+    y0, x0 = h // 2 - 10, max(0, w // 2 - 250)
+    s = np.ascontiguousarray(rgba[y0:y0 + 20, x0:x0 + 500]).reshape(-1)
+    d = torch.from_numpy(s.view(np.int32)).cuda()
+    res = torch.empty(ctypes.sizeof(_gcut.GcGmmFitResult), dtype=torch.uint8, device="cuda")
+    L = _gcut.lib()
+    ms = []
+    for rep in range(6):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        _gcut.check(L.gc_gmm_fit(_gcut.ptr(d), s.size, 4, 65, 0.01, 1e-3, 30.0, 0,
+                                 _gcut.ptr(res), _gcut.stream_handle(stream)))
+        ev1.record(stream)
+        ev1.synchronize()
+        if rep >= 2:
+            ms.append(ev0.elapsed_time(ev1))
+    r = _gcut.GcGmmFitResult.from_buffer_copy(res.cpu().numpy().tobytes())
+    out = {"samples": int(s.size), "components": 4, "max_iterations": 65,
+           "iterations": int(r.iterations), "converged": bool(r.converged),
+           "ms": sum(ms) / len(ms), "launches": 1}
+    if with_cpu:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        ref = O.gmm_fit(s, 4, 65, tolerance=0.01)
+        out["cpu_baseline_ms"] = 1000 * (time.perf_counter() - t0)
+        out["cpu_baseline"] = "float64 numpy EM restatement (oracle gmm_fit), 1 process"
+        out["parity"] = bool(ref["iterations"] == r.iterations and np.allclose(
+            ref["means"], np.array([list(r.means[k]) for k in range(4)]), rtol=1e-7, atol=1e-7))
+    return out
+
+
 def cpu_baseline(graph, threads, budget_s=12.0):
     """The reference schedule restated (oracle ref_tiled) on the host cores."""
     from oracle import oracle as O
@@ -396,6 +442,8 @@ def main():
                           "api": "RGBA (host, pinned) -> gmm_tlinks.tlinks (2x2-component "
                                  "full-covariance models) -> GraphCut.upload_image -> cut -> "
                                  "labels_host + flow"}
+            e2e_models["gmm_fit"] = time_gmm_fit(g, stream, rank == 0 and world == 1
+                                                 and not args.no_cpu_baseline)
 
     # roofline of the dominant kernel (largest summed event time)
     peak, peak_kind = measured_peak()

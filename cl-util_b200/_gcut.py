@@ -55,6 +55,14 @@ class GcGauss(ctypes.Structure):
                 ("li", ctypes.c_double * 6)]
 
 
+class GcGmmFitResult(ctypes.Structure):
+    """gc_gmm_fit's result: the model (covariances as lower triangles) and how the fit ended."""
+    _fields_ = [("weights", ctypes.c_double * 8), ("means", (ctypes.c_double * 3) * 8),
+                ("covars", (ctypes.c_double * 6) * 8), ("log_likelihood", ctypes.c_double),
+                ("iterations", ctypes.c_int32), ("converged", ctypes.c_int32),
+                ("status", ctypes.c_int32), ("n_components", ctypes.c_int32)]
+
+
 GC_NKERN = 10
 GC_COMPACT_NOALLOC_MAX_N = 4194304
 GC_GMM_MAX_COMPONENTS = 8
@@ -76,6 +84,8 @@ SIGNATURES = {
     "gc_upload_rgba": [_P, _P, _P, _P],
     "gc_upload_rgba_host": [_P, _P, _P, _P],
     "gc_tlinks_gmm": [_P, _I, _I, _I, _P, _I, _P, _I, ctypes.c_double, _I32, _P, _P],
+    "gc_gmm_fit": [_P, _I, _I, _I, ctypes.c_double, ctypes.c_double, ctypes.c_double, _I,
+                   _P, _P],
     "gc_solve": [_P, _P],
     "gc_push": [_P, _P],
     "gc_relabel": [_P, _P],

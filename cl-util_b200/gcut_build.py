@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libgcut.so")
-SOURCES = ["gcut_scan.cu", "gcut_solver.cu", "gcut_api.cu", "gcut_noalloc.cu", "gcut_gmm.cu"]
+SOURCES = ["gcut_scan.cu", "gcut_solver.cu", "gcut_api.cu", "gcut_noalloc.cu", "gcut_gmm.cu",
+           "gcut_gmmfit.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

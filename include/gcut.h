@@ -157,6 +157,41 @@ int gc_tlinks_gmm(const uint32_t* rgba, int width, int height, int pitch, const 
                   int n_fg, const gc_gauss* bg, int n_bg, double scale, int32_t clamp,
                   int32_t* excess, void* stream);
 
+/* Result of gc_gmm_fit (written to DEVICE memory). */
+typedef struct gc_gmm_fit_result {
+  double weights[GC_GMM_MAX_COMPONENTS];
+  double means[GC_GMM_MAX_COMPONENTS][3];
+  double covars[GC_GMM_MAX_COMPONENTS][6]; /* lower triangle: S00, S10, S11, S20, S21, S22 */
+  double log_likelihood;  /* sum over the samples of log p(x) under the returned model */
+  int32_t iterations;     /* EM iterations run */
+  int32_t converged;      /* 1: the likelihood test stopped the loop before max_iterations */
+  int32_t status;         /* 0; 1: a covariance stopped being positive definite */
+  int32_t n_components;
+} gc_gmm_fit_result;
+
+/* Colour-model fit on the device: GMM.fit (GMM.pyx:165-372; initA, em1, em2, eval and
+   check_converge, gmm.cl:33-372), in float64.
+   - samples: DEVICE uint32 [n] RGBA words (R in bits 0-7, G 8-15, B 16-23), n >= n_components.
+   - Start (initA): weights 1/K; mean_k = the colour of sample k * (n - 1) / (K - 1) (integer
+     division; sample 0 when K = 1); covariance init_covar * I.
+   - Iteration: responsibilities r_k(x) = w_k N(x | mean_k, S_k) / p(x) under the current
+     model; N_k = sum r_k; w_k = N_k / sum_j N_j; mean_k = sum r_k x / N_k;
+     S_k = sum r_k x x^T / N_k - mean_k mean_k^T + min_covar * I, off-diagonal terms set to 0
+     unless full_covariance.  A component whose N_k is 0 keeps its mean and covariance with
+     weight 0.
+   - Stop: L_i, the log-likelihood of the samples under the model of iteration i, is
+     evaluated after each iteration; for i > 1 the loop stops when |L_i - L_{i-1}| < tolerance
+     (the reference uses 0.01), else after max_iterations.
+   - 1 <= n_components <= GC_GMM_MAX_COMPONENTS, 1 <= max_iterations <= 100000, tolerance,
+     min_covar >= 0 and init_covar > 0 finite; otherwise GC_ERR_INVALID.
+   - One launch of one thread-block cluster whose blocks add their sums through distributed
+     shared memory in a fixed order, so results are deterministic; they equal a float64 host
+     evaluation of the same steps up to rounding.  *result is complete when the stream
+     reaches the end of the call; result->status 1 means the fit stopped early. */
+int gc_gmm_fit(const uint32_t* samples, int n, int n_components, int max_iterations,
+               double tolerance, double min_covar, double init_covar, int full_covariance,
+               gc_gmm_fit_result* result, void* stream);
+
 /* Max-flow to the final cut.  Replaces GraphCut.cut (GraphCut.pyx:348-418); warm-starts
    from the current residual graph when called again after gc_edit_tlinks.  Blocks the
    calling host thread until the solve is done (it polls the active-tile count). */

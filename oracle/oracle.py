@@ -14,6 +14,7 @@ this module to check results; the product never imports it.
   incremental_tile_list.cl:40-154 (stamp predicates).  Pinned by the reference's own
   known-answer checks (test_PrefixSum.py:35, test_StreamCompact.py:40-41,
   test_IncrementalTileList.py:38-40) in tests/test_oracle.py.
+* ``gmm_fit``         EM fit of a colour model (GMM.fit, GMM.pyx:165-372; gmm.cl:33-372).
 * ``tlinks_gmm``      t-links from a foreground and a background colour model (GMM.score,
                       gmm.cl:373-491, and scoreBg - scoreFg, test_GraphCut.py:44-47).
 """
@@ -202,3 +203,68 @@ def tiles_view(tiles, tile_w, tile_h, iteration, width, height):
         stamp = tiles[np.minimum(ty, th - 1), np.minimum(tx, tw - 1)]
         on = inside & (stamp == iteration)
     return np.where(on, np.uint32(0xFF0000FF), np.uint32(0xFF000000)).astype(np.uint32)
+
+
+# --- colour-model fit (GMM.fit) ----------------------------------------------------------
+
+def _colours(samples):
+    p = np.asarray(samples).view(np.uint32).reshape(-1)
+    return np.stack([p & 0xFF, (p >> 8) & 0xFF, (p >> 16) & 0xFF], 1).astype(np.float64)
+
+
+def _log_joint(x, w, mu, S):
+    """log(w_k N(x | mu_k, S_k)) for every sample and component (float64 [n, K])."""
+    e = np.empty((x.shape[0], len(w)))
+    for k in range(len(w)):
+        L = np.linalg.cholesky(S[k])
+        y = np.linalg.solve(L, (x - mu[k]).T)
+        logdet = 2.0 * np.log(np.diag(L)).sum()
+        with np.errstate(divide="ignore"):
+            e[:, k] = np.log(w[k]) - 0.5 * (3 * np.log(2 * np.pi) + logdet) - 0.5 * (y * y).sum(0)
+    return e
+
+
+def gmm_fit(samples, n_components, max_iterations, tolerance=0.01, min_covar=1e-3,
+            init_covar=30.0, full=False):
+    """EM restating GMM.fit (GMM.pyx:165-372) with initA / em1 / em2 / eval /
+    check_converge (gmm.cl:33-372) in float64: means start at the colours of samples
+    k (n - 1) / (K - 1), covariances at init_covar I, weights 1/K; each iteration takes the
+    responsibilities under the current model, then N_k = sum r, w = N / sum N,
+    mean = sum r x / N, S = sum r x x^T / N - mean mean^T + min_covar I (diagonal unless
+    ``full``); L_i, the log-likelihood under the model of iteration i, stops the loop when
+    i > 1 and |L_i - L_{i-1}| < tolerance.  (initA reads green through the mask 0xFF0,
+    gmm.cl:54; the green byte is used here.)  Returns a dict: weights [K], means [K, 3],
+    covars [K, 3, 3], iterations, converged, log_likelihood."""
+    x = _colours(samples)
+    n, K = x.shape[0], n_components
+    idx = [k * (n - 1) // (K - 1) for k in range(K)] if K > 1 else [0]
+    w = np.full(K, 1.0 / K)
+    mu = x[idx].copy()
+    S = np.stack([np.eye(3) * init_covar for _ in range(K)])
+    lprev, t, converged = 0.0, 0, False
+    while True:
+        e = _log_joint(x, w, mu, S)
+        m = e.max(1)
+        lpr = m + np.log(np.exp(e - m[:, None]).sum(1))
+        L = float(lpr.sum())
+        stop = False
+        if t >= 1:
+            if t - 1 > 1 and abs(L - lprev) < tolerance:
+                stop = converged = True
+            lprev = L
+        if not stop and t == max_iterations:
+            stop = True
+        if stop:
+            return {"weights": w, "means": mu, "covars": S, "iterations": t,
+                    "converged": converged, "log_likelihood": L}
+        r = np.exp(e - lpr[:, None])
+        nk = r.sum(0)
+        for k in range(K):
+            if not nk[k] > 0:
+                w[k] = 0.0
+                continue
+            w[k] = nk[k] / nk.sum()
+            mu[k] = (r[:, k] @ x) / nk[k]
+            c = (r[:, k, None] * x).T @ x / nk[k] - np.outer(mu[k], mu[k])
+            S[k] = (c if full else np.diag(np.diag(c))) + min_covar * np.eye(3)
+        t += 1
