@@ -84,6 +84,11 @@ def parse():
                     help="warm up, then run one host-driven solve of the --size grid inside the "
                          "NVTX range 'profiled_solve' and print its per-kernel launches and "
                          "tiles (the command the ncu summaries are made from)")
+    ap.add_argument("--profile-models", action="store_true",
+                    help="one gc_tlinks_gmm launch on the --size image (two 2-component "
+                         "full-covariance models) and one gc_gmm_fit launch (10000 samples, 4 "
+                         "components, 65 iterations), after a warm-up of each: the command the "
+                         "ncu summaries of those two kernels are made from")
     ap.add_argument("--host-driven", action="store_true",
                     help="solve loops decided by the host (use_graph=0); ncu does not profile "
                          "kernels inside conditional CUDA-graph nodes, so profiling runs use this")
@@ -274,6 +279,8 @@ def main():
         return run_serving(args)
     if args.profile_solve:
         return run_profile_solve(args)
+    if args.profile_models:
+        return run_profile_models(args)
     import torch
     import torch.distributed as dist
 
@@ -538,6 +545,33 @@ def run_profile_solve(args):
                       "flow": gc.flow, "stats": gc.stats(),
                       "kernels": {k: v for k, v in prof.items() if v["launches"]}}), flush=True)
     gc.close()
+
+
+def run_profile_models(args):
+    """See --profile-models.  Prints the two kernels' CUDA-event times."""
+    import torch
+
+    import synth
+    from gmm_tlinks import Mixture, tlinks
+    from GraphCut import _as_rgba32
+    W = H = args.size
+    g = synth.make_graph(W, H, 1, keep_image=True)
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    rgba = torch.from_numpy(np.ascontiguousarray(_as_rgba32(g.image)).view(np.int32)).cuda()
+    ex = torch.empty((H, W), dtype=torch.int32, device="cuda")
+    models = tuple(Mixture.from_components(c) for c in g.models)
+    with torch.cuda.stream(stream):
+        tlinks(rgba, *models, out=ex, stream=stream)       # warm-up
+        stream.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        tlinks(rgba, *models, out=ex, stream=stream)
+        ev[1].record(stream)
+        ev[1].synchronize()
+    fit = time_gmm_fit(g, stream, False)
+    print(json.dumps({"tlinks_gmm_ms": ev[0].elapsed_time(ev[1]), "gmm_fit_ms": fit["ms"],
+                      "size": [W, H], "fit": fit}), flush=True)
 
 
 def _percentile(xs, p):
