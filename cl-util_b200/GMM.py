@@ -28,6 +28,11 @@ TOLERANCE = 0.01     # GMM.pyx:329
 
 
 class GMM:
+    """``GMM(n_iterations, n_components, cap_samples, min_covar, init_covar)`` as in the
+    reference (GMM.pyx:59-93).  ``cap_samples`` is accepted and ignored: the reference sizes
+    its per-sample responsibility buffers with it, and the device fit keeps no per-sample
+    state."""
+
     def __init__(self, n_iterations: int, n_components: int, cap_samples=None,
                  min_covar=None, init_covar=None, tolerance: float = TOLERANCE,
                  full_covariance: bool = False, device=0):

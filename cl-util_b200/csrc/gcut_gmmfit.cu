@@ -19,7 +19,6 @@
 #include <cooperative_groups.h>
 
 #include <cmath>
-#include <cstdio>
 
 #include "gcut_internal.h"
 
