@@ -26,6 +26,12 @@ int fail(int code, const char* msg) {
   return code;
 }
 
+// Serialises CUDA-graph construction and destruction across the handles of the process.
+std::mutex& graph_build_mutex() {
+  static std::mutex mu;
+  return mu;
+}
+
 int cuda_fail(cudaError_t e, const char* where) {
   g_err = std::string(where) + ": " + cudaGetErrorString(e);
   return GC_ERR_CUDA;
@@ -600,19 +606,34 @@ struct Pool {
     return GC_OK;
   }
 
+  // The kernels read a conditional handle of value 0 as "not launched from a graph" (the
+  // host-driven loop passes 0).  The runtime does not promise that 0 is never a valid handle,
+  // so a handle that comes out as 0 is left unused in the graph and another one is created.
+  int cond_handle(cudaGraphConditionalHandle* h, cudaGraph_t g) {
+    for (int tries = 0; tries < 4; ++tries) {
+      CK(cudaGraphConditionalHandleCreate(h, g, 0, 0));
+      if (*h != 0) return GC_OK;
+    }
+    return fail(GC_ERR_INTERNAL, "cudaGraphConditionalHandleCreate gave only handle 0");
+  }
+
   int build_graph(int variant) {
+    // One graph construction at a time in the process: building, instantiating and
+    // destroying graphs with nested conditional nodes from several threads at once is the
+    // suspected trigger of an intermittent fault under concurrent serving.
+    std::lock_guard<std::mutex> lock(graph_build_mutex());
     if (!cap_stream) CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
     cudaGraph_t g;
     CK(cudaGraphCreate(&g, 0));
     graph[variant] = g;
     std::vector<cudaGraphNode_t> L;
     cudaGraphConditionalHandle hmain, hflood;
-    CK(cudaGraphConditionalHandleCreate(&hmain, g, 0, 0));
-    CK(cudaGraphConditionalHandleCreate(&hflood, g, 0, 0));
+    RK(cond_handle(&hmain, g));
+    RK(cond_handle(&hflood, g));
     RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs); }));
     if (variant) {  // exact global relabel before the first push
       cudaGraphConditionalHandle h0;
-      CK(cudaGraphConditionalHandleCreate(&h0, g, 0, 0));
+      RK(cond_handle(&h0, g));
       RK(capture(g, L, [&](cudaStream_t cs) {
         RK(launch_masks(P, grid_warps, cs));
         return launch_bfs_round(P, 1, h0, grid_warps, cs);
@@ -630,7 +651,7 @@ struct Pool {
     {
       std::vector<cudaGraphNode_t> Lm;
       cudaGraphConditionalHandle hb;
-      CK(cudaGraphConditionalHandleCreate(&hb, bm, 0, 0));
+      RK(cond_handle(&hb, bm));
       RK(capture(bm, Lm, [&](cudaStream_t cs) {
         for (int p = 0; p < opts.pulses_per_relabel; ++p)
           RK(launch_discharge(P, opts.discharge_iters, grid_dis, cs));
@@ -681,6 +702,7 @@ struct Pool {
   }
 
   void release_graphs() {
+    std::lock_guard<std::mutex> lock(graph_build_mutex());
     for (int v = 0; v < 2; ++v) {
       if (gexec[v]) cudaGraphExecDestroy(gexec[v]);
       if (graph[v]) cudaGraphDestroy(graph[v]);
