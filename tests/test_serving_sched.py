@@ -209,3 +209,17 @@ def test_image_larger_than_budget_is_refused():
         srv.drain(timeout=10)
     srv.close()
     assert [r.session for r in srv.results] == [1]
+
+
+def test_new_image_shape_for_every_request_form():
+    """A new session may carry the five capacity planes, (image, t-links) or (image, models);
+    its size comes from the t-link plane or, with models, from the image."""
+    h, w = 30, 50
+    planes = tuple(np.zeros((h, w), np.int32) for _ in range(5))
+    rgba32 = np.zeros((h, w), np.uint32)
+    rgb8 = np.zeros((h, w, 3), np.uint8)
+    fg = bg = np.zeros((1, 10))
+    assert NewImage(0, planes).shape == (h, w)
+    assert NewImage(0, (rgba32, planes[4])).shape == (h, w)
+    assert NewImage(0, (rgba32, (fg, bg))).shape == (h, w)
+    assert NewImage(0, (rgb8, (fg, bg))).shape == (h, w)
