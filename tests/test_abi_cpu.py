@@ -73,3 +73,39 @@ def test_arena_bytes_host_only():
     assert sizes[(4096, 4096)] > 28 * 4096 * 4096            # 7 int32 planes at least
     assert sizes[(4096, 4096)] < 32 * 4096 * 4096
     assert lib.gc_arena_bytes(0, 5, ctypes.byref(out)) == 1   # GC_ERR_INVALID
+
+
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """The ctypes mirrors of the header's structs have the sizes and field offsets gcc gives
+    the C declarations (a drift here would corrupt every call that passes them)."""
+    import shutil
+    import subprocess
+
+    import _gcut
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not found")
+    fields = {
+        "gc_opts": (_gcut.GcOpts, ["device", "discharge_iters", "max_cycles", "use_graph"]),
+        "gc_stats": (_gcut.GcStats, ["cycles", "launches", "tiles_discharged"]),
+        "gc_gauss": (_gcut.GcGauss, ["c", "mean", "li"]),
+        "gc_gmm_fit_result": (_gcut.GcGmmFitResult,
+                              ["weights", "means", "covars", "log_likelihood", "iterations",
+                               "converged", "status", "n_components"]),
+    }
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "gcut.h"', "int main(void) {"]
+    for name, (_, fs) in fields.items():
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for f in fs:
+            lines.append(f'  printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)],
+                   check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                       text=True).stdout.splitlines())
+    for name, (cls, fs) in fields.items():
+        assert int(got[name]) == ctypes.sizeof(cls), name
+        for f in fs:
+            assert int(got[f"{name}.{f}"]) == getattr(cls, f).offset, (name, f)
