@@ -94,6 +94,9 @@ class GMM:
         self.iterations = int(r.iterations)
         self.has_converged = bool(r.converged)
         self.log_likelihood = float(r.log_likelihood)
+        # the model's evaluation form as the device computed it ([K, 10] rows of gc_gauss)
+        self.device_components = np.array(
+            [[r.components[k].c, *r.components[k].mean, *r.components[k].li] for k in range(K)])
         if r.status:
             raise _gcut.GCError(_gcut.GC_ERR_NOT_CONVERGED,
                                 "gc_gmm_fit: a covariance stopped being positive definite "

@@ -60,7 +60,8 @@ class GcGmmFitResult(ctypes.Structure):
     _fields_ = [("weights", ctypes.c_double * 8), ("means", (ctypes.c_double * 3) * 8),
                 ("covars", (ctypes.c_double * 6) * 8), ("log_likelihood", ctypes.c_double),
                 ("iterations", ctypes.c_int32), ("converged", ctypes.c_int32),
-                ("status", ctypes.c_int32), ("n_components", ctypes.c_int32)]
+                ("status", ctypes.c_int32), ("n_components", ctypes.c_int32),
+                ("components", GcGauss * 8)]
 
 
 GC_NKERN = 10

@@ -243,6 +243,14 @@ k_gmm_fit(const uint32_t* __restrict__ samples, int n, int K, int max_iter, doub
       for (int j = 0; j < 3; ++j) out->means[k][j] = on ? sh.mu[k][j] : 0.0;
       for (int j = 0; j < 6; ++j) out->covars[k][j] = on ? sh.S[k][j] : 0.0;
     }
+    // the evaluation form computed at the top of the last iteration belongs to the returned
+    // model: the loop stops before an M-step
+    for (int k = 0; k < kMaxK; ++k) {
+      const bool on = k < K && !sh.status;
+      out->components[k].c = on ? sh.c[k] : 0.0;
+      for (int j = 0; j < 3; ++j) out->components[k].mean[j] = on ? sh.mu[k][j] : 0.0;
+      for (int j = 0; j < 6; ++j) out->components[k].li[j] = on ? sh.li[k][j] : 0.0;
+    }
     out->log_likelihood = sh.lcur;
     out->iterations = sh.iterations;
     out->converged = sh.converged;

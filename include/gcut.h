@@ -167,6 +167,9 @@ typedef struct gc_gmm_fit_result {
   int32_t converged;      /* 1: the likelihood test stopped the loop before max_iterations */
   int32_t status;         /* 0; 1: a covariance stopped being positive definite */
   int32_t n_components;
+  /* the returned model in the form gc_tlinks_gmm takes (all zero when status is 1); leave
+     out components of weight 0, whose c is -infinity */
+  gc_gauss components[GC_GMM_MAX_COMPONENTS];
 } gc_gmm_fit_result;
 
 /* Colour-model fit on the device: GMM.fit (GMM.pyx:165-372; initA, em1, em2, eval and

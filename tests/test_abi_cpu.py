@@ -90,7 +90,7 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
         "gc_gauss": (_gcut.GcGauss, ["c", "mean", "li"]),
         "gc_gmm_fit_result": (_gcut.GcGmmFitResult,
                               ["weights", "means", "covars", "log_likelihood", "iterations",
-                               "converged", "status", "n_components"]),
+                               "converged", "status", "n_components", "components"]),
     }
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "gcut.h"', "int main(void) {"]
     for name, (_, fs) in fields.items():

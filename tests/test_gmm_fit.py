@@ -99,7 +99,7 @@ def test_abi_argument_checks(L):
 
 def test_result_layout_matches_header():
     import _gcut
-    assert ctypes.sizeof(_gcut.GcGmmFitResult) == 8 * (8 + 24 + 48 + 1) + 4 * 4
+    assert ctypes.sizeof(_gcut.GcGmmFitResult) == 8 * (8 + 24 + 48 + 1) + 4 * 4 + 8 * 80
 
 
 def test_gmm_class_checks():

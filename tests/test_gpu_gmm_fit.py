@@ -41,6 +41,12 @@ def test_fit_matches_oracle(cuda, oracle, K, full, n, iters, tol):
     g = GMM(iters, K, tolerance=tol, full_covariance=full)
     g.fit(s)
     _compare(g, oracle.gmm_fit(s, K, iters, tolerance=tol, full=full), full)
+    # the evaluation form the device returns is that of the returned model
+    from gmm_tlinks import components
+    keep = g.weights > 0
+    np.testing.assert_allclose(g.device_components[keep],
+                               components(g.weights[keep], g.means[keep], g.covars[keep]),
+                               rtol=1e-9, atol=1e-9)
 
 
 def test_fit_is_deterministic_and_takes_device_samples(cuda):
