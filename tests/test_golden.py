@@ -38,6 +38,18 @@ def test_oracle_reproduces_golden(oracle, name):
     assert oracle.cut_capacity(up, down, left, right, ex, labels) == flow
 
 
+@pytest.mark.parametrize("name", NAMES)
+def test_restated_reference_schedule_gives_the_golden_flow(oracle, name):
+    """ref_tiled (GraphCut.cut + graphcut.cl restated) on the fixture padded to whole tiles
+    with isolated pixels, which carry no flow."""
+    planes, ex, flow, _ = load(name)
+    h, w = ex.shape
+    ph, pw = -(-h // 32) * 32, -(-w // 32) * 32
+    pad = [np.pad(a, ((0, ph - h), (0, pw - w))) for a in (*planes, ex)]
+    f, _, _ = oracle.ref_tiled(*pad)
+    assert f == flow
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", NAMES)
 def test_cuda_reproduces_golden(cuda, name):
