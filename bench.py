@@ -74,8 +74,8 @@ def parse():
     ap.add_argument("--duration", type=float, default=60.0, help="seconds of --config serving trace")
     ap.add_argument("--rate", type=float, default=200.0, help="requests/s of --config serving")
     ap.add_argument("--slots", type=int, default=1,
-                    help="requests in flight, --config serving (more than 1 raised an "
-                         "intermittent device fault whose cause is not yet found)")
+                    help="requests in flight, --config serving; only 1 is accepted (more "
+                         "raised an intermittent device fault whose cause is not found)")
     ap.add_argument("--verify-s", type=float, default=90.0,
                     help="wall-time cap of the --config serving result verification")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -269,6 +269,9 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.slots != 1:
+        sys.exit("bench.py: --slots must be 1 (concurrent serving slots raised an "
+                 "intermittent device fault whose cause is not found)")
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "batch":

@@ -15,10 +15,11 @@ on a button press (test_GraphCut.py:78-99).  Here many sessions share one GPU:
   of the least-recently-used idle session of its size, else evicts least-recently-used
   idle sessions until a range fits.  Creating and evicting sessions therefore never calls
   cudaMalloc / cudaFree, which synchronise the device, on the request path;
-* continuous batching: up to ``slots`` requests are on the GPU at once, each on its own
-  worker thread and stream; a request starts as soon as a slot is free and its session is
-  idle (a stroke waits only for its own session), so solves of different sizes overlap on
-  the device.  The solver calls release the Python GIL;
+* slots: each slot is a worker thread with its own stream; a request starts as soon as a
+  slot is free and its session is idle (a stroke waits only for its own session).  The
+  device server accepts one slot (``MAX_SLOTS``): several requests in flight on separate
+  streams raised an intermittent device fault whose cause is not established.  The
+  solver calls release the Python GIL;
 * scheduling is earliest-arrival-first over the head new image and the sessions with a
   queued stroke, with one slot kept for strokes (at most ``slots - 1`` new images in
   flight), so an edit never waits behind a wall of image uploads.  Strokes of one session
@@ -152,8 +153,18 @@ class _Session:
 class GraphCutServer:
     """Serves NewImage / Stroke requests on one GPU (see the module docstring)."""
 
-    def __init__(self, slots: int = 4, hbm_budget: int = 16 << 30, device: int = 0,
+    # Requests in flight at once.  Several requests on separate streams raised an
+    # intermittent "unspecified launch failure" on the B200 whose cause is not established,
+    # so the device server runs one at a time; the scheduler itself handles any number
+    # (its host-side tests run it with several slots against a fake solver).
+    MAX_SLOTS = 1
+
+    def __init__(self, slots: int = 1, hbm_budget: int = 16 << 30, device: int = 0,
                  solver_kw=None, max_pixels: int = 4096 * 4096):
+        if not 1 <= slots <= self.MAX_SLOTS:
+            raise ValueError(f"GraphCutServer: slots must be between 1 and {self.MAX_SLOTS} "
+                             "(concurrent slots raised an intermittent device fault whose "
+                             "cause is not found)")
         import torch
         self.torch = torch
         self.device = device

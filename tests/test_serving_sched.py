@@ -60,6 +60,8 @@ class FakeContext:
 
 
 class FakeServer(GraphCutServer):
+    MAX_SLOTS = 8   # the scheduler's own limit; the device server accepts 1
+
     def __init__(self, *a, **k):
         self.images_running = 0
         self.max_images_running = 0
