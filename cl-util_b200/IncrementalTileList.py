@@ -4,14 +4,17 @@ Mirrors of the reference classes beneath GraphCut (IncrementalTileList.pyx:26-20
 StreamCompact.pyx:22-82, PrefixSum.pyx:121-226) with the same method names, argument
 meaning and ValueError on capacity overflow.  Buffers are torch int32 CUDA tensors; every
 build / compact / scan is one kernel launch (decoupled look-back) instead of the
-reference's flag + copy + 1-3 scan launches + scatter.
+reference's flag + copy + 1-3 scan launches + scatter.  Each object owns its look-back
+state (as each reference object owns its buffers), so objects on different streams do not
+interfere; a look-back error of an earlier call raises GCError at the next call, and a
+compacted length of -1 (a wait that gave up) raises when `length` is read.
 """
 from __future__ import annotations
 
 import ctypes
 
 import _gcut
-from _gcut import check, lib, ptr, stream_handle
+from _gcut import ScanState, check, lib, ptr, stream_handle
 
 
 class Operator:
@@ -49,6 +52,7 @@ class PrefixSum:
         import torch
         self.capacity = int(capacity)
         self.device = torch.device("cuda", device) if isinstance(device, int) else device
+        self.state = ScanState(self.device.index or 0, self.capacity)
 
     def factory(self, length=None):
         """A scan buffer; its size is rounded up to a power of two (PrefixSum.pyx:168-176)."""
@@ -64,8 +68,8 @@ class PrefixSum:
             length = dArray.numel()
         if length > self.capacity:
             raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
-        check(lib().gc_scan_exclusive(ptr(dArray), ptr(dArray), ptr(dTotal), int(length),
-                                      stream_handle(stream)))
+        check(lib().gc_scan_exclusive(self.state.handle, ptr(dArray), ptr(dArray), ptr(dTotal),
+                                      int(length), stream_handle(stream)))
 
 
 class StreamCompact:
@@ -75,6 +79,7 @@ class StreamCompact:
         import torch
         self.capacity = int(capacity)
         self.device = torch.device("cuda", device) if isinstance(device, int) else device
+        self.state = ScanState(self.device.index or 0, self.capacity)
 
     def flagFactory(self, length=None):
         if length is None:
@@ -96,8 +101,8 @@ class StreamCompact:
             length = dFlags.numel()
         elif length > self.capacity:
             raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
-        check(lib().gc_compact(ptr(dFlags), ptr(dList), ptr(dLength), int(length),
-                               stream_handle(stream)))
+        check(lib().gc_compact(self.state.handle, ptr(dFlags), ptr(dList), ptr(dLength),
+                               int(length), stream_handle(stream)))
 
 
 class IncrementalTileList:
@@ -112,6 +117,7 @@ class IncrementalTileList:
         self.device = torch.device("cuda", device) if isinstance(device, int) else device
         n = self.dim[0] * self.dim[1]
         self.d_tiles = torch.zeros((self.dim[1], self.dim[0]), dtype=torch.int32, device=self.device)
+        self.state = ScanState(self.device.index or 0, n)
         self.d_list = _i32(n, self.device)
         self.d_length = _i32(1, self.device)
         self.init_iteration = -1
@@ -127,7 +133,11 @@ class IncrementalTileList:
     def length(self) -> int:
         """Number of tiles in d_list (one device->host read when dirty)."""
         if self.is_dirty:
-            self._length = int(self.d_length[0].item())
+            n = int(self.d_length[0].item())
+            if n < 0:
+                raise _gcut.GCError(_gcut.GC_ERR_INTERNAL, "the tile-list compaction gave up "
+                                    f"a bounded look-back wait (error {self.state.error()})")
+            self._length = n
             self.is_dirty = False
         return self._length
 
@@ -142,9 +152,9 @@ class IncrementalTileList:
             operator = Operator.EQUAL
         if operand is None:
             operand = self.iteration
-        check(lib().gc_tiles_build(ptr(self.d_tiles), int(operator), int(operand),
-                                   ptr(self.d_list), ptr(self.d_length), self.n_tiles,
-                                   stream_handle(stream)))
+        check(lib().gc_tiles_build(self.state.handle, ptr(self.d_tiles), int(operator),
+                                   int(operand), ptr(self.d_list), ptr(self.d_length),
+                                   self.n_tiles, stream_handle(stream)))
         self.is_dirty = True
 
     def incorporate(self, d_tiles2, operator1, operand1, operator2, operand2, logical,
@@ -157,10 +167,11 @@ class IncrementalTileList:
 
     def buildLogical(self, d_tiles2, operator1, operand1, operator2, operand2, logical,
                      stream=None):
-        check(lib().gc_tiles_build_logical(ptr(self.d_tiles), ptr(d_tiles2), int(operator1),
-                                           int(operand1), int(operator2), int(operand2),
-                                           int(logical), ptr(self.d_list), ptr(self.d_length),
-                                           self.n_tiles, stream_handle(stream)))
+        check(lib().gc_tiles_build_logical(self.state.handle, ptr(self.d_tiles),
+                                           ptr(d_tiles2), int(operator1), int(operand1),
+                                           int(operator2), int(operand2), int(logical),
+                                           ptr(self.d_list), ptr(self.d_length), self.n_tiles,
+                                           stream_handle(stream)))
         self.is_dirty = True
 
     def execute(self, out=None, stream=None):

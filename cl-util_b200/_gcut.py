@@ -106,11 +106,15 @@ SIGNATURES = {
     "gc_get_profile": [_P, _P, _I],
     "gc_kernel_name": [_I],
     "gc_last_error": [],
-    "gc_scan_exclusive": [_P, _P, _P, _I, _P],
-    "gc_compact": [_P, _P, _P, _I, _P],
+    "gc_scan_state_create": [_I, _I, _P],
+    "gc_scan_state_destroy": [_P],
+    "gc_scan_state_error": [_P, _P, _P],
+    "gc_scan_state_selftest": [_P, _I, _P, _P],
+    "gc_scan_exclusive": [_P, _P, _P, _P, _I, _P],
+    "gc_compact": [_P, _P, _P, _P, _I, _P],
     "gc_compact_noalloc": [_P, _P, _P, _I, _P],
-    "gc_tiles_build": [_P, _I, _I32, _P, _P, _I, _P],
-    "gc_tiles_build_logical": [_P, _P, _I, _I32, _I, _I32, _I, _P, _P, _I, _P],
+    "gc_tiles_build": [_P, _P, _I, _I32, _P, _P, _I, _P],
+    "gc_tiles_build_logical": [_P, _P, _P, _I, _I32, _I, _I32, _I, _P, _P, _I, _P],
     "gc_tiles_incorporate": [_P, _P, _I, _I32, _I, _I32, _I, _I32, _I, _P],
     "gc_tiles_fill": [_P, _I32, _I, _P],
     "gc_tiles_view": [_P, _I, _I, _I, _I, _I32, _I, _I, _P, _P],
@@ -149,6 +153,46 @@ def check(rc: int):
     if rc != GC_OK:
         msg = lib().gc_last_error()
         raise GCError(rc, msg.decode() if msg else "")
+
+
+class ScanState:
+    """One look-back state of the scan primitives (gc_scan_state): every PrefixSum,
+    StreamCompact and IncrementalTileList owns one, as each reference object owns its own
+    buffers, so objects used on different streams never share look-back words."""
+
+    def __init__(self, device: int, max_items: int):
+        h = ctypes.c_void_p()
+        check(lib().gc_scan_state_create(int(device), int(max_items), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def error(self, stream=None) -> int:
+        """The error word (0: none; 1: a look-back wait gave up; 2: a scatter index was out
+        of range), read synchronously and cleared."""
+        e = ctypes.c_int(0)
+        check(lib().gc_scan_state_error(self._h, ctypes.byref(e), stream_handle(stream)))
+        return int(e.value)
+
+    def selftest(self, spins: int, stream=None) -> int:
+        """Runs gc_scan_state_selftest: a bounded look-back wait that must run out."""
+        e = ctypes.c_int(0)
+        check(lib().gc_scan_state_selftest(self._h, int(spins), ctypes.byref(e),
+                                           stream_handle(stream)))
+        return int(e.value)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gc_scan_state_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def default_opts(**overrides) -> GcOpts:

@@ -817,27 +817,112 @@ struct gcb_handle {
 };
 
 // ------------------------------------------------------------------------------------
-// Per-device look-back state for the stand-alone primitives.
+// Look-back state of the stand-alone primitives (gc_scan_state).  The reference gives every
+// tile list its own StreamCompact and PrefixSum objects (IncrementalTileList.pyx:74,
+// StreamCompact.pyx:39, PrefixSum.pyx:46); here every such object owns one state, so calls
+// from different objects on different streams never share tickets or status words.  A state
+// passed as NULL selects one shared state per device.
+//
+// The device error word is sticky: a launch that gives up a look-back wait (or whose scatter
+// index is out of range) sets it and it stays set until the host reports it.  After each
+// launch the word is copied into pinned host memory on the caller's stream; the next call on
+// the state returns GC_ERR_INTERNAL once that copy has landed with a non-zero word, and
+// gc_scan_state_error reads it synchronously.
 // ------------------------------------------------------------------------------------
-namespace {
-std::mutex g_scan_mu;
-std::unordered_map<int, ScanBuffers> g_scan;
+struct gc_scan_state {
+  int device = 0;
+  ScanBuffers buf;
+  int32_t* h_err = nullptr;     // pinned mirror of the device error word
+  cudaEvent_t ev = nullptr;     // the last mirror copy
+  bool pending = false;
+  std::mutex mu;                // one call at a time on a state
+  ~gc_scan_state() {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    if (ev) { cudaEventSynchronize(ev); cudaEventDestroy(ev); }
+    buf.release();
+    if (h_err) cudaFreeHost(h_err);
+    cudaSetDevice(cur);
+  }
+};
 
-int device_scan_state(ScanState* out) {
+namespace {
+constexpr int kDefaultScanChunks = 1 << 16;   // the shared per-device state: 2^28 items
+
+int scan_state_init(gc_scan_state* S, int device, int chunks) {
+  S->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e) return cuda_fail(e, "cudaSetDevice");
+  preload_kernels();
+  e = S->buf.alloc(chunks);
+  if (e) { cudaGetLastError(); return e == cudaErrorMemoryAllocation ? fail(GC_ERR_OOM, "scan state") : cuda_fail(e, "scan state"); }
+  e = cudaHostAlloc((void**)&S->h_err, sizeof(int32_t), cudaHostAllocPortable);
+  if (e) { S->h_err = nullptr; cudaGetLastError(); return fail(GC_ERR_OOM, "pinned host allocation failed"); }
+  *S->h_err = 0;
+  e = cudaEventCreateWithFlags(&S->ev, cudaEventDisableTiming);
+  if (e) { S->ev = nullptr; return cuda_fail(e, "event"); }
+  return GC_OK;
+}
+
+std::mutex g_scan_mu;
+std::unordered_map<int, gc_scan_state*> g_scan;   // shared per-device states (never freed)
+
+// The state a primitive runs on (the caller's, or the device's shared one), with the device
+// made current.
+int resolve_scan_state(gc_scan_state* S, gc_scan_state** out) {
+  if (S) {
+    cudaError_t e = cudaSetDevice(S->device);
+    if (e) return cuda_fail(e, "cudaSetDevice");
+    *out = S;
+    return GC_OK;
+  }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e) return cuda_fail(e, "cudaGetDevice");
-  preload_kernels();
   std::lock_guard<std::mutex> lock(g_scan_mu);
   auto it = g_scan.find(dev);
   if (it == g_scan.end()) {
-    ScanBuffers b;
-    e = b.alloc(1 << 16);
-    if (e) { b.release(); return e == cudaErrorMemoryAllocation ? fail(GC_ERR_OOM, "scan state") : cuda_fail(e, "scan state"); }
-    it = g_scan.emplace(dev, b).first;
+    gc_scan_state* n = new (std::nothrow) gc_scan_state();
+    if (!n) return fail(GC_ERR_OOM, "host allocation");
+    const int r = scan_state_init(n, dev, kDefaultScanChunks);
+    if (r) { delete n; return r; }
+    it = g_scan.emplace(dev, n).first;
   }
-  *out = it->second.st;
+  *out = it->second;
   return GC_OK;
+}
+
+// An error recorded by an earlier launch whose mirror copy has landed (no wait).
+int scan_state_take_error(gc_scan_state* S, cudaStream_t s) {
+  if (!S->pending || cudaEventQuery(S->ev) != cudaSuccess) { cudaGetLastError(); return GC_OK; }
+  S->pending = false;
+  if (*S->h_err == 0) return GC_OK;
+  const int code = *S->h_err;
+  *S->h_err = 0;
+  CK(cudaMemsetAsync(S->buf.st.err, 0, sizeof(int32_t), s));
+  return fail(GC_ERR_INTERNAL, code == 1 ? "an earlier call on this scan state gave up a bounded look-back wait"
+                                         : "an earlier call on this scan state computed an out-of-range index");
+}
+
+// After a launch: mirror the error word into pinned memory on the caller's stream.
+int scan_state_track(gc_scan_state* S, cudaStream_t s) {
+  CK(cudaMemcpyAsync(S->h_err, S->buf.st.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaEventRecord(S->ev, s));
+  S->pending = true;
+  return GC_OK;
+}
+
+// Runs one primitive launch on a state: reports an earlier error, launches, mirrors.
+template <class F>
+int with_scan_state(gc_scan_state* state, cudaStream_t s, F&& launch) {
+  gc_scan_state* S = nullptr;
+  RK(resolve_scan_state(state, &S));
+  std::lock_guard<std::mutex> lock(S->mu);
+  RK(scan_state_take_error(S, s));
+  const int r = launch(S->buf.st);
+  if (r) return r == GC_ERR_INVALID ? fail(r, "input larger than the scan state holds") : fail(r, "launch failed");
+  return scan_state_track(S, s);
 }
 }  // namespace
 
@@ -1162,47 +1247,113 @@ int gc_set_collect_stats(gc_handle* h, int on) {
 }
 
 // ---- primitives -------------------------------------------------------------------
-int gc_scan_exclusive(const int32_t* in, int32_t* out, int32_t* total, int n, void* stream) {
+int gc_scan_state_create(int device, int max_items, gc_scan_state** out) {
   g_err.clear();
-  if (n < 0 || (n > 0 && (!in || !out)) || !total) return fail(GC_ERR_INVALID, "bad argument");
-  ScanState st;
-  RK(device_scan_state(&st));
-  return launch_scan(GC_SCAN_MODE_SCAN, in, nullptr, nullptr, out, nullptr, total, n, 0, 0, 0,
-                     0, 0, st, (cudaStream_t)stream);
+  if (!out || max_items < 0) return fail(GC_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  gc_scan_state* S = new (std::nothrow) gc_scan_state();
+  if (!S) return fail(GC_ERR_OOM, "host allocation");
+  // chunks of the widest launch on max_items: the scan's (4096 items each), at least two
+  // (the look-back self-test uses two)
+  int chunks = scan_chunks(max_items);
+  if (chunks < 2) chunks = 2;
+  const int r = scan_state_init(S, device, chunks);
+  if (r) { delete S; return r; }
+  *out = S;
+  return GC_OK;
 }
 
-int gc_compact(const int32_t* flags, int32_t* list, int32_t* length, int n, void* stream) {
+int gc_scan_state_destroy(gc_scan_state* S) {
+  if (!S) return GC_OK;
+  std::lock_guard<std::mutex> lock(g_scan_mu);
+  for (auto& kv : g_scan)
+    if (kv.second == S) return fail(GC_ERR_INVALID, "the shared per-device state is not destroyed");
+  delete S;
+  return GC_OK;
+}
+
+int gc_scan_state_error(gc_scan_state* state, int* err, void* stream) {
+  g_err.clear();
+  if (!err) return fail(GC_ERR_INVALID, "null argument");
+  gc_scan_state* S = nullptr;
+  RK(resolve_scan_state(state, &S));
+  std::lock_guard<std::mutex> lock(S->mu);
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(S->h_err, S->buf.st.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *err = *S->h_err;
+  S->pending = false;
+  if (*err) {
+    *S->h_err = 0;
+    CK(cudaMemsetAsync(S->buf.st.err, 0, sizeof(int32_t), s));
+    CK(cudaStreamSynchronize(s));
+  }
+  return GC_OK;
+}
+
+int gc_scan_state_selftest(gc_scan_state* state, int spins, int* err, void* stream) {
+  g_err.clear();
+  if (spins < 1) return fail(GC_ERR_INVALID, "bad argument");
+  gc_scan_state* S = nullptr;
+  RK(resolve_scan_state(state, &S));
+  {
+    std::lock_guard<std::mutex> lock(S->mu);
+    ScanState st = S->buf.st;
+    st.spin_limit = spins;
+    const int r = launch_lookback_selftest(st, (cudaStream_t)stream);
+    if (r) return fail(r, "self-test launch failed");
+    if (!err) return scan_state_track(S, (cudaStream_t)stream);   // reported like any error
+  }
+  return gc_scan_state_error(S, err, stream);
+}
+
+int gc_scan_exclusive(gc_scan_state* state, const int32_t* in, int32_t* out, int32_t* total,
+                      int n, void* stream) {
+  g_err.clear();
+  if (n < 0 || (n > 0 && (!in || !out)) || !total) return fail(GC_ERR_INVALID, "bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  return with_scan_state(state, s, [&](const ScanState& st) {
+    return launch_scan(GC_SCAN_MODE_SCAN, in, nullptr, nullptr, out, nullptr, total, n, 0, 0, 0,
+                       0, 0, st, s);
+  });
+}
+
+int gc_compact(gc_scan_state* state, const int32_t* flags, int32_t* list, int32_t* length,
+               int n, void* stream) {
   g_err.clear();
   if (n < 0 || (n > 0 && (!flags || !list)) || !length) return fail(GC_ERR_INVALID, "bad argument");
   if (n > 0 && flags == list) return fail(GC_ERR_INVALID, "list must not alias flags");
-  ScanState st;
-  RK(device_scan_state(&st));
-  return launch_scan(GC_SCAN_MODE_COMPACT, flags, nullptr, nullptr, nullptr, list, length, n, 0,
-                     0, 0, 0, 0, st, (cudaStream_t)stream);
+  cudaStream_t s = (cudaStream_t)stream;
+  return with_scan_state(state, s, [&](const ScanState& st) {
+    return launch_scan(GC_SCAN_MODE_COMPACT, flags, nullptr, nullptr, nullptr, list, length, n, 0,
+                       0, 0, 0, 0, st, s);
+  });
 }
 
-int gc_tiles_build(const int32_t* tiles, int op, int32_t operand, int32_t* list,
-                   int32_t* length, int n, void* stream) {
+int gc_tiles_build(gc_scan_state* state, const int32_t* tiles, int op, int32_t operand,
+                   int32_t* list, int32_t* length, int n, void* stream) {
   g_err.clear();
   if (n < 0 || (n > 0 && (!tiles || !list)) || !length || op < 0 || op > 4)
     return fail(GC_ERR_INVALID, "bad argument");
-  ScanState st;
-  RK(device_scan_state(&st));
-  return launch_scan(GC_SCAN_MODE_FLAG, tiles, nullptr, nullptr, nullptr, list, length, n, op,
-                     operand, 0, 0, 0, st, (cudaStream_t)stream);
+  cudaStream_t s = (cudaStream_t)stream;
+  return with_scan_state(state, s, [&](const ScanState& st) {
+    return launch_scan(GC_SCAN_MODE_FLAG, tiles, nullptr, nullptr, nullptr, list, length, n, op,
+                       operand, 0, 0, 0, st, s);
+  });
 }
 
-int gc_tiles_build_logical(const int32_t* tiles, const int32_t* tiles2, int op1, int32_t a1,
-                           int op2, int32_t a2, int logical, int32_t* list, int32_t* length,
-                           int n, void* stream) {
+int gc_tiles_build_logical(gc_scan_state* state, const int32_t* tiles, const int32_t* tiles2,
+                           int op1, int32_t a1, int op2, int32_t a2, int logical, int32_t* list,
+                           int32_t* length, int n, void* stream) {
   g_err.clear();
   if (n < 0 || (n > 0 && (!tiles || !tiles2 || !list)) || !length || op1 < 0 || op1 > 4 ||
       op2 < 0 || op2 > 4 || logical < 0 || logical > 1)
     return fail(GC_ERR_INVALID, "bad argument");
-  ScanState st;
-  RK(device_scan_state(&st));
-  return launch_scan(GC_SCAN_MODE_LOGICAL, tiles, tiles2, nullptr, nullptr, list, length, n, op1,
-                     a1, op2, a2, logical, st, (cudaStream_t)stream);
+  cudaStream_t s = (cudaStream_t)stream;
+  return with_scan_state(state, s, [&](const ScanState& st) {
+    return launch_scan(GC_SCAN_MODE_LOGICAL, tiles, tiles2, nullptr, nullptr, list, length, n,
+                       op1, a1, op2, a2, logical, st, s);
+  });
 }
 
 int gc_tiles_incorporate(int32_t* tiles, const int32_t* tiles2, int op1, int32_t a1, int op2,

@@ -98,8 +98,9 @@ struct ScanState {
   int32_t* ticket;             // dynamic chunk ids (reset by the last CTA)
   int32_t* done;               // finished CTAs (reset by the last CTA)
   uint32_t* seq;               // launch sequence tag (bumped by the last CTA)
-  int32_t* err;                // set when a look-back wait gives up
+  int32_t* err;                // set when a look-back wait gives up (sticky until read)
   int max_chunks;
+  int spin_limit;              // polls before a look-back wait gives up; 0: GC_SPIN_LIMIT
 };
 
 enum ScanStateFlag : unsigned { SS_NONE = 0, SS_AGG = 1, SS_PREFIX = 2 };
@@ -112,6 +113,10 @@ __device__ __forceinline__ unsigned long long ss_pack(uint32_t tag, unsigned st,
 // Spin limit for look-back waits: after this many polls the wait gives up, records an
 // error and continues, so a scheduling anomaly can never hang the GPU.
 #define GC_SPIN_LIMIT (1 << 22)
+
+__device__ __forceinline__ int spin_limit_of(const ScanState& st) {
+  return st.spin_limit > 0 ? st.spin_limit : GC_SPIN_LIMIT;
+}
 
 // Called by one thread (thread 0) of the CTA owning chunk `chunk` after it knows its own
 // aggregate.  Publishes the aggregate, walks back over predecessors and returns the
@@ -130,12 +135,13 @@ __device__ __forceinline__ int32_t lookback_exclusive(const ScanState& st, uint3
   int32_t excl = 0;
   int j = chunk - 1;
   int spins = 0;
+  const int limit = spin_limit_of(st);
   while (j >= 0) {
     unsigned long long s = status[j];
     uint32_t stag = (uint32_t)(s >> 34);
     unsigned sst = (unsigned)((s >> 32) & 3u);
     if (stag != (tag & 0x3fffffffu) || sst == SS_NONE) {
-      if (++spins > GC_SPIN_LIMIT) {
+      if (++spins > limit) {
         atomicExch(st.err, 1);
         break;
       }
@@ -167,6 +173,7 @@ __device__ __forceinline__ int32_t lookback_exclusive_warp(const ScanState& st, 
   int32_t excl = 0;
   int j = chunk - 1;
   int spins = 0;
+  const int limit = spin_limit_of(st);
   bool gave_up = false;
   while (j >= 0) {
     const int idx = j - lane;
@@ -181,7 +188,7 @@ __device__ __forceinline__ int32_t lookback_exclusive_warp(const ScanState& st, 
       v = (int32_t)(uint32_t)(s & 0xffffffffull);
     }
     if (!__all_sync(0xffffffffu, ready)) {
-      if (++spins > GC_SPIN_LIMIT) { gave_up = true; break; }
+      if (++spins > limit) { gave_up = true; break; }
       __nanosleep(32);
       continue;
     }
@@ -202,18 +209,22 @@ __device__ __forceinline__ int32_t lookback_exclusive_warp(const ScanState& st, 
   return excl;
 }
 
-// Last CTA to finish resets the tickets and bumps the tag for the next launch.
-__device__ __forceinline__ void scan_finish(const ScanState& st, int nchunks) {
+// Last CTA to finish resets the tickets and bumps the tag for the next launch; returns
+// true in that CTA (every other CTA's writes are visible to it).
+__device__ __forceinline__ bool scan_finish(const ScanState& st, int nchunks) {
   __threadfence();
   int d = atomicAdd(st.done, 1);
   if (d == nchunks - 1) {
+    __threadfence();
     *st.ticket = 0;
     *st.done = 0;
     uint32_t s = *st.seq + 1;
     if ((s & 0x3fffffffu) == 0) s = 1;
     *st.seq = s;
     __threadfence();
+    return true;
   }
+  return false;
 }
 
 // Block-wide exclusive scan of one int per thread (blockDim.x multiple of 32, <= 1024).

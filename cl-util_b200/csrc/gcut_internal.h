@@ -24,6 +24,9 @@ int launch_scan(int mode, const int32_t* in, const int32_t* in2, int32_t* clear,
                 int32_t* scan_out, int32_t* list_out, int32_t* total_out, int n, int op1,
                 int32_t a1, int op2, int32_t a2, int logical, const ScanState& st,
                 cudaStream_t s);
+// One warp waits on a look-back predecessor that never publishes, until st.spin_limit
+// polls run out (sets *st.err); needs st.max_chunks >= 2.
+int launch_lookback_selftest(const ScanState& st, cudaStream_t s);
 int launch_increment_logical(const int32_t* in1, const int32_t* in2, int32_t* out, int n,
                              int op1, int op2, int32_t a1, int32_t a2, int logical,
                              int32_t iteration, cudaStream_t s);

@@ -2,8 +2,7 @@
 //
 // gc_compact keeps the look-back scratch of its single-pass scan (a ticket counter, a
 // finish counter, an error word, a sequence tag and one status word per 4096-item chunk)
-// in device memory that the library obtains with cudaMalloc on the first call on each
-// device.  Some callers cannot allow that: code that must keep a fixed device-memory
+// in a gc_scan_state, whose device memory the library obtains with cudaMalloc.  Some callers cannot allow that: code that must keep a fixed device-memory
 // footprint (a serving process whose memory is carved up in advance, or one that runs next
 // to other jobs on a shared GPU), and code that cannot afford the implicit device-wide
 // synchronisation that cudaMalloc / cudaFree may cause while other work is in flight.
@@ -41,6 +40,9 @@ int scratch_address(void** out) {
   if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(GC_ERR_INVALID, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_mu);
   if (!g_scratch_addr[dev]) {
+    // every kernel of the library is loaded here, once per device, so a later call never
+    // loads one lazily (inside a stream capture or next to other threads' launches)
+    gcut::preload_kernels();
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_compact_scratch);
     if (e != cudaSuccess || !p) return noalloc_fail(GC_ERR_CUDA, "cudaGetSymbolAddress of the compaction scratch failed");

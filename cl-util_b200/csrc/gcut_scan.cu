@@ -119,7 +119,24 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan(ScanArgs a, ScanState st)
     run += v[k];
   }
   if (chunk == nchunks - 1 && threadIdx.x == 0 && a.total_out) *a.total_out = s_excl + agg;
-  if (threadIdx.x == 0) scan_finish(st, nchunks);
+  // The last CTA to finish sees every CTA's error report: a compaction whose look-back gave
+  // up returns length -1 (a list length is never negative), so the result itself says so.
+  if (threadIdx.x == 0 && scan_finish(st, nchunks) && a.mode != GC_SCAN_MODE_SCAN &&
+      a.total_out && *((volatile int32_t*)st.err) != 0)
+    *a.total_out = -1;
+}
+
+// Exercises the bounded look-back wait.  One warp looks back from chunk 1 to a chunk 0 that
+// never publishes (the host cleared its status word, whose tag 0 never matches a launch
+// tag), so the wait gives up after st.spin_limit polls, sets the error word and returns.
+// The launch then closes like a one-chunk scan (tickets reset, tag bumped), so the status
+// word it published cannot be mistaken for a later launch's.
+__global__ void k_lookback_selftest(ScanState st) {
+  __shared__ uint32_t s_tag;
+  if (threadIdx.x == 0) s_tag = *((volatile uint32_t*)st.seq);
+  __syncthreads();
+  if (threadIdx.x < 32) lookback_exclusive_warp(st, s_tag, 1, 0);
+  if (threadIdx.x == 0) scan_finish(st, 1);
 }
 
 // IncrementalTileList.incorporate (incremental_tile_list.cl:110-154): stamp `iteration`
@@ -157,8 +174,16 @@ __global__ void k_tiles_view(const int32_t* __restrict__ tiles, int tiles_w, int
   }
 }
 
+int launch_lookback_selftest(const ScanState& st, cudaStream_t s) {
+  if (st.max_chunks < 2) return GC_ERR_INVALID;
+  if (cudaMemsetAsync(st.status, 0, sizeof(unsigned long long), s) != cudaSuccess) return GC_ERR_CUDA;
+  k_lookback_selftest<<<1, 32, 0, s>>>(st);
+  return cudaGetLastError() == cudaSuccess ? GC_OK : GC_ERR_CUDA;
+}
+
 void preload_scan_kernels() {
   cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, (const void*)k_lookback_selftest);
   cudaFuncGetAttributes(&a, (const void*)k_scan);
   cudaFuncGetAttributes(&a, (const void*)k_increment_logical);
   cudaFuncGetAttributes(&a, (const void*)k_fill);

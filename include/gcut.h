@@ -263,42 +263,77 @@ const char* gc_kernel_name(int kind);
 const char* gc_last_error(void);
 
 /* ---- data-parallel primitives beneath IncrementalTileList ---------------------------
-   All pointers are DEVICE pointers; n items; one launch each.  The library keeps the
-   look-back state per device. */
+   All pointers are DEVICE pointers; n items; one launch each.
+
+   Each primitive runs on a look-back state (the single-pass scan's tickets, per-chunk status
+   words, launch tag and error word).  The reference gives every tile list its own
+   StreamCompact and PrefixSum (IncrementalTileList.pyx:74, StreamCompact.pyx:39,
+   PrefixSum.pyx:46); the counterpart here is one gc_scan_state per such object.  Calls on
+   one state must not overlap on the GPU (one stream per state, or host ordering); calls on
+   different states never interfere.  A NULL state selects one state shared by every caller
+   on the current device: calls on it from different streams must not overlap either.
+
+   Errors found on the device (a bounded look-back wait that gave up, an out-of-range
+   scatter index) set the state's error word, which stays set until reported:
+   - compactions (gc_compact, gc_tiles_build, gc_tiles_build_logical) then write length -1;
+   - the next call on the state returns GC_ERR_INTERNAL once the word has reached the host
+     (it is copied back after every launch, on the caller's stream);
+   - gc_scan_state_error reads it synchronously. */
+typedef struct gc_scan_state gc_scan_state;
+/* A state for launches of up to max_items items on `device`.  No counterpart in the
+   reference (the objects above own their buffers). */
+int gc_scan_state_create(int device, int max_items, gc_scan_state** out);
+/* Waits for the state's last launch, then frees it. */
+int gc_scan_state_destroy(gc_scan_state* state);
+/* *err = the state's error word (0 none, 1 a look-back wait gave up, 2 a scatter index was
+   out of range), then clears it.  Synchronises `stream`. */
+int gc_scan_state_error(gc_scan_state* state, int* err, void* stream);
+/* Diagnostic of the bounded wait: one warp waits, with a limit of `spins` polls, for a
+   look-back predecessor that never publishes, gives up, and records error 1.  With err
+   non-NULL, *err gets the error word as gc_scan_state_error reads it (1 when the wait ran
+   out as designed); with err NULL the word is left on the state and reported like any
+   device error (the next call on the state returns GC_ERR_INTERNAL).  The state stays
+   usable. */
+int gc_scan_state_selftest(gc_scan_state* state, int spins, int* err, void* stream);
 
 /* PrefixSum.scan (PrefixSum.pyx:83-129, prefixsum.cl): exclusive scan of in[0..n) into
    out (may alias in) and the sum into *total (int32 wrap-around). */
-int gc_scan_exclusive(const int32_t* in, int32_t* out, int32_t* total, int n, void* stream);
+int gc_scan_exclusive(gc_scan_state* state, const int32_t* in, int32_t* out, int32_t* total,
+                      int n, void* stream);
 /* StreamCompact.compact (StreamCompact.pyx:66-82, streamcompact.cl): indices i with
    flags[i] != 0, increasing, into list; their number into *length.  list must not alias
    flags. */
-int gc_compact(const int32_t* flags, int32_t* list, int32_t* length, int n, void* stream);
+int gc_compact(gc_scan_state* state, const int32_t* flags, int32_t* list, int32_t* length,
+               int n, void* stream);
 /* IncrementalTileList.build(operator, operand) (IncrementalTileList.pyx:119-136,
    incremental_tile_list.cl:40-64 + compaction). */
-int gc_tiles_build(const int32_t* tiles, int op, int32_t operand, int32_t* list,
-                   int32_t* length, int n, void* stream);
+int gc_tiles_build(gc_scan_state* state, const int32_t* tiles, int op, int32_t operand,
+                   int32_t* list, int32_t* length, int n, void* stream);
 /* Same compaction as gc_compact for callers that cannot allocate device memory.  No
-   counterpart in the reference.  gc_compact obtains its look-back scratch with cudaMalloc
-   on its first call on a device; code that must keep a fixed device-memory footprint (for
-   example a serving process with a pre-divided budget on a shared GPU) or that cannot risk
-   the implicit synchronisation of cudaMalloc/cudaFree while other work runs, calls this
-   variant instead.  Its scratch is a fixed 8208-byte array compiled into the library,
-   present on every GPU that loads the library until the process exits; it calls no
-   cudaMalloc, cudaFree or allocating library routine.
+   counterpart in the reference.  gc_compact keeps its look-back scratch in a gc_scan_state,
+   whose device memory comes from cudaMalloc (in gc_scan_state_create, or on the first call
+   on a device for the shared NULL state); code that must keep a fixed device-memory
+   footprint (for example a serving process with a pre-divided budget on a shared GPU) or
+   that cannot risk the implicit synchronisation of cudaMalloc/cudaFree while other work
+   runs, calls this variant instead.  Its scratch is a fixed 8208-byte array compiled into
+   the library, present on every GPU that loads the library until the process exits; it
+   calls no cudaMalloc, cudaFree or allocating library routine.
    - n must not exceed GC_COMPACT_NOALLOC_MAX_N (4194304 items); larger n returns
      GC_ERR_INVALID.
-   - The first call on each device looks up the array's device address (with that device
-     current); make that first call before any stream capture.
+   - The first call on each device looks up the array's device address and loads the
+     library's kernels (with that device current); make that first call before any stream
+     capture.
    - All calls share the one array and each call clears the part it uses, so calls whose
      work overlaps on the GPU (different streams, or different host threads) race and must
-     be serialised by the caller. */
+     be serialised by the caller.
+   - A look-back wait that gives up is reported in the result: *length is -1. */
 #define GC_COMPACT_NOALLOC_MAX_N 4194304
 int gc_compact_noalloc(const int32_t* flags, int32_t* list, int32_t* length, int n, void* stream);
 /* IncrementalTileList.buildLogical (IncrementalTileList.pyx:157-176,
    incremental_tile_list.cl:66-108 + compaction). */
-int gc_tiles_build_logical(const int32_t* tiles, const int32_t* tiles2, int op1, int32_t a1,
-                           int op2, int32_t a2, int logical, int32_t* list, int32_t* length,
-                           int n, void* stream);
+int gc_tiles_build_logical(gc_scan_state* state, const int32_t* tiles, const int32_t* tiles2,
+                           int op1, int32_t a1, int op2, int32_t a2, int logical, int32_t* list,
+                           int32_t* length, int n, void* stream);
 /* IncrementalTileList.incorporate (IncrementalTileList.pyx:138-155,
    incremental_tile_list.cl:110-154): tiles[i] = iteration where the predicate holds. */
 int gc_tiles_incorporate(int32_t* tiles, const int32_t* tiles2, int op1, int32_t a1, int op2,

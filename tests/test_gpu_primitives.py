@@ -143,3 +143,76 @@ def test_tile_list_execute_view(cuda, oracle, global_dim, tiles_dim):
         assert np.array_equal(got, want)
     out = torch.zeros((global_dim[1], global_dim[0]), dtype=torch.int32, device="cuda")
     assert tl.execute(out=out) is out
+
+
+def test_lookback_wait_runs_out_and_reports(cuda):
+    """A bounded look-back wait made to run out on purpose (a predecessor that never
+    publishes, a short poll limit) records error 1; the state reports it once, is clear
+    afterwards and still compacts correctly."""
+    import _gcut
+    torch = cuda
+    st = _gcut.ScanState(0, 1 << 16)
+    assert st.selftest(spins=2000) == 1
+    assert st.error() == 0
+    flags = (np.random.default_rng(5).random(50000) < 0.4).astype(np.int32)
+    dF = _dev(flags, torch)
+    dL = torch.zeros(50000, dtype=torch.int32, device="cuda")
+    dN = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _gcut.check(_gcut.lib().gc_compact(st.handle, _gcut.ptr(dF), _gcut.ptr(dL), _gcut.ptr(dN),
+                                       flags.size, _gcut.stream_handle()))
+    m = int(dN.item())
+    assert m == int(flags.sum()) and np.array_equal(np.flatnonzero(flags), dL[:m].cpu().numpy())
+    assert st.error() == 0
+    st.close()
+
+
+def test_lookback_error_surfaces_at_next_call(cuda):
+    """An error left on a state by an earlier launch makes the next call on it return
+    GC_ERR_INTERNAL (after which the state is clear again)."""
+    import _gcut
+    torch = cuda
+    st = _gcut.ScanState(0, 1 << 16)
+    L = _gcut.lib()
+    s = _gcut.stream_handle()
+    # the wait runs out and its error word is left on the state, unread
+    assert L.gc_scan_state_selftest(st.handle, 1000, None, s) == 0
+    torch.cuda.synchronize()
+    flags = np.ones(10000, np.int32)
+    dF = _dev(flags, torch)
+    dL = torch.zeros(10000, dtype=torch.int32, device="cuda")
+    dN = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert L.gc_compact(st.handle, _gcut.ptr(dF), _gcut.ptr(dL), _gcut.ptr(dN), 10000, s) == \
+        _gcut.GC_ERR_INTERNAL
+    assert b"look-back" in L.gc_last_error()
+    # reported once: the same call now runs and is right
+    assert L.gc_compact(st.handle, _gcut.ptr(dF), _gcut.ptr(dL), _gcut.ptr(dN), 10000, s) == 0
+    torch.cuda.synchronize()
+    assert int(dN.item()) == 10000
+    assert np.array_equal(dL.cpu().numpy(), np.arange(10000))
+    assert st.error() == 0
+    st.close()
+
+
+def test_objects_on_different_streams_do_not_interfere(cuda):
+    """Two StreamCompact objects compacting at the same time on two streams (each with its
+    own look-back state) both return np.flatnonzero of their flags, many times over."""
+    torch = cuda
+    rng = np.random.default_rng(17)
+    n = 1_500_000
+    objs = [StreamCompact(n), StreamCompact(n)]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    flags = [(rng.random(n) < p).astype(np.int32) for p in (0.2, 0.6)]
+    dF = [_dev(f, torch) for f in flags]
+    dL = [o.listFactory() for o in objs]
+    dN = [torch.zeros(1, dtype=torch.int32, device="cuda") for _ in objs]
+    torch.cuda.synchronize()
+    for _ in range(20):
+        for k in range(2):
+            with torch.cuda.stream(streams[k]):
+                objs[k].compact(dF[k], dL[k], dN[k], n, stream=streams[k])
+    torch.cuda.synchronize()
+    for k in range(2):
+        m = int(dN[k].item())
+        assert m == int(flags[k].sum())
+        assert np.array_equal(np.flatnonzero(flags[k]), dL[k][:m].cpu().numpy())
+        assert objs[k].state.error() == 0
