@@ -146,14 +146,19 @@ class GraphCut:
                 check(lib().gc_upload_host(self._h, *[ptr(a) for a in host], stream_handle(stream)))
         self._solved = False
 
-    def upload_image(self, rgba, excess, stream=None):
+    def upload_image(self, rgba, excess, stream=None, lamda=None):
         """Builds the capacities on the device from an image and the t-links (gc_upload_rgba):
-        n-link = floor(50 * exp(-beta * |dI|^2) + 0.5), beta = 1 / (2 * mean |dI|^2).  `rgba`
-        is uint32 [H, W] (RGBA bytes viewed as uint32) or uint8 [H, W, 3|4]; `excess` int32
-        [H, W], or a pair (fg, bg) of colour models (gmm_tlinks.Mixture) from which the t-links
-        are computed on the device (gc_tlinks_gmm, 100 * (score_bg - score_fg) rounded).
-        Torch CUDA tensors are read in place; numpy arrays are copied."""
+        n-link = floor(50 * exp(-beta * |dI|^2) + 0.5), beta = 1 / (2 * mean |dI|^2).  With
+        `lamda` (an integer, the reference's LAMBDA; 60 in GraphCut.pyx:25) the n-links follow
+        the reference's own rule instead, lamda / (0.1 * sqrt(|dI|^2) + 0.05) rounded to the
+        nearest integer (gc_upload_rgba_lambda; graphcut.cl:1018-1031).  `rgba` is uint32
+        [H, W] (RGBA bytes viewed as uint32) or uint8 [H, W, 3|4]; `excess` int32 [H, W], or a
+        pair (fg, bg) of colour models (gmm_tlinks.Mixture) from which the t-links are
+        computed on the device (gc_tlinks_gmm, 100 * (score_bg - score_fg) rounded).  Torch
+        CUDA tensors are read in place; numpy arrays are copied."""
         import torch
+        if lamda is not None and (int(lamda) != lamda or not 1 <= lamda <= 1000):
+            raise ValueError("lamda must be an integer in [1, 1000]")
         rgba = _as_rgba32(rgba)
         if isinstance(excess, tuple):
             import gmm_tlinks
@@ -172,14 +177,23 @@ class GraphCut:
             with _on(stream):
                 ex = _as_i32_device(excess, self.device)
                 img = rgba.contiguous()
-            check(lib().gc_upload_rgba(self._h, ptr(img), ptr(ex), stream_handle(stream)))
+            if lamda is None:
+                check(lib().gc_upload_rgba(self._h, ptr(img), ptr(ex), stream_handle(stream)))
+            else:
+                check(lib().gc_upload_rgba_lambda(self._h, ptr(img), ptr(ex), int(lamda),
+                                                  stream_handle(stream)))
             self._keep = (img, ex)
         else:
             img = np.ascontiguousarray(rgba.cpu().numpy() if isinstance(rgba, torch.Tensor) else rgba)
             ex = np.ascontiguousarray(excess.cpu().numpy() if isinstance(excess, torch.Tensor) else excess,
                                       dtype=np.int32)
             with torch.cuda.device(self.device):
-                check(lib().gc_upload_rgba_host(self._h, ptr(img), ptr(ex), stream_handle(stream)))
+                if lamda is None:
+                    check(lib().gc_upload_rgba_host(self._h, ptr(img), ptr(ex),
+                                                    stream_handle(stream)))
+                else:
+                    check(lib().gc_upload_rgba_lambda_host(self._h, ptr(img), ptr(ex),
+                                                           int(lamda), stream_handle(stream)))
         self._solved = False
 
     # ---- solve ------------------------------------------------------------------
@@ -287,6 +301,18 @@ class GraphCut:
             raise ValueError("xs and ys must be 1-D arrays of the same length")
         check(lib().gc_edit_stroke(self._h, ptr(xs), ptr(ys), int(xs.shape[0]), int(radius),
                                    int(value), stream_handle(stream)))
+        self._solved = False
+
+    def edit_brush(self, xs, ys, radius: int, value: int, stream=None):
+        """Every pixel the reference Brush covers for the polyline (brush.pyx:138-161: line
+        pixels widened by the disc of the radius, centred; pixels outside the image skipped)
+        gets t-link `value`; warm-starts cut()."""
+        xs = np.ascontiguousarray(xs, dtype=np.int32)
+        ys = np.ascontiguousarray(ys, dtype=np.int32)
+        if xs.shape != ys.shape or xs.ndim != 1:
+            raise ValueError("xs and ys must be 1-D arrays of the same length")
+        check(lib().gc_edit_brush(self._h, ptr(xs), ptr(ys), int(xs.shape[0]), int(radius),
+                                  int(value), stream_handle(stream)))
         self._solved = False
 
     # ---- read-only planes (GraphCut.pyx:57-79) ----------------------------------

@@ -84,6 +84,8 @@ SIGNATURES = {
     "gc_upload_host": [_P] * 6 + [_P],
     "gc_upload_rgba": [_P, _P, _P, _P],
     "gc_upload_rgba_host": [_P, _P, _P, _P],
+    "gc_upload_rgba_lambda": [_P, _P, _P, _I32, _P],
+    "gc_upload_rgba_lambda_host": [_P, _P, _P, _I32, _P],
     "gc_tlinks_gmm": [_P, _I, _I, _I, _P, _I, _P, _I, ctypes.c_double, _I32, _P, _P],
     "gc_gmm_fit": [_P, _I, _I, _I, ctypes.c_double, ctypes.c_double, ctypes.c_double, _I,
                    _P, _P],
@@ -99,6 +101,7 @@ SIGNATURES = {
     "gc_labels_packed_host": [_P, _P, _P],
     "gc_edit_tlinks": [_P, _P, _P, _I, _P],
     "gc_edit_stroke": [_P, _P, _P, _I, _I, _I32, _P],
+    "gc_edit_brush": [_P, _P, _P, _I, _I, _I32, _P],
     "gc_download_state": [_P] * 7 + [_P],
     "gc_get_stats": [_P, _P],
     "gc_set_collect_stats": [_P, _I],

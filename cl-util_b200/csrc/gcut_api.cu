@@ -153,7 +153,6 @@ struct Pool {
   size_t arena_bytes = 0;
   bool own_arena = true;       // false: caller-owned memory (gc_create_in)
   cudaEvent_t done_ev = nullptr;   // recorded after every call's work (see track)
-  cudaEvent_t dsum_ev = nullptr;   // the |dI|^2 sum of gc_upload_rgba reached the host
   void* pin = nullptr;         // pinned block holding h_count, h_ctl, h_acc
   size_t pin_bytes = 0;
   int32_t* h_count = nullptr;  // pinned
@@ -162,7 +161,7 @@ struct Pool {
   ImageAcc* h_acc = nullptr;   // pinned
   int grid_dis = 0, grid_warps = 0, sms = 1;
   unsigned long long* dsum = nullptr;     // device: sum of |dI|^2 (gc_upload_rgba)
-  unsigned long long* h_dsum = nullptr;   // pinned copy
+  int32_t* ntab = nullptr;                // device: n-link thresholds (gc_upload_rgba)
   bool uploaded = false, solved = false, edited = false, collect = false;
   bool list_valid = false, bfs_fresh = false;
   gc_stats stats{};
@@ -230,10 +229,6 @@ struct Pool {
   }
 
   void release() {
-    if (dsum_ev) {
-      cudaEventDestroy(dsum_ev);
-      dsum_ev = nullptr;
-    }
     if (done_ev) {
       if (!own_arena) cudaEventSynchronize(done_ev);
       cudaEventDestroy(done_ev);
@@ -252,7 +247,7 @@ struct Pool {
     P = PoolView{};
     tl = list = counts = stage = pts = nullptr;
     acc = nullptr; lstage = nullptr; h_count = nullptr; h_ctl = nullptr; h_acc = nullptr;
-    dsum = nullptr; h_dsum = nullptr;
+    dsum = nullptr; ntab = nullptr;
   }
 
   // places every device buffer of the pool (see Carve)
@@ -287,6 +282,7 @@ struct Pool {
     scan.st.max_chunks = chunks;
     c.take(&pts, 2 * 1024);
     c.take(&dsum, 1);
+    c.take(&ntab, GC_NLINK_LEVELS);
     if (imgs.size() == 1) c.take(&lstage, (size_t)imgs[0].W * imgs[0].H);
   }
 
@@ -335,8 +331,6 @@ struct Pool {
     }
     e = cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming);
     if (e) { done_ev = nullptr; release(); return cuda_fail(e, "event"); }
-    e = cudaEventCreateWithFlags(&dsum_ev, cudaEventDisableTiming);
-    if (e) { dsum_ev = nullptr; release(); return cuda_fail(e, "event"); }
     Carve place{arena, 0};
     layout(place);
     list = P.queue[0];
@@ -355,7 +349,6 @@ struct Pool {
     pin = pinned_take(pin_bytes);
     if (!pin) { release(); return fail(GC_ERR_OOM, "pinned host allocation failed"); }
     h_count = static_cast<int32_t*>(pin);
-    h_dsum = reinterpret_cast<unsigned long long*>(static_cast<char*>(pin) + 64);
     h_ctl = reinterpret_cast<int32_t*>(static_cast<char*>(pin) + 256);
     h_acc = reinterpret_cast<ImageAcc*>(static_cast<char*>(pin) + 512);
     std::vector<int4> nb(nt);
@@ -397,68 +390,33 @@ struct Pool {
     return GC_OK;
   }
 
-  // Capacities from an RGBA image (n-links) and int32 t-links: the sum of |dI|^2 over all
-  // 4-neighbour pairs is taken on the device (exact), the host turns it into beta and the
-  // n-link table, and the upload kernel builds the tile planes from the image.
-  int upload_rgba(int i, const uint32_t* rgba, const int32_t* excess, cudaStream_t s) {
-    RK(rgba_sum_begin(i, rgba, s));
-    return upload_rgba_finish(i, rgba, excess, s);
-  }
-
-  // first half of upload_rgba: the sum of |dI|^2 on the device and its copy to the host,
-  // marked by dsum_ev (work queued after it, such as another input copy, overlaps the wait)
-  int rgba_sum_begin(int i, const uint32_t* rgba, cudaStream_t s) {
+  // Capacities from an RGBA image (n-links) and int32 t-links, all on the device with no
+  // host wait.  lambda == 0: the exp weighting, whose scale comes from the mean |dI|^2 over
+  // all 4-neighbour pairs (k_dsum sums it exactly, k_nlink_table turns it into the weight
+  // thresholds); lambda > 0: the reference's weighting with that LAMBDA.
+  int upload_rgba(int i, const uint32_t* rgba, const int32_t* excess, int lambda, cudaStream_t s) {
     if (i < 0 || i >= (int)imgs.size()) return fail(GC_ERR_INVALID, "image index");
-    if (!rgba) return fail(GC_ERR_INVALID, "null plane");
+    if (!rgba || !excess) return fail(GC_ERR_INVALID, "null plane");
+    if (lambda < 0 || lambda > GC_NLINK_MAX_LAMBDA) return fail(GC_ERR_INVALID, "lambda out of range");
     CK(cudaSetDevice(device));
     const ImageDesc& im = imgs[i];
-    CK(cudaMemsetAsync(dsum, 0, sizeof(unsigned long long), s));
-    RK(launch_dsum(rgba, im.W, im.H, dsum, sms, s));
-    CK(cudaMemcpyAsync(h_dsum, dsum, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    CK(cudaEventRecord(dsum_ev, s));
-    return GC_OK;
-  }
-
-  // second half: wait for the sum, build the n-link table, launch the upload
-  int upload_rgba_finish(int i, const uint32_t* rgba, const int32_t* excess, cudaStream_t s) {
-    if (!excess) return fail(GC_ERR_INVALID, "null plane");
-    const ImageDesc& im = imgs[i];
-    CK(cudaEventSynchronize(dsum_ev));
-    const long long npairs = (long long)(im.H - 1) * im.W + (long long)im.H * (im.W - 1);
-    NlinkTable tab;
-    nlink_table(*h_dsum, npairs, &tab);
+    if (lambda == 0) {
+      const long long npairs = (long long)(im.H - 1) * im.W + (long long)im.H * (im.W - 1);
+      CK(cudaMemsetAsync(dsum, 0, sizeof(unsigned long long), s));
+      RK(launch_dsum(rgba, im.W, im.H, dsum, sms, s));
+      RK(launch_nlink_table(dsum, npairs, ntab, s));
+    }
     CK(cudaMemsetAsync(acc + i, 0, sizeof(ImageAcc), s));
     P.ktiles = nullptr;
-    RK(timed(K_UPLOAD, s, [&] { return launch_upload_rgba(P, im, i, rgba, excess, tab, tl, acc, s); }));
+    RK(timed(K_UPLOAD, s, [&] {
+      return launch_upload_rgba(P, im, i, rgba, excess, lambda ? nullptr : ntab, lambda, tl, acc, s);
+    }));
     uploaded = true;
     solved = false;
     edited = false;
     list_valid = false;
     bfs_fresh = false;
     return GC_OK;
-  }
-
-  // weight(d) = floor(50 * exp(-beta * d) + 0.5), beta = 1 / (2 * mean |dI|^2) (0 when the
-  // mean is 0), for d = |dI|^2 in [0, 3 * 255^2]; the weight does not increase with d, so it
-  // is stored as t[k - 1] = the largest d with weight >= k.  Each entry is located from the
-  // real root and then settled by evaluating the formula itself at the integers around it.
-  static void nlink_table(unsigned long long sum, long long npairs, NlinkTable* tab) {
-    const long kMax = 3L * 255 * 255;
-    const double mean = (double)sum / (double)(npairs > 1 ? npairs : 1);
-    const double beta = mean > 0 ? 1.0 / (2.0 * mean) : 0.0;
-    auto w = [&](long d) {
-      const double x = std::exp(-beta * (double)d);
-      const double y = 50.0 * x;
-      return (int)std::floor(y + 0.5);
-    };
-    for (int k = 1; k <= GC_NLINK_LEVELS; ++k) {
-      if (beta <= 0) { tab->t[k - 1] = (int32_t)kMax; continue; }
-      const double root = std::log(50.0 / (k - 0.5)) / beta;   // w(d) >= k  <=>  d <= root
-      long d = root >= (double)kMax ? kMax : (root < 0 ? 0 : (long)std::floor(root));
-      while (d < kMax && w(d + 1) >= k) ++d;
-      while (d >= 0 && w(d) < k) --d;
-      tab->t[k - 1] = (int32_t)d;
-    }
   }
 
   // exact BFS distances to the sink pixels (global relabel); sets tact.  h: condition
@@ -1045,16 +1003,17 @@ int gc_upload_host(gc_handle* h, const int32_t* up, const int32_t* down, const i
   return GC_OK;
 }
 
-int gc_upload_rgba(gc_handle* h, const uint32_t* rgba, const int32_t* excess, void* stream) {
+static int upload_rgba_dev(gc_handle* h, const uint32_t* rgba, const int32_t* excess, int lambda,
+                           void* stream) {
   g_err.clear();
   if (!h) return fail(GC_ERR_INVALID, "null handle");
-  const int r = h->pool.upload_rgba(0, rgba, excess, (cudaStream_t)stream);
+  const int r = h->pool.upload_rgba(0, rgba, excess, lambda, (cudaStream_t)stream);
   h->pool.track((cudaStream_t)stream);
   return r;
 }
 
-int gc_upload_rgba_host(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
-                        void* stream) {
+static int upload_rgba_host(gc_handle* h, const uint32_t* rgba, const int32_t* excess, int lambda,
+                            void* stream) {
   g_err.clear();
   if (!h || !rgba || !excess) return fail(GC_ERR_INVALID, "null argument");
   Pool& p = h->pool;
@@ -1066,15 +1025,34 @@ int gc_upload_rgba_host(gc_handle* h, const uint32_t* rgba, const int32_t* exces
   }
   cudaStream_t s = (cudaStream_t)stream;
   const uint32_t* img = reinterpret_cast<const uint32_t*>(p.stage);
-  // the image first: its |dI|^2 sum travels to the host while the t-links are copied
   CK(cudaMemcpyAsync(p.stage, rgba, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-  RK(p.rgba_sum_begin(0, img, s));
   CK(cudaMemcpyAsync(p.stage + n, excess, n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-  int r = p.upload_rgba_finish(0, img, p.stage + n, s);
+  int r = p.upload_rgba(0, img, p.stage + n, lambda, s);
   p.track(s);
   if (r) return r;
   CK(cudaStreamSynchronize(s));
   return GC_OK;
+}
+
+int gc_upload_rgba(gc_handle* h, const uint32_t* rgba, const int32_t* excess, void* stream) {
+  return upload_rgba_dev(h, rgba, excess, 0, stream);
+}
+
+int gc_upload_rgba_host(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
+                        void* stream) {
+  return upload_rgba_host(h, rgba, excess, 0, stream);
+}
+
+int gc_upload_rgba_lambda(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
+                          int32_t lambda, void* stream) {
+  if (lambda < 1) return fail(GC_ERR_INVALID, "lambda out of range");
+  return upload_rgba_dev(h, rgba, excess, lambda, stream);
+}
+
+int gc_upload_rgba_lambda_host(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
+                               int32_t lambda, void* stream) {
+  if (lambda < 1) return fail(GC_ERR_INVALID, "lambda out of range");
+  return upload_rgba_host(h, rgba, excess, lambda, stream);
 }
 
 int gc_solve(gc_handle* h, void* stream) {
@@ -1161,6 +1139,26 @@ int gc_edit_stroke(gc_handle* h, const int32_t* xs, const int32_t* ys, int npts,
   cudaStream_t s = (cudaStream_t)stream;
   CK(cudaMemcpyAsync(p.pts, pts.data(), pts.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   RK(launch_stroke(p.P, p.imgs[0], 0, p.pts, pts.data(), npts, radius, value, p.tl, p.acc, s));
+  p.track(s);
+  CK(cudaStreamSynchronize(s));  // pts (host vector) must outlive the copy
+  p.edited = true;
+  p.bfs_fresh = false;
+  return GC_OK;
+}
+
+int gc_edit_brush(gc_handle* h, const int32_t* xs, const int32_t* ys, int npts, int radius,
+                  int32_t value, void* stream) {
+  g_err.clear();
+  if (!h || !xs || !ys || npts < 1 || npts > 1024 || radius > 1024)
+    return fail(GC_ERR_INVALID, "bad brush stroke");
+  Pool& p = h->pool;
+  if (!p.uploaded) return fail(GC_ERR_STATE, "edit before upload");
+  CK(cudaSetDevice(p.device));
+  std::vector<int32_t> pts(2 * npts);
+  for (int k = 0; k < npts; ++k) { pts[2 * k] = xs[k]; pts[2 * k + 1] = ys[k]; }
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(p.pts, pts.data(), pts.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  RK(launch_brush(p.P, p.imgs[0], 0, p.pts, pts.data(), npts, radius, value, p.tl, p.acc, s));
   p.track(s);
   CK(cudaStreamSynchronize(s));  // pts (host vector) must outlive the copy
   p.edited = true;

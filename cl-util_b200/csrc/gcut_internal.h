@@ -64,11 +64,13 @@ int launch_masks(const PoolView& P, int grid, cudaStream_t s);
 // n-link table of gc_upload_rgba: weight(d) = floor(50 * exp(-beta * d) + 0.5) for d = |dI|^2
 // equals the number of entries t[k] >= d (t[k] = largest d with weight >= k + 1).
 constexpr int GC_NLINK_LEVELS = 50;
-struct NlinkTable {
-  int32_t t[GC_NLINK_LEVELS];
-};
+// tab: the 50 device thresholds (exp weighting), or null for the reference's weighting
+// floor(lambda / (0.1 sqrt(d) + 0.05) + 0.5) (gc_upload_rgba_lambda)
 int launch_upload_rgba(const PoolView& P, const ImageDesc& im, int img, const uint32_t* rgba,
-                       const int32_t* excess, const NlinkTable& tab, int32_t* tl, ImageAcc* acc,
+                       const int32_t* excess, const int32_t* tab, int lambda, int32_t* tl,
+                       ImageAcc* acc, cudaStream_t s);
+// tab[0..50) from the |dI|^2 sum (device) and the number of 4-neighbour pairs
+int launch_nlink_table(const unsigned long long* sum, long long npairs, int32_t* tab,
                        cudaStream_t s);
 int launch_dsum(const uint32_t* rgba, int W, int H, unsigned long long* sum, int sms,
                 cudaStream_t s);
@@ -99,6 +101,11 @@ int launch_edit(const PoolView& P, const ImageDesc& im, int img, const int32_t* 
 int launch_stroke(const PoolView& P, const ImageDesc& im, int img, const int32_t* pts_dev,
                   const int32_t* pts_host, int npts, int radius, int32_t value, int32_t* tl,
                   ImageAcc* acc, cudaStream_t s);
+// The reference brush's pixel set (gc_edit_brush); radius <= 0 counts as 1; GC_ERR_INVALID
+// above 1024.
+int launch_brush(const PoolView& P, const ImageDesc& im, int img, const int32_t* pts_dev,
+                 const int32_t* pts_host, int npts, int radius, int32_t value, int32_t* tl,
+                 ImageAcc* acc, cudaStream_t s);
 // Loads every kernel of the library on the current device (once per device; called by the
 // first handle creation and the first stand-alone primitive on a device).
 void preload_kernels();

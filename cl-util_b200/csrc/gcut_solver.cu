@@ -140,24 +140,50 @@ __device__ __forceinline__ int rgb_dist2(uint32_t a, uint32_t b) {
   return dr * dr + dg * dg + db * db;
 }
 
+// Weight of the reference's n-link rule, rounded to an integer: floor(x + 0.5) for
+// x = lambda / (0.1 sqrt(d) + 0.05) = 20 lambda / (2 sqrt(d) + 1) (graphcut.cl:1018-1031,
+// LAMBDA and EPSILON from GraphCut.pyx:25-26,92-93), exactly.  For k >= 1,
+// floor(x + 0.5) >= k  <=>  b = 40 lambda - 2k + 1 >= 0  and  4 (2k - 1)^2 d <= b^2,
+// so the weight is the largest k satisfying that integer test (monotone in k).  A double
+// estimate of k is settled by the test itself; with lambda <= 1000 and d <= 3 * 255^2 every
+// product fits in 64 bits.
+__device__ __forceinline__ bool ref_weight_at_least(long long k, long long d, long long a40) {
+  if (k < 1) return true;
+  const long long b = a40 - 2 * k + 1, a = 2 * k - 1;
+  return b >= 0 && 4 * a * a * d <= b * b;
+}
+__device__ __forceinline__ int ref_weight(int d, int lambda) {
+  const long long a40 = 40LL * lambda;
+  const double sd = sqrt((double)d);
+  long long k = (long long)floor(((double)a40 + 1.0 + 2.0 * sd) / (4.0 * sd + 2.0));
+  if (k < 0) k = 0;
+  while (k > 0 && !ref_weight_at_least(k, d, a40)) --k;
+  while (ref_weight_at_least(k + 1, d, a40)) ++k;
+  return (int)k;
+}
+
 struct RgbaSource {
   const uint32_t* rgba;
   const int32_t* excess;
-  NlinkTable tab;
+  const int32_t* tab;   // exp weighting: the 50 thresholds on the device; null: reference rule
+  int lambda;           // reference weighting
   static constexpr bool vec = false;
   __device__ __forceinline__ void pixel4(const ImageDesc&, int, int, int (&)[4], int (&)[4],
                                          int (&)[4], int (&)[4], int (&)[4]) const {}
   __device__ __forceinline__ void prepare(int32_t* s_tab) const {
-    if (threadIdx.x < GC_NLINK_LEVELS) s_tab[threadIdx.x] = tab.t[threadIdx.x];
+    if (tab && threadIdx.x < GC_NLINK_LEVELS) s_tab[threadIdx.x] = tab[threadIdx.x];
   }
-  // weight of |dI|^2 = d: the number of table entries >= d (the entries do not increase)
-  __device__ __forceinline__ static int weight(const int32_t* s_tab, int d) {
+  // exp weighting: the number of table entries >= d (the entries do not increase)
+  __device__ __forceinline__ static int table_weight(const int32_t* s_tab, int d) {
     int lo = 0, hi = GC_NLINK_LEVELS;
     while (lo < hi) {
       const int mid = (lo + hi) >> 1;
       if (s_tab[mid] >= d) lo = mid + 1; else hi = mid;
     }
     return lo;
+  }
+  __device__ __forceinline__ int weight(const int32_t* s_tab, int d) const {
+    return tab ? table_weight(s_tab, d) : ref_weight(d, lambda);
   }
   __device__ __forceinline__ void pixel(const ImageDesc& im, const int32_t* s_tab, int x, int y,
                                         int& e, int& cu, int& cd, int& cl, int& cr) const {
@@ -170,6 +196,28 @@ struct RgbaSource {
     cr = x < im.W - 1 ? weight(s_tab, rgb_dist2(c, rgba[i + 1])) : 0;
   }
 };
+
+// The exp weighting's table on the device, from the |dI|^2 sum of k_dsum: weight(d) =
+// floor(50 exp(-beta d) + 0.5) with beta = 1 / (2 mean |dI|^2) (0 when the mean is 0) does
+// not increase with d, so it is stored as t[k - 1] = the largest d in [0, 3 * 255^2] with
+// weight >= k.  Thread k - 1 locates t[k - 1] from the real root of 50 exp(-beta d) + 0.5
+// = k and settles it by evaluating the formula itself at the integers around it, in double,
+// so the table reproduces a float64 evaluation of the formula pixel by pixel.
+__global__ void k_nlink_table(const unsigned long long* __restrict__ sum, long long npairs,
+                              int32_t* __restrict__ tab) {
+  const int k = (int)threadIdx.x + 1;
+  if (k > GC_NLINK_LEVELS) return;
+  const long kMax = 3L * 255 * 255;
+  const double mean = (double)(*sum) / (double)(npairs > 1 ? npairs : 1);
+  const double beta = mean > 0 ? 1.0 / (2.0 * mean) : 0.0;
+  if (beta <= 0) { tab[k - 1] = (int32_t)kMax; return; }
+  auto w = [&](long d) { return (int)floor(50.0 * exp(-beta * (double)d) + 0.5); };
+  const double root = log(50.0 / (k - 0.5)) / beta;   // weight(d) >= k  <=>  d <= root
+  long d = root >= (double)kMax ? kMax : (root < 0 ? 0 : (long)floor(root));
+  while (d < kMax && w(d + 1) >= k) ++d;
+  while (d >= 0 && w(d) < k) --d;
+  tab[k - 1] = (int32_t)d;
+}
 
 template <class Source>
 __global__ void __launch_bounds__(DIS_THREADS)
@@ -1347,6 +1395,78 @@ __global__ void k_stroke(PoolView P, ImageDesc im, int img, const int32_t* __res
   apply_tlink(P, im, img, x, y, value, tl, acc);
 }
 
+// Reference brush (gc_edit_brush): the pixel set of Brush.points (brush.pyx:138-161), the
+// line pixels of each segment (skimage.draw.line: Bresenham, the minor axis stepping while
+// the error term d = 2 dr - dc + ... is >= 0) widened by the disc of skimage.draw.circle, whose
+// points satisfy (dy / R)^2 + (dx / R)^2 < 1 in float64.  The disc is centred on every line
+// pixel (the reference adds circle(R, R, R), a disc shifted by +R) and pixels outside the
+// image are skipped (the reference's y * W + x wraps them).
+//
+// Along the major axis (n steps, minor-axis travel m) Bresenham's i-th pixel has minor
+// offset floor((2 m i + n) / (2 n)): the loop steps the minor axis once for every time the
+// error term 2 m (i + 1) - n - 2 n k reaches 0, which is rounding m i / n to the nearest
+// integer with halves up.  Each thread tests one pixel of the bounding box against the
+// line pixels within R - 1 of it along the major axis, so every pixel is written once.
+constexpr int GC_BRUSH_MAX_RADIUS = 1024;
+
+// skimage's disc test for the offset (dy, dx): two quotients, two squares and a sum, each
+// rounded on its own as numpy evaluates ((y - cy) / ry) ** 2 + ((x - cx) / rx) ** 2 < 1.
+__device__ __forceinline__ bool brush_disk(int dy, int dx, int R) {
+  const double a = __ddiv_rn((double)dy, (double)R), b = __ddiv_rn((double)dx, (double)R);
+  return __dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)) < 1.0;
+}
+
+__device__ __forceinline__ bool in_brush(int px, int py, const int32_t* pts, int npts, int R,
+                                         const int32_t* half) {
+  const int nseg = npts > 1 ? npts - 1 : 1;
+  for (int k = 0; k < nseg; ++k) {
+    const int x0 = pts[2 * k], y0 = pts[2 * k + 1];
+    const int x1 = npts > 1 ? pts[2 * k + 2] : x0, y1 = npts > 1 ? pts[2 * k + 3] : y0;
+    const int dr = abs(y1 - y0), dc = abs(x1 - x0);
+    const int sr = (y1 - y0) > 0 ? 1 : -1, sc = (x1 - x0) > 0 ? 1 : -1;
+    const bool steep = dr > dc;
+    const int n = steep ? dr : dc, m = steep ? dc : dr;       // major steps, minor travel
+    const int a0 = steep ? y0 : x0, b0 = steep ? x0 : y0;     // major / minor start
+    const int sa = steep ? sr : sc, sb = steep ? sc : sr;
+    const int pa = steep ? py : px;
+    const int t = sa * (pa - a0);                             // pixel's major-axis step
+    const int ilo = max(t - (R - 1), 0), ihi = min(t + (R - 1), n);
+    for (int i = ilo; i <= ihi; ++i) {
+      const int bi = n > 0 ? b0 + sb * (int)((2LL * m * i + n) / (2LL * n)) : b0;
+      const int ai = a0 + sa * i;
+      const int dy = py - (steep ? ai : bi), dx = px - (steep ? bi : ai);
+      if (dy < 1 - R || dy > R - 1) continue;
+      const int w = half[dy + R - 1];
+      if (dx >= -w && dx <= w) return true;
+    }
+  }
+  return false;
+}
+
+__global__ void k_brush(PoolView P, ImageDesc im, int img, const int32_t* __restrict__ pts,
+                        int npts, int R, int32_t value, int x0, int y0, int bw, int bh,
+                        int32_t* tl, ImageAcc* acc) {
+  // half[dy + R - 1] = the largest dx >= 0 with the offset (dy, dx) inside the disc (the
+  // test is monotone in |dx|; dx = 0 is inside for |dy| <= R - 1)
+  __shared__ int32_t half[2 * GC_BRUSH_MAX_RADIUS - 1];
+  for (int j = threadIdx.x; j < 2 * R - 1; j += blockDim.x) {
+    const int dy = j - (R - 1);
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (brush_disk(dy, mid, R)) lo = mid; else hi = mid - 1;
+    }
+    half[j] = lo;
+  }
+  __syncthreads();
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)bw * bh) return;
+  const int x = x0 + (int)(i % bw), y = y0 + (int)(i / bw);
+  if (x < 0 || y < 0 || x >= im.W || y >= im.H) return;
+  if (!in_brush(x, y, pts, npts, R, half)) return;
+  apply_tlink(P, im, img, x, y, value, tl, acc);
+}
+
 // ------------------------------------------------------------------------------------
 // Launchers
 // ------------------------------------------------------------------------------------
@@ -1363,10 +1483,16 @@ int launch_upload(const PoolView& P, const ImageDesc& im, int img, const int32_t
 }
 
 int launch_upload_rgba(const PoolView& P, const ImageDesc& im, int img, const uint32_t* rgba,
-                       const int32_t* excess, const NlinkTable& tab, int32_t* tl, ImageAcc* acc,
-                       cudaStream_t s) {
-  const RgbaSource src{rgba, excess, tab};
+                       const int32_t* excess, const int32_t* tab, int lambda, int32_t* tl,
+                       ImageAcc* acc, cudaStream_t s) {
+  const RgbaSource src{rgba, excess, tab, lambda};
   k_upload<<<im.tw * im.th, DIS_THREADS, 0, s>>>(P, im, img, src, tl, acc);
+  return ok();
+}
+
+int launch_nlink_table(const unsigned long long* sum, long long npairs, int32_t* tab,
+                       cudaStream_t s) {
+  k_nlink_table<<<1, 64, 0, s>>>(sum, npairs, tab);
   return ok();
 }
 
@@ -1514,6 +1640,30 @@ int launch_stroke(const PoolView& P, const ImageDesc& im, int img, const int32_t
   return ok();
 }
 
+int launch_brush(const PoolView& P, const ImageDesc& im, int img, const int32_t* pts_dev,
+                 const int32_t* pts_host, int npts, int radius, int32_t value, int32_t* tl,
+                 ImageAcc* acc, cudaStream_t s) {
+  const int R = radius < 1 ? 1 : radius;
+  if (R > GC_BRUSH_MAX_RADIUS) return GC_ERR_INVALID;
+  int xmin = pts_host[0], xmax = pts_host[0], ymin = pts_host[1], ymax = pts_host[1];
+  for (int k = 1; k < npts; ++k) {
+    xmin = xmin < pts_host[2 * k] ? xmin : pts_host[2 * k];
+    xmax = xmax > pts_host[2 * k] ? xmax : pts_host[2 * k];
+    ymin = ymin < pts_host[2 * k + 1] ? ymin : pts_host[2 * k + 1];
+    ymax = ymax > pts_host[2 * k + 1] ? ymax : pts_host[2 * k + 1];
+  }
+  long long x0 = (long long)xmin - (R - 1), y0 = (long long)ymin - (R - 1);
+  long long x1 = (long long)xmax + (R - 1), y1 = (long long)ymax + (R - 1);
+  x0 = x0 < 0 ? 0 : x0; y0 = y0 < 0 ? 0 : y0;
+  x1 = x1 > im.W - 1 ? im.W - 1 : x1; y1 = y1 > im.H - 1 ? im.H - 1 : y1;
+  if (x1 < x0 || y1 < y0) return GC_OK;
+  const int bw = (int)(x1 - x0 + 1), bh = (int)(y1 - y0 + 1);
+  const long long n = (long long)bw * bh;
+  k_brush<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, im, img, pts_dev, npts, R, value,
+                                                     (int)x0, (int)y0, bw, bh, tl, acc);
+  return ok();
+}
+
 // Loads every kernel of the library on the current device.  With lazy module loading (the
 // CUDA default) a kernel is loaded at its first launch or graph instantiation; doing it
 // here, once per device under a lock, keeps that loading away from threads that solve on
@@ -1528,11 +1678,13 @@ void preload_kernels() {
   cudaFuncAttributes a;
   const void* kernels[] = {
       (const void*)k_upload<PlaneSource>, (const void*)k_upload<RgbaSource>, (const void*)k_dsum,
+      (const void*)k_nlink_table,
       (const void*)k_masks, (const void*)k_discharge, (const void*)k_edge_relabel_build,
       (const void*)k_bfs_round, (const void*)k_flood_round, (const void*)k_ctl_begin,
       (const void*)k_active_list, (const void*)k_ctl_cycle,
       (const void*)k_acc_reset, (const void*)k_labels_out, (const void*)k_labels_packed,
-      (const void*)k_state_out, (const void*)k_edit, (const void*)k_stroke};
+      (const void*)k_state_out, (const void*)k_edit, (const void*)k_stroke,
+      (const void*)k_brush};
   for (const void* k : kernels) cudaFuncGetAttributes(&a, k);
   preload_scan_kernels();
   cudaGetLastError();

@@ -115,11 +115,29 @@ int gc_upload_host(gc_handle* h, const int32_t* up, const int32_t* down, const i
    uniform image); t-links are the int32 excess plane (positive: source).  rgba: DEVICE
    uint32 [height][width], R in bits 0-7, G 8-15, B 16-23 (alpha ignored), i.e. RGBA bytes
    viewed as uint32 (test_GraphCut.py:21); excess: DEVICE int32 [height][width].  Replaces
-   the 20 bytes per pixel of gc_upload with 8. */
+   the 20 bytes per pixel of gc_upload with 8.  The scale beta is computed on the device
+   (no host wait): the call only enqueues work on the stream. */
 int gc_upload_rgba(gc_handle* h, const uint32_t* rgba, const int32_t* excess, void* stream);
 /* Same with HOST arrays (copied through a device staging buffer; synchronous). */
 int gc_upload_rgba_host(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
                         void* stream);
+/* Capacities from an image with the reference's own n-link rule: GraphCut(context, devices,
+   dImg, lamda) (GraphCut.pyx:80-116) weighs the edge between 4-neighbours i, j as
+   LAMBDA / (BETA * sqrt(|I_i - I_j|^2) + EPSILON) with BETA = 0.1, EPSILON = 0.05 and
+   LAMBDA = lamda (60 by default) in float (weight(), graphcut.cl:1018-1031; load_tiles
+   :1033-1132).  Here the capacity is that value rounded to the nearest integer (halves up),
+   computed exactly: floor(x + 0.5) >= k  <=>  b = 40 lambda - 2k + 1 >= 0 and
+   4 (2k - 1)^2 d <= b^2, for d = |I_i - I_j|^2.  It differs from the reference's float32
+   value by at most 0.5 plus float rounding.  The reference's load_tiles bugs (assigning
+   instead of adding the last row/column, zeroing the right boundary in the last tile only)
+   are not reproduced: every pair gets the weight both ways and capacities out of the image
+   are 0.  1 <= lambda <= GC_NLINK_MAX_LAMBDA.  Layouts as gc_upload_rgba; no host wait. */
+#define GC_NLINK_MAX_LAMBDA 1000
+int gc_upload_rgba_lambda(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
+                          int32_t lambda, void* stream);
+/* Same with HOST arrays (synchronous). */
+int gc_upload_rgba_lambda_host(gc_handle* h, const uint32_t* rgba, const int32_t* excess,
+                               int32_t lambda, void* stream);
 
 /* One Gaussian component of a colour model, in the form its log-density is evaluated in:
    log(w N(x | mean, S)) = c - 0.5 * |Li (x - mean)|^2 for the pixel colour x = (R, G, B),
@@ -237,6 +255,19 @@ int gc_edit_tlinks(gc_handle* h, const int32_t* idx, const int32_t* value, int n
    arrays, integer pixel centres) gets t-link `value`.  Rasterised on the device. */
 int gc_edit_stroke(gc_handle* h, const int32_t* xs, const int32_t* ys, int npts, int radius,
                    int32_t value, void* stream);
+
+/* Brush edit with the reference's own pixel set (Brush.points, brush.pyx:138-161): for one
+   point, the disc skimage.draw.circle(y, x, radius) around it; for a polyline, the Bresenham
+   pixels of every segment (skimage.draw.line) each widened by that disc, whose offsets
+   (dy, dx) satisfy (dy / radius)^2 + (dx / radius)^2 < 1 in float64.  Every covered pixel
+   gets t-link `value` (the reference paints label 7 there, brush.cl:1-13).  radius <= 0
+   counts as 1, as Brush.setRadius does; radius <= 1024, 1 <= npts <= 1024 (host arrays).
+   Two reference bugs are not reproduced: the reference widens segments by
+   circle(radius, radius, radius), a disc shifted by +radius in x and y, where this centres
+   it on the line; and it flattens pixels outside the image into y * width + x (wrapping
+   into other rows), where this skips them. */
+int gc_edit_brush(gc_handle* h, const int32_t* xs, const int32_t* ys, int npts, int radius,
+                  int32_t value, void* stream);
 
 /* Residual state back to row-major DEVICE buffers (any pointer may be NULL): excess,
    height, residual capacities.  Inspection and tests. */

@@ -17,6 +17,11 @@ this module to check results; the product never imports it.
 * ``gmm_fit``         EM fit of a colour model (GMM.fit, GMM.pyx:165-372; gmm.cl:33-372).
 * ``tlinks_gmm``      t-links from a foreground and a background colour model (GMM.score,
                       gmm.cl:373-491, and scoreBg - scoreFg, test_GraphCut.py:44-47).
+* ``nlinks_reference`` the reference's n-link rule (weight(), graphcut.cl:1018-1031, with
+                      LAMBDA / EPSILON of GraphCut.pyx:25-26) rounded to integers, in exact
+                      integer arithmetic; ``weight_reference_float32`` is the reference's own
+                      float evaluation it is pinned against.
+* ``brush_pixels``    the pixel set of a brush stroke (brush.pyx:138-161).
 """
 from __future__ import annotations
 
@@ -268,3 +273,154 @@ def gmm_fit(samples, n_components, max_iterations, tolerance=0.01, min_covar=1e-
             c = (r[:, k, None] * x).T @ x / nk[k] - np.outer(mu[k], mu[k])
             S[k] = (c if full else np.diag(np.diag(c))) + min_covar * np.eye(3)
         t += 1
+
+
+# ---- n-links of the reference (graphcut.cl:1018-1031) ------------------------------------
+REF_BETA = np.float32(1.0) / np.float32(10.0)   # #define BETA 1.0f/10 (graphcut.cl:13)
+REF_EPSILON = 0.05                             # DEF EPSILON = 0.05 (GraphCut.pyx:26)
+REF_LAMBDA = 60                                # DEF LAMDA_DEFAULT = 60 (GraphCut.pyx:25)
+
+
+def weight_reference_float32(d, lam=REF_LAMBDA):
+    """The reference's capacity LAMBDA * weight(c1, c2) for |dRGB|^2 = d, evaluated as its
+    OpenCL C does: sqrt of the float distance, times BETA (float), plus EPSILON (a double
+    literal, so the sum and the reciprocal are double), the reciprocal rounded to float, then
+    times LAMBDA in float (graphcut.cl:1030, :1089)."""
+    d = np.asarray(d)
+    s = np.sqrt(d.astype(np.float32))                       # float sqrt
+    den = (REF_BETA * s).astype(np.float64) + REF_EPSILON   # float * float + double
+    w = (1.0 / den).astype(np.float32)                      # returned as float
+    return (np.float32(lam) * w).astype(np.float32)
+
+
+def weight_reference(d, lam=REF_LAMBDA):
+    """That weight rounded to the nearest integer, halves up, computed exactly:
+    x = lam / (0.1 sqrt(d) + 0.05) = 20 lam / (2 sqrt(d) + 1), and for k >= 1
+    floor(x + 0.5) >= k  <=>  b = 40 lam - 2k + 1 >= 0 and 4 (2k - 1)^2 d <= b^2.
+    Python integers, one distinct distance at a time."""
+    d = np.asarray(d, dtype=np.int64)
+    out = np.empty(d.shape, np.int64)
+    cache = {}
+    a40 = 40 * int(lam)
+
+    def ok(k, dd):
+        if k < 1:
+            return True
+        b, a = a40 - 2 * k + 1, 2 * k - 1
+        return b >= 0 and 4 * a * a * dd <= b * b
+
+    flat = out.reshape(-1)
+    for i, dd in enumerate(d.reshape(-1).tolist()):
+        w = cache.get(dd)
+        if w is None:
+            # the largest k with ok(k): ok is monotone in k, bisect over [0, 20 lam]
+            lo, hi = 0, 20 * int(lam)
+            while lo < hi:
+                mid = (lo + hi + 1) // 2
+                if ok(mid, dd):
+                    lo = mid
+                else:
+                    hi = mid - 1
+            w = cache[dd] = lo
+        flat[i] = w
+    return out
+
+
+def _dist2(a, b):
+    a = a.astype(np.int64)
+    b = b.astype(np.int64)
+    return sum(((a >> s & 255) - (b >> s & 255)) ** 2 for s in (0, 8, 16))
+
+
+def nlinks_reference(rgba, lam=REF_LAMBDA):
+    """Capacity planes (up, down, left, right) of an RGBA image (uint32 [H, W], R in the low
+    byte) under the reference's weighting rounded as ``weight_reference``: every 4-neighbour
+    pair gets its weight in both directions and capacities pointing out of the image are 0
+    (load_tiles, graphcut.cl:1033-1132, without its last-row/column and right-border bugs)."""
+    img = np.asarray(rgba).astype(np.uint32)
+    H, W = img.shape
+    wv = weight_reference(_dist2(img[1:], img[:-1]), lam).astype(np.int32)    # (y, y-1) pairs
+    wh = weight_reference(_dist2(img[:, 1:], img[:, :-1]), lam).astype(np.int32)
+    up = np.zeros((H, W), np.int32)
+    down = np.zeros((H, W), np.int32)
+    left = np.zeros((H, W), np.int32)
+    right = np.zeros((H, W), np.int32)
+    up[1:] = wv
+    down[:-1] = wv
+    left[:, 1:] = wh
+    right[:, :-1] = wh
+    return up, down, left, right
+
+
+# ---- the reference brush (brush.pyx:138-161) ---------------------------------------------
+def bresenham_line(r0, c0, r1, c1):
+    """Pixels (rows, cols) of the segment from (r0, c0) to (r1, c1) as skimage.draw.line
+    produces them (Bresenham with the error term d = 2 dr - dc, a step of the minor axis
+    while d >= 0, and the end point appended), the rasteriser brush.pyx:150 calls."""
+    r, c = int(r0), int(c0)
+    dr, dc = abs(int(r1) - r), abs(int(c1) - c)
+    sc = 1 if int(c1) - c > 0 else -1
+    sr = 1 if int(r1) - r > 0 else -1
+    steep = dr > dc
+    if steep:
+        r, c = c, r
+        dr, dc = dc, dr
+        sr, sc = sc, sr
+    d = 2 * dr - dc
+    rr, cc = [], []
+    for _ in range(dc):
+        if steep:
+            rr.append(c)
+            cc.append(r)
+        else:
+            rr.append(r)
+            cc.append(c)
+        while d >= 0:
+            r += sr
+            d -= 2 * dc
+        c += sc
+        d += 2 * dr
+    rr.append(int(r1))
+    cc.append(int(c1))
+    return np.array(rr, np.int64), np.array(cc, np.int64)
+
+
+def disk_offsets(radius):
+    """Offsets (dr, dc) of skimage.draw.circle(0, 0, radius): the integer points with
+    (dr / radius)^2 + (dc / radius)^2 < 1, evaluated in float64 as skimage's ellipse test
+    does (brush.pyx:147, :151)."""
+    R = int(radius)
+    o = np.arange(-R, R + 1, dtype=np.float64)
+    a = (o / float(R)) ** 2
+    inside = (a[:, None] + a[None, :]) < 1.0
+    dr, dc = np.nonzero(inside)
+    return dr - R, dc - R
+
+
+def brush_pixels(xs, ys, radius, width, height):
+    """Flat indices (y * width + x, increasing) of the pixels the reference Brush covers for
+    the polyline (xs[i], ys[i]) (Brush.points, brush.pyx:138-161): one point gives the disc
+    circle(y, x, radius) around it; each segment gives its line pixels, each widened by the
+    disc offsets.  radius <= 0 counts as 1 (Brush.setRadius).  Two reference bugs are fixed:
+    the segment disc is centred on each line pixel (the reference adds the pixels of
+    circle(radius, radius, radius), i.e. offsets shifted by +radius in x and y), and pixels
+    outside the image are dropped (the reference's y * width + x wraps them into other rows or
+    out of the buffer)."""
+    R = max(1, int(radius))
+    odr, odc = disk_offsets(R)
+    xs = [int(v) for v in xs]
+    ys = [int(v) for v in ys]
+    pts_r, pts_c = [], []
+    if len(xs) == 1:
+        pts_r.append(np.array([ys[0]]))
+        pts_c.append(np.array([xs[0]]))
+    for k in range(len(xs) - 1):
+        lr, lc = bresenham_line(ys[k], xs[k], ys[k + 1], xs[k + 1])
+        pts_r.append(lr)
+        pts_c.append(lc)
+    lr = np.concatenate(pts_r)
+    lc = np.concatenate(pts_c)
+    yy = (lr[:, None] + odr[None, :]).reshape(-1)
+    xx = (lc[:, None] + odc[None, :]).reshape(-1)
+    keep = (yy >= 0) & (yy < height) & (xx >= 0) & (xx < width)
+    return np.unique(yy[keep] * width + xx[keep])

@@ -128,6 +128,49 @@ def test_upload_image_builds_the_generator_planes(cuda, oracle, w, h, seed, kind
             assert np.array_equal(gc.labels_host(), l_ref)
 
 
+@pytest.mark.parametrize("w,h,lam", [(96, 64, 60), (257, 131, 60), (64, 64, 7), (300, 211, 1000)])
+def test_upload_image_reference_weighting(cuda, oracle, w, h, lam):
+    """gc_upload_rgba_lambda(_host): the reference's n-link rule (graphcut.cl:1018-1031),
+    rounded exactly, built on the device equals the oracle's planes bit for bit, and the
+    solve on them matches the exact max-flow."""
+    import torch
+    g = synth.make_graph(w, h, 5, keep_image=True)
+    from GraphCut import _as_rgba32
+    rgba = _as_rgba32(g.image)
+    planes = oracle.nlinks_reference(rgba, lam) + (g.excess,)
+    f_ref, l_ref = oracle.maxflow_bk(*planes)
+    for host in (False, True):
+        with GraphCut(w, h) as gc:
+            if host:
+                gc.upload_image(g.image, g.excess, lamda=lam)
+            else:
+                gc.upload_image(torch.from_numpy(g.image).cuda(), torch.from_numpy(g.excess).cuda(),
+                                lamda=lam)
+            for name, ref in zip(("dUp", "dDown", "dLeft", "dRight", "dExcess"), planes):
+                assert np.array_equal(getattr(gc, name).cpu().numpy(), ref), (name, host)
+            gc.cut()
+            assert gc.flow == f_ref
+            assert np.array_equal(gc.labels().cpu().numpy(), l_ref)
+
+
+def test_upload_image_many_contrasts(cuda, oracle):
+    """The device-side scale and weight table of gc_upload_rgba over images of many contrasts
+    (so many values of beta): the capacities equal the generator's float64 formula."""
+    import torch
+    rng = np.random.default_rng(77)
+    for k in range(24):
+        h, w = int(rng.integers(8, 90)), int(rng.integers(8, 90))
+        amp = float(rng.choice([1, 2, 5, 20, 60, 128, 255]))
+        img = np.clip(rng.normal(128, amp, (h, w, 3)), 0, 255).astype(np.uint8)
+        excess = rng.integers(-50, 50, (h, w)).astype(np.int32)
+        wv, wh = synth.nlinks(img)
+        planes = synth.planes_from_weights(wv, wh, excess) + (excess,)
+        with GraphCut(w, h) as gc:
+            gc.upload_image(torch.from_numpy(img).cuda(), torch.from_numpy(excess).cuda())
+            for name, ref in zip(("dUp", "dDown", "dLeft", "dRight"), planes):
+                assert np.array_equal(getattr(gc, name).cpu().numpy(), ref), (k, name)
+
+
 @pytest.mark.parametrize("iters,pulses,init", [(1, 1, 0), (4, 1, 1), (64, 5, 0), (32, 1, 1)])
 def test_schedules_agree(cuda, oracle, iters, pulses, init):
     g = synth.random_graph(160, 128, 11, cap_max=80, tlink_max=120, symmetric=False)
@@ -252,6 +295,50 @@ def test_stroke_raster_matches_host(cuda):
             t = strokes.apply(t, s)
         # the excess plane before any solve is exactly the edited t-links
         assert np.array_equal(gc.dExcess.cpu().numpy(), t)
+
+
+def test_brush_pixel_set_matches_oracle(cuda, oracle):
+    """gc_edit_brush: the reference Brush's pixel set (brush.pyx:138-161; centred disc,
+    clipped to the image) equals the oracle's restatement, for points, segments and
+    polylines, radii 0..40 and strokes that leave the image."""
+    g = synth.random_graph(257, 131, 3, cap_max=5, tlink_max=5)
+    rng = np.random.default_rng(8)
+    with GraphCut(g.width, g.height) as gc:
+        gc.upload_capacities(*g.planes())
+        t = g.excess.copy()
+        for k in range(40):
+            n = int(rng.integers(1, 6))
+            xs = rng.integers(-30, g.width + 30, n).astype(np.int32)
+            ys = rng.integers(-30, g.height + 30, n).astype(np.int32)
+            r = int(rng.integers(0, 41))
+            v = int(rng.choice([strokes.HARD, -strokes.HARD, 0, 17]))
+            gc.edit_brush(xs, ys, r, v)
+            t.reshape(-1)[oracle.brush_pixels(xs, ys, r, g.width, g.height)] = v
+            if k % 8 == 7:
+                assert np.array_equal(gc.dExcess.cpu().numpy(), t), k
+        assert np.array_equal(gc.dExcess.cpu().numpy(), t)
+
+
+def test_brush_warm_solves_match_cold(cuda, oracle):
+    """Brush strokes on a solved graph re-solve warm to the exact cut of the edited graph."""
+    g = synth.make_graph(384, 256, 12)
+    rng = np.random.default_rng(9)
+    with GraphCut(g.width, g.height) as gc:
+        gc.upload_capacities(*g.planes())
+        gc.cut()
+        t = g.excess.copy()
+        for _ in range(4):
+            n = int(rng.integers(1, 5))
+            xs = rng.integers(0, g.width, n).astype(np.int32)
+            ys = rng.integers(0, g.height, n).astype(np.int32)
+            r = int(rng.integers(4, 24))
+            v = strokes.HARD if rng.random() < 0.5 else -strokes.HARD
+            gc.edit_brush(xs, ys, r, v)
+            t.reshape(-1)[oracle.brush_pixels(xs, ys, r, g.width, g.height)] = v
+            gc.cut()
+            f_ref, l_ref = oracle.maxflow_bk(*(list(g.planes())[:4] + [t]))
+            assert gc.flow == f_ref
+            assert np.array_equal(gc.labels().cpu().numpy(), l_ref)
 
 
 def test_batch_matches_per_image(cuda, oracle):
