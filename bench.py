@@ -8,10 +8,13 @@ int32 planes) -> tile upload -> push-relabel with global relabels -> canonical c
 -> labels in a device buffer + the flow value on the host.  `value` is the whole-job
 throughput (pixels solved by all ranks / max-over-ranks device time), timed with CUDA
 events on the solver's stream; L2 is flushed (256 MiB write) between steps, outside the
-timed region.  `e2e` is the same metric through the public API with host buffers: the
-pinned RGBA image and t-link plane -> GraphCut.upload_image (n-links built on the device)
--> cut -> labels_host + flow, copies included.  `e2e_image_and_models` starts one step
-earlier, from the image and the two colour models (t-links from gmm_tlinks.tlinks).
+timed region.  `e2e` is the same metric through the public API with host buffers: every
+step copies the pinned RGBA image and t-link plane to the device, builds the graph there
+(GraphCut.upload_image, n-links on the device), solves, and reads the flow and the
+bit-packed cut back (pipeline.SolvePipeline, which overlaps step k+1's copies with step
+k's solve); `e2e_serial` runs the same calls one step after another.
+`e2e_image_and_models` starts one step earlier, from the image and the two colour models
+(t-links from gmm_tlinks.tlinks).
 
 Workload (`--config single`, the default): one 2048x2048 grid per rank built as in the
 synthetic generator (12 blurred ellipses + noise, 2-component GMM t-links, exp n-links),
@@ -371,20 +374,45 @@ def main():
         gc.set_profile(False)
 
         # e2e through the public API with host buffers
-        e2e = e2e_models = None
+        e2e = e2e_serial = e2e_models = None
         if not args.no_e2e:
             # the reference's own inputs: the RGBA image (n-links are built on the device)
-            # and the t-link plane, from pinned host memory; labels back to host memory
-            from GraphCut import _as_rgba32
+            # and the t-link plane, from pinned host memory; the cut comes back bit-packed
+            from GraphCut import _as_rgba32, unpack_labels
+            from pipeline import SolvePipeline
             rgba_pin = torch.from_numpy(np.ascontiguousarray(_as_rgba32(g.image))).pin_memory()
             exc_pin = torch.from_numpy(g.excess).pin_memory()
             rgba_host, exc_host = rgba_pin.numpy(), exc_pin.numpy()
-            out_host = torch.empty((H, W), dtype=torch.uint8).pin_memory().numpy()
+            bits_host = torch.empty((H, (W + 7) // 8), dtype=torch.uint8).pin_memory().numpy()
+            h2d, d2h = 2 * 4 * W * H, H * ((W + 7) // 8) + 8
+            # pipelined: frame k+1's copies overlap frame k's solve (SolvePipeline)
+            pipe = SolvePipeline(W, H, device=local)
+            frames = [(rgba_host, exc_host)] * args.steps
+            for fl, bits in pipe.run(frames[:3]):
+                pass
+            e2e_parity = bool(fl == f_ref and np.array_equal(unpack_labels(bits, W), l_ref))
+            barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            n_out = 0
+            for fl, bits in pipe.run(frames):
+                n_out += 1
+            e_tot = reduce_max(1000 * (time.perf_counter() - t0), torch.device("cuda", local))
+            e2e_parity &= bool(n_out == args.steps and fl == f_ref and
+                               np.array_equal(unpack_labels(bits, W), l_ref))
+            pipe.close()
+            e2e = {"value": mpix_all / (e_tot / 1000), "unit": UNIT,
+                   "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                   "ms_per_step": e_tot / args.steps, "parity": e2e_parity,
+                   "api": "pipeline.SolvePipeline.run over pinned (RGBA, int32 t-links) frames: "
+                          "per frame H2D copy, GraphCut.upload_image, cut, flow and packed "
+                          "labels D2H; frame k+1's copies overlap frame k's solve"}
+            # serial: one frame after another, every call blocking
             for _ in range(2):
                 gc.upload_image(rgba_host, exc_host, stream=stream)
                 gc.cut(stream=stream)
-                gc.labels_host(out=out_host, stream=stream)
-            e2e_parity = bool(gc.flow == f_ref and np.array_equal(out_host, l_ref))
+                gc.labels_packed_host(out=bits_host, stream=stream)
+            s_parity = bool(gc.flow == f_ref and np.array_equal(unpack_labels(bits_host, W), l_ref))
             e_ms = []
             barrier()
             for _ in range(args.steps):
@@ -393,15 +421,17 @@ def main():
                 t0 = time.perf_counter()
                 gc.upload_image(rgba_host, exc_host, stream=stream)
                 gc.cut(stream=stream)
-                gc.labels_host(out=out_host, stream=stream)
+                gc.labels_packed_host(out=bits_host, stream=stream)
                 _ = gc.flow
                 e_ms.append(1000 * (time.perf_counter() - t0))
-            e_tot = reduce_max(sum(e_ms), torch.device("cuda", local))
-            e2e = {"value": mpix_all / (e_tot / 1000), "unit": UNIT,
-                   "h2d_bytes_per_step": 2 * 4 * W * H, "d2h_bytes_per_step": W * H + 8,
-                   "ms_per_step": e_tot / args.steps, "parity": e2e_parity,
-                   "api": "GraphCut.upload_image (RGBA + int32 t-links, host) -> cut -> "
-                          "labels_host + flow"}
+            es_tot = reduce_max(sum(e_ms), torch.device("cuda", local))
+            e2e_serial = {"value": mpix_all / (es_tot / 1000), "unit": UNIT,
+                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                          "ms_per_step": es_tot / args.steps, "parity": s_parity,
+                          "api": "GraphCut.upload_image (RGBA + int32 t-links, host) -> cut -> "
+                                 "labels_packed_host + flow, one frame at a time, L2 flushed "
+                                 "before each"}
+            out_host = bits_host
 
             # one step further back in the reference's pipeline: the image and the two colour
             # models only (t-links from gc_tlinks_gmm, n-links from gc_upload_rgba; 4 B/px up)
@@ -417,12 +447,12 @@ def main():
                 tlinks(rgba_dev, *models, out=ex_dev, stream=stream)
                 gc.upload_image(rgba_dev, ex_dev, stream=stream)
                 gc.cut(stream=stream)
-                gc.labels_host(out=out_host, stream=stream)
+                gc.labels_packed_host(out=out_host, stream=stream)
                 return gc.flow
 
             for _ in range(2):
                 fm = model_step()
-            m_parity = bool(fm == f_ref and np.array_equal(out_host, l_ref))
+            m_parity = bool(fm == f_ref and np.array_equal(unpack_labels(out_host, W), l_ref))
             m_ms = []
             barrier()
             for _ in range(args.steps):
@@ -445,13 +475,13 @@ def main():
                 tl_ms.append(ev0.elapsed_time(ev1))
             tl_avg = sum(tl_ms) / len(tl_ms)
             e2e_models = {"value": mpix_all / (m_tot / 1000), "unit": UNIT,
-                          "h2d_bytes_per_step": 4 * W * H, "d2h_bytes_per_step": W * H + 8,
+                          "h2d_bytes_per_step": 4 * W * H, "d2h_bytes_per_step": d2h,
                           "ms_per_step": m_tot / args.steps, "parity": m_parity,
                           "tlinks_gmm_ms": tl_avg,
                           "tlinks_gmm_gbs": 8 * W * H / (tl_avg / 1000) / 1e9,
                           "api": "RGBA (host, pinned) -> gmm_tlinks.tlinks (2x2-component "
                                  "full-covariance models) -> GraphCut.upload_image -> cut -> "
-                                 "labels_host + flow"}
+                                 "labels_packed_host + flow"}
             e2e_models["gmm_fit"] = time_gmm_fit(g, stream, rank == 0 and world == 1
                                                  and not args.no_cpu_baseline)
 
@@ -492,6 +522,7 @@ def main():
             "parity": parity,
             "flow": flow,
             "e2e": e2e,
+            "e2e_serial": e2e_serial,
             "e2e_image_and_models": e2e_models,
             "gpu_launches": launches,
             "ms_per_step_host_driven": sum(prof_ms) / len(prof_ms),

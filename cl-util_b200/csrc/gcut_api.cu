@@ -270,6 +270,7 @@ struct Pool {
     c.take(&P.dq, nt);
     c.take(&P.dcount, 2);
     c.take(&P.img_live, imgs.size());
+    c.take(&P.img_hit, imgs.size());
     c.take(&P.tpos, nt);
     c.take(&P.rcnt, 2);
     c.take(&P.ctl, CTL_N);
@@ -429,11 +430,11 @@ struct Pool {
 
   // host-driven rounds over the marked tiles until a round finds none; the host reads
   // the control words once per batch of rounds
-  int frontier_rounds(cudaStream_t s, bool flood) {
+  int frontier_rounds(cudaStream_t s, bool flood, int abort_hit = 0) {
     int batch = 4;
     while (true) {
       for (int k = 0; k < batch; ++k) {
-        if (flood) RK(timed(K_FLOOD, s, [&] { return launch_flood_round(P, 0, 0, acc, grid_warps, s); }));
+        if (flood) RK(timed(K_FLOOD, s, [&] { return launch_flood_round(P, 0, abort_hit, 0, acc, grid_warps, s); }));
         else RK(timed(K_BFS, s, [&] { return launch_bfs_round(P, 0, 0, grid_warps, s); }));
       }
       RK(read_ctl(s));
@@ -487,18 +488,31 @@ struct Pool {
   }
 
   // Host-driven solve (profiling, stats collection): same kernels, host decides the loops.
+  //
+  // The solve (both paths): a solve that starts from a previous flow (relabel_first) floods
+  // every image first and relabels the images whose flood reaches a sink pixel; a fresh
+  // upload starts from the trivial labelling.  Then, while tiles are active: pulses of
+  // discharge, a mask rebuild, the flood of the live images with its termination check, and
+  // for the images that are not solved a global relabel and the next active-tile list.  The
+  // last flood of every image is its canonical cut, so no separate flood phase follows.
   int solve_host(cudaStream_t s, bool relabel_first) {
     RK(prof_begin(s));
     RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, s));
     int n = 0;
-    if (relabel_first) RK(global_relabel(s));
-    RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 0, 0, 0, s); }));
-    bool go = true;
     if (relabel_first) {
+      RK(flood_phase(s, /*mode=*/1));
+      RK(timed(K_COMPACT, s, [&] { return launch_flood_check(P, 1, 0, 0, s); }));
+      RK(read_ctl(s));
+      if (h_ctl[CTL_LEFT] > 0) {
+        RK(bfs_phase(s));
+        RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 0, 0, 1, 0, acc, s); }));
+        RK(read_count(s, &n));
+      }
+    } else {
+      RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 0, 0, 0, 0, acc, s); }));
       RK(read_count(s, &n));
-      go = n > 0;
     }
-    for (int cycle = 0; go; ++cycle) {
+    for (int cycle = 0; n > 0; ++cycle) {
       if (cycle >= opts.max_cycles) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
       stats.cycles++;
       for (int p = 0; p < opts.pulses_per_relabel; ++p) {
@@ -510,18 +524,33 @@ struct Pool {
         RK(timed(K_DISCHARGE, s, [&] { return launch_discharge(P, opts.discharge_iters, grid_dis, s); }));
         stats.pulses++;
       }
-      RK(global_relabel(s, 2));
-      RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 1, 1, 0, s); }));
-      RK(read_count(s, &n));
-      go = n > 0;
+      RK(timed(K_MASKS, s, [&] { return launch_masks(P, grid_warps, s); }));
+      RK(flood_phase(s, /*mode=*/2));
+      RK(timed(K_COMPACT, s, [&] { return launch_flood_check(P, 0, 0, 0, s); }));
+      RK(read_ctl(s));
+      n = 0;
+      if (h_ctl[CTL_LEFT] > 0) {
+        RK(bfs_phase(s));
+        RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 1, 1, 1, 0, acc, s); }));
+        RK(read_count(s, &n));
+      }
     }
-    RK(launch_acc_reset(acc, (int)imgs.size(), s));
-    RK(timed(K_FLOOD_FIRST, s, [&] { return launch_flood_round(P, 1, 0, acc, grid_warps, s); }));
-    RK(frontier_rounds(s, /*flood=*/true));
     CK(cudaMemcpyAsync(h_acc, acc, sizeof(ImageAcc) * imgs.size(), cudaMemcpyDeviceToHost, s));
     RK(read_ctl(s));
     RK(prof_end(s));
     return GC_OK;
+  }
+
+  // global relabel of the live images: first round, then frontier rounds until none is left
+  int bfs_phase(cudaStream_t s) {
+    RK(timed(K_BFS_FIRST, s, [&] { return launch_bfs_round(P, 2, 0, grid_warps, s); }));
+    return frontier_rounds(s, /*flood=*/false);
+  }
+
+  // flood of every image (mode 1) or of the live images (mode 2), to its end
+  int flood_phase(cudaStream_t s, int mode) {
+    RK(timed(K_FLOOD_FIRST, s, [&] { return launch_flood_round(P, mode, 1, 0, acc, grid_warps, s); }));
+    return frontier_rounds(s, /*flood=*/true, /*abort_hit=*/1);
   }
 
   // ---- CUDA graph solve: the whole solve is one graph launch.  The loops are WHILE nodes
@@ -550,18 +579,26 @@ struct Pool {
     return GC_OK;
   }
 
-  int add_while(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves,
-                cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  int add_cond(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves,
+               cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaGraph_t* body) {
     cudaGraphNodeParams p{};
     p.type = cudaGraphNodeTypeConditional;
     p.conditional.handle = h;
-    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.type = type;
     p.conditional.size = 1;
     cudaGraphNode_t node;
     CK(cudaGraphAddNode(&node, g, leaves.empty() ? nullptr : leaves.data(), leaves.size(), &p));
     *body = p.conditional.phGraph_out[0];
     leaves.assign(1, node);
     return GC_OK;
+  }
+  int add_while(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves,
+                cudaGraphConditionalHandle h, cudaGraph_t* body) {
+    return add_cond(g, leaves, h, cudaGraphCondTypeWhile, body);
+  }
+  int add_if(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves,
+             cudaGraphConditionalHandle h, cudaGraph_t* body) {
+    return add_cond(g, leaves, h, cudaGraphCondTypeIf, body);
   }
 
   // The kernels read a conditional handle of value 0 as "not launched from a graph" (the
@@ -575,63 +612,69 @@ struct Pool {
     return fail(GC_ERR_INTERNAL, "cudaGraphConditionalHandleCreate gave only handle 0");
   }
 
+  // Appends to g: flood first round (mode) + WHILE(frontier rounds) + the check, then
+  // IF(images left) { global relabel + active list (bump, count_cycle) }.
+  int graph_cycle_tail(cudaGraph_t g, std::vector<cudaGraphNode_t>& L, int mode, int all,
+                       int bump, cudaGraphConditionalHandle hmain) {
+    cudaGraphConditionalHandle hf, hbfs, hb;
+    RK(cond_handle(&hf, g));
+    RK(cond_handle(&hbfs, g));
+    RK(capture(g, L, [&](cudaStream_t cs) { return launch_flood_round(P, mode, 1, hf, acc, grid_warps, cs); }));
+    cudaGraph_t bf;
+    RK(add_while(g, L, hf, &bf));
+    {
+      std::vector<cudaGraphNode_t> Lf;
+      RK(capture(bf, Lf, [&](cudaStream_t cs) { return launch_flood_round(P, 0, 1, hf, acc, grid_warps, cs); }));
+    }
+    RK(capture(g, L, [&](cudaStream_t cs) { return launch_flood_check(P, all, hbfs, hmain, cs); }));
+    cudaGraph_t bi;
+    RK(add_if(g, L, hbfs, &bi));
+    std::vector<cudaGraphNode_t> Li;
+    RK(cond_handle(&hb, bi));
+    RK(capture(bi, Li, [&](cudaStream_t cs) { return launch_bfs_round(P, 2, hb, grid_warps, cs); }));
+    cudaGraph_t bb;
+    RK(add_while(bi, Li, hb, &bb));
+    {
+      std::vector<cudaGraphNode_t> Lb;
+      RK(capture(bb, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, hb, grid_warps, cs); }));
+    }
+    return capture(bi, Li, [&](cudaStream_t cs) {
+      return launch_active_list(P, scan.st, list, counts, bump, bump, 1, hmain, acc, cs);
+    });
+  }
+
   int build_graph(int variant) {
-    // One graph construction at a time in the process: building, instantiating and
-    // destroying graphs with nested conditional nodes from several threads at once is the
-    // suspected trigger of an intermittent fault under concurrent serving.
+    // One graph construction at a time in the process (building, instantiating and
+    // destroying graphs with nested conditional nodes from several threads at once was the
+    // suspected trigger of an intermittent fault under concurrent serving).
     std::lock_guard<std::mutex> lock(graph_build_mutex());
     if (!cap_stream) CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
     cudaGraph_t g;
     CK(cudaGraphCreate(&g, 0));
     graph[variant] = g;
     std::vector<cudaGraphNode_t> L;
-    cudaGraphConditionalHandle hmain, hflood;
+    cudaGraphConditionalHandle hmain;
     RK(cond_handle(&hmain, g));
-    RK(cond_handle(&hflood, g));
     RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs); }));
-    if (variant) {  // exact global relabel before the first push
-      cudaGraphConditionalHandle h0;
-      RK(cond_handle(&h0, g));
+    if (variant) {
+      // from a previous flow: flood every image; relabel the ones that are not solved
+      RK(capture(g, L, [&](cudaStream_t cs) { return launch_masks(P, grid_warps, cs); }));
+      RK(graph_cycle_tail(g, L, /*mode=*/1, /*all=*/1, /*bump=*/0, hmain));
+    } else {
       RK(capture(g, L, [&](cudaStream_t cs) {
-        RK(launch_masks(P, grid_warps, cs));
-        return launch_bfs_round(P, 1, h0, grid_warps, cs);
+        return launch_active_list(P, scan.st, list, counts, 0, 0, 0, hmain, acc, cs);
       }));
-      cudaGraph_t b0;
-      RK(add_while(g, L, h0, &b0));
-      std::vector<cudaGraphNode_t> Lb;
-      RK(capture(b0, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, h0, grid_warps, cs); }));
     }
-    RK(capture(g, L, [&](cudaStream_t cs) {
-      return launch_active_list(P, scan.st, list, counts, 0, 0, hmain, cs);
-    }));
     cudaGraph_t bm;
     RK(add_while(g, L, hmain, &bm));
     {
       std::vector<cudaGraphNode_t> Lm;
-      cudaGraphConditionalHandle hb;
-      RK(cond_handle(&hb, bm));
       RK(capture(bm, Lm, [&](cudaStream_t cs) {
         for (int p = 0; p < opts.pulses_per_relabel; ++p)
           RK(launch_discharge(P, opts.discharge_iters, grid_dis, cs));
-        RK(launch_masks(P, grid_warps, cs));
-        return launch_bfs_round(P, 2, hb, grid_warps, cs);
+        return launch_masks(P, grid_warps, cs);
       }));
-      cudaGraph_t bb;
-      RK(add_while(bm, Lm, hb, &bb));
-      std::vector<cudaGraphNode_t> Lb;
-      RK(capture(bb, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, hb, grid_warps, cs); }));
-      RK(capture(bm, Lm, [&](cudaStream_t cs) {
-        return launch_active_list(P, scan.st, list, counts, 1, 1, hmain, cs);
-      }));
-    }
-    RK(capture(g, L, [&](cudaStream_t cs) {   // k_ctl_begin cleared the sums
-      return launch_flood_round(P, 1, hflood, acc, grid_warps, cs);
-    }));
-    cudaGraph_t bf;
-    RK(add_while(g, L, hflood, &bf));
-    {
-      std::vector<cudaGraphNode_t> Lf;
-      RK(capture(bf, Lf, [&](cudaStream_t cs) { return launch_flood_round(P, 0, hflood, acc, grid_warps, cs); }));
+      RK(graph_cycle_tail(bm, Lm, /*mode=*/2, /*all=*/0, /*bump=*/1, hmain));
     }
     RK(capture(g, L, [&](cudaStream_t cs) {
       // control words and per-image sums are adjacent on both sides: one copy
@@ -690,8 +733,10 @@ struct Pool {
     if (stats.launches < 0) {  // graph solve: count the kernel nodes that ran
       stats.cycles = h_ctl[CTL_CYCLES];
       stats.pulses = stats.cycles * opts.pulses_per_relabel;
-      stats.launches = 4 + stats.cycles * (1LL * opts.pulses_per_relabel + 3) + stats.bfs_rounds +
-                       1 + stats.flood_rounds;
+      // ctl_begin, the pulses, one mask rebuild per flood check, the checks, the active
+      // lists and every BFS / flood round
+      stats.launches = 1 + stats.pulses + 2LL * h_ctl[CTL_NCHECK] + h_ctl[CTL_NACT] +
+                       stats.bfs_rounds + stats.flood_rounds;
     }
     solved = true;
     edited = false;
@@ -735,7 +780,7 @@ struct Pool {
     *done = n == 0;
     if (*done) {
       RK(launch_acc_reset(acc, (int)imgs.size(), s));
-      RK(launch_flood_round(P, 1, 0, acc, grid_warps, s));
+      RK(launch_flood_round(P, 1, 0, 0, acc, grid_warps, s));
       RK(frontier_rounds(s, /*flood=*/true));
       CK(cudaMemcpyAsync(h_acc, acc, sizeof(ImageAcc) * imgs.size(), cudaMemcpyDeviceToHost, s));
       RK(read_ctl(s));

@@ -53,6 +53,7 @@ struct PoolView {
   long long* tpos;        // [nt] sum of max(excess, 0) over the tile (with the masks)
   int nimg;               // images in the pool
   int32_t* img_live;      // [nimg] cycle stamp of images that still have active tiles
+  int32_t* img_hit;       // [nimg] cycle stamp: the image's flood reached a sink pixel
   unsigned long long* ktiles;  // [K_COUNT] tiles processed per kernel kind (profiling)
 };
 
@@ -77,6 +78,9 @@ enum CtlSlot {
                       // 5: frontier append, 6: frontier length, 7: dirty append,
                       // 8: dirty length
   CTL_KDONE = 14,     // CTAs finished in k_masks
+  CTL_NCHECK = 15,    // flood checks run (k_flood_check launches)
+  CTL_NACT = 16,      // active-list rebuilds run (k_active_list launches)
+  CTL_LEFT = 17,      // images still running after the last flood check
   CTL_N = 64          // the control words fill 256 bytes; the per-image sums follow them
 };
 

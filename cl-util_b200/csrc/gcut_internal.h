@@ -82,12 +82,19 @@ int launch_edge_relabel_build(const PoolView& P, int32_t* list, int32_t* count,
 // images that still had active tiles at the previous check.
 int launch_bfs_round(const PoolView& P, int first, cudaGraphConditionalHandle h, int grid,
                      cudaStream_t s);
-int launch_flood_round(const PoolView& P, int first, cudaGraphConditionalHandle h, ImageAcc* acc,
-                       int grid, cudaStream_t s);
+// mode: 0 frontier round, 1 first round over every tile, 2 first round over the tiles of the
+// images live in this cycle; abort_hit: frontier rounds skip images that reached a sink
+int launch_flood_round(const PoolView& P, int mode, int abort_hit, cudaGraphConditionalHandle h,
+                       ImageAcc* acc, int grid, cudaStream_t s);
+// retires the images whose flood reached no sink; all: every image takes part
+int launch_flood_check(const PoolView& P, int all, cudaGraphConditionalHandle hbfs,
+                       cudaGraphConditionalHandle hmain, cudaStream_t s);
 int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc* acc,
                      cudaStream_t s);
+// filter_live: only tiles of the images a flood check kept (img_live == the cycle stamp)
 int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, int32_t* count,
-                       int bump, int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s);
+                       int bump, int count_cycle, int filter_live, cudaGraphConditionalHandle h,
+                       ImageAcc* acc, cudaStream_t s);
 int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s);
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s);

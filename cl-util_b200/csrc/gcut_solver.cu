@@ -260,6 +260,7 @@ k_upload(PoolView P, ImageDesc im, int img, Source src, int32_t* __restrict__ tl
   *(int4*)(P.cap[DLEFT] + off) = make_int4(cl[0], cl[1], cl[2], cl[3]);
   *(int4*)(P.cap[DRIGHT] + off) = make_int4(cr[0], cr[1], cr[2], cr[3]);
   write_tile_masks(P, t, e, cu, cd, cl, cr);
+  if (threadIdx.x < 32) P.mreach[(long long)t * 32 + threadIdx.x] = 0u;   // no flood yet
   __shared__ long long wpos[DIS_THREADS / 32];
 #pragma unroll
   for (int o = 16; o; o >>= 1) pos += __shfl_xor_sync(0xffffffffu, pos, o);
@@ -1011,6 +1012,7 @@ __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc
   for (int i = threadIdx.x; i < CTL_N; i += blockDim.x) P.ctl[i] = 0;
   for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) {
     P.img_live[i] = 0;
+    P.img_hit[i] = 0;
     acc[i].sumpos_e = 0;   // the flood of this solve accumulates it
   }
   if (threadIdx.x == 0) {
@@ -1035,17 +1037,17 @@ constexpr int ACT_CHUNK = ACT_THREADS * ACT_ITEMS;
 
 __global__ void __launch_bounds__(ACT_THREADS)
 k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
-              int count_cycle, cudaGraphConditionalHandle h) {
+              int count_cycle, int filter_live, cudaGraphConditionalHandle h, ImageAcc* acc) {
   __shared__ int32_t sm[32];
-  __shared__ int32_t s_chunk, s_excl, s_stamp;
+  __shared__ int32_t s_chunk, s_excl, s_cur;
   __shared__ uint32_t s_tag;
   if (threadIdx.x == 0) {
     s_chunk = atomicAdd(st.ticket, 1);
     s_tag = *((volatile uint32_t*)st.seq);
-    s_stamp = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1 + bump;
+    s_cur = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1;
   }
   __syncthreads();
-  const int chunk = s_chunk, stamp = s_stamp;
+  const int chunk = s_chunk, cur = s_cur, stamp = cur + bump;
   const int nt = P.nt;
   const int nchunks = (nt + ACT_CHUNK - 1) / ACT_CHUNK;
   const int base = chunk * ACT_CHUNK + threadIdx.x * ACT_ITEMS;
@@ -1059,6 +1061,17 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
   } else {
 #pragma unroll
     for (int k = 0; k < ACT_ITEMS; ++k) v[k] = (base + k < nt) ? (P.tact[base + k] != 0) : 0;
+  }
+  // after a flood check only the images it kept take part (a solved image keeps the
+  // activity flags of its last relabel); the stamp this launch writes counts as live too
+  if (filter_live) {
+#pragma unroll
+    for (int k = 0; k < ACT_ITEMS; ++k) {
+      if (!v[k]) continue;
+      const int img = P.img_of[base + k];
+      const int il = (unsigned)img < (unsigned)P.nimg ? *((volatile int32_t*)&P.img_live[img]) : 0;
+      v[k] = il == cur || il == stamp;
+    }
   }
   int32_t tsum = 0;
 #pragma unroll
@@ -1078,8 +1091,15 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
       if ((unsigned)run < (unsigned)nt) list[run] = t;
       else atomicExch(st.err, 2);   // only after a look-back that gave up
       const int img = P.img_of[t];
-      if ((unsigned)img < (unsigned)P.nimg) P.img_live[img] = stamp;
-      else record_bad(P, 4, img);
+      if ((unsigned)img < (unsigned)P.nimg) {
+        P.img_live[img] = stamp;
+        // the image's next flood starts afresh: its sum and its sink-reached stamp (the
+        // first cycle of a warm solve reuses the stamp of the flood before it)
+        acc[img].sumpos_e = 0;
+        P.img_hit[img] = 0;
+      } else {
+        record_bad(P, 4, img);
+      }
       ++run;
     }
   }
@@ -1101,6 +1121,7 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
   P.qcount[1] = 0;
   const int cycles = ctl[CTL_CYCLES] + (count_cycle ? 1 : 0);
   ctl[CTL_CYCLES] = cycles;
+  ctl[CTL_NACT] = ctl[CTL_NACT] + 1;
   bool more = n > 0 && ctl[CTL_ERR] < 3;
   if (more && cycles >= ctl[CTL_MAXCYCLES]) {
     ctl[CTL_ERR] = 2;
@@ -1225,11 +1246,23 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
 // ------------------------------------------------------------------------------------
 // Canonical cut: flood from excess pixels over residual edges (forward direction).
 // The first flood round also sums max(excess, 0) per image for the flow value.
+//
+// The flood also decides termination: an excess pixel can reach a sink pixel exactly when
+// the flood from the excess pixels reaches one, so an image whose flood reaches no sink
+// pixel is solved (its flood is the canonical cut) and one whose flood does needs another
+// global relabel and push cycle.  Every round stamps img_hit[img] with the cycle stamp
+// (ctl[CTL_CYCLES] + 1) when a tile's reached set meets its sink pixels.
+//
+// mode: 0 frontier round; 1 first round over every tile; 2 first round over the tiles of
+// the images live in this cycle (img_live == stamp).  abort_hit: frontier rounds skip the
+// tiles of images already stamped (their flood is redone in a later cycle).
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
-k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc) {
+k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h, ImageAcc* acc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int first = mode != 0;
   const int in = frontier_round_number(P, first) & 1, out = in ^ 1;
+  const int stamp = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1;
   int32_t* const markin = P.mark[in];
   int done = 0;
   int n, parts;
@@ -1238,6 +1271,13 @@ k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc
   for (int i = blockIdx.x * WARPS_PER_CTA + warp; i < n; i += parts * WARPS_PER_CTA) {
     const int t = first ? i : P.fq[in][i];
     if (!first && lane == 0) markin[t] = 0;
+    const int img = P.img_of[t];
+    if ((unsigned)img >= (unsigned)P.nimg) {   // self-check
+      if (lane == 0) record_bad(P, 4, img);
+      continue;
+    }
+    if (mode == 2 && P.img_live[img] != stamp) continue;
+    if (mode == 0 && abort_hit && *((volatile int32_t*)&P.img_hit[img]) == stamp) continue;
     ++done;
     const int4 nb = P.nbr[t];
     const uint32_t* mc = P.mcan + (long long)t * 128;
@@ -1246,14 +1286,9 @@ k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc
     if (first) {
       R = P.mexc[(long long)t * 32 + lane];
       R0 = 0;
-      // Σ max(excess, 0) of the tile was taken with its masks at the last global relabel,
-      // after which the tile did not change
+      // Σ max(excess, 0) of the tile was taken with its masks after the tile last changed
       const long long ps = P.tpos[t];
-      const int img = P.img_of[t];
-      if (lane == 0 && ps) {
-        if ((unsigned)img < (unsigned)P.nimg) atomicAdd(&acc[img].sumpos_e, (unsigned long long)ps);
-        else record_bad(P, 4, img);   // self-check
-      }
+      if (lane == 0 && ps) atomicAdd(&acc[img].sumpos_e, (unsigned long long)ps);
     } else {
       R = R0 = P.mreach[(long long)t * 32 + lane];
       if (lane == 0 && nb.x >= 0)
@@ -1275,6 +1310,9 @@ k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc
       R = N;
     }
     P.mreach[(long long)t * 32 + lane] = R;
+    if (__any_sync(0xffffffffu, (R & P.msink[(long long)t * 32 + lane]) != 0) && lane == 0 &&
+        *((volatile int32_t*)&P.img_hit[img]) != stamp)
+      P.img_hit[img] = stamp;
     const uint32_t nw = first ? R : (R & ~R0);
     const int sU = __any_sync(0xffffffffu, lane == 0 && (nw & canU));
     const int sD = __any_sync(0xffffffffu, lane == 31 && (nw & canD));
@@ -1292,6 +1330,42 @@ k_flood_round(PoolView P, int first, cudaGraphConditionalHandle h, ImageAcc* acc
     if (P.ktiles) atomicAdd(&P.ktiles[first ? K_FLOOD_FIRST : K_FLOOD], (unsigned long long)done);
   }
   frontier_round_end(P, first, in, CTL_FLOOD_TOTAL, parts, h);
+}
+
+// After a flood: an image whose flood reached no sink pixel is solved (its flood is the
+// canonical cut, its sums are final) and leaves the live set; the others go on to a global
+// relabel.  all != 0: every image takes part (the first check of a solve that starts with a
+// relabel); else the images live in this cycle.  Sets the condition of the IF node around
+// the relabel (hbfs) and, when no image is left, ends the solve loop (hmain); the last cycle
+// of a solve is counted here.  One CTA.
+__global__ void k_flood_check(PoolView P, int all, cudaGraphConditionalHandle hbfs,
+                              cudaGraphConditionalHandle hmain) {
+  __shared__ int s_left;
+  if (threadIdx.x == 0) s_left = 0;
+  __syncthreads();
+  volatile int32_t* ctl = P.ctl;
+  const int stamp = ctl[CTL_CYCLES] + 1;
+  int left = 0;
+  for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) {
+    if (!all && P.img_live[i] != stamp) continue;
+    if (P.img_hit[i] == stamp) {
+      P.img_live[i] = stamp;
+      ++left;
+    } else {
+      P.img_live[i] = 0;   // solved: no later stamp equals 0
+    }
+  }
+  if (left) atomicAdd(&s_left, left);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  int n = s_left;
+  if (ctl[CTL_ERR] != 0) n = 0;   // a cap or a self-check ends the loops
+  ctl[CTL_LEFT] = n;
+  ctl[CTL_NCHECK] = ctl[CTL_NCHECK] + 1;
+  if (n == 0 && !all) ctl[CTL_CYCLES] = ctl[CTL_CYCLES] + 1;
+  __threadfence();
+  if (hbfs) cudaGraphSetConditional(hbfs, n > 0 ? 1u : 0u);
+  if (hmain && n == 0) cudaGraphSetConditional(hmain, 0u);
 }
 
 // Labels of one image, row-major, padding excluded.  One thread writes the 32 pixels of
@@ -1554,9 +1628,15 @@ int launch_bfs_round(const PoolView& P, int first, cudaGraphConditionalHandle h,
   return ok();
 }
 
-int launch_flood_round(const PoolView& P, int first, cudaGraphConditionalHandle h, ImageAcc* acc,
-                       int grid, cudaStream_t s) {
-  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, first, h, acc);
+int launch_flood_round(const PoolView& P, int mode, int abort_hit, cudaGraphConditionalHandle h,
+                       ImageAcc* acc, int grid, cudaStream_t s) {
+  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, mode, abort_hit, h, acc);
+  return ok();
+}
+
+int launch_flood_check(const PoolView& P, int all, cudaGraphConditionalHandle hbfs,
+                       cudaGraphConditionalHandle hmain, cudaStream_t s) {
+  k_flood_check<<<1, 256, 0, s>>>(P, all, hbfs, hmain);
   return ok();
 }
 
@@ -1577,10 +1657,12 @@ int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc
 }
 
 int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, int32_t* count,
-                       int bump, int count_cycle, cudaGraphConditionalHandle h, cudaStream_t s) {
+                       int bump, int count_cycle, int filter_live, cudaGraphConditionalHandle h,
+                       ImageAcc* acc, cudaStream_t s) {
   const int nch = (P.nt + ACT_CHUNK - 1) / ACT_CHUNK;
   if (nch > st.max_chunks) return GC_ERR_INVALID;
-  k_active_list<<<nch > 0 ? nch : 1, ACT_THREADS, 0, s>>>(P, st, list, count, bump, count_cycle, h);
+  k_active_list<<<nch > 0 ? nch : 1, ACT_THREADS, 0, s>>>(P, st, list, count, bump, count_cycle,
+                                                          filter_live, h, acc);
   return ok();
 }
 
@@ -1681,7 +1763,7 @@ void preload_kernels() {
       (const void*)k_nlink_table,
       (const void*)k_masks, (const void*)k_discharge, (const void*)k_edge_relabel_build,
       (const void*)k_bfs_round, (const void*)k_flood_round, (const void*)k_ctl_begin,
-      (const void*)k_active_list, (const void*)k_ctl_cycle,
+      (const void*)k_active_list, (const void*)k_ctl_cycle, (const void*)k_flood_check,
       (const void*)k_acc_reset, (const void*)k_labels_out, (const void*)k_labels_packed,
       (const void*)k_state_out, (const void*)k_edit, (const void*)k_stroke,
       (const void*)k_brush};

@@ -1,0 +1,74 @@
+"""The benchmark's multi-grid and interactive configurations at their stated sizes.
+
+* The 64-grid batch: sides drawn from {256, 384, ..., 1536} (width and height independent),
+  one synthetic grid per seed 10000 + i, all solved together in one tile pool; every grid's
+  flow and canonical cut equal the exact max-flow oracle's, on the CUDA-graph path and on
+  the host-driven path.
+* A slice of the interactive workload: one 4096 x 4096 grid, then brush strokes (radius
+  8-32, t-links +-10^6), each re-solved warm from the previous residual graph; after every
+  stroke the cut equals a cold solve of the edited graph and the flow equals the capacity
+  of the cut (weak duality certifies both optimal).
+"""
+import numpy as np
+import pytest
+
+import strokes
+import synth
+from GraphCut import GraphCut
+from GraphCutBatch import GraphCutBatch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def batch64():
+    shapes = synth.batch_shapes(64, seed=2)
+    graphs = synth.make_graphs([(w, h, 10_000 + i) for i, (w, h) in enumerate(shapes)])
+    return shapes, graphs
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_of_64_mixed_grids_matches_oracle(cuda, oracle, batch64, use_graph):
+    torch = cuda
+    shapes, graphs = batch64
+    assert len(shapes) == 64 and {w % 128 for w, _ in shapes} == {0}
+    assert min(min(s) for s in shapes) >= 256 and max(max(s) for s in shapes) <= 1536
+    b = GraphCutBatch(shapes, use_graph=use_graph)
+    try:
+        for i, g in enumerate(graphs):
+            b.upload(i, *[torch.from_numpy(p).cuda() for p in g.planes()])
+        b.cut()
+        for i, g in enumerate(graphs):
+            f_ref, l_ref = oracle.maxflow_bk(*g.planes())
+            assert b.flow(i) == f_ref, i
+            assert np.array_equal(b.labels(i).cpu().numpy(), l_ref), i
+    finally:
+        b.close()
+
+
+def test_strokes_on_4096_grid_warm_equals_cold(cuda, oracle):
+    torch = cuda
+    g = synth.make_graph(4096, 4096, 1001)
+    dev = [torch.from_numpy(p).cuda() for p in g.planes()]
+    rng = np.random.default_rng(31)
+    t = g.excess.copy()
+    warm = GraphCut(g.width, g.height)
+    cold = GraphCut(g.width, g.height)
+    try:
+        warm.upload_capacities(*dev)
+        warm.cut()
+        for k in range(24):
+            s = strokes.random_stroke(rng, g.width, g.height)
+            warm.edit_stroke(s.xs, s.ys, s.radius, s.value)
+            t = strokes.apply(t, s)
+            warm.cut()
+            cold.upload_capacities(*dev[:4], torch.from_numpy(t).cuda())
+            cold.cut()
+            lw, lc = warm.labels_host(), cold.labels_host()
+            assert warm.flow == cold.flow, k
+            assert np.array_equal(lw, lc), k
+            if k % 6 == 5:   # certificate: flow == capacity of the cut
+                assert oracle.cut_capacity(g.up, g.down, g.left, g.right, t, lw) == warm.flow, k
+    finally:
+        warm.close()
+        cold.close()
