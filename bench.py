@@ -270,8 +270,29 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def spawn_ranks(args):
+    """`--gpus N` without a launcher: re-run this command under torch.distributed.run with N
+    processes on this node (one per GPU, rendezvous on 127.0.0.1) and return its exit code.
+    The ranks print the JSON line (rank 0) exactly as under an external torchrun."""
+    import socket
+
+    import torch
+    if torch.cuda.device_count() < args.gpus:
+        sys.exit(f"bench.py: --gpus {args.gpus} needs {args.gpus} GPUs, "
+                 f"{torch.cuda.device_count()} visible")
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args))
     if args.slots != 1:
         sys.exit("bench.py: --slots must be 1 (concurrent serving slots raised an "
                  "intermittent device fault whose cause is not found)")

@@ -81,6 +81,12 @@ class GraphCut:
         import torch
         self.width, self.height = int(width), int(height)
         self.device = torch.device("cuda", device)
+        if bfs is None and discharge_iters is None and initial_relabel is None:
+            # the run-time autotuner's choice for this size class on this device
+            import autotune
+            sched = autotune.default_tuner().schedule(device, self.width, self.height)
+            bfs, discharge_iters = sched["pulses_per_relabel"], sched["discharge_iters"]
+            initial_relabel = bool(sched["initial_relabel"])
         opts = _gcut.default_opts(device=device, discharge_iters=discharge_iters,
                                   pulses_per_relabel=bfs,
                                   initial_relabel=None if initial_relabel is None else int(initial_relabel),

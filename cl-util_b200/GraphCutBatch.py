@@ -18,11 +18,6 @@ import _gcut
 from _gcut import check, lib, ptr, stream_handle
 
 
-# schedule tuned by autotune.py on the 64-grid mixed batch (sides 256..1536)
-BATCH_DISCHARGE_ITERS = 4
-BATCH_PULSES = 2
-
-
 class GraphCutBatch:
     def __init__(self, shapes, device: int = 0, bfs=None, discharge_iters=None,
                  initial_relabel=None, max_cycles=None, max_bfs_rounds=None,
@@ -30,8 +25,13 @@ class GraphCutBatch:
         import torch
         self.shapes = [(int(w), int(h)) for (w, h) in shapes]
         self.device = torch.device("cuda", device)
-        if discharge_iters is None and bfs is None:
-            discharge_iters, bfs = BATCH_DISCHARGE_ITERS, BATCH_PULSES
+        if discharge_iters is None and bfs is None and initial_relabel is None:
+            # the run-time autotuner's choice for a pool of this many pixels on this device
+            import autotune
+            sched = autotune.default_tuner().schedule(
+                device, 0, 0, kind="batch", pixels=sum(w * h for w, h in self.shapes))
+            discharge_iters, bfs = sched["discharge_iters"], sched["pulses_per_relabel"]
+            initial_relabel = bool(sched["initial_relabel"])
         opts = _gcut.default_opts(device=device, discharge_iters=discharge_iters,
                                   pulses_per_relabel=bfs,
                                   initial_relabel=None if initial_relabel is None else int(initial_relabel),

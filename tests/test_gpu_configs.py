@@ -72,3 +72,26 @@ def test_strokes_on_4096_grid_warm_equals_cold(cuda, oracle):
     finally:
         warm.close()
         cold.close()
+
+
+def test_runtime_autotuner_on_the_device(cuda, tmp_path):
+    """The tuner times every candidate schedule on a grid of the class, each candidate's cut
+    must equal the others' (tune raises otherwise), and the choice is cached: asking again
+    does no device work, a new tuner reads it from the file, and GraphCut picks it up."""
+    import autotune
+    grid = {"discharge_iters": [2, 4], "pulses_per_relabel": [1, 2], "initial_relabel": [0, 1]}
+    t = autotune.Autotuner(cache_path=str(tmp_path / "sched.json"), grid=grid, repeats=1)
+    best = t.ensure(0, 320, 320)          # class of grids up to 512 x 512
+    assert set(best) == set(autotune.KNOBS) and t.tunings == 1
+    assert t.ensure(0, 300, 333) == best and t.tunings == 1
+    t2 = autotune.Autotuner(cache_path=str(tmp_path / "sched.json"), grid=grid)
+    assert t2.schedule(0, 256, 256) == best
+    old = autotune._default
+    autotune._default = t2
+    try:
+        gc = GraphCut(256, 256)
+        assert (gc.opts.discharge_iters, gc.opts.pulses_per_relabel, gc.opts.initial_relabel) == \
+            (best["discharge_iters"], best["pulses_per_relabel"], best["initial_relabel"])
+        gc.close()
+    finally:
+        autotune._default = old
