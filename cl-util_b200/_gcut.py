@@ -130,6 +130,21 @@ SIGNATURES = {
     "gcb_get_stats": [_P, _P],
     "gcb_set_profile": [_P, _I],
     "gcb_get_profile": [_P, _P, _I],
+    "gcp_arena_bytes": [_I, _I, _P],
+    "gcp_create": [_I, _I, _P, _P],
+    "gcp_create_in": [_I, _I, _P, _P, ctypes.c_int64, _P],
+    "gcp_destroy": [_P],
+    "gcp_open": [_P, _I, _I, _I, _I, _P],
+    "gcp_close": [_P, _I],
+    "gcp_upload": [_P, _I] + [_P] * 5 + [_P],
+    "gcp_upload_rgba": [_P, _I, _P, _P, _P],
+    "gcp_edit_stroke": [_P, _I, _P, _P, _I, _I, _I32, _P],
+    "gcp_edit_brush": [_P, _I, _P, _P, _I, _I, _I32, _P],
+    "gcp_solve": [_P, _P, _I, _P],
+    "gcp_flow": [_P, _I, _P],
+    "gcp_labels": [_P, _I, _P, _P],
+    "gcp_labels_packed": [_P, _I, _P, _P],
+    "gcp_get_stats": [_P, _P],
 }
 _RESTYPE = {"gc_last_error": ctypes.c_char_p, "gc_kernel_name": ctypes.c_char_p}
 

@@ -164,6 +164,13 @@ struct Pool {
   int32_t* ntab = nullptr;                // device: n-link thresholds (gc_upload_rgba)
   bool uploaded = false, solved = false, edited = false, collect = false;
   bool list_valid = false, bfs_fresh = false;
+  // per image: uploaded, solved since its upload or last edit, edited since its last solve
+  std::vector<uint8_t> img_up, img_solved, img_edited;
+  bool dynamic = false;        // a session pool: images open and close at run time
+  // the selection block (ranges, modes, counts) in device memory and its pinned mirror
+  char* d_sel = nullptr;
+  char* h_sel = nullptr;
+  size_t sel_bytes = 0;
   gc_stats stats{};
   // profiling: event pairs around every launch, tiles processed per kernel kind
   bool prof = false;
@@ -247,7 +254,7 @@ struct Pool {
     P = PoolView{};
     tl = list = counts = stage = pts = nullptr;
     acc = nullptr; lstage = nullptr; h_count = nullptr; h_ctl = nullptr; h_acc = nullptr;
-    dsum = nullptr; ntab = nullptr;
+    dsum = nullptr; ntab = nullptr; d_sel = nullptr; h_sel = nullptr;
   }
 
   // places every device buffer of the pool (see Carve)
@@ -271,6 +278,13 @@ struct Pool {
     c.take(&P.dcount, 2);
     c.take(&P.img_live, imgs.size());
     c.take(&P.img_hit, imgs.size());
+    c.take(&P.img_mode, imgs.size());
+    c.take(&d_sel, sel_bytes);
+    if (d_sel) {
+      P.nsel = reinterpret_cast<int32_t*>(d_sel);
+      P.sel = reinterpret_cast<int4*>(d_sel + 16);
+      P.sel_mode = reinterpret_cast<int32_t*>(P.sel + imgs.size());
+    }
     c.take(&P.tpos, nt);
     c.take(&P.rcnt, 2);
     c.take(&P.ctl, CTL_N);
@@ -301,8 +315,24 @@ struct Pool {
       nt += (int)tiles;
       imgs.push_back(d);
     }
+    return finish_describe();
+  }
+
+  // a session pool: room for max_tiles tiles and max_images images, none open yet
+  int describe_dynamic(int max_tiles, int max_images) {
+    if (max_tiles < 1 || max_tiles > (1 << 26) || max_images < 1 || max_images > (1 << 16))
+      return fail(GC_ERR_INVALID, "session pool size out of range");
+    nt = max_tiles;
+    imgs.assign(max_images, ImageDesc{0, 0, 0, 0, 0});
+    dynamic = true;
+    return finish_describe();
+  }
+
+  int finish_describe() {
     P.nt = nt;
     P.nimg = (int)imgs.size();
+    // selection block: counts (16 bytes), one int4 range and one mode per image
+    sel_bytes = 16 + imgs.size() * (sizeof(int4) + sizeof(int32_t));
     Carve sizing;
     layout(sizing);
     arena_bytes = sizing.off + 256;   // slack after the last buffer
@@ -313,9 +343,24 @@ struct Pool {
   int create(int n, const int* W, const int* H, const gc_opts* o, void* ext = nullptr,
              size_t ext_bytes = 0) {
     opts = *o;
+    RK(describe(n, W, H));
+    return create_common(ext, ext_bytes);
+  }
+
+  // a session pool of max_tiles tiles and max_images image slots
+  int create_dynamic(int max_tiles, int max_images, const gc_opts* o, void* ext = nullptr,
+                     size_t ext_bytes = 0) {
+    opts = *o;
+    RK(describe_dynamic(max_tiles, max_images));
+    return create_common(ext, ext_bytes);
+  }
+
+  int create_common(void* ext, size_t ext_bytes) {
     device = opts.device;
     use_graph = opts.use_graph != 0;
-    RK(describe(n, W, H));
+    img_up.assign(imgs.size(), 0);
+    img_solved.assign(imgs.size(), 0);
+    img_edited.assign(imgs.size(), 0);
     if (ext) {
       if ((reinterpret_cast<uintptr_t>(ext) & 255) != 0) return fail(GC_ERR_INVALID, "arena not 256-byte aligned");
       if (ext_bytes < arena_bytes) return fail(GC_ERR_INVALID, "arena smaller than gc_arena_bytes");
@@ -346,23 +391,28 @@ struct Pool {
       release();
       return fail(GC_ERR_INTERNAL, "arena layout");
     }
-    pin_bytes = 512 + imgs.size() * sizeof(ImageAcc);
+    // pinned: counts, control words, per-image sums, then the selection mirror
+    const size_t acc_end = (512 + imgs.size() * sizeof(ImageAcc) + 15) & ~(size_t)15;
+    pin_bytes = acc_end + sel_bytes;
     pin = pinned_take(pin_bytes);
     if (!pin) { release(); return fail(GC_ERR_OOM, "pinned host allocation failed"); }
     h_count = static_cast<int32_t*>(pin);
     h_ctl = reinterpret_cast<int32_t*>(static_cast<char*>(pin) + 256);
     h_acc = reinterpret_cast<ImageAcc*>(static_cast<char*>(pin) + 512);
-    std::vector<int4> nb(nt);
-    for (const auto& d : imgs)
-      for (int ty = 0; ty < d.th; ++ty)
-        for (int tx = 0; tx < d.tw; ++tx) {
-          int t = d.tile0 + ty * d.tw + tx;
-          nb[t] = make_int4(ty > 0 ? t - d.tw : -1, ty < d.th - 1 ? t + d.tw : -1,
-                            tx > 0 ? t - 1 : -1, tx < d.tw - 1 ? t + 1 : -1);
-        }
+    h_sel = static_cast<char*>(pin) + acc_end;
     // every buffer starts at zero; the look-back tag starts at 1
     CK(cudaMemset(arena, 0, arena_bytes));
-    CK(cudaMemcpy(P.nbr, nb.data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
+    if (!dynamic) {   // a session pool sets its tiles up as images open
+      std::vector<int4> nb(nt);
+      for (const auto& d : imgs)
+        for (int ty = 0; ty < d.th; ++ty)
+          for (int tx = 0; tx < d.tw; ++tx) {
+            int t = d.tile0 + ty * d.tw + tx;
+            nb[t] = make_int4(ty > 0 ? t - d.tw : -1, ty < d.th - 1 ? t + d.tw : -1,
+                              tx > 0 ? t - 1 : -1, tx < d.tw - 1 ? t + 1 : -1);
+          }
+      CK(cudaMemcpy(P.nbr, nb.data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
+    }
     const uint32_t one = 1;
     CK(cudaMemcpy(scan.st.seq, &one, sizeof(one), cudaMemcpyHostToDevice));
     // These clears were issued on the legacy default stream, which non-blocking streams
@@ -383,11 +433,7 @@ struct Pool {
     CK(cudaMemsetAsync(acc + i, 0, sizeof(ImageAcc), s));
     P.ktiles = nullptr;
     RK(timed(K_UPLOAD, s, [&] { return launch_upload(P, imgs[i], i, up, down, left, right, excess, tl, acc, s); }));
-    uploaded = true;
-    solved = false;
-    edited = false;
-    list_valid = false;
-    bfs_fresh = false;
+    uploaded_image(i);
     return GC_OK;
   }
 
@@ -412,12 +458,61 @@ struct Pool {
     RK(timed(K_UPLOAD, s, [&] {
       return launch_upload_rgba(P, im, i, rgba, excess, lambda ? nullptr : ntab, lambda, tl, acc, s);
     }));
+    uploaded_image(i);
+    return GC_OK;
+  }
+
+  void uploaded_image(int i) {
+    img_up[i] = 1;
+    img_solved[i] = 0;
+    img_edited[i] = 0;
     uploaded = true;
     solved = false;
     edited = false;
     list_valid = false;
     bfs_fresh = false;
+  }
+
+  void edited_image(int i) {
+    img_edited[i] = 1;
+    img_solved[i] = 0;
+    edited = true;
+    bfs_fresh = false;
+  }
+
+  // Writes the selection of a solve (the listed images, in order) to the pinned mirror and
+  // queues its copy to the device.  An image is fresh (mode 1: trivial labelling, no flood
+  // before its first pulses) right after its upload, else it continues from its previous
+  // flow (mode 2); initial_relabel makes every image mode 2.  *any_warm: some image is mode 2.
+  int set_selection(const int* idx, int n, bool* any_warm, cudaStream_t s) {
+    int32_t* cnt = reinterpret_cast<int32_t*>(h_sel);
+    int4* rng = reinterpret_cast<int4*>(h_sel + 16);
+    int32_t* mode = reinterpret_cast<int32_t*>(rng + imgs.size());
+    long long start = 0;
+    bool warm = false;
+    for (int k = 0; k < n; ++k) {
+      const int i = idx[k];
+      const ImageDesc& im = imgs[i];
+      const int tiles = im.tw * im.th;
+      rng[k] = make_int4(im.tile0, tiles, (int)start, i);
+      mode[k] = (opts.initial_relabel || img_solved[i] || img_edited[i]) ? 2 : 1;
+      warm |= mode[k] == 2;
+      start += tiles;
+    }
+    if (start > nt) return fail(GC_ERR_INTERNAL, "selection larger than the pool");
+    cnt[0] = n;
+    cnt[1] = (int)start;
+    *any_warm = warm;
+    // one copy: counts, the n ranges, then (at their fixed place) the modes
+    CK(cudaMemcpyAsync(d_sel, h_sel, 16 + sizeof(int4) * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(P.sel_mode, mode, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
     return GC_OK;
+  }
+
+  int select_all(bool* any_warm, cudaStream_t s) {
+    std::vector<int> all(imgs.size());
+    for (size_t i = 0; i < imgs.size(); ++i) all[i] = (int)i;
+    return set_selection(all.data(), (int)all.size(), any_warm, s);
   }
 
   // exact BFS distances to the sink pixels (global relabel); sets tact.  h: condition
@@ -477,41 +572,60 @@ struct Pool {
     return GC_OK;
   }
 
+  // Solves every image of a fixed pool.
   int solve(cudaStream_t s) {
-    if (!uploaded) return fail(GC_ERR_STATE, "solve before upload");
+    std::vector<int> all(imgs.size());
+    for (size_t i = 0; i < imgs.size(); ++i) all[i] = (int)i;
+    return solve_images(all.data(), (int)all.size(), s);
+  }
+
+  // Solves the listed images together (distinct, uploaded); the pool's other images keep
+  // their state and results.
+  int solve_images(const int* idx, int n, cudaStream_t s) {
+    if (n < 1 || !idx) return fail(GC_ERR_INVALID, "no images to solve");
+    std::vector<uint8_t> seen(imgs.size(), 0);
+    for (int k = 0; k < n; ++k) {
+      const int i = idx[k];
+      if (i < 0 || i >= (int)imgs.size() || seen[i]) return fail(GC_ERR_INVALID, "bad image list");
+      if (!img_up[i]) return fail(GC_ERR_STATE, "solve before upload");
+      seen[i] = 1;
+    }
     CK(cudaSetDevice(device));
     stats = gc_stats{};
-    const bool relabel_first = opts.initial_relabel || edited || solved;
-    int r = (prof || collect || !use_graph) ? solve_host(s, relabel_first) : solve_graph(s, relabel_first);
+    bool warm = false;
+    RK(set_selection(idx, n, &warm, s));
+    int r = (prof || collect || !use_graph) ? solve_host(s, warm) : solve_graph(s, warm);
     if (r) return r;
-    return finish_check(s);
+    RK(finish_check(s, idx, n));
+    for (int k = 0; k < n; ++k) {
+      img_solved[idx[k]] = 1;
+      img_edited[idx[k]] = 0;
+    }
+    return GC_OK;
   }
 
   // Host-driven solve (profiling, stats collection): same kernels, host decides the loops.
   //
-  // The solve (both paths): a solve that starts from a previous flow (relabel_first) floods
-  // every image first and relabels the images whose flood reaches a sink pixel; a fresh
-  // upload starts from the trivial labelling.  Then, while tiles are active: pulses of
-  // discharge, a mask rebuild, the flood of the live images with its termination check, and
-  // for the images that are not solved a global relabel and the next active-tile list.  The
-  // last flood of every image is its canonical cut, so no separate flood phase follows.
-  int solve_host(cudaStream_t s, bool relabel_first) {
+  // The solve (both paths) over the selected images: the images that continue from a
+  // previous flow (warm) are flooded first, and those whose flood reaches a sink pixel get a
+  // global relabel; freshly uploaded images start from the trivial labelling.  Then, while
+  // tiles are active: pulses of discharge, a mask rebuild, the flood of the live images with
+  // its termination check, and for the images that are not solved a global relabel and the
+  // next active-tile list.  The last flood of every image is its canonical cut, so no
+  // separate flood phase follows.
+  int solve_host(cudaStream_t s, bool warm) {
     RK(prof_begin(s));
     RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, s));
     int n = 0;
-    if (relabel_first) {
-      RK(flood_phase(s, /*mode=*/1));
+    if (warm) {
+      RK(timed(K_MASKS, s, [&] { return launch_masks(P, grid_warps, s); }));
+      RK(flood_phase(s, /*mode=*/3));
       RK(timed(K_COMPACT, s, [&] { return launch_flood_check(P, 1, 0, 0, s); }));
       RK(read_ctl(s));
-      if (h_ctl[CTL_LEFT] > 0) {
-        RK(bfs_phase(s));
-        RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 0, 0, 1, 0, acc, s); }));
-        RK(read_count(s, &n));
-      }
-    } else {
-      RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 0, 0, 0, 0, acc, s); }));
-      RK(read_count(s, &n));
+      if (h_ctl[CTL_LEFT] > 0) RK(bfs_phase(s));
     }
+    RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 0, 0, 2, 0, acc, s); }));
+    RK(read_count(s, &n));
     for (int cycle = 0; n > 0; ++cycle) {
       if (cycle >= opts.max_cycles) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
       stats.cycles++;
@@ -613,7 +727,7 @@ struct Pool {
   }
 
   // Appends to g: flood first round (mode) + WHILE(frontier rounds) + the check, then
-  // IF(images left) { global relabel + active list (bump, count_cycle) }.
+  // IF(images left) { global relabel [+ active list (bump = count_cycle = 1), in the loop] }.
   int graph_cycle_tail(cudaGraph_t g, std::vector<cudaGraphNode_t>& L, int mode, int all,
                        int bump, cudaGraphConditionalHandle hmain) {
     cudaGraphConditionalHandle hf, hbfs, hb;
@@ -626,7 +740,7 @@ struct Pool {
       std::vector<cudaGraphNode_t> Lf;
       RK(capture(bf, Lf, [&](cudaStream_t cs) { return launch_flood_round(P, 0, 1, hf, acc, grid_warps, cs); }));
     }
-    RK(capture(g, L, [&](cudaStream_t cs) { return launch_flood_check(P, all, hbfs, hmain, cs); }));
+    RK(capture(g, L, [&](cudaStream_t cs) { return launch_flood_check(P, all, hbfs, all ? 0 : hmain, cs); }));
     cudaGraph_t bi;
     RK(add_if(g, L, hbfs, &bi));
     std::vector<cudaGraphNode_t> Li;
@@ -638,8 +752,9 @@ struct Pool {
       std::vector<cudaGraphNode_t> Lb;
       RK(capture(bb, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, hb, grid_warps, cs); }));
     }
+    if (!bump) return GC_OK;   // the first list of a solve follows the IF node
     return capture(bi, Li, [&](cudaStream_t cs) {
-      return launch_active_list(P, scan.st, list, counts, bump, bump, 1, hmain, acc, cs);
+      return launch_active_list(P, scan.st, list, counts, 1, 1, 1, hmain, acc, cs);
     });
   }
 
@@ -657,14 +772,13 @@ struct Pool {
     RK(cond_handle(&hmain, g));
     RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs); }));
     if (variant) {
-      // from a previous flow: flood every image; relabel the ones that are not solved
+      // images that continue from a previous flow: flood them; relabel the ones not solved
       RK(capture(g, L, [&](cudaStream_t cs) { return launch_masks(P, grid_warps, cs); }));
-      RK(graph_cycle_tail(g, L, /*mode=*/1, /*all=*/1, /*bump=*/0, hmain));
-    } else {
-      RK(capture(g, L, [&](cudaStream_t cs) {
-        return launch_active_list(P, scan.st, list, counts, 0, 0, 0, hmain, acc, cs);
-      }));
+      RK(graph_cycle_tail(g, L, /*mode=*/3, /*all=*/1, /*bump=*/0, hmain));
     }
+    RK(capture(g, L, [&](cudaStream_t cs) {   // the first active list (fresh and live images)
+      return launch_active_list(P, scan.st, list, counts, 0, 0, 2, hmain, acc, cs);
+    }));
     cudaGraph_t bm;
     RK(add_while(g, L, hmain, &bm));
     {
@@ -686,8 +800,9 @@ struct Pool {
     return GC_OK;
   }
 
-  int solve_graph(cudaStream_t s, bool relabel_first) {
-    const int v = relabel_first ? 1 : 0;
+  // variant 1: some selected image continues from a previous flow (the graph floods first)
+  int solve_graph(cudaStream_t s, bool warm) {
+    const int v = warm ? 1 : 0;
     if (!gexec[v]) {
       const int r = build_graph(v);
       if (r) {
@@ -715,7 +830,7 @@ struct Pool {
   }
 
   // errors and results common to both paths (h_acc / h_ctl are filled and synchronised)
-  int finish_check(cudaStream_t s) {
+  int finish_check(cudaStream_t s, const int* idx = nullptr, int n = 0) {
     RK(check_device_error(s));
     if (h_ctl[CTL_ERR] == 1) return fail(GC_ERR_NOT_CONVERGED, "BFS round cap reached");
     if (h_ctl[CTL_ERR] == 2) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
@@ -726,8 +841,8 @@ struct Pool {
                h_ctl[CTL_BAD], h_ctl[CTL_BADWHERE]);
       return fail(GC_ERR_INTERNAL, msg);
     }
-    for (size_t i = 0; i < imgs.size(); ++i)
-      if (h_acc[i].bad_caps) return fail(GC_ERR_INVALID, "negative capacity in the upload");
+    for (int k = 0; k < (idx ? n : (int)imgs.size()); ++k)
+      if (h_acc[idx ? idx[k] : k].bad_caps) return fail(GC_ERR_INVALID, "negative capacity in the upload");
     stats.bfs_rounds = h_ctl[CTL_BFS_TOTAL];
     stats.flood_rounds = h_ctl[CTL_FLOOD_TOTAL];
     if (stats.launches < 0) {  // graph solve: count the kernel nodes that ran
@@ -737,6 +852,10 @@ struct Pool {
       // lists and every BFS / flood round
       stats.launches = 1 + stats.pulses + 2LL * h_ctl[CTL_NCHECK] + h_ctl[CTL_NACT] +
                        stats.bfs_rounds + stats.flood_rounds;
+    }
+    for (int k = 0; k < (idx ? n : (int)imgs.size()); ++k) {
+      img_solved[idx ? idx[k] : k] = 1;
+      img_edited[idx ? idx[k] : k] = 0;
     }
     solved = true;
     edited = false;
@@ -753,6 +872,8 @@ struct Pool {
     }
     solved = false;
     bfs_fresh = false;
+    img_solved.assign(imgs.size(), 0);
+    img_edited.assign(imgs.size(), 1);   // the next solve starts by flooding
     return launch_discharge(P, opts.discharge_iters, grid_dis, s);
   }
   int step_relabel(cudaStream_t s) {
@@ -760,11 +881,15 @@ struct Pool {
     solved = false;
     bfs_fresh = false;
     list_valid = true;
+    img_solved.assign(imgs.size(), 0);
+    img_edited.assign(imgs.size(), 1);
     RK(launch_edge_relabel_build(P, list, counts, scan.st, s));
     return launch_ctl_cycle(P, counts, 0, 0, s);
   }
   int step_start_bfs(cudaStream_t s) {
     if (!uploaded) return fail(GC_ERR_STATE, "startBfs before upload");
+    bool warm;
+    RK(select_all(&warm, s));
     RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, s));
     RK(global_relabel(s));
     RK(compact(P.tact, nullptr, s));
@@ -790,22 +915,22 @@ struct Pool {
   }
 
   int flow(int i, int64_t* out) {
-    if (!solved) return fail(GC_ERR_STATE, "flow before solve");
     if (i < 0 || i >= (int)imgs.size() || !out) return fail(GC_ERR_INVALID, "bad argument");
+    if (!img_solved[i]) return fail(GC_ERR_STATE, "flow before solve");
     *out = (int64_t)(h_acc[i].sumpos_t - h_acc[i].sumpos_e);
     return GC_OK;
   }
 
   int labels(int i, uint8_t* out, cudaStream_t s) {
-    if (!solved) return fail(GC_ERR_STATE, "labels before solve");
     if (i < 0 || i >= (int)imgs.size() || !out) return fail(GC_ERR_INVALID, "bad argument");
+    if (!img_solved[i]) return fail(GC_ERR_STATE, "labels before solve");
     CK(cudaSetDevice(device));
     return timed(K_LABELS, s, [&] { return launch_labels_out(P, imgs[i], out, s); });
   }
 
   int labels_packed(int i, uint8_t* out, cudaStream_t s) {
-    if (!solved) return fail(GC_ERR_STATE, "labels before solve");
     if (i < 0 || i >= (int)imgs.size() || !out) return fail(GC_ERR_INVALID, "bad argument");
+    if (!img_solved[i]) return fail(GC_ERR_STATE, "labels before solve");
     CK(cudaSetDevice(device));
     return timed(K_LABELS, s, [&] { return launch_labels_packed(P, imgs[i], out, s); });
   }
@@ -817,6 +942,11 @@ struct gc_handle {
 
 struct gcb_handle {
   Pool pool;
+};
+
+struct gcp_handle {
+  Pool pool;
+  std::vector<uint8_t> open;   // slot is open
 };
 
 // ------------------------------------------------------------------------------------
@@ -1166,8 +1296,7 @@ int gc_edit_tlinks(gc_handle* h, const int32_t* idx, const int32_t* value, int n
   CK(cudaSetDevice(p.device));
   RK(launch_edit(p.P, p.imgs[0], 0, idx, value, n, p.tl, p.acc, (cudaStream_t)stream));
   p.track((cudaStream_t)stream);
-  p.edited = true;
-  p.bfs_fresh = false;
+  p.edited_image(0);
   return GC_OK;
 }
 
@@ -1186,8 +1315,7 @@ int gc_edit_stroke(gc_handle* h, const int32_t* xs, const int32_t* ys, int npts,
   RK(launch_stroke(p.P, p.imgs[0], 0, p.pts, pts.data(), npts, radius, value, p.tl, p.acc, s));
   p.track(s);
   CK(cudaStreamSynchronize(s));  // pts (host vector) must outlive the copy
-  p.edited = true;
-  p.bfs_fresh = false;
+  p.edited_image(0);
   return GC_OK;
 }
 
@@ -1206,8 +1334,7 @@ int gc_edit_brush(gc_handle* h, const int32_t* xs, const int32_t* ys, int npts, 
   RK(launch_brush(p.P, p.imgs[0], 0, p.pts, pts.data(), npts, radius, value, p.tl, p.acc, s));
   p.track(s);
   CK(cudaStreamSynchronize(s));  // pts (host vector) must outlive the copy
-  p.edited = true;
-  p.bfs_fresh = false;
+  p.edited_image(0);
   return GC_OK;
 }
 
@@ -1493,6 +1620,179 @@ int gcb_get_profile(const gcb_handle* b, gc_kernel_prof* out, int n) {
 int gcb_get_stats(const gcb_handle* b, gc_stats* st) {
   if (!b || !st) return fail(GC_ERR_INVALID, "null argument");
   *st = b->pool.stats;
+  return GC_OK;
+}
+
+// ---- session pools -----------------------------------------------------------------
+int gcp_arena_bytes(int max_tiles, int max_sessions, int64_t* bytes) {
+  g_err.clear();
+  if (!bytes) return fail(GC_ERR_INVALID, "null out");
+  Pool p;
+  RK(p.describe_dynamic(max_tiles, max_sessions));
+  *bytes = (int64_t)p.arena_bytes;
+  return GC_OK;
+}
+
+static int gcp_make(int max_tiles, int max_sessions, const gc_opts* opts, void* arena,
+                    int64_t bytes, gcp_handle** out) {
+  g_err.clear();
+  if (!out) return fail(GC_ERR_INVALID, "null out");
+  *out = nullptr;
+  gc_opts o;
+  if (opts) o = *opts; else gc_opts_default(&o);
+  RK(check_opts(&o));
+  gcp_handle* h = new (std::nothrow) gcp_handle();
+  if (!h) return fail(GC_ERR_OOM, "host allocation");
+  int r = h->pool.create_dynamic(max_tiles, max_sessions, &o, arena, (size_t)bytes);
+  if (r) { delete h; return r; }
+  h->open.assign(max_sessions, 0);
+  *out = h;
+  return GC_OK;
+}
+
+int gcp_create(int max_tiles, int max_sessions, const gc_opts* opts, gcp_handle** out) {
+  return gcp_make(max_tiles, max_sessions, opts, nullptr, 0, out);
+}
+
+int gcp_create_in(int max_tiles, int max_sessions, const gc_opts* opts, void* arena,
+                  int64_t bytes, gcp_handle** out) {
+  if (!arena || bytes <= 0) return fail(GC_ERR_INVALID, "null arena");
+  return gcp_make(max_tiles, max_sessions, opts, arena, bytes, out);
+}
+
+int gcp_destroy(gcp_handle* p) {
+  if (!p) return GC_OK;
+  cudaSetDevice(p->pool.device);
+  delete p;
+  return GC_OK;
+}
+
+static int gcp_slot(gcp_handle* p, int slot, bool must_be_open) {
+  if (!p) return fail(GC_ERR_INVALID, "null handle");
+  if (slot < 0 || slot >= (int)p->open.size()) return fail(GC_ERR_INVALID, "slot out of range");
+  if (must_be_open && !p->open[slot]) return fail(GC_ERR_STATE, "slot not open");
+  return GC_OK;
+}
+
+int gcp_open(gcp_handle* p, int slot, int width, int height, int tile0, void* stream) {
+  g_err.clear();
+  RK(gcp_slot(p, slot, false));
+  if (p->open[slot]) return fail(GC_ERR_STATE, "slot already open");
+  if (width < 1 || height < 1 || width > (1 << 16) || height > (1 << 16))
+    return fail(GC_ERR_INVALID, "image size out of range");
+  Pool& pool = p->pool;
+  const ImageDesc d{width, height, (width + 31) / 32, (height + 31) / 32, tile0};
+  const long long tiles = (long long)d.tw * d.th;
+  if (tile0 < 0 || tile0 + tiles > pool.nt) return fail(GC_ERR_INVALID, "tile range outside the pool");
+  for (size_t k = 0; k < p->open.size(); ++k) {   // no two open slots share a tile
+    if (!p->open[k]) continue;
+    const ImageDesc& o = pool.imgs[k];
+    const long long a0 = o.tile0, a1 = o.tile0 + (long long)o.tw * o.th;
+    if (tile0 < a1 && a0 < tile0 + tiles) return fail(GC_ERR_INVALID, "tile range overlaps an open slot");
+  }
+  CK(cudaSetDevice(pool.device));
+  pool.imgs[slot] = d;
+  RK(launch_image_tiles(pool.P, d, slot, (cudaStream_t)stream));
+  pool.img_up[slot] = pool.img_solved[slot] = pool.img_edited[slot] = 0;
+  p->open[slot] = 1;
+  pool.track((cudaStream_t)stream);
+  return GC_OK;
+}
+
+int gcp_close(gcp_handle* p, int slot) {
+  g_err.clear();
+  RK(gcp_slot(p, slot, true));
+  p->open[slot] = 0;
+  p->pool.img_up[slot] = p->pool.img_solved[slot] = 0;
+  return GC_OK;
+}
+
+int gcp_upload(gcp_handle* p, int slot, const int32_t* up, const int32_t* down,
+               const int32_t* left, const int32_t* right, const int32_t* excess, void* stream) {
+  g_err.clear();
+  RK(gcp_slot(p, slot, true));
+  const int r = p->pool.upload(slot, up, down, left, right, excess, (cudaStream_t)stream);
+  p->pool.track((cudaStream_t)stream);
+  return r;
+}
+
+int gcp_upload_rgba(gcp_handle* p, int slot, const uint32_t* rgba, const int32_t* excess,
+                    void* stream) {
+  g_err.clear();
+  RK(gcp_slot(p, slot, true));
+  const int r = p->pool.upload_rgba(slot, rgba, excess, 0, (cudaStream_t)stream);
+  p->pool.track((cudaStream_t)stream);
+  return r;
+}
+
+static int gcp_edit(gcp_handle* p, int slot, const int32_t* xs, const int32_t* ys, int npts,
+                    int radius, int32_t value, bool brush, void* stream) {
+  g_err.clear();
+  RK(gcp_slot(p, slot, true));
+  if (!xs || !ys || npts < 1 || npts > 1024 || radius > (brush ? 1024 : 4096) ||
+      (!brush && radius < 0))
+    return fail(GC_ERR_INVALID, "bad stroke");
+  Pool& pool = p->pool;
+  if (!pool.img_up[slot]) return fail(GC_ERR_STATE, "edit before upload");
+  CK(cudaSetDevice(pool.device));
+  std::vector<int32_t> pts(2 * npts);
+  for (int k = 0; k < npts; ++k) { pts[2 * k] = xs[k]; pts[2 * k + 1] = ys[k]; }
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemcpyAsync(pool.pts, pts.data(), pts.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  if (brush)
+    RK(launch_brush(pool.P, pool.imgs[slot], slot, pool.pts, pts.data(), npts, radius, value, pool.tl, pool.acc, s));
+  else
+    RK(launch_stroke(pool.P, pool.imgs[slot], slot, pool.pts, pts.data(), npts, radius, value, pool.tl, pool.acc, s));
+  pool.track(s);
+  CK(cudaStreamSynchronize(s));  // pts (host vector) must outlive the copy
+  pool.edited_image(slot);
+  return GC_OK;
+}
+
+int gcp_edit_stroke(gcp_handle* p, int slot, const int32_t* xs, const int32_t* ys, int npts,
+                    int radius, int32_t value, void* stream) {
+  return gcp_edit(p, slot, xs, ys, npts, radius, value, false, stream);
+}
+
+int gcp_edit_brush(gcp_handle* p, int slot, const int32_t* xs, const int32_t* ys, int npts,
+                   int radius, int32_t value, void* stream) {
+  return gcp_edit(p, slot, xs, ys, npts, radius, value, true, stream);
+}
+
+int gcp_solve(gcp_handle* p, const int* slots, int n, void* stream) {
+  g_err.clear();
+  if (!p || !slots || n < 1) return fail(GC_ERR_INVALID, "bad argument");
+  for (int k = 0; k < n; ++k) RK(gcp_slot(p, slots[k], true));
+  const int r = p->pool.solve_images(slots, n, (cudaStream_t)stream);
+  p->pool.track((cudaStream_t)stream);
+  return r;
+}
+
+int gcp_flow(gcp_handle* p, int slot, int64_t* flow) {
+  g_err.clear();
+  RK(gcp_slot(p, slot, true));
+  return p->pool.flow(slot, flow);
+}
+
+int gcp_labels(gcp_handle* p, int slot, uint8_t* labels, void* stream) {
+  g_err.clear();
+  RK(gcp_slot(p, slot, true));
+  const int r = p->pool.labels(slot, labels, (cudaStream_t)stream);
+  p->pool.track((cudaStream_t)stream);
+  return r;
+}
+
+int gcp_labels_packed(gcp_handle* p, int slot, uint8_t* bits, void* stream) {
+  g_err.clear();
+  RK(gcp_slot(p, slot, true));
+  const int r = p->pool.labels_packed(slot, bits, (cudaStream_t)stream);
+  p->pool.track((cudaStream_t)stream);
+  return r;
+}
+
+int gcp_get_stats(const gcp_handle* p, gc_stats* st) {
+  if (!p || !st) return fail(GC_ERR_INVALID, "null argument");
+  *st = p->pool.stats;
   return GC_OK;
 }
 

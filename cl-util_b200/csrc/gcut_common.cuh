@@ -54,6 +54,13 @@ struct PoolView {
   int nimg;               // images in the pool
   int32_t* img_live;      // [nimg] cycle stamp of images that still have active tiles
   int32_t* img_hit;       // [nimg] cycle stamp: the image's flood reached a sink pixel
+  int32_t* img_mode;      // [nimg] the image's part in this solve: 0 none, 1 fresh upload
+                          // (trivial labelling), 2 continues from its previous flow
+  // The solve's selection: the tile ranges of the images it solves (first rounds and
+  // active-tile lists walk these instead of the whole pool)
+  int4* sel;              // [nimg] first tile, tiles, first selected index, image
+  int32_t* sel_mode;      // [nimg] img_mode of the range's image
+  int32_t* nsel;          // [2] ranges, selected tiles in all
   unsigned long long* ktiles;  // [K_COUNT] tiles processed per kernel kind (profiling)
 };
 
@@ -81,7 +88,31 @@ enum CtlSlot {
   CTL_NCHECK = 15,    // flood checks run (k_flood_check launches)
   CTL_NACT = 16,      // active-list rebuilds run (k_active_list launches)
   CTL_LEFT = 17,      // images still running after the last flood check
+  CTL_DTICKET = 18,   // next worklist position a discharge CTA takes (dynamic fetch)
   CTL_N = 64          // the control words fill 256 bytes; the per-image sums follow them
+};
+
+// Walks consecutive selected indices: the tile of index i, with the range found once by a
+// binary search over the ranges' first indices and then followed range by range.
+struct SelCursor {
+  const int4* sel;
+  int nr, k;
+  int4 cur;
+  __device__ __forceinline__ SelCursor(const PoolView& P, int nranges, int i) : sel(P.sel), nr(nranges) {
+    int lo = 0, hi = nr - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sel[mid].z <= i) lo = mid; else hi = mid - 1;
+    }
+    k = lo;
+    cur = nr > 0 ? sel[k] : make_int4(0, 0, 0, 0);
+  }
+  // tile of selected index i (i >= the previous index asked for)
+  __device__ __forceinline__ int tile(int i) {
+    while (i >= cur.z + cur.y && k + 1 < nr) cur = sel[++k];
+    return cur.x + (i - cur.z);
+  }
+  __device__ __forceinline__ int image() const { return cur.w; }
 };
 
 // A self-check found a worklist value outside the pool: keep the first one, flag the solve

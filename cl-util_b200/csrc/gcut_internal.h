@@ -91,13 +91,16 @@ int launch_flood_check(const PoolView& P, int all, cudaGraphConditionalHandle hb
                        cudaGraphConditionalHandle hmain, cudaStream_t s);
 int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc* acc,
                      cudaStream_t s);
-// filter_live: only tiles of the images a flood check kept (img_live == the cycle stamp)
+// over the solve's selected tiles; filter 1: only tiles of the images a flood check kept
+// (img_live == the cycle stamp), 2: those and the tiles of freshly uploaded images
 int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, int32_t* count,
-                       int bump, int count_cycle, int filter_live, cudaGraphConditionalHandle h,
+                       int bump, int count_cycle, int filter, cudaGraphConditionalHandle h,
                        ImageAcc* acc, cudaStream_t s);
 int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s);
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s);
+// neighbour ids and image index of the tiles of image img (a session-pool slot)
+int launch_image_tiles(const PoolView& P, const ImageDesc& im, int img, cudaStream_t s);
 int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s);
 int launch_labels_packed(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s);
 int launch_state_out(const PoolView& P, const ImageDesc& im, const int32_t* plane,

@@ -345,24 +345,35 @@ k_masks(PoolView P) {
 // ------------------------------------------------------------------------------------
 // Discharge.  Thread (r, q) owns pixels (r, 4q .. 4q+3) of the tile.
 //
-// Every pixel pushes along all admissible edges and relabels, tile-edge pixels included,
-// but a tile-edge pixel rises by at most 2 above its height at the start of the launch.
-// A neighbouring CTA that pushes into an edge pixel v saw either v's start height or its
-// final height; with h_final(v) <= h_start(v) + 2 every such push leaves a valid labelling
-// (h(v) <= h(u) + 1 on the new residual edge v -> u), and pushes out of the tile read the
-// neighbour's height under the same bound.  Flow leaving the tile is added to the
-// neighbour's excess and reverse residual with atomics at the end of the tile.
+// A sweep is: take the flow the other threads pushed into my pixels in the previous sweep,
+// push along every admissible edge (heights as they were at the start of the sweep), let
+// the flow between my own four pixels land at once, relabel (Jacobi), publish my pushes and
+// heights.  One barrier per sweep: the exchange arrays are double-buffered by sweep parity,
+// so a sweep writes one half while its neighbours may still read the other.  A pixel learns
+// of the flow other threads pushed into it only in the next sweep, so its relabel in this
+// sweep may not see the residual edges that flow created; a rise of at most 2 per sweep
+// keeps the labelling valid all the same (a neighbour u pushed into v only if h(u) =
+// h_start(v) + 1, so h(v) <= h_start(v) + 2 = h(u) + 1 on the new edge v -> u).
+//
+// Every pixel pushes and relabels, tile-edge pixels included, but a tile-edge pixel rises by
+// at most 2 above its height at the start of the launch.  A neighbouring CTA that pushes
+// into an edge pixel v saw either v's start height or its final height; with h_final(v) <=
+// h_start(v) + 2 every such push leaves a valid labelling (h(v) <= h(u) + 1 on the new
+// residual edge v -> u), and pushes out of the tile read the neighbour's height under the
+// same bound.  Flow leaving the tile is added to the neighbour's excess and reverse residual
+// with atomics at the end of the tile.
 //
 // Active tiles form a worklist: the launch reads queue[c] (c = pulse parity, device-side)
 // and appends, deduplicated by inq[c ^ 1], every tile that is still active or received flow
-// to queue[c ^ 1]; the last CTA advances the parity.  One launch per pulse, no compaction.
+// to queue[c ^ 1]; the last CTA advances the parity.  CTAs take list positions from a
+// counter as they finish tiles, so the work spreads evenly.  One launch per pulse.
 // ------------------------------------------------------------------------------------
 struct DisSmem {
-  int32_t hs[GC_TILE_PX];   // heights
-  int32_t fu[GC_TILE_PX];   // flow pushed up by each pixel this round
-  int32_t fd[GC_TILE_PX];   // flow pushed down
-  int32_t fl[GC_TILE * 8];  // flow pushed left by the first pixel of each 4-pixel strip
-  int32_t fr[GC_TILE * 8];  // flow pushed right by the last pixel of each strip
+  int32_t hs[2][GC_TILE_PX];   // heights published by a sweep, by sweep parity
+  int32_t fu[2][GC_TILE_PX];   // flow pushed up by each pixel in a sweep
+  int32_t fd[2][GC_TILE_PX];   // flow pushed down
+  int32_t fl[2][GC_TILE * 8];  // flow pushed left by the first pixel of each 4-pixel strip
+  int32_t fr[2][GC_TILE * 8];  // flow pushed right by the last pixel of each strip
   int32_t hu[GC_TILE], hd[GC_TILE], hl[GC_TILE], hr[GC_TILE];  // halo heights
   // launch-start values of the tile-edge pixels that also receive atomics from the
   // neighbouring tiles (written back as deltas against these)
@@ -370,6 +381,7 @@ struct DisSmem {
   int32_t cu_top[GC_TILE], cd_bot[GC_TILE], cl_left[GC_TILE], cr_right[GC_TILE];
   // flow leaving the tile, per edge pixel, delivered at the end of the tile
   int32_t xu[GC_TILE], xd[GC_TILE], xl[GC_TILE], xr[GC_TILE];
+  int32_t next;                // the list position of the CTA's next tile
 };
 
 __device__ __forceinline__ void worklist_add(const PoolView& P, int nxt, int t) {
@@ -449,18 +461,35 @@ __device__ __forceinline__ void dis_prefetch(const PoolView& P, int t, int32_t* 
     bulk_g2s(buf + k * GC_TILE_PX, dis_plane(P, k) + (long long)t * GC_TILE_PX, GC_TILE_PX * 4, mbar);
 }
 
+// Takes the flow the neighbouring threads pushed into my pixels in a sweep (from the half
+// `b` of the exchange arrays): excess rises, and each receiving pixel gains the reverse
+// residual of the edge the flow came over.
+__device__ __forceinline__ void dis_gather(const DisSmem& S, int b, int r, int q, int pix,
+                                           int (&e)[4], int (&cu)[4], int (&cd)[4],
+                                           int (&cl)[4], int (&cr)[4]) {
+  const int4 a = r < 31 ? lds4(S.fu[b] + pix + GC_TILE) : make_int4(0, 0, 0, 0);   // from below
+  const int4 d = r > 0 ? lds4(S.fd[b] + pix - GC_TILE) : make_int4(0, 0, 0, 0);    // from above
+  const int fin_l = q > 0 ? S.fr[b][r * 8 + q - 1] : 0;   // from the strip on the left
+  const int fin_r = q < 7 ? S.fl[b][r * 8 + q + 1] : 0;   // from the strip on the right
+  e[0] += a.x + d.x + fin_l; cd[0] += a.x; cu[0] += d.x; cl[0] += fin_l;
+  e[1] += a.y + d.y;         cd[1] += a.y; cu[1] += d.y;
+  e[2] += a.z + d.z;         cd[2] += a.z; cu[2] += d.z;
+  e[3] += a.w + d.w + fin_r; cd[3] += a.w; cu[3] += d.w; cr[3] += fin_r;
+}
+
 __global__ void __launch_bounds__(DIS_THREADS, 4)
 k_discharge(PoolView P, int iters) {
   extern __shared__ __align__(128) int32_t dsm[];
   int32_t* const buf = dsm;                                    // [6][1024] staging
   DisSmem& S = *reinterpret_cast<DisSmem*>(dsm + DIS_PLANES * GC_TILE_PX);
   __shared__ uint64_t mbar;
-  __shared__ int s_cur, s_n;
+  __shared__ int s_cur, s_n, s_li;
   const int tid = threadIdx.x;
   const int r = tid >> 3, q = tid & 7, c0 = q * 4;
   if (tid == 0) {
     s_cur = *((volatile int32_t*)&P.ctl[CTL_PULSE]) & 1;
     s_n = *((volatile int32_t*)&P.qcount[s_cur]);
+    s_li = atomicAdd(&P.ctl[CTL_DTICKET], 1);
     mbar_init(&mbar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -476,10 +505,12 @@ k_discharge(PoolView P, int iters) {
   auto entry = [&](int li) { return P.queue[cur][li]; };
   const bool erow = (r == 0) || (r == 31);
   const int pix = r * GC_TILE + c0;
+  const int sq = r * 8 + q;
   unsigned phase = 0;
   bool failed = false, pending = false;
-  if (tid == 0 && (int)blockIdx.x < n) dis_prefetch(P, entry(blockIdx.x), buf, &mbar);
-  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+  int li = s_li;
+  if (tid == 0 && li < n) dis_prefetch(P, entry(li), buf, &mbar);
+  while (li < n) {
     const int t = entry(li);
     const int4 nb = P.nbr[t];
     if (tid < 32) S.hu[tid] = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + tid] : GC_HINF;
@@ -490,7 +521,10 @@ k_discharge(PoolView P, int iters) {
     else if (tid < 192) S.xd[tid - 160] = 0;
     else if (tid < 224) S.xl[tid - 192] = 0;
     else S.xr[tid - 224] = 0;
-    if (tid == 0) P.inq[cur][t] = 0;
+    if (tid == 0) {
+      P.inq[cur][t] = 0;
+      S.next = atomicAdd(&P.ctl[CTL_DTICKET], 1);
+    }
     const bool ok = mbar_wait(&mbar, phase);
     if (__syncthreads_or(!ok)) { failed = true; pending = true; break; }  // block-uniform
     phase ^= 1u;
@@ -522,22 +556,30 @@ k_discharge(PoolView P, int iters) {
       const bool edge = erow || c == 0 || c == 31;
       hcap[j] = edge ? (h[j] >= GC_HINF - 2 ? GC_HINF : h[j] + 2) : GC_HINF;
     }
-    sts4(S.hs + pix, h[0], h[1], h[2], h[3]);
+    // sweep 0 reads the launch-start heights and no inflow
+    sts4(S.hs[0] + pix, h[0], h[1], h[2], h[3]);
+    sts4(S.fu[0] + pix, 0, 0, 0, 0);
+    sts4(S.fd[0] + pix, 0, 0, 0, 0);
+    S.fl[0][sq] = 0;
+    S.fr[0][sq] = 0;
     __syncthreads();   // every thread has its values in registers: the buffer is free
+    const int nli = S.next;
     // prefetch this CTA's next tile into the buffer while this one is worked on
-    if (tid == 0 && li + (int)gridDim.x < n) dis_prefetch(P, entry(li + gridDim.x), buf, &mbar);
+    if (tid == 0 && nli < n) dis_prefetch(P, entry(nli), buf, &mbar);
 
+    int b = 0;   // the half of the exchange arrays the current sweep reads
     for (int it = 0; it < iters; ++it) {
-      // neighbour heights (fixed during the push phase)
+      dis_gather(S, b, r, q, pix, e, cu, cd, cl, cr);
+      // neighbour heights at the start of the sweep
       int hnu[4], hnd[4], hnl[4], hnr[4];
-      if (r > 0) { const int4 v = lds4(S.hs + pix - GC_TILE); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
+      if (r > 0) { const int4 v = lds4(S.hs[b] + pix - GC_TILE); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
       else { const int4 v = lds4(S.hu + c0); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
-      if (r < 31) { const int4 v = lds4(S.hs + pix + GC_TILE); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
+      if (r < 31) { const int4 v = lds4(S.hs[b] + pix + GC_TILE); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
       else { const int4 v = lds4(S.hd + c0); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
-      hnl[0] = c0 > 0 ? S.hs[pix - 1] : S.hl[r];
+      hnl[0] = c0 > 0 ? S.hs[b][pix - 1] : S.hl[r];
       hnl[1] = h[0]; hnl[2] = h[1]; hnl[3] = h[2];
       hnr[0] = h[1]; hnr[1] = h[2]; hnr[2] = h[3];
-      hnr[3] = c0 < 28 ? S.hs[pix + 4] : S.hr[r];
+      hnr[3] = c0 < 28 ? S.hs[b][pix + 4] : S.hr[r];
 
       // push phase.  `rem` marks pixels that still hold excess after pushing: every
       // admissible edge of theirs is then saturated, and inflow only adds residual towards
@@ -565,6 +607,12 @@ k_discharge(PoolView P, int iters) {
           }
         }
       }
+      // flow between my own pixels lands now, with its reverse residual
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        e[j + 1] += orr[j]; cl[j + 1] += orr[j];
+        e[j] += ol[j + 1]; cr[j] += ol[j + 1];
+      }
       // flow leaving the tile is delivered at the end of the tile
       if (r == 0) {
 #pragma unroll
@@ -576,31 +624,12 @@ k_discharge(PoolView P, int iters) {
       }
       if (q == 0) { S.xl[r] += ol[0]; ol[0] = 0; }
       if (q == 7) { S.xr[r] += orr[3]; orr[3] = 0; }
-      sts4(S.fu + pix, ou[0], ou[1], ou[2], ou[3]);
-      sts4(S.fd + pix, od[0], od[1], od[2], od[3]);
-      S.fl[r * 8 + q] = ol[0];
-      S.fr[r * 8 + q] = orr[3];
-      __syncthreads();
-      // gather inflow; a pixel receiving flow gains the reverse residual
-      {
-        const int4 a = r < 31 ? lds4(S.fu + pix + GC_TILE) : make_int4(0, 0, 0, 0);
-        const int4 bb = r > 0 ? lds4(S.fd + pix - GC_TILE) : make_int4(0, 0, 0, 0);
-        const int fb[4] = {a.x, a.y, a.z, a.w}, fa[4] = {bb.x, bb.y, bb.z, bb.w};
-        int fromleft[4], fromright[4];
-        fromleft[0] = q > 0 ? S.fr[r * 8 + q - 1] : 0;
-        fromleft[1] = orr[0]; fromleft[2] = orr[1]; fromleft[3] = orr[2];
-        fromright[0] = ol[1]; fromright[1] = ol[2]; fromright[2] = ol[3];
-        fromright[3] = q < 7 ? S.fl[r * 8 + q + 1] : 0;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          e[j] += fb[j] + fa[j] + fromleft[j] + fromright[j];
-          cd[j] += fb[j];
-          cu[j] += fa[j];
-          cl[j] += fromleft[j];
-          cr[j] += fromright[j];
-        }
-      }
-      // relabel phase (Jacobi; tile-edge pixels are capped at hcap)
+      sts4(S.fu[b ^ 1] + pix, ou[0], ou[1], ou[2], ou[3]);
+      sts4(S.fd[b ^ 1] + pix, od[0], od[1], od[2], od[3]);
+      S.fl[b ^ 1][sq] = ol[0];
+      S.fr[b ^ 1][sq] = orr[3];
+      // relabel phase (Jacobi on the sweep-start heights; at most +2 per sweep, and
+      // tile-edge pixels at most hcap)
       int nh[4] = {h[0], h[1], h[2], h[3]};
       const bool any_need = (e[0] > 0 && h[0] < hcap[0]) || (e[1] > 0 && h[1] < hcap[1]) ||
                             (e[2] > 0 && h[2] < hcap[2]) || (e[3] > 0 && h[3] < hcap[3]);
@@ -618,19 +647,20 @@ k_discharge(PoolView P, int iters) {
               if (cu[j] > 0) m = imin(m, hnu[j] + 1);
               if (cr[j] > 0) m = imin(m, hnr[j] + 1);
               if (cl[j] > 0) m = imin(m, hnl[j] + 1);
-              nh[j] = imin(imin(m, GC_HINF), hcap[j]);
+              nh[j] = imin(imin(m, hcap[j]), h[j] + 2);
               changed |= nh[j] != h[j];
             }
           }
         }
       }
-      // every read of S.hs in this iteration happened before the flow barrier above, so the
-      // new heights can be written now; the next reads follow the barrier below
 #pragma unroll
       for (int j = 0; j < 4; ++j) h[j] = nh[j];
-      sts4(S.hs + pix, h[0], h[1], h[2], h[3]);
+      sts4(S.hs[b ^ 1] + pix, h[0], h[1], h[2], h[3]);
+      b ^= 1;
       if (!__syncthreads_or(changed)) break;
     }
+    // the flow the last sweep pushed between threads
+    dis_gather(S, b, r, q, pix, e, cu, cd, cl, cr);
 
     // write back: interior values are owned by this CTA; tile-edge excess and the
     // outward residual of edge pixels also receive atomics from neighbouring tiles, so
@@ -731,7 +761,8 @@ k_discharge(PoolView P, int iters) {
     if (sent_d) { P.touched[nb.y] = 1; mark_dirty(P, nb.y); worklist_add(P, nxt, nb.y); }
     if (sent_l) { P.touched[nb.z] = 1; mark_dirty(P, nb.z); worklist_add(P, nxt, nb.z); }
     if (sent_r) { P.touched[nb.w] = 1; mark_dirty(P, nb.w); worklist_add(P, nxt, nb.w); }
-    // the block-wide reductions also order every read of this buffer before its reuse
+    // the block-wide reductions also order every read of this tile's shared memory before
+    // the next tile's writes
     const int any_act = __syncthreads_or(act);
     act_int = __syncthreads_or(act_int);
     if (tid == 0) {
@@ -741,6 +772,7 @@ k_discharge(PoolView P, int iters) {
       if (any_act) worklist_add(P, nxt, t);
       if (P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
     }
+    li = nli;
   }
   if (failed) {
     // a bulk copy did not complete in time: record it, let our copy drain, stop
@@ -759,6 +791,7 @@ k_discharge(PoolView P, int iters) {
       P.qcount[cur] = 0;
       P.ctl[CTL_PULSE] = P.ctl[CTL_PULSE] + 1;
       P.ctl[CTL_DDONE] = 0;
+      P.ctl[CTL_DTICKET] = 0;
       __threadfence();
     }
   }
@@ -938,8 +971,9 @@ __device__ __forceinline__ uint32_t tile_bfs_seeded(int* row, uint32_t sink, uin
   return vis;
 }
 
-// Frontier rounds.  The first round of a relabel or flood processes every tile (grid-stride);
-// round r > 0 processes the list fq[r & 1] built by round r - 1.  A tile whose boundary
+// Frontier rounds.  The first round of a relabel or flood processes the solve's selected
+// tiles (grid-stride over the selection); round r > 0 processes the list fq[r & 1] built by
+// round r - 1.  A tile whose boundary
 // values changed queues its neighbours in fq[(r + 1) & 1], deduplicated by mark[(r + 1) & 1];
 // the round that processes a tile clears its mark.  Only the CTAs the list needs take part
 // (at least one, so every launched round is finalised), and the last of them consumes the
@@ -949,22 +983,30 @@ __device__ __forceinline__ int frontier_round_number(const PoolView& P, int firs
   return first ? 0 : *((volatile int32_t*)&P.ctl[CTL_RND]);
 }
 
-// Work of this round: *count tiles (all tiles for a first round) and the number of CTAs that
-// take part; CTAs beyond it return at once.  Called by every thread of the CTA.
+// Work of this round: *count tiles (the selected tiles for a first round, the frontier list
+// otherwise), *nranges the selection's ranges, and the number of CTAs that take part; CTAs
+// beyond it return at once.  Called by every thread of the CTA.
 __device__ __forceinline__ void frontier_work(const PoolView& P, int first, int in, int per_cta,
-                                              int* count, int* participants) {
-  __shared__ int s_n;
+                                              int* count, int* participants, int* nranges) {
+  __shared__ int s_n, s_nr;
   if (threadIdx.x == 0) {
-    int n = first ? P.nt : *((volatile int32_t*)&P.fcount[in]);
+    int n = first ? *((volatile int32_t*)&P.nsel[1]) : *((volatile int32_t*)&P.fcount[in]);
+    int nr = *((volatile int32_t*)&P.nsel[0]);
     if (n < 0 || n > P.nt) {   // self-check: a list holds each tile at most once
       record_bad(P, 6, n);
       n = 0;
     }
+    if (nr < 0 || nr > P.nimg) {   // self-check: one range per image at most
+      record_bad(P, 9, nr);
+      n = nr = 0;
+    }
     s_n = n;
+    s_nr = nr;
   }
   __syncthreads();
   const int n = s_n;
   *count = n;
+  *nranges = s_nr;
   const int need = first ? (int)gridDim.x : (n + per_cta - 1) / per_cta;
   *participants = need < 1 ? 1 : (need < (int)gridDim.x ? need : (int)gridDim.x);
 }
@@ -1007,13 +1049,23 @@ __device__ __forceinline__ void frontier_round_end(const PoolView& P, int first,
   if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 
-// Solve prologue: reset the control words and the image stamps.
+// Solve prologue: reset the control words and the image stamps; the images of the
+// selection take their mode for this solve and restart their flow sums (the others keep
+// their results).  One CTA.
 __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc* acc) {
   for (int i = threadIdx.x; i < CTL_N; i += blockDim.x) P.ctl[i] = 0;
   for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) {
     P.img_live[i] = 0;
     P.img_hit[i] = 0;
-    acc[i].sumpos_e = 0;   // the flood of this solve accumulates it
+    P.img_mode[i] = 0;
+  }
+  __syncthreads();
+  const int nr = *((volatile int32_t*)&P.nsel[0]);
+  for (int k = threadIdx.x; k < nr && k < P.nimg; k += blockDim.x) {
+    const int img = P.sel[k].w;
+    if ((unsigned)img >= (unsigned)P.nimg) continue;
+    P.img_mode[img] = P.sel_mode[k];
+    acc[img].sumpos_e = 0;   // the floods of this solve accumulate it
   }
   if (threadIdx.x == 0) {
     P.ctl[CTL_MAXROUNDS] = max_rounds;
@@ -1026,87 +1078,95 @@ __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc
 }
 
 // The active-tile list after a global relabel, in one launch: a single-pass scan (chunks by
-// arrival ticket, decoupled look-back) of the tiles' activity flags writes the ids of the
-// active tiles in order and stamps their images live for the next cycle (stamp = cycles + 1
-// + bump); the last CTA to finish closes the scan and applies the cycle check: another cycle
-// runs while tiles are active and the cycle cap is not reached (`count_cycle` counts this
-// check as a finished cycle).  Replaces a compaction and a separate stamping launch.
+// arrival ticket, decoupled look-back) of the activity flags of the selected tiles writes the
+// ids of the active tiles in order and stamps their images live for the next cycle (stamp =
+// cycles + 1 + bump); the last CTA to finish closes the scan and applies the cycle check:
+// another cycle runs while tiles are active and the cycle cap is not reached (`count_cycle`
+// counts this check as a finished cycle).  Replaces a compaction and a separate stamping
+// launch.  filter: 1 only tiles of the images a flood check kept (img_live == the cycle
+// stamp; a solved image keeps the activity flags of its last relabel), 2 those and the tiles
+// of freshly uploaded images (the first list of a solve).  The grid covers the whole pool;
+// CTAs whose ticket is past the selection's chunks only count themselves done.
 constexpr int ACT_THREADS = 256;
 constexpr int ACT_ITEMS = 16;
 constexpr int ACT_CHUNK = ACT_THREADS * ACT_ITEMS;
 
 __global__ void __launch_bounds__(ACT_THREADS)
 k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
-              int count_cycle, int filter_live, cudaGraphConditionalHandle h, ImageAcc* acc) {
+              int count_cycle, int filter, cudaGraphConditionalHandle h, ImageAcc* acc) {
   __shared__ int32_t sm[32];
-  __shared__ int32_t s_chunk, s_excl, s_cur;
+  __shared__ int32_t s_chunk, s_excl, s_cur, s_n, s_nr;
   __shared__ uint32_t s_tag;
   if (threadIdx.x == 0) {
     s_chunk = atomicAdd(st.ticket, 1);
     s_tag = *((volatile uint32_t*)st.seq);
     s_cur = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1;
+    int n = *((volatile int32_t*)&P.nsel[1]), nr = *((volatile int32_t*)&P.nsel[0]);
+    if (n < 0 || n > P.nt || nr < 0 || nr > P.nimg) {   // self-check
+      record_bad(P, 9, n);
+      n = nr = 0;
+    }
+    s_n = n;
+    s_nr = nr;
   }
   __syncthreads();
   const int chunk = s_chunk, cur = s_cur, stamp = cur + bump;
-  const int nt = P.nt;
-  const int nchunks = (nt + ACT_CHUNK - 1) / ACT_CHUNK;
-  const int base = chunk * ACT_CHUNK + threadIdx.x * ACT_ITEMS;
-  int32_t v[ACT_ITEMS];
-  if (base + ACT_ITEMS <= nt) {
-#pragma unroll
-    for (int k = 0; k < ACT_ITEMS; k += 4) {
-      const int4 q = *reinterpret_cast<const int4*>(P.tact + base + k);
-      v[k] = q.x != 0; v[k + 1] = q.y != 0; v[k + 2] = q.z != 0; v[k + 3] = q.w != 0;
-    }
-  } else {
-#pragma unroll
-    for (int k = 0; k < ACT_ITEMS; ++k) v[k] = (base + k < nt) ? (P.tact[base + k] != 0) : 0;
-  }
-  // after a flood check only the images it kept take part (a solved image keeps the
-  // activity flags of its last relabel); the stamp this launch writes counts as live too
-  if (filter_live) {
+  const int n = s_n;
+  const int nchunks = (n + ACT_CHUNK - 1) / ACT_CHUNK;
+  if (chunk < nchunks) {
+    const int base = chunk * ACT_CHUNK + threadIdx.x * ACT_ITEMS;
+    SelCursor cursor(P, s_nr, base < n ? base : 0);
+    int32_t v[ACT_ITEMS], tl[ACT_ITEMS];
 #pragma unroll
     for (int k = 0; k < ACT_ITEMS; ++k) {
-      if (!v[k]) continue;
-      const int img = P.img_of[base + k];
-      const int il = (unsigned)img < (unsigned)P.nimg ? *((volatile int32_t*)&P.img_live[img]) : 0;
-      v[k] = il == cur || il == stamp;
+      tl[k] = base + k < n ? cursor.tile(base + k) : -1;
+      v[k] = tl[k] >= 0 ? P.tact[tl[k]] != 0 : 0;
     }
-  }
-  int32_t tsum = 0;
+    if (filter) {
 #pragma unroll
-  for (int k = 0; k < ACT_ITEMS; ++k) tsum += v[k];
-  int32_t agg;
-  const int32_t tex = block_exclusive_scan(tsum, sm, &agg);
-  if (threadIdx.x < 32) {
-    const int32_t ex = lookback_exclusive_warp(st, s_tag, chunk, agg);
-    if (threadIdx.x == 0) s_excl = ex;
-  }
-  __syncthreads();
-  int32_t run = s_excl + tex;
-#pragma unroll
-  for (int k = 0; k < ACT_ITEMS; ++k) {
-    if (v[k]) {
-      const int t = base + k;
-      if ((unsigned)run < (unsigned)nt) list[run] = t;
-      else atomicExch(st.err, 2);   // only after a look-back that gave up
-      const int img = P.img_of[t];
-      if ((unsigned)img < (unsigned)P.nimg) {
-        P.img_live[img] = stamp;
-        // the image's next flood starts afresh: its sum and its sink-reached stamp (the
-        // first cycle of a warm solve reuses the stamp of the flood before it)
-        acc[img].sumpos_e = 0;
-        P.img_hit[img] = 0;
-      } else {
-        record_bad(P, 4, img);
+      for (int k = 0; k < ACT_ITEMS; ++k) {
+        if (!v[k]) continue;
+        const int img = P.img_of[tl[k]];
+        if ((unsigned)img >= (unsigned)P.nimg) { v[k] = 0; continue; }
+        const int il = *((volatile int32_t*)&P.img_live[img]);
+        v[k] = il == cur || il == stamp || (filter == 2 && P.img_mode[img] == 1);
       }
-      ++run;
     }
+    int32_t tsum = 0;
+#pragma unroll
+    for (int k = 0; k < ACT_ITEMS; ++k) tsum += v[k];
+    int32_t agg;
+    const int32_t tex = block_exclusive_scan(tsum, sm, &agg);
+    if (threadIdx.x < 32) {
+      const int32_t ex = lookback_exclusive_warp(st, s_tag, chunk, agg);
+      if (threadIdx.x == 0) s_excl = ex;
+    }
+    __syncthreads();
+    int32_t run = s_excl + tex;
+#pragma unroll
+    for (int k = 0; k < ACT_ITEMS; ++k) {
+      if (v[k]) {
+        const int t = tl[k];
+        if ((unsigned)run < (unsigned)P.nt) list[run] = t;
+        else atomicExch(st.err, 2);   // only after a look-back that gave up
+        const int img = P.img_of[t];
+        if ((unsigned)img < (unsigned)P.nimg) {
+          P.img_live[img] = stamp;
+          // the image's next flood starts afresh: its sum and its sink-reached stamp (the
+          // first cycle of a warm solve reuses the stamp of the flood before it)
+          acc[img].sumpos_e = 0;
+          P.img_hit[img] = 0;
+        } else {
+          record_bad(P, 4, img);
+        }
+        ++run;
+      }
+    }
+    if (chunk == nchunks - 1 && threadIdx.x == 0) *count = s_excl + agg;
   }
-  if (chunk == nchunks - 1 && threadIdx.x == 0) *count = s_excl + agg;
   if (threadIdx.x != 0) return;
   __threadfence();
-  if (atomicAdd(st.done, 1) != nchunks - 1) return;
+  if (atomicAdd(st.done, 1) != (int)gridDim.x - 1) return;
   // last CTA: close the scan (tickets, tag) and apply the cycle check
   __threadfence();
   *st.ticket = 0;
@@ -1115,14 +1175,15 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
   if ((sq & 0x3fffffffu) == 0) sq = 1;
   *st.seq = sq;
   volatile int32_t* ctl = P.ctl;
-  const int n = *((volatile int32_t*)count);
+  if (nchunks == 0) *count = 0;
+  const int nact = *((volatile int32_t*)count);
   ctl[CTL_PULSE] = 0;   // the list sits in queue[0]
   ctl[CTL_DDONE] = 0;
   P.qcount[1] = 0;
   const int cycles = ctl[CTL_CYCLES] + (count_cycle ? 1 : 0);
   ctl[CTL_CYCLES] = cycles;
   ctl[CTL_NACT] = ctl[CTL_NACT] + 1;
-  bool more = n > 0 && ctl[CTL_ERR] < 3;
+  bool more = nact > 0 && ctl[CTL_ERR] < 3;
   if (more && cycles >= ctl[CTL_MAXCYCLES]) {
     ctl[CTL_ERR] = 2;
     more = false;
@@ -1162,11 +1223,13 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
   // first == 2: a global relabel inside the solve loop skips images whose cut was final at
   // the previous check (no active tile); their state no longer changes
   const int live = first == 2 ? *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1 : 0;
-  int n, parts;
-  frontier_work(P, first, in, WARPS_PER_CTA, &n, &parts);
+  int n, parts, nr;
+  frontier_work(P, first, in, WARPS_PER_CTA, &n, &parts, &nr);
   if ((int)blockIdx.x >= parts) return;
-  for (int i = blockIdx.x * WARPS_PER_CTA + warp; i < n; i += parts * WARPS_PER_CTA) {
-    const int t = first ? i : P.fq[in][i];
+  const int i0 = blockIdx.x * WARPS_PER_CTA + warp;
+  SelCursor cursor(P, first ? nr : 0, i0);
+  for (int i = i0; i < n; i += parts * WARPS_PER_CTA) {
+    const int t = first ? cursor.tile(i) : P.fq[in][i];
     if (!first) {
       if (lane == 0) markin[t] = 0;
     } else {
@@ -1253,9 +1316,10 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
 // global relabel and push cycle.  Every round stamps img_hit[img] with the cycle stamp
 // (ctl[CTL_CYCLES] + 1) when a tile's reached set meets its sink pixels.
 //
-// mode: 0 frontier round; 1 first round over every tile; 2 first round over the tiles of
-// the images live in this cycle (img_live == stamp).  abort_hit: frontier rounds skip the
-// tiles of images already stamped (their flood is redone in a later cycle).
+// mode: 0 frontier round; first rounds over the selected tiles: 1 all of them, 2 those of the
+// images live in this cycle (img_live == stamp), 3 those of the images that continue from a
+// previous flow (img_mode == 2).  abort_hit: frontier rounds skip the tiles of images already
+// stamped (their flood is redone in a later cycle).
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
 k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h, ImageAcc* acc) {
@@ -1265,11 +1329,13 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
   const int stamp = *((volatile int32_t*)&P.ctl[CTL_CYCLES]) + 1;
   int32_t* const markin = P.mark[in];
   int done = 0;
-  int n, parts;
-  frontier_work(P, first, in, WARPS_PER_CTA, &n, &parts);
+  int n, parts, nr;
+  frontier_work(P, first, in, WARPS_PER_CTA, &n, &parts, &nr);
   if ((int)blockIdx.x >= parts) return;
-  for (int i = blockIdx.x * WARPS_PER_CTA + warp; i < n; i += parts * WARPS_PER_CTA) {
-    const int t = first ? i : P.fq[in][i];
+  const int i0 = blockIdx.x * WARPS_PER_CTA + warp;
+  SelCursor cursor(P, first ? nr : 0, i0);
+  for (int i = i0; i < n; i += parts * WARPS_PER_CTA) {
+    const int t = first ? cursor.tile(i) : P.fq[in][i];
     if (!first && lane == 0) markin[t] = 0;
     const int img = P.img_of[t];
     if ((unsigned)img >= (unsigned)P.nimg) {   // self-check
@@ -1277,6 +1343,7 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
       continue;
     }
     if (mode == 2 && P.img_live[img] != stamp) continue;
+    if (mode == 3 && P.img_mode[img] != 2) continue;
     if (mode == 0 && abort_hit && *((volatile int32_t*)&P.img_hit[img]) == stamp) continue;
     ++done;
     const int4 nb = P.nbr[t];
@@ -1334,10 +1401,10 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
 
 // After a flood: an image whose flood reached no sink pixel is solved (its flood is the
 // canonical cut, its sums are final) and leaves the live set; the others go on to a global
-// relabel.  all != 0: every image takes part (the first check of a solve that starts with a
-// relabel); else the images live in this cycle.  Sets the condition of the IF node around
-// the relabel (hbfs) and, when no image is left, ends the solve loop (hmain); the last cycle
-// of a solve is counted here.  One CTA.
+// relabel.  all != 0: the images that continue from a previous flow (img_mode == 2; the
+// first check of a solve); else the images live in this cycle.  Sets the condition of the
+// IF node around the relabel (hbfs) and, when no image is left, ends the solve loop (hmain);
+// the last cycle of a solve is counted here.  One CTA.
 __global__ void k_flood_check(PoolView P, int all, cudaGraphConditionalHandle hbfs,
                               cudaGraphConditionalHandle hmain) {
   __shared__ int s_left;
@@ -1347,7 +1414,7 @@ __global__ void k_flood_check(PoolView P, int all, cudaGraphConditionalHandle hb
   const int stamp = ctl[CTL_CYCLES] + 1;
   int left = 0;
   for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) {
-    if (!all && P.img_live[i] != stamp) continue;
+    if (all ? P.img_mode[i] != 2 : P.img_live[i] != stamp) continue;
     if (P.img_hit[i] == stamp) {
       P.img_live[i] = stamp;
       ++left;
@@ -1366,6 +1433,17 @@ __global__ void k_flood_check(PoolView P, int all, cudaGraphConditionalHandle hb
   __threadfence();
   if (hbfs) cudaGraphSetConditional(hbfs, n > 0 ? 1u : 0u);
   if (hmain && n == 0) cudaGraphSetConditional(hmain, 0u);
+}
+
+// Neighbour tile ids and image index of one image's tiles (row-major from im.tile0), for an
+// image placed in a session pool.
+__global__ void k_image_tiles(PoolView P, ImageDesc im, int img) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= im.tw * im.th) return;
+  const int tx = k % im.tw, ty = k / im.tw, t = im.tile0 + k;
+  P.nbr[t] = make_int4(ty > 0 ? t - im.tw : -1, ty < im.th - 1 ? t + im.tw : -1,
+                       tx > 0 ? t - 1 : -1, tx < im.tw - 1 ? t + 1 : -1);
+  P.img_of[t] = img;
 }
 
 // Labels of one image, row-major, padding excluded.  One thread writes the 32 pixels of
@@ -1652,23 +1730,30 @@ int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s) {
 
 int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc* acc,
                      cudaStream_t s) {
-  k_ctl_begin<<<1, 32, 0, s>>>(P, max_rounds, max_cycles, acc);
+  k_ctl_begin<<<1, 256, 0, s>>>(P, max_rounds, max_cycles, acc);
   return ok();
 }
 
 int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, int32_t* count,
-                       int bump, int count_cycle, int filter_live, cudaGraphConditionalHandle h,
+                       int bump, int count_cycle, int filter, cudaGraphConditionalHandle h,
                        ImageAcc* acc, cudaStream_t s) {
-  const int nch = (P.nt + ACT_CHUNK - 1) / ACT_CHUNK;
+  const int nch = (P.nt + ACT_CHUNK - 1) / ACT_CHUNK;   // enough for any selection
   if (nch > st.max_chunks) return GC_ERR_INVALID;
   k_active_list<<<nch > 0 ? nch : 1, ACT_THREADS, 0, s>>>(P, st, list, count, bump, count_cycle,
-                                                          filter_live, h, acc);
+                                                          filter, h, acc);
   return ok();
 }
 
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s) {
   k_ctl_cycle<<<1, 32, 0, s>>>(P, count, count_cycle, h);
+  return ok();
+}
+
+int launch_image_tiles(const PoolView& P, const ImageDesc& im, int img, cudaStream_t s) {
+  const int n = im.tw * im.th;
+  if (n <= 0) return GC_OK;
+  k_image_tiles<<<(n + 255) / 256, 256, 0, s>>>(P, im, img);
   return ok();
 }
 
@@ -1764,6 +1849,7 @@ void preload_kernels() {
       (const void*)k_masks, (const void*)k_discharge, (const void*)k_edge_relabel_build,
       (const void*)k_bfs_round, (const void*)k_flood_round, (const void*)k_ctl_begin,
       (const void*)k_active_list, (const void*)k_ctl_cycle, (const void*)k_flood_check,
+      (const void*)k_image_tiles,
       (const void*)k_acc_reset, (const void*)k_labels_out, (const void*)k_labels_packed,
       (const void*)k_state_out, (const void*)k_edit, (const void*)k_stroke,
       (const void*)k_brush};

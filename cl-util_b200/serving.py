@@ -492,3 +492,274 @@ def poisson_trace(rng, rate_hz, duration_s, n_images, p_new=0.3):
         if t >= duration_s:
             return out
         out.append((t, "image" if rng.random() < p_new else "stroke", int(rng.integers(n_images))))
+
+
+class _PoolSession:
+    def __init__(self, sid, slot, tile0, width, height):
+        self.sid, self.slot, self.tile0 = sid, slot, tile0
+        self.width, self.height = width, height
+        self.last_use = time.perf_counter()
+
+
+class BatchingServer:
+    """Continuous batching on one GPU: every session lives in one SessionPool, and each tick
+    of the worker solves all the requests that are ready at that moment in one launch.
+
+    A tick takes, under the lock, the head stroke of every resident session with queued
+    strokes (one per session, so strokes of a session stay in order) and the queued new
+    images in arrival order, as far as free tiles, free slots (evicting least-recently-used
+    idle sessions) and `tick_pixels` allow (at least one image per tick).  It uploads the
+    images and applies the strokes, solves all of them together (gcp_solve), and reads every
+    flow and bit-packed cut back.  Requests that arrive meanwhile join the next tick, so the
+    solves of different sizes overlap on the device inside one launch instead of on
+    concurrent streams, and no request waits for a CUDA-graph construction: the pool's graph
+    is built at start-up.  Results do not depend on the mix: each session's flow value and
+    canonical cut are unique for its graph.
+
+    Same request / result interface as GraphCutServer (submit, drain, close, results,
+    misses, evictions)."""
+
+    def __init__(self, hbm_budget: int = 16 << 30, device: int = 0, max_sessions: int = 512,
+                 tick_pixels: int = 24 << 20, solver_kw=None, warm_up: bool = True):
+        import torch
+
+        from session_pool import SessionPool
+        self.torch = torch
+        self.device = device
+        self.tick_pixels = int(tick_pixels)
+        max_tiles = self._tiles_for(hbm_budget, max_sessions)
+        self.budget = SessionPool.arena_bytes(max_tiles, max_sessions)
+        self.pool = SessionPool(max_tiles, max_sessions, device=device, **(solver_kw or {}))
+        self.lock = threading.Condition()
+        self.images = collections.deque()              # (NewImage, arrival)
+        self.strokes = collections.defaultdict(collections.deque)  # session -> (Stroke, arrival)
+        self.sessions: dict[int, _PoolSession] = {}
+        self.lru = collections.OrderedDict()           # resident sessions, oldest first
+        self.free_slots = list(range(max_sessions - 1, -1, -1))
+        self.queued_images = set()
+        self.results: list[Result] = []
+        self.misses = 0
+        self.evictions = 0
+        self.ticks = 0
+        self.errors = []
+        self.stop = False
+        self.inflight = 0
+        with torch.cuda.device(device):
+            self.stream = torch.cuda.Stream()
+        if warm_up:
+            self._warm_up()
+        self.worker = threading.Thread(target=self._worker, daemon=True)
+        self.worker.start()
+
+    @staticmethod
+    def _tiles_for(budget, max_sessions):
+        """The most tiles whose pool fits in `budget` bytes."""
+        from session_pool import SessionPool
+        lo, hi = 1, 1 << 26
+        if SessionPool.arena_bytes(lo, max_sessions) > budget:
+            raise MemoryError("the HBM budget does not hold a session pool")
+        while lo < hi:
+            mid = (lo + hi + 1) // 2
+            if SessionPool.arena_bytes(mid, max_sessions) <= budget:
+                lo = mid
+            else:
+                hi = mid - 1
+        return lo
+
+    def _warm_up(self):
+        """Builds the pool's CUDA graphs before the first request: a fresh solve and a warm
+        one of a small image."""
+        torch = self.torch
+        t0 = self.pool.alloc_tiles(64, 64)
+        slot = self.free_slots[-1]
+        z = torch.zeros((64, 64), dtype=torch.int32, device=self.pool.device)
+        ex = torch.zeros((64, 64), dtype=torch.int32, device=self.pool.device)
+        ex[0, 0], ex[-1, -1] = 5, -5
+        with torch.cuda.stream(self.stream):
+            self.pool.open(slot, 64, 64, t0, stream=self.stream)
+            self.pool.upload_capacities(slot, z + 1, z + 1, z + 1, z + 1, ex, stream=self.stream)
+            self.pool.solve([slot], stream=self.stream)
+            self.pool.edit_stroke(slot, [3], [3], 2, 7, stream=self.stream)
+            self.pool.solve([slot], stream=self.stream)
+        self.pool.close(slot)
+        self.pool.free_tiles(t0, 64, 64)
+
+    # ---- client side ------------------------------------------------------------
+    def submit(self, request, arrival=None):
+        arrival = time.perf_counter() if arrival is None else arrival
+        with self.lock:
+            sid = request.session
+            if isinstance(request, Stroke):
+                if sid not in self.sessions and sid not in self.queued_images:
+                    self.misses += 1      # evicted (or never opened)
+                    return
+                self.strokes[sid].append((request, arrival))
+            else:
+                self.queued_images.add(sid)
+                self.images.append((request, arrival))
+            self.lock.notify()
+
+    def drain(self, timeout=600.0):
+        t0 = time.perf_counter()
+        with self.lock:
+            while ((self.images or self.inflight or
+                    any(q and (s in self.sessions or s in self.queued_images)
+                        for s, q in self.strokes.items()))
+                   and time.perf_counter() - t0 < timeout):
+                self.lock.wait(0.05)
+        if self.errors:
+            raise self.errors[0]
+
+    def close(self):
+        with self.lock:
+            self.stop = True
+            self.lock.notify_all()
+        self.worker.join()
+        self.pool.close_pool()
+
+    @property
+    def used_tiles(self) -> int:
+        """Tiles of the pool held by resident sessions."""
+        return self.pool.tiles.used
+
+    # ---- scheduling (under self.lock) ---------------------------------------------
+    def _evict_one(self, keep):
+        for sid, s in self.lru.items():
+            if sid in keep or self.strokes.get(sid):
+                continue
+            del self.lru[sid]
+            del self.sessions[sid]
+            self.strokes.pop(sid, None)
+            self.pool.close(s.slot)
+            self.pool.free_tiles(s.tile0, s.width, s.height)
+            self.free_slots.append(s.slot)
+            self.evictions += 1
+            return True
+        return False
+
+    def _take_tick(self):
+        """(strokes, images) of the next tick, or None."""
+        strokes = []
+        for sid, q in self.strokes.items():
+            if q and sid in self.sessions:
+                req, arr = q.popleft()
+                strokes.append((req, arr, self.sessions[sid]))
+        keep = {req.session for req, _, _ in strokes}
+        images, px = [], 0
+        while self.images:
+            req, arr = self.images[0]
+            h, w = req.shape
+            if images and px + w * h > self.tick_pixels:
+                break
+            from session_pool import tiles_of
+            if tiles_of(w, h) > self.pool.max_tiles:
+                self.images.popleft()
+                self.queued_images.discard(req.session)
+                self.strokes.pop(req.session, None)
+                self.errors.append(MemoryError(f"session {req.session}: {w}x{h} needs more "
+                                               "than the pool holds"))
+                continue
+            t0 = self.pool.alloc_tiles(w, h)
+            while (t0 is None or not self.free_slots) and self._evict_one(keep):
+                if t0 is None:
+                    t0 = self.pool.alloc_tiles(w, h)
+            if t0 is None or not self.free_slots:
+                if t0 is not None:
+                    self.pool.free_tiles(t0, w, h)
+                break
+            self.images.popleft()
+            slot = self.free_slots.pop()
+            s = _PoolSession(req.session, slot, t0, w, h)
+            images.append((req, arr, s))
+            keep.add(req.session)
+            px += w * h
+        if not strokes and not images:
+            return None
+        return strokes, images
+
+    # ---- worker -----------------------------------------------------------------------
+    def _worker(self):
+        torch = self.torch
+        while True:
+            with self.lock:
+                tick = None
+                while not self.stop:
+                    tick = self._take_tick()
+                    if tick is not None:
+                        break
+                    self.lock.wait(0.02)
+                if tick is None:
+                    return
+                strokes, images = tick
+                self.inflight += len(strokes) + len(images)
+            try:
+                start = time.perf_counter()
+                with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+                    for req, _, s in images:
+                        self.pool.open(s.slot, s.width, s.height, s.tile0, stream=self.stream)
+                        self._upload(s, req.planes)
+                    for req, _, s in strokes:
+                        self.pool.edit_stroke(s.slot, req.xs, req.ys, req.radius, req.value,
+                                              stream=self.stream)
+                    t1 = time.perf_counter()
+                    jobs = images + strokes
+                    self.pool.solve([s.slot for _, _, s in jobs], stream=self.stream)
+                    t2 = time.perf_counter()
+                    flows = [self.pool.flow(s.slot) for _, _, s in jobs]
+                    dev = [self.pool.labels_packed(s.slot, stream=self.stream) for _, _, s in jobs]
+                    host = [d.to("cpu", non_blocking=True) for d in dev]
+                    self.stream.synchronize()
+                done = time.perf_counter()
+                phases = (1e3 * (t1 - start), 1e3 * (t2 - t1), 1e3 * (done - t2))
+                with self.lock:
+                    self.ticks += 1
+                    for (req, arr, s), f, bits in zip(jobs, flows, host):
+                        kind = "stroke" if isinstance(req, Stroke) else "image"
+                        self.results.append(Result(s.sid, kind, f, bits.numpy(), s.width, arr,
+                                                   start, done, s.width * s.height, phases))
+                        if kind == "image":
+                            self.sessions[s.sid] = s
+                            self.queued_images.discard(s.sid)
+                        s.last_use = done
+                        self.lru.pop(s.sid, None)
+                        self.lru[s.sid] = s
+            except Exception as exc:  # surfaced by drain()
+                with self.lock:
+                    self.errors.append(exc)
+                    for req, _, s in images:
+                        self.queued_images.discard(req.session)
+                        if s.sid not in self.sessions:
+                            try:
+                                self.pool.close(s.slot)
+                            except Exception:
+                                pass
+                            self.pool.free_tiles(s.tile0, s.width, s.height)
+                            self.free_slots.append(s.slot)
+            finally:
+                with self.lock:
+                    self.inflight -= len(strokes) + len(images)
+                    self.lock.notify_all()
+
+    def _upload(self, s, planes):
+        """A new session's inputs (the same three forms as GraphCutServer's) to its slot."""
+        torch = self.torch
+        w, h = s.width, s.height
+        if isinstance(planes[-1], tuple):   # (rgba, (fg, bg)): t-links from the models
+            import gmm_tlinks
+            from GraphCut import _as_rgba32
+            img = torch.from_numpy(np.ascontiguousarray(_as_rgba32(planes[0])).view(np.int32)).to(
+                self.pool.device, non_blocking=True)
+            ex = gmm_tlinks.tlinks(img, *planes[1], stream=self.stream)
+            self.pool.upload_image(s.slot, img, ex, stream=self.stream)
+            return
+        dev = []
+        for p in planes:
+            src = np.ascontiguousarray(p)
+            if src.dtype == np.uint32:
+                src = src.view(np.int32)
+            dev.append(torch.from_numpy(np.ascontiguousarray(src, dtype=np.int32)).to(
+                self.pool.device, non_blocking=True))
+        if len(dev) == 2:
+            self.pool.upload_image(s.slot, dev[0], dev[1], stream=self.stream)
+        else:
+            self.pool.upload_capacities(s.slot, *dev, stream=self.stream)

@@ -397,6 +397,49 @@ int gcb_get_stats(const gcb_handle* b, gc_stats* stats);
 int gcb_set_profile(gcb_handle* b, int on);
 int gcb_get_profile(const gcb_handle* b, gc_kernel_prof* out, int n);
 
+/* ---- session pools: many resident images, solved together a few at a time ------------
+   A pool of max_tiles 32x32 tiles and max_sessions image slots in one arena.  An image
+   (a serving session) opens on a slot with a caller-chosen range of tiles, keeps its
+   residual graph there between requests, and any set of slots is solved together by one
+   launch of the pool's CUDA graph; the other slots keep their state and results.  The graph
+   is built on the pool's first solves (one for solves of fresh uploads only, one when some
+   slot continues from a previous flow), so requests never wait for a graph construction.
+   No counterpart in the reference (one GraphCut object per image, GraphCut.pyx:80-154).
+   One caller thread and one stream per pool at a time. */
+typedef struct gcp_handle gcp_handle;
+/* Device bytes of a pool (host-only computation). */
+int gcp_arena_bytes(int max_tiles, int max_sessions, int64_t* bytes);
+int gcp_create(int max_tiles, int max_sessions, const gc_opts* opts, gcp_handle** out);
+/* In caller-owned device memory (256-byte aligned, at least gcp_arena_bytes bytes). */
+int gcp_create_in(int max_tiles, int max_sessions, const gc_opts* opts, void* arena,
+                  int64_t bytes, gcp_handle** out);
+int gcp_destroy(gcp_handle* p);
+/* Opens slot `slot` for a width x height image on tiles [tile0, tile0 + ceil(W/32) *
+   ceil(H/32)) of the pool, which must not overlap another open slot's. */
+int gcp_open(gcp_handle* p, int slot, int width, int height, int tile0, void* stream);
+/* Closes a slot; its tiles may be given to another slot. */
+int gcp_close(gcp_handle* p, int slot);
+/* Uploads and edits of one slot, as gc_upload / gc_upload_rgba / gc_edit_stroke /
+   gc_edit_brush do for a handle. */
+int gcp_upload(gcp_handle* p, int slot, const int32_t* up, const int32_t* down,
+               const int32_t* left, const int32_t* right, const int32_t* excess, void* stream);
+int gcp_upload_rgba(gcp_handle* p, int slot, const uint32_t* rgba, const int32_t* excess,
+                    void* stream);
+int gcp_edit_stroke(gcp_handle* p, int slot, const int32_t* xs, const int32_t* ys, int npts,
+                    int radius, int32_t value, void* stream);
+int gcp_edit_brush(gcp_handle* p, int slot, const int32_t* xs, const int32_t* ys, int npts,
+                   int radius, int32_t value, void* stream);
+/* Solves the n listed slots (distinct, open, uploaded) together: one graph launch; a slot
+   uploaded since its last solve starts fresh, an edited or solved one warm-starts from its
+   previous flow.  Blocks the calling thread until the solve is done. */
+int gcp_solve(gcp_handle* p, const int* slots, int n, void* stream);
+int gcp_flow(gcp_handle* p, int slot, int64_t* flow);
+/* Canonical labels of a slot's last solve into DEVICE buffers (as gc_labels /
+   gc_labels_packed). */
+int gcp_labels(gcp_handle* p, int slot, uint8_t* labels, void* stream);
+int gcp_labels_packed(gcp_handle* p, int slot, uint8_t* bits, void* stream);
+int gcp_get_stats(const gcp_handle* p, gc_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

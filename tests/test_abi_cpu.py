@@ -13,7 +13,7 @@ def header_functions():
     with open(os.path.join(ROOT, "include", "gcut.h")) as f:
         src = f.read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(gcb?_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(gc[bp]?_[a-z_]+)\s*\(", src)))
 
 
 @pytest.fixture(scope="module")

@@ -144,3 +144,54 @@ def test_image_requests_from_colour_models(cuda):
         g, strks = hist[r.session]
         f, lab = _alone(g, strks[:k])
         assert r.flow == f and np.array_equal(r.labels, lab), (r.session, k)
+
+
+@pytest.mark.parametrize("budget_images", [100, 2])
+def test_batching_server_same_alone_and_in_mix(cuda, budget_images):
+    """Continuous batching (BatchingServer): requests submitted in bursts are solved several
+    per launch, sessions of different sizes together, with evictions when the pool is small;
+    every result equals the solve of its session's graph alone."""
+    from serving import BatchingServer
+    from session_pool import SessionPool, tiles_of
+    rng = np.random.default_rng(20 + budget_images)
+    shapes = [(int(rng.integers(64, 400)), int(rng.integers(64, 400))) for _ in range(5)]
+    graphs = [synth.make_graph(w, h, 700 + i) for i, (w, h) in enumerate(shapes)]
+    max_sessions = 32
+    tiles = int(budget_images * max(tiles_of(w, h) for w, h in shapes))
+    srv = BatchingServer(hbm_budget=SessionPool.arena_bytes(tiles, max_sessions),
+                         max_sessions=max_sessions)
+    history = {}
+    sid = 0
+    n_req = 0
+    for burst in range(10):
+        for step in range(6):
+            if step == 0 or not history:
+                img = (burst + step) % len(graphs)
+                history[sid] = (img, [])
+                srv.submit(NewImage(sid, graphs[img].planes()))
+                sid += 1
+            else:
+                target = max(history) - int(rng.integers(0, min(3, len(history))))
+                g = graphs[history[target][0]]
+                s = strokes.random_stroke(rng, g.width, g.height, rmin=4, rmax=12)
+                history[target][1].append(s)
+                srv.submit(Stroke(target, s.xs, s.ys, s.radius, s.value))
+            n_req += 1
+        if burst % 3 == 2:
+            srv.drain()
+    srv.drain()
+    results = sorted(srv.results, key=lambda r: r.arrival)
+    ticks, evictions, misses = srv.ticks, srv.evictions, srv.misses
+    srv.close()
+    assert results and ticks < len(results)          # several requests per launch
+    if budget_images <= 2:
+        assert evictions > 0
+    seen = {}
+    for r in results:
+        k = seen.get(r.session, 0)
+        seen[r.session] = k + 1
+        img, strks = history[r.session]
+        f, lab = _alone(graphs[img], strks[:k])
+        assert r.flow == f, (r.session, k)
+        assert np.array_equal(r.labels, lab), (r.session, k)
+    assert len(results) + misses == n_req
