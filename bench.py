@@ -830,14 +830,19 @@ def serving_images(n=12, seed=4):
                              keep_image=True)
 
 
-def run_trace(graphs, host_planes, trace, slots, budget, seed=5, solver_kw=None):
-    """Replays a (time, kind, image) trace against a GraphCutServer in real time.  A stroke
-    targets one of the 8 most recently opened sessions (random polyline, radius 8-32,
-    t-links +-10**6).  Returns (results, history, server counters, wall seconds)."""
+def run_trace(graphs, host_planes, trace, server, budget, seed=5, solver_kw=None):
+    """Replays a (time, kind, image) trace in real time against a server: "batching"
+    (BatchingServer: continuous batching over one session pool) or "single"
+    (GraphCutServer: one request at a time, one handle per session).  A stroke targets one
+    of the 8 most recently opened sessions (random polyline, radius 8-32, t-links +-10**6).
+    Returns (results, history, server counters, wall seconds)."""
     import strokes
-    from serving import GraphCutServer, NewImage, Stroke
+    from serving import BatchingServer, GraphCutServer, NewImage, Stroke
     rng = np.random.default_rng(seed)
-    srv = GraphCutServer(slots=slots, hbm_budget=budget, solver_kw=solver_kw)
+    if server == "batching":
+        srv = BatchingServer(hbm_budget=budget, solver_kw=solver_kw)
+    else:
+        srv = GraphCutServer(slots=1, hbm_budget=budget, solver_kw=solver_kw)
     history = {}     # session -> (image index, [strokes in submission order])
     sid = 0
     t0 = time.perf_counter()
@@ -860,6 +865,9 @@ def run_trace(graphs, host_planes, trace, slots, budget, seed=5, solver_kw=None)
     wall = time.perf_counter() - t0
     results = sorted(srv.results, key=lambda r: r.arrival)
     counters = {"misses": srv.misses, "evictions": srv.evictions}
+    if server == "batching":
+        counters["launches"] = srv.ticks
+        counters["requests_per_launch"] = len(results) / max(1, srv.ticks)
     srv.close()
     return results, history, counters, wall
 
@@ -935,11 +943,12 @@ def verify_results(graphs, dev_planes, results, history, cap_s):
 def run_serving(args):
     """Config 4: a Poisson request stream (`--rate` 200 req/s for `--duration` 60 s), 30 %
     new images (sides uniform in [256, 4096]) and 70 % brush strokes on resident sessions,
-    served by GraphCutServer with `--slots` requests in flight under a 64 GiB HBM budget,
-    then the same trace served one request at a time (slots=1).  Latency = result on the
-    host - arrival; every request's inputs come from pinned host memory and its labels go
-    back to host memory.  A time-capped sample of the results (whole sessions) is checked
-    bit-exactly against cold solves."""
+    served with continuous batching (BatchingServer: every session in one session pool under
+    a 64 GiB HBM budget, each tick solves all ready requests in one launch), then the same
+    trace served by the plain one-at-a-time solver (GraphCutServer, one handle per session).
+    Latency = result on the host - arrival; every request's inputs come from pinned host
+    memory and its labels go back to host memory.  A time-capped sample of the results
+    (whole sessions) is checked bit-exactly against cold solves."""
     import torch
 
     from serving import poisson_trace
@@ -958,12 +967,13 @@ def run_serving(args):
     # CUDA-graph instantiations in a process are slow, which is start-up, not serving
     warm = poisson_trace(np.random.default_rng(7), args.rate, min(args.duration, 15.0),
                          len(graphs))
-    run_trace(graphs, host_planes, warm, args.slots, budget, seed=8)
+    run_trace(graphs, host_planes, warm, "batching", budget, seed=8)
     clocks = ClockSampler(0)
     with clocks:
-        res, hist, cnt, wall = run_trace(graphs, host_planes, trace, args.slots, budget)
+        res, hist, cnt, wall = run_trace(graphs, host_planes, trace, "batching", budget)
     main_sum = _latency_summary(res, wall)
-    res1, hist1, cnt1, wall1 = run_trace(graphs, host_planes, trace, 1, budget)
+    run_trace(graphs, host_planes, warm, "single", budget, seed=8)
+    res1, hist1, cnt1, wall1 = run_trace(graphs, host_planes, trace, "single", budget)
     one_sum = _latency_summary(res1, wall1)
     checked, bad, examples = verify_results(graphs, dev_planes, res, hist, args.verify_s)
     line = {
@@ -975,7 +985,8 @@ def run_serving(args):
                                "image (pool of 12 synthetic grids, sides uniform in [256, 4096], "
                                "seeds 20000+i; each request opens its own session), 70% stroke "
                                "(radius 8-32, t-links +-10^6) on one of the 8 newest sessions",
-                   "slots": args.slots, "hbm_budget_gib": budget >> 30,
+                   "server": "continuous batching (BatchingServer, one session pool, one "
+                             "launch per tick)", "hbm_budget_gib": budget >> 30,
                    "latency": "arrival to labels in host memory (queueing included)"},
         **main_sum, **cnt,
         "one_at_a_time": {**one_sum, **cnt1},

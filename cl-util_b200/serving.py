@@ -1,7 +1,17 @@
 """Serving loop: image sessions and brush-stroke edits arriving over time.
 
 The reference is an interactive tool: one image, strokes from the GUI, ``GraphCut.cut`` run
-on a button press (test_GraphCut.py:78-99).  Here many sessions share one GPU:
+on a button press (test_GraphCut.py:78-99).  Here many sessions share one GPU, served by
+one of two servers with the same request / result interface:
+
+* ``BatchingServer``: continuous batching.  Every session lives in one session pool
+  (session_pool.SessionPool, gcp_* in include/gcut.h); each tick of its worker takes every
+  request ready at that moment and solves them all in one launch of the pool's CUDA graph,
+  so requests of different sizes overlap on the device and none waits for a graph build;
+* ``GraphCutServer``: the plain one-at-a-time solver, one GraphCut handle per session,
+  described below.
+
+GraphCutServer:
 
 * a request is either a NEW image (capacity planes in host memory) or a STROKE on a
   resident session; every request returns the flow value and the canonical labels of its
