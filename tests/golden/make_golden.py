@@ -14,7 +14,7 @@ present where the tests run, so this script turns windows of them into fixtures:
   in the final residual graph, bit-packed rows) from the oracle's Boykov-Kolmogorov solver,
   cross-checked against the restated reference schedule (same flow).
 
-    python tests/golden/make_golden.py [path to the reference tree]
+    python tests/golden/make_golden.py REFERENCE_DIR
 """
 from __future__ import annotations
 
@@ -76,4 +76,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py REFERENCE_DIR  (the checkout of "
+                 "rheiland/cl-util holding scoreFg.npy and scoreBg.npy)")
+    main(sys.argv[1])
