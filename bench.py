@@ -221,17 +221,26 @@ def time_gmm_fit(g, stream, with_cpu):
     return out
 
 
-def cpu_baseline(graph, threads, budget_s=12.0):
-    """The reference schedule restated (oracle ref_tiled) on the host cores."""
+def _cpu_build():
     from oracle import oracle as O
+    return "-O3 -march=native (built on this host)" if O.native_lib() else \
+        "-O3 -march=x86-64-v2 (portable build)"
+
+
+def cpu_baseline(graph, threads, budget_s=12.0):
+    """The reference schedule restated (oracle ref_tiled) on the host cores, built for this
+    host's CPU."""
+    from oracle import oracle as O
+    build = _cpu_build()
     reps, t_total = 0, 0.0
     while t_total < budget_s and reps < 50:
         t0 = time.perf_counter()
-        O.ref_tiled(*graph.planes(), bfs=5, threads=threads)
+        O.ref_tiled(*graph.planes(), bfs=5, threads=threads, native=True)
         t_total += time.perf_counter() - t0
         reps += 1
     mpix = graph.width * graph.height / 1e6
     return {"value": reps * mpix / t_total, "unit": UNIT, "cores": threads, "kind": "port",
+            "build": build,
             "sample": f"{reps} full solves of the {graph.width}x{graph.height} grid "
                       f"({t_total:.1f} s), oracle ref_tiled (GraphCut.cut + graphcut.cl "
                       f"restated, int32, OpenMP)"}
@@ -245,12 +254,13 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     g = synth.make_graph(args.size, args.size, 1)
     from oracle import oracle as O
+    build = _cpu_build()
     for _ in range(max(1, args.warmup)):
-        O.ref_tiled(*g.planes(), bfs=5, threads=threads)
+        O.ref_tiled(*g.planes(), bfs=5, threads=threads, native=True)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.ref_tiled(*g.planes(), bfs=5, threads=threads)
+        O.ref_tiled(*g.planes(), bfs=5, threads=threads, native=True)
         times.append(time.perf_counter() - t0)
     mpix = g.width * g.height / 1e6
     ms = 1000 * statistics.mean(times)
@@ -264,6 +274,7 @@ def run_reference(args):
                    "impl": "oracle ref_tiled: the reference schedule (GraphCut.pyx:348-418 + "
                            "graphcut.cl) restated in int32 C++, OpenMP over tiles"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "build": build,
                          "sample": f"{args.steps} full solves of the {args.size}^2 grid"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }

@@ -59,6 +59,32 @@ def lib():
     return _LIB
 
 
+_NATIVE = None
+
+
+def native_lib():
+    """The oracle built with -O3 -march=native for the host that runs it (compiled into a
+    temporary directory on first use, so a build never travels to another CPU), for timing
+    the CPU baseline; None when the compiler is unavailable."""
+    global _NATIVE
+    if _NATIVE is None:
+        import tempfile
+        out = os.path.join(tempfile.mkdtemp(prefix="gcut_oracle_"), "liboracle_native.so")
+        cmd = ["g++", "-O3", "-march=native", "-fopenmp", "-fPIC", "-std=c++17", "-shared",
+               "-o", out, os.path.join(_HERE, "gc_oracle.cpp")]
+        try:
+            subprocess.run(cmd, check=True, capture_output=True, timeout=300)
+        except (OSError, subprocess.SubprocessError):
+            _NATIVE = False
+            return None
+        L = ctypes.CDLL(out)
+        P = ctypes.c_void_p
+        L.orc_ref_tiled.argtypes = ([ctypes.c_int, ctypes.c_int] + [P] * 5 +
+                                    [ctypes.c_int, ctypes.c_longlong, ctypes.c_int, P, P, P])
+        _NATIVE = L
+    return _NATIVE or None
+
+
 def _p(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
@@ -81,15 +107,18 @@ def maxflow_bk(up, down, left, right, excess, return_excess=False):
     return (int(flow[0]), labels, fe) if return_excess else (int(flow[0]), labels)
 
 
-def ref_tiled(up, down, left, right, excess, bfs=5, max_iters=10 ** 7, threads=0):
-    """The reference schedule restated: (flow, labels, stats[iterations, relabels, bfs])."""
+def ref_tiled(up, down, left, right, excess, bfs=5, max_iters=10 ** 7, threads=0,
+              native=False):
+    """The reference schedule restated: (flow, labels, stats[iterations, relabels, bfs]).
+    native=True runs the -march=native build (native_lib) when it is available."""
     up, down, left, right, excess = map(_i32, (up, down, left, right, excess))
     h, w = excess.shape
     flow = np.zeros(1, np.int64)
     labels = np.zeros((h, w), np.uint8)
     stats = np.zeros(3, np.int64)
-    rc = lib().orc_ref_tiled(w, h, _p(up), _p(down), _p(left), _p(right), _p(excess), bfs,
-                             max_iters, threads, _p(flow), _p(labels), _p(stats))
+    L = (native_lib() if native else None) or lib()
+    rc = L.orc_ref_tiled(w, h, _p(up), _p(down), _p(left), _p(right), _p(excess), bfs,
+                         max_iters, threads, _p(flow), _p(labels), _p(stats))
     if rc != 0:
         raise RuntimeError(f"orc_ref_tiled failed ({rc})")
     return int(flow[0]), labels, stats
