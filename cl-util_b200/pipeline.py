@@ -12,6 +12,11 @@ two device staging slots, and copies the previous frame's packed labels back:
     for flow, bits in pipe.run(frames):      # frames: (rgba uint32 [H, W], excess int32 [H, W])
         ...                                  # bits: packed labels, GraphCut.unpack_labels(bits, W)
 
+A frame may carry two colour models instead of the t-links, (rgba, (fg, bg)) with
+gmm_tlinks.Mixture models: then only the image is copied (4 bytes per pixel) and the t-links
+are computed on the device (gc_tlinks_gmm), as the reference scores the image under its
+models on the device before the cut (GMM.score, test_GraphCut.py:44-47).
+
 Only copies overlap kernels; the solver's kernels never run concurrently with each other.
 Frames should be in pinned host memory (``torch.empty(..., pin_memory=True).numpy()``) for the
 copies to be asynchronous; pageable arrays work, with the copy done on the calling thread.
@@ -51,6 +56,7 @@ class SolvePipeline:
             self.landed = [ev() for _ in range(2)]     # packed labels are in host memory
             for e in self.consumed + self.landed:
                 e.record(self.compute)
+        self.models = [None, None]
         self._n = n
 
     def _host_i32(self, a):
@@ -64,15 +70,19 @@ class SolvePipeline:
 
     def _copy_in(self, j, rgba, excess):
         """Queues the host->device copies of one frame into slot j (after the slot's last
-        upload has read it)."""
+        upload has read it); colour models stay on the host until the t-links are built."""
         rgba = _as_rgba32(rgba)
-        if tuple(rgba.shape) != (self.height, self.width) or tuple(excess.shape) != (self.height, self.width):
+        models = isinstance(excess, tuple)
+        if tuple(rgba.shape) != (self.height, self.width) or \
+                (not models and tuple(excess.shape) != (self.height, self.width)):
             raise ValueError("frame shape differs from the pipeline's")
         with self.torch.cuda.stream(self.copy):
             self.copy.wait_event(self.consumed[j])
             self.stage_img[j].copy_(self._host_i32(rgba), non_blocking=True)
-            self.stage_exc[j].copy_(self._host_i32(excess), non_blocking=True)
+            if not models:
+                self.stage_exc[j].copy_(self._host_i32(excess), non_blocking=True)
             self.copied[j].record(self.copy)
+        self.models[j] = excess if models else None
 
     def run(self, frames):
         """Yields (flow, packed labels) for every (rgba, excess) frame, in order.  The packed
@@ -93,6 +103,10 @@ class SolvePipeline:
                 with torch.cuda.stream(self.compute):
                     self.compute.wait_event(self.copied[j])
                     self.compute.wait_event(self.landed[j])   # dbits[j] / hbits[j] are free
+                    if self.models[j] is not None:            # t-links from the two models
+                        import gmm_tlinks
+                        gmm_tlinks.tlinks(self.stage_img[j], *self.models[j],
+                                          out=self.stage_exc[j], stream=self.compute)
                     self.gc.upload_image(self.stage_img[j], self.stage_exc[j], stream=self.compute,
                                          lamda=self.lamda)
                     self.consumed[j].record(self.compute)
