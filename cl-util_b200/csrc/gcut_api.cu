@@ -797,6 +797,10 @@ struct Pool {
       return GC_OK;
     }));
     CK(cudaGraphInstantiate(&gexec[variant], g, 0));
+    // upload the executable graph here, under the construction lock, rather than implicitly
+    // at its first launch next to other threads' graph work
+    CK(cudaGraphUpload(gexec[variant], cap_stream));
+    CK(cudaStreamSynchronize(cap_stream));
     return GC_OK;
   }
 
