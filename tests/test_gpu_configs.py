@@ -95,3 +95,29 @@ def test_runtime_autotuner_on_the_device(cuda, tmp_path):
         gc.close()
     finally:
         autotune._default = old
+
+
+def test_solve_pipeline_frames_match_single_solves(cuda, oracle):
+    """SolvePipeline (copies of frame k+1 overlapping the solve of frame k) returns, frame by
+    frame and in order, the exact flow and cut of each frame: from (image, t-links) frames and
+    from (image, colour models) frames, with frames that differ from one another."""
+    import torch
+
+    from GraphCut import _as_rgba32, unpack_labels
+    from gmm_tlinks import Mixture
+    from pipeline import SolvePipeline
+    graphs = [synth.make_graph(300, 200, 900 + k, keep_image=True) for k in range(5)]
+    refs = [oracle.maxflow_bk(*g.planes()) for g in graphs]
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    frames = [(pin(_as_rgba32(g.image)), pin(g.excess)) for g in graphs]
+    with SolvePipeline(300, 200) as pipe:
+        out = list(pipe.run(frames + frames[::-1]))
+        assert len(out) == 10
+        for (f, bits), k in zip(out, list(range(5)) + list(range(4, -1, -1))):
+            assert f == refs[k][0], k
+            assert np.array_equal(unpack_labels(bits, 300), refs[k][1]), k
+        mframes = [(pin(_as_rgba32(g.image)), tuple(Mixture.from_components(c) for c in g.models))
+                   for g in graphs]
+        for (f, bits), k in zip(pipe.run(mframes), range(5)):
+            assert f == refs[k][0], k
+            assert np.array_equal(unpack_labels(bits, 300), refs[k][1]), k
