@@ -88,7 +88,6 @@ enum CtlSlot {
   CTL_NCHECK = 15,    // flood checks run (k_flood_check launches)
   CTL_NACT = 16,      // active-list rebuilds run (k_active_list launches)
   CTL_LEFT = 17,      // images still running after the last flood check
-  CTL_DTICKET = 18,   // next worklist position a discharge CTA takes (dynamic fetch)
   CTL_N = 64          // the control words fill 256 bytes; the per-image sums follow them
 };
 

@@ -345,35 +345,24 @@ k_masks(PoolView P) {
 // ------------------------------------------------------------------------------------
 // Discharge.  Thread (r, q) owns pixels (r, 4q .. 4q+3) of the tile.
 //
-// A sweep is: take the flow the other threads pushed into my pixels in the previous sweep,
-// push along every admissible edge (heights as they were at the start of the sweep), let
-// the flow between my own four pixels land at once, relabel (Jacobi), publish my pushes and
-// heights.  One barrier per sweep: the exchange arrays are double-buffered by sweep parity,
-// so a sweep writes one half while its neighbours may still read the other.  A pixel learns
-// of the flow other threads pushed into it only in the next sweep, so its relabel in this
-// sweep may not see the residual edges that flow created; a rise of at most 2 per sweep
-// keeps the labelling valid all the same (a neighbour u pushed into v only if h(u) =
-// h_start(v) + 1, so h(v) <= h_start(v) + 2 = h(u) + 1 on the new edge v -> u).
-//
-// Every pixel pushes and relabels, tile-edge pixels included, but a tile-edge pixel rises by
-// at most 2 above its height at the start of the launch.  A neighbouring CTA that pushes
-// into an edge pixel v saw either v's start height or its final height; with h_final(v) <=
-// h_start(v) + 2 every such push leaves a valid labelling (h(v) <= h(u) + 1 on the new
-// residual edge v -> u), and pushes out of the tile read the neighbour's height under the
-// same bound.  Flow leaving the tile is added to the neighbour's excess and reverse residual
-// with atomics at the end of the tile.
+// Every pixel pushes along all admissible edges and relabels, tile-edge pixels included,
+// but a tile-edge pixel rises by at most 2 above its height at the start of the launch.
+// A neighbouring CTA that pushes into an edge pixel v saw either v's start height or its
+// final height; with h_final(v) <= h_start(v) + 2 every such push leaves a valid labelling
+// (h(v) <= h(u) + 1 on the new residual edge v -> u), and pushes out of the tile read the
+// neighbour's height under the same bound.  Flow leaving the tile is added to the
+// neighbour's excess and reverse residual with atomics at the end of the tile.
 //
 // Active tiles form a worklist: the launch reads queue[c] (c = pulse parity, device-side)
 // and appends, deduplicated by inq[c ^ 1], every tile that is still active or received flow
-// to queue[c ^ 1]; the last CTA advances the parity.  CTAs take list positions from a
-// counter as they finish tiles, so the work spreads evenly.  One launch per pulse.
+// to queue[c ^ 1]; the last CTA advances the parity.  One launch per pulse, no compaction.
 // ------------------------------------------------------------------------------------
 struct DisSmem {
-  int32_t hs[2][GC_TILE_PX];   // heights published by a sweep, by sweep parity
-  int32_t fu[2][GC_TILE_PX];   // flow pushed up by each pixel in a sweep
-  int32_t fd[2][GC_TILE_PX];   // flow pushed down
-  int32_t fl[2][GC_TILE * 8];  // flow pushed left by the first pixel of each 4-pixel strip
-  int32_t fr[2][GC_TILE * 8];  // flow pushed right by the last pixel of each strip
+  int32_t hs[GC_TILE_PX];   // heights
+  int32_t fu[GC_TILE_PX];   // flow pushed up by each pixel this round
+  int32_t fd[GC_TILE_PX];   // flow pushed down
+  int32_t fl[GC_TILE * 8];  // flow pushed left by the first pixel of each 4-pixel strip
+  int32_t fr[GC_TILE * 8];  // flow pushed right by the last pixel of each strip
   int32_t hu[GC_TILE], hd[GC_TILE], hl[GC_TILE], hr[GC_TILE];  // halo heights
   // launch-start values of the tile-edge pixels that also receive atomics from the
   // neighbouring tiles (written back as deltas against these)
@@ -381,7 +370,6 @@ struct DisSmem {
   int32_t cu_top[GC_TILE], cd_bot[GC_TILE], cl_left[GC_TILE], cr_right[GC_TILE];
   // flow leaving the tile, per edge pixel, delivered at the end of the tile
   int32_t xu[GC_TILE], xd[GC_TILE], xl[GC_TILE], xr[GC_TILE];
-  int32_t next;                // the list position of the CTA's next tile
 };
 
 __device__ __forceinline__ void worklist_add(const PoolView& P, int nxt, int t) {
@@ -461,35 +449,18 @@ __device__ __forceinline__ void dis_prefetch(const PoolView& P, int t, int32_t* 
     bulk_g2s(buf + k * GC_TILE_PX, dis_plane(P, k) + (long long)t * GC_TILE_PX, GC_TILE_PX * 4, mbar);
 }
 
-// Takes the flow the neighbouring threads pushed into my pixels in a sweep (from the half
-// `b` of the exchange arrays): excess rises, and each receiving pixel gains the reverse
-// residual of the edge the flow came over.
-__device__ __forceinline__ void dis_gather(const DisSmem& S, int b, int r, int q, int pix,
-                                           int (&e)[4], int (&cu)[4], int (&cd)[4],
-                                           int (&cl)[4], int (&cr)[4]) {
-  const int4 a = r < 31 ? lds4(S.fu[b] + pix + GC_TILE) : make_int4(0, 0, 0, 0);   // from below
-  const int4 d = r > 0 ? lds4(S.fd[b] + pix - GC_TILE) : make_int4(0, 0, 0, 0);    // from above
-  const int fin_l = q > 0 ? S.fr[b][r * 8 + q - 1] : 0;   // from the strip on the left
-  const int fin_r = q < 7 ? S.fl[b][r * 8 + q + 1] : 0;   // from the strip on the right
-  e[0] += a.x + d.x + fin_l; cd[0] += a.x; cu[0] += d.x; cl[0] += fin_l;
-  e[1] += a.y + d.y;         cd[1] += a.y; cu[1] += d.y;
-  e[2] += a.z + d.z;         cd[2] += a.z; cu[2] += d.z;
-  e[3] += a.w + d.w + fin_r; cd[3] += a.w; cu[3] += d.w; cr[3] += fin_r;
-}
-
 __global__ void __launch_bounds__(DIS_THREADS, 4)
 k_discharge(PoolView P, int iters) {
   extern __shared__ __align__(128) int32_t dsm[];
   int32_t* const buf = dsm;                                    // [6][1024] staging
   DisSmem& S = *reinterpret_cast<DisSmem*>(dsm + DIS_PLANES * GC_TILE_PX);
   __shared__ uint64_t mbar;
-  __shared__ int s_cur, s_n, s_li;
+  __shared__ int s_cur, s_n;
   const int tid = threadIdx.x;
   const int r = tid >> 3, q = tid & 7, c0 = q * 4;
   if (tid == 0) {
     s_cur = *((volatile int32_t*)&P.ctl[CTL_PULSE]) & 1;
     s_n = *((volatile int32_t*)&P.qcount[s_cur]);
-    s_li = atomicAdd(&P.ctl[CTL_DTICKET], 1);
     mbar_init(&mbar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -505,12 +476,10 @@ k_discharge(PoolView P, int iters) {
   auto entry = [&](int li) { return P.queue[cur][li]; };
   const bool erow = (r == 0) || (r == 31);
   const int pix = r * GC_TILE + c0;
-  const int sq = r * 8 + q;
   unsigned phase = 0;
   bool failed = false, pending = false;
-  int li = s_li;
-  if (tid == 0 && li < n) dis_prefetch(P, entry(li), buf, &mbar);
-  while (li < n) {
+  if (tid == 0 && (int)blockIdx.x < n) dis_prefetch(P, entry(blockIdx.x), buf, &mbar);
+  for (int li = blockIdx.x; li < n; li += gridDim.x) {
     const int t = entry(li);
     const int4 nb = P.nbr[t];
     if (tid < 32) S.hu[tid] = nb.x >= 0 ? P.hgt[(long long)nb.x * GC_TILE_PX + 31 * GC_TILE + tid] : GC_HINF;
@@ -521,10 +490,7 @@ k_discharge(PoolView P, int iters) {
     else if (tid < 192) S.xd[tid - 160] = 0;
     else if (tid < 224) S.xl[tid - 192] = 0;
     else S.xr[tid - 224] = 0;
-    if (tid == 0) {
-      P.inq[cur][t] = 0;
-      S.next = atomicAdd(&P.ctl[CTL_DTICKET], 1);
-    }
+    if (tid == 0) P.inq[cur][t] = 0;
     const bool ok = mbar_wait(&mbar, phase);
     if (__syncthreads_or(!ok)) { failed = true; pending = true; break; }  // block-uniform
     phase ^= 1u;
@@ -556,30 +522,22 @@ k_discharge(PoolView P, int iters) {
       const bool edge = erow || c == 0 || c == 31;
       hcap[j] = edge ? (h[j] >= GC_HINF - 2 ? GC_HINF : h[j] + 2) : GC_HINF;
     }
-    // sweep 0 reads the launch-start heights and no inflow
-    sts4(S.hs[0] + pix, h[0], h[1], h[2], h[3]);
-    sts4(S.fu[0] + pix, 0, 0, 0, 0);
-    sts4(S.fd[0] + pix, 0, 0, 0, 0);
-    S.fl[0][sq] = 0;
-    S.fr[0][sq] = 0;
+    sts4(S.hs + pix, h[0], h[1], h[2], h[3]);
     __syncthreads();   // every thread has its values in registers: the buffer is free
-    const int nli = S.next;
     // prefetch this CTA's next tile into the buffer while this one is worked on
-    if (tid == 0 && nli < n) dis_prefetch(P, entry(nli), buf, &mbar);
+    if (tid == 0 && li + (int)gridDim.x < n) dis_prefetch(P, entry(li + gridDim.x), buf, &mbar);
 
-    int b = 0;   // the half of the exchange arrays the current sweep reads
     for (int it = 0; it < iters; ++it) {
-      dis_gather(S, b, r, q, pix, e, cu, cd, cl, cr);
-      // neighbour heights at the start of the sweep
+      // neighbour heights (fixed during the push phase)
       int hnu[4], hnd[4], hnl[4], hnr[4];
-      if (r > 0) { const int4 v = lds4(S.hs[b] + pix - GC_TILE); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
+      if (r > 0) { const int4 v = lds4(S.hs + pix - GC_TILE); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
       else { const int4 v = lds4(S.hu + c0); hnu[0] = v.x; hnu[1] = v.y; hnu[2] = v.z; hnu[3] = v.w; }
-      if (r < 31) { const int4 v = lds4(S.hs[b] + pix + GC_TILE); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
+      if (r < 31) { const int4 v = lds4(S.hs + pix + GC_TILE); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
       else { const int4 v = lds4(S.hd + c0); hnd[0] = v.x; hnd[1] = v.y; hnd[2] = v.z; hnd[3] = v.w; }
-      hnl[0] = c0 > 0 ? S.hs[b][pix - 1] : S.hl[r];
+      hnl[0] = c0 > 0 ? S.hs[pix - 1] : S.hl[r];
       hnl[1] = h[0]; hnl[2] = h[1]; hnl[3] = h[2];
       hnr[0] = h[1]; hnr[1] = h[2]; hnr[2] = h[3];
-      hnr[3] = c0 < 28 ? S.hs[b][pix + 4] : S.hr[r];
+      hnr[3] = c0 < 28 ? S.hs[pix + 4] : S.hr[r];
 
       // push phase.  `rem` marks pixels that still hold excess after pushing: every
       // admissible edge of theirs is then saturated, and inflow only adds residual towards
@@ -607,12 +565,6 @@ k_discharge(PoolView P, int iters) {
           }
         }
       }
-      // flow between my own pixels lands now, with its reverse residual
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        e[j + 1] += orr[j]; cl[j + 1] += orr[j];
-        e[j] += ol[j + 1]; cr[j] += ol[j + 1];
-      }
       // flow leaving the tile is delivered at the end of the tile
       if (r == 0) {
 #pragma unroll
@@ -624,12 +576,31 @@ k_discharge(PoolView P, int iters) {
       }
       if (q == 0) { S.xl[r] += ol[0]; ol[0] = 0; }
       if (q == 7) { S.xr[r] += orr[3]; orr[3] = 0; }
-      sts4(S.fu[b ^ 1] + pix, ou[0], ou[1], ou[2], ou[3]);
-      sts4(S.fd[b ^ 1] + pix, od[0], od[1], od[2], od[3]);
-      S.fl[b ^ 1][sq] = ol[0];
-      S.fr[b ^ 1][sq] = orr[3];
-      // relabel phase (Jacobi on the sweep-start heights; at most +2 per sweep, and
-      // tile-edge pixels at most hcap)
+      sts4(S.fu + pix, ou[0], ou[1], ou[2], ou[3]);
+      sts4(S.fd + pix, od[0], od[1], od[2], od[3]);
+      S.fl[r * 8 + q] = ol[0];
+      S.fr[r * 8 + q] = orr[3];
+      __syncthreads();
+      // gather inflow; a pixel receiving flow gains the reverse residual
+      {
+        const int4 a = r < 31 ? lds4(S.fu + pix + GC_TILE) : make_int4(0, 0, 0, 0);
+        const int4 bb = r > 0 ? lds4(S.fd + pix - GC_TILE) : make_int4(0, 0, 0, 0);
+        const int fb[4] = {a.x, a.y, a.z, a.w}, fa[4] = {bb.x, bb.y, bb.z, bb.w};
+        int fromleft[4], fromright[4];
+        fromleft[0] = q > 0 ? S.fr[r * 8 + q - 1] : 0;
+        fromleft[1] = orr[0]; fromleft[2] = orr[1]; fromleft[3] = orr[2];
+        fromright[0] = ol[1]; fromright[1] = ol[2]; fromright[2] = ol[3];
+        fromright[3] = q < 7 ? S.fl[r * 8 + q + 1] : 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          e[j] += fb[j] + fa[j] + fromleft[j] + fromright[j];
+          cd[j] += fb[j];
+          cu[j] += fa[j];
+          cl[j] += fromleft[j];
+          cr[j] += fromright[j];
+        }
+      }
+      // relabel phase (Jacobi; tile-edge pixels are capped at hcap)
       int nh[4] = {h[0], h[1], h[2], h[3]};
       const bool any_need = (e[0] > 0 && h[0] < hcap[0]) || (e[1] > 0 && h[1] < hcap[1]) ||
                             (e[2] > 0 && h[2] < hcap[2]) || (e[3] > 0 && h[3] < hcap[3]);
@@ -647,20 +618,19 @@ k_discharge(PoolView P, int iters) {
               if (cu[j] > 0) m = imin(m, hnu[j] + 1);
               if (cr[j] > 0) m = imin(m, hnr[j] + 1);
               if (cl[j] > 0) m = imin(m, hnl[j] + 1);
-              nh[j] = imin(imin(m, hcap[j]), h[j] + 2);
+              nh[j] = imin(imin(m, GC_HINF), hcap[j]);
               changed |= nh[j] != h[j];
             }
           }
         }
       }
+      // every read of S.hs in this iteration happened before the flow barrier above, so the
+      // new heights can be written now; the next reads follow the barrier below
 #pragma unroll
       for (int j = 0; j < 4; ++j) h[j] = nh[j];
-      sts4(S.hs[b ^ 1] + pix, h[0], h[1], h[2], h[3]);
-      b ^= 1;
+      sts4(S.hs + pix, h[0], h[1], h[2], h[3]);
       if (!__syncthreads_or(changed)) break;
     }
-    // the flow the last sweep pushed between threads
-    dis_gather(S, b, r, q, pix, e, cu, cd, cl, cr);
 
     // write back: interior values are owned by this CTA; tile-edge excess and the
     // outward residual of edge pixels also receive atomics from neighbouring tiles, so
@@ -761,8 +731,7 @@ k_discharge(PoolView P, int iters) {
     if (sent_d) { P.touched[nb.y] = 1; mark_dirty(P, nb.y); worklist_add(P, nxt, nb.y); }
     if (sent_l) { P.touched[nb.z] = 1; mark_dirty(P, nb.z); worklist_add(P, nxt, nb.z); }
     if (sent_r) { P.touched[nb.w] = 1; mark_dirty(P, nb.w); worklist_add(P, nxt, nb.w); }
-    // the block-wide reductions also order every read of this tile's shared memory before
-    // the next tile's writes
+    // the block-wide reductions also order every read of this buffer before its reuse
     const int any_act = __syncthreads_or(act);
     act_int = __syncthreads_or(act_int);
     if (tid == 0) {
@@ -772,7 +741,6 @@ k_discharge(PoolView P, int iters) {
       if (any_act) worklist_add(P, nxt, t);
       if (P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
     }
-    li = nli;
   }
   if (failed) {
     // a bulk copy did not complete in time: record it, let our copy drain, stop
@@ -791,7 +759,6 @@ k_discharge(PoolView P, int iters) {
       P.qcount[cur] = 0;
       P.ctl[CTL_PULSE] = P.ctl[CTL_PULSE] + 1;
       P.ctl[CTL_DDONE] = 0;
-      P.ctl[CTL_DTICKET] = 0;
       __threadfence();
     }
   }
