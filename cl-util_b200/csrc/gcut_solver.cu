@@ -373,6 +373,7 @@ struct DisSmem {
 };
 
 __device__ __forceinline__ void worklist_add(const PoolView& P, int nxt, int t) {
+  if (*((volatile int32_t*)&P.inq[nxt][t]) != 0) return;   // common case: already queued
   if (atomicExch(&P.inq[nxt][t], 1) == 0) {
     const int pos = atomicAdd(&P.qcount[nxt], 1);
     if (pos < P.nt) P.queue[nxt][pos] = t;   // inq deduplicates, so pos < nt always holds
@@ -455,7 +456,7 @@ k_discharge(PoolView P, int iters) {
   int32_t* const buf = dsm;                                    // [6][1024] staging
   DisSmem& S = *reinterpret_cast<DisSmem*>(dsm + DIS_PLANES * GC_TILE_PX);
   __shared__ uint64_t mbar;
-  __shared__ int s_cur, s_n;
+  __shared__ int s_cur, s_n, s_sent;
   const int tid = threadIdx.x;
   const int r = tid >> 3, q = tid & 7, c0 = q * 4;
   if (tid == 0) {
@@ -490,7 +491,7 @@ k_discharge(PoolView P, int iters) {
     else if (tid < 192) S.xd[tid - 160] = 0;
     else if (tid < 224) S.xl[tid - 192] = 0;
     else S.xr[tid - 224] = 0;
-    if (tid == 0) P.inq[cur][t] = 0;
+    if (tid == 0) { P.inq[cur][t] = 0; s_sent = 0; }
     const bool ok = mbar_wait(&mbar, phase);
     if (__syncthreads_or(!ok)) { failed = true; pending = true; break; }  // block-uniform
     phase ^= 1u;
@@ -727,19 +728,22 @@ k_discharge(PoolView P, int iters) {
       act |= a;
       act_int |= a && !erow && c > 0 && c < 31;
     }
-    if (sent_u) { P.touched[nb.x] = 1; mark_dirty(P, nb.x); worklist_add(P, nxt, nb.x); }
-    if (sent_d) { P.touched[nb.y] = 1; mark_dirty(P, nb.y); worklist_add(P, nxt, nb.y); }
-    if (sent_l) { P.touched[nb.z] = 1; mark_dirty(P, nb.z); worklist_add(P, nxt, nb.z); }
-    if (sent_r) { P.touched[nb.w] = 1; mark_dirty(P, nb.w); worklist_add(P, nxt, nb.w); }
+    const int sent = (sent_u ? 1 : 0) | (sent_d ? 2 : 0) | (sent_l ? 4 : 0) | (sent_r ? 8 : 0);
+    if (sent) atomicOr(&s_sent, sent);
     // the block-wide reductions also order every read of this buffer before its reuse
     const int any_act = __syncthreads_or(act);
     act_int = __syncthreads_or(act_int);
-    if (tid == 0) {
-      P.touched[t] = 1;
-      mark_dirty(P, t);
-      P.act_int[t] = act_int;
-      if (any_act) worklist_add(P, nxt, t);
-      if (P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
+    // the tile itself (lane 0) and the neighbours that received flow (lanes 1-4), in parallel
+    if (tid < 5) {
+      const int bits = s_sent;
+      const int target = tid == 0 ? t : tid == 1 ? nb.x : tid == 2 ? nb.y : tid == 3 ? nb.z : nb.w;
+      if (tid == 0 || ((bits >> (tid - 1)) & 1)) {
+        P.touched[target] = 1;
+        mark_dirty(P, target);
+        if (tid == 0) P.act_int[t] = act_int;
+        if (tid != 0 || any_act) worklist_add(P, nxt, target);
+        if (tid == 0 && P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
+      }
     }
   }
   if (failed) {
