@@ -386,6 +386,18 @@ def main():
         mpix_all = world * args.steps * W * H / 1e6
         value = mpix_all / (total_ms / 1000)
 
+        # the graph-mode timeline from the device-side trace (kernel start stamps inside the
+        # CUDA graph, which host profilers do not list): one solve, outside the timed region
+        import _gcut
+        flush.fill_(1)
+        stream.synchronize()
+        gc.set_trace(True, stream=stream)
+        step()
+        trace = gc.trace(stream=stream)
+        gc.set_trace(False, stream=stream)
+        timeline = {k: [v[0], round(v[1] / 1000, 2)] for k, v in _gcut.trace_summary(trace).items()}
+        timeline_total = round((trace[-1][1] - trace[0][1]) / 1000, 2) if len(trace) > 1 else None
+
         # per-kernel CUDA-event timing (host-driven loop, same kernels) for the roofline
         gc.set_profile(True)
         prof_tot = {}
@@ -575,6 +587,9 @@ def main():
             "e2e_image_and_models": e2e_models,
             "gpu_launches": launches,
             "ms_per_step_host_driven": sum(prof_ms) / len(prof_ms),
+            "graph_timeline_us": {"kernels": timeline, "upload_start_to_labels_start": timeline_total,
+                                  "how": "device-side trace of one graph solve: per kernel kind "
+                                         "[launches, us from its start to the next kernel's start]"},
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,

@@ -280,6 +280,14 @@ class GraphCut:
     def profile(self) -> dict:
         return _gcut.kernel_profile(lib().gc_get_profile, self._h)
 
+    def set_trace(self, on: bool, stream=None):
+        """Device-side trace of the following solves (gc_set_trace): see trace()."""
+        check(lib().gc_set_trace(self._h, int(on), stream_handle(stream)))
+
+    def trace(self, stream=None):
+        """[(kernel kind, start ns)] recorded since set_trace(True), in launch order."""
+        return _gcut.read_trace(lib().gc_get_trace, self._h, stream)
+
     def set_collect_stats(self, on: bool):
         check(lib().gc_set_collect_stats(self._h, int(on)))
 

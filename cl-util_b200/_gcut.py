@@ -104,6 +104,12 @@ SIGNATURES = {
     "gc_edit_brush": [_P, _P, _P, _I, _I, _I32, _P],
     "gc_download_state": [_P] * 7 + [_P],
     "gc_get_stats": [_P, _P],
+    "gc_set_trace": [_P, _I, _P],
+    "gc_get_trace": [_P, _P, _I, _P, _P],
+    "gcb_set_trace": [_P, _I, _P],
+    "gcb_get_trace": [_P, _P, _I, _P, _P],
+    "gcp_set_trace": [_P, _I, _P],
+    "gcp_get_trace": [_P, _P, _I, _P, _P],
     "gc_set_collect_stats": [_P, _I],
     "gc_set_profile": [_P, _I],
     "gc_get_profile": [_P, _P, _I],
@@ -236,6 +242,34 @@ def ptr(t):
     if hasattr(t, "data_ptr"):
         return ctypes.c_void_p(t.data_ptr())
     return t.ctypes.data_as(ctypes.c_void_p)
+
+
+TRACE_KINDS = ("begin", "active_list", "discharge", "masks", "flood_first", "flood", "check",
+               "bfs_first", "bfs", "upload", "labels", "end")
+GC_TRACE_MAX = 2048
+
+
+def read_trace(get_fn, handle, stream=None):
+    """[(kind name, start ns)] of a handle's device-side trace (gc_get_trace and kin)."""
+    import numpy as np
+    buf = np.zeros(2 * GC_TRACE_MAX, np.uint64)
+    n = ctypes.c_int(0)
+    check(get_fn(handle, buf.ctypes.data_as(ctypes.c_void_p), GC_TRACE_MAX, ctypes.byref(n),
+                 stream_handle(stream)))
+    k = min(n.value, GC_TRACE_MAX)
+    return [(TRACE_KINDS[int(buf[2 * i + 1])] if int(buf[2 * i + 1]) < len(TRACE_KINDS)
+             else str(int(buf[2 * i + 1])), int(buf[2 * i])) for i in range(k)]
+
+
+def trace_summary(entries):
+    """{kind: [count, total ns]} from consecutive start times (each kernel's span runs to the
+    next entry's start; the last entry closes the trace)."""
+    out = {}
+    for (k, t0), (_, t1) in zip(entries, entries[1:]):
+        a = out.setdefault(k, [0, 0])
+        a[0] += 1
+        a[1] += t1 - t0
+    return out
 
 
 def kernel_profile(get_fn, handle) -> dict:

@@ -290,6 +290,8 @@ struct Pool {
     c.take(&P.ctl, CTL_N);
     c.take(&acc, imgs.size());
     c.take(&ktiles, GC_NKERN);
+    c.take(&P.trace, 2 * GC_TRACE_MAX);
+    c.take(&P.trace_ctl, 2);
     // look-back slots: the scan uses one per 4096 items, the list rebuild one per 64 tiles
     const int chunks = scan_chunks(nt) > nt / 64 + 1 ? scan_chunks(nt) : nt / 64 + 1;
     c.take(&scan.st.status, chunks);
@@ -932,6 +934,31 @@ struct Pool {
     return timed(K_LABELS, s, [&] { return launch_labels_out(P, imgs[i], out, s); });
   }
 
+  // device-side trace: on/off and a fresh start (ordered on the stream)
+  int set_trace(int on, cudaStream_t s) {
+    CK(cudaSetDevice(device));
+    int32_t* w = reinterpret_cast<int32_t*>(static_cast<char*>(pin) + 64);
+    CK(cudaStreamSynchronize(s));   // the words' previous copy has been read
+    w[0] = on ? 1 : 0;
+    w[1] = 0;
+    CK(cudaMemcpyAsync(P.trace_ctl, w, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return GC_OK;
+  }
+
+  int get_trace(unsigned long long* out, int max, int* n, cudaStream_t s) {
+    if (!n || max < 0 || (max > 0 && !out)) return fail(GC_ERR_INVALID, "bad argument");
+    CK(cudaSetDevice(device));
+    int32_t cnt[2];
+    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpy(cnt, P.trace_ctl, sizeof(cnt), cudaMemcpyDeviceToHost));
+    const int have = cnt[1] < GC_TRACE_MAX ? cnt[1] : GC_TRACE_MAX;
+    *n = cnt[1];
+    const int k = have < max ? have : max;
+    if (k > 0) CK(cudaMemcpy(out, P.trace, sizeof(unsigned long long) * 2 * k, cudaMemcpyDeviceToHost));
+    return GC_OK;
+  }
+
   int labels_packed(int i, uint8_t* out, cudaStream_t s) {
     if (i < 0 || i >= (int)imgs.size() || !out) return fail(GC_ERR_INVALID, "bad argument");
     if (!img_solved[i]) return fail(GC_ERR_STATE, "labels before solve");
@@ -1389,6 +1416,32 @@ int gc_is_completed(gc_handle* h, int* completed, void* stream) {
   return r;
 }
 
+int gc_set_trace(gc_handle* h, int on, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  return h->pool.set_trace(on, (cudaStream_t)stream);
+}
+
+int gc_get_trace(gc_handle* h, uint64_t* entries, int max_entries, int* n, void* stream) {
+  g_err.clear();
+  if (!h) return fail(GC_ERR_INVALID, "null handle");
+  return h->pool.get_trace(reinterpret_cast<unsigned long long*>(entries), max_entries, n,
+                           (cudaStream_t)stream);
+}
+
+int gcb_set_trace(gcb_handle* b, int on, void* stream) {
+  g_err.clear();
+  if (!b) return fail(GC_ERR_INVALID, "null handle");
+  return b->pool.set_trace(on, (cudaStream_t)stream);
+}
+
+int gcb_get_trace(gcb_handle* b, uint64_t* entries, int max_entries, int* n, void* stream) {
+  g_err.clear();
+  if (!b) return fail(GC_ERR_INVALID, "null handle");
+  return b->pool.get_trace(reinterpret_cast<unsigned long long*>(entries), max_entries, n,
+                           (cudaStream_t)stream);
+}
+
 int gc_get_stats(const gc_handle* h, gc_stats* st) {
   if (!h || !st) return fail(GC_ERR_INVALID, "null argument");
   *st = h->pool.stats;
@@ -1792,6 +1845,19 @@ int gcp_labels_packed(gcp_handle* p, int slot, uint8_t* bits, void* stream) {
   const int r = p->pool.labels_packed(slot, bits, (cudaStream_t)stream);
   p->pool.track((cudaStream_t)stream);
   return r;
+}
+
+int gcp_set_trace(gcp_handle* p, int on, void* stream) {
+  g_err.clear();
+  if (!p) return fail(GC_ERR_INVALID, "null handle");
+  return p->pool.set_trace(on, (cudaStream_t)stream);
+}
+
+int gcp_get_trace(gcp_handle* p, uint64_t* entries, int max_entries, int* n, void* stream) {
+  g_err.clear();
+  if (!p) return fail(GC_ERR_INVALID, "null handle");
+  return p->pool.get_trace(reinterpret_cast<unsigned long long*>(entries), max_entries, n,
+                           (cudaStream_t)stream);
 }
 
 int gcp_get_stats(const gcp_handle* p, gc_stats* st) {

@@ -62,6 +62,10 @@ struct PoolView {
   int32_t* sel_mode;      // [nimg] img_mode of the range's image
   int32_t* nsel;          // [2] ranges, selected tiles in all
   unsigned long long* ktiles;  // [K_COUNT] tiles processed per kernel kind (profiling)
+  // device-side trace of the solve: trace_ctl[0] on, trace_ctl[1] entries written; entry i
+  // is (start time in ns of %globaltimer, kind) in trace[2i], trace[2i + 1]
+  unsigned long long* trace;
+  int32_t* trace_ctl;
 };
 
 // Device-side loop control words.  The last CTA of every frontier round advances the round
@@ -119,6 +123,30 @@ struct SelCursor {
 __device__ __forceinline__ void record_bad(const PoolView& P, int where, int value) {
   if (atomicCAS(&P.ctl[CTL_BADWHERE], 0, where) == 0) P.ctl[CTL_BAD] = value;
   atomicCAS(&P.ctl[CTL_ERR], 0, 4);
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Kinds of the device-side trace (gc_set_trace); the values are part of the C ABI.
+enum TraceKind { TR_BEGIN = 0, TR_ACTIVE_LIST, TR_DISCHARGE, TR_MASKS, TR_FLOOD_FIRST, TR_FLOOD,
+                 TR_CHECK, TR_BFS_FIRST, TR_BFS, TR_UPLOAD, TR_LABELS, TR_END };
+#ifndef GC_TRACE_MAX
+#define GC_TRACE_MAX 2048
+#endif
+
+// Records the start of a kernel in the solve's trace (CTA 0, thread 0, when tracing is on).
+__device__ __forceinline__ void trace_mark(const PoolView& P, int kind) {
+  if (blockIdx.x != 0 || threadIdx.x != 0 || !P.trace_ctl) return;
+  if (*((volatile int32_t*)&P.trace_ctl[0]) == 0) return;
+  const int i = atomicAdd(&P.trace_ctl[1], 1);
+  if (i < GC_TRACE_MAX) {
+    P.trace[2 * i] = global_ns();
+    P.trace[2 * i + 1] = (unsigned long long)kind;
+  }
 }
 
 // Kernel kinds for profiling (launch counts, event time, tiles processed).

@@ -222,6 +222,7 @@ __global__ void k_nlink_table(const unsigned long long* __restrict__ sum, long l
 template <class Source>
 __global__ void __launch_bounds__(DIS_THREADS)
 k_upload(PoolView P, ImageDesc im, int img, Source src, int32_t* __restrict__ tl, ImageAcc* acc) {
+  trace_mark(P, TR_UPLOAD);
   __shared__ int32_t s_tab[GC_NLINK_LEVELS];
   src.prepare(s_tab);
   __syncthreads();
@@ -291,6 +292,7 @@ k_upload(PoolView P, ImageDesc im, int img, Source src, int32_t* __restrict__ tl
 // last of them empties the list.
 __global__ void __launch_bounds__(DIS_THREADS)
 k_masks(PoolView P) {
+  trace_mark(P, TR_MASKS);
   __shared__ int s_n;
   __shared__ long long wpos[DIS_THREADS / 32];
   if (threadIdx.x == 0) {
@@ -409,11 +411,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, unsigned parity) {
                : "=r"(ok) : "r"(a), "r"(parity) : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
 // A tile copy normally lands in microseconds; a wait gives up after this long.  The bound
 // is on time, not on polls: try_wait may return at once, and a poll count then would allow
 // only milliseconds under load (a CTA that gave up early would leave while its copy is
@@ -452,6 +449,7 @@ __device__ __forceinline__ void dis_prefetch(const PoolView& P, int t, int32_t* 
 
 __global__ void __launch_bounds__(DIS_THREADS, 4)
 k_discharge(PoolView P, int iters) {
+  trace_mark(P, TR_DISCHARGE);
   extern __shared__ __align__(128) int32_t dsm[];
   int32_t* const buf = dsm;                                    // [6][1024] staging
   DisSmem& S = *reinterpret_cast<DisSmem*>(dsm + DIS_PLANES * GC_TILE_PX);
@@ -1024,6 +1022,7 @@ __device__ __forceinline__ void frontier_round_end(const PoolView& P, int first,
 // selection take their mode for this solve and restart their flow sums (the others keep
 // their results).  One CTA.
 __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc* acc) {
+  trace_mark(P, TR_BEGIN);
   for (int i = threadIdx.x; i < CTL_N; i += blockDim.x) P.ctl[i] = 0;
   for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) {
     P.img_live[i] = 0;
@@ -1065,6 +1064,7 @@ constexpr int ACT_CHUNK = ACT_THREADS * ACT_ITEMS;
 __global__ void __launch_bounds__(ACT_THREADS)
 k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
               int count_cycle, int filter, cudaGraphConditionalHandle h, ImageAcc* acc) {
+  trace_mark(P, TR_ACTIVE_LIST);
   __shared__ int32_t sm[32];
   __shared__ int32_t s_chunk, s_excl, s_cur, s_n, s_nr;
   __shared__ uint32_t s_tag;
@@ -1185,6 +1185,7 @@ __global__ void k_ctl_cycle(PoolView P, const int32_t* count, int count_cycle,
 
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
 k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
+  trace_mark(P, first ? TR_BFS_FIRST : TR_BFS);
   __shared__ int32_t tr[WARPS_PER_CTA][32 * 33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int in = frontier_round_number(P, first) & 1, out = in ^ 1;
@@ -1294,6 +1295,7 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
 k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h, ImageAcc* acc) {
+  trace_mark(P, mode ? TR_FLOOD_FIRST : TR_FLOOD);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int first = mode != 0;
   const int in = frontier_round_number(P, first) & 1, out = in ^ 1;
@@ -1378,6 +1380,7 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
 // the last cycle of a solve is counted here.  One CTA.
 __global__ void k_flood_check(PoolView P, int all, cudaGraphConditionalHandle hbfs,
                               cudaGraphConditionalHandle hmain) {
+  trace_mark(P, TR_CHECK);
   __shared__ int s_left;
   if (threadIdx.x == 0) s_left = 0;
   __syncthreads();
@@ -1404,6 +1407,7 @@ __global__ void k_flood_check(PoolView P, int all, cudaGraphConditionalHandle hb
   __threadfence();
   if (hbfs) cudaGraphSetConditional(hbfs, n > 0 ? 1u : 0u);
   if (hmain && n == 0) cudaGraphSetConditional(hmain, 0u);
+  if (n == 0) trace_mark(P, TR_END);
 }
 
 // Neighbour tile ids and image index of one image's tiles (row-major from im.tile0), for an
@@ -1420,6 +1424,7 @@ __global__ void k_image_tiles(PoolView P, ImageDesc im, int img) {
 // Labels of one image, row-major, padding excluded.  One thread writes the 32 pixels of
 // one tile row (one mask word); consecutive threads take consecutive tiles of an image row.
 __global__ void k_labels_out(PoolView P, ImageDesc im, uint8_t* __restrict__ out) {
+  trace_mark(P, TR_LABELS);
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)im.H * im.tw) return;
   const int y = (int)(i / im.tw), tx = (int)(i % im.tw);
@@ -1443,6 +1448,7 @@ __global__ void k_labels_out(PoolView P, ImageDesc im, uint8_t* __restrict__ out
 // (row stride (W + 7) / 8 bytes, little bit order).  Pixels of a ragged tile beyond the
 // image have no capacities and no excess, so their reach bits are 0.
 __global__ void k_labels_packed(PoolView P, ImageDesc im, uint8_t* __restrict__ out) {
+  trace_mark(P, TR_LABELS);
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)im.H * im.tw) return;
   const int y = (int)(i / im.tw), tx = (int)(i % im.tw);

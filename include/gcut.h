@@ -290,6 +290,20 @@ int gc_set_profile(gc_handle* h, int on);
 int gc_get_profile(const gc_handle* h, gc_kernel_prof* out, int n);
 const char* gc_kernel_name(int kind);
 
+/* Device-side trace of the solves, for looking inside a CUDA-graph solve (whose kernels a
+   host profiler does not list): while on, the first thread of every solver kernel appends
+   (start time in ns of the GPU's global timer, kind) to a buffer of GC_TRACE_MAX entries in
+   the handle's memory; the difference of consecutive start times is a kernel's duration
+   including its launch.  Kinds: 0 solve start, 1 active-tile list, 2 discharge, 3 mask
+   rebuild, 4 flood first round, 5 flood round, 6 flood check, 7 BFS first round, 8 BFS
+   round, 9 upload, 10 labels, 11 solve end.  gc_set_trace turns it on or off and empties
+   the buffer; gc_get_trace copies up to max_entries entries (two uint64 each) and sets *n
+   to the number written since (it may exceed the buffer).  Both synchronise `stream`.
+   No counterpart in the reference (its host loop timed kernels with OpenCL events). */
+#define GC_TRACE_MAX 2048
+int gc_set_trace(gc_handle* h, int on, void* stream);
+int gc_get_trace(gc_handle* h, uint64_t* entries, int max_entries, int* n, void* stream);
+
 /* Message of the last error on this thread ("" if none). */
 const char* gc_last_error(void);
 
@@ -396,6 +410,8 @@ int gcb_labels(gcb_handle* b, int i, uint8_t* labels, void* stream);
 int gcb_get_stats(const gcb_handle* b, gc_stats* stats);
 int gcb_set_profile(gcb_handle* b, int on);
 int gcb_get_profile(const gcb_handle* b, gc_kernel_prof* out, int n);
+int gcb_set_trace(gcb_handle* b, int on, void* stream);
+int gcb_get_trace(gcb_handle* b, uint64_t* entries, int max_entries, int* n, void* stream);
 
 /* ---- session pools: many resident images, solved together a few at a time ------------
    A pool of max_tiles 32x32 tiles and max_sessions image slots in one arena.  An image
@@ -439,6 +455,8 @@ int gcp_flow(gcp_handle* p, int slot, int64_t* flow);
 int gcp_labels(gcp_handle* p, int slot, uint8_t* labels, void* stream);
 int gcp_labels_packed(gcp_handle* p, int slot, uint8_t* bits, void* stream);
 int gcp_get_stats(const gcp_handle* p, gc_stats* stats);
+int gcp_set_trace(gcp_handle* p, int on, void* stream);
+int gcp_get_trace(gcp_handle* p, uint64_t* entries, int max_entries, int* n, void* stream);
 
 #ifdef __cplusplus
 }

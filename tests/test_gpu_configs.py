@@ -121,3 +121,31 @@ def test_solve_pipeline_frames_match_single_solves(cuda, oracle):
         for (f, bits), k in zip(pipe.run(mframes), range(5)):
             assert f == refs[k][0], k
             assert np.array_equal(unpack_labels(bits, 300), refs[k][1]), k
+
+
+def test_device_trace_of_a_graph_solve(cuda):
+    """The device-side trace sees inside a CUDA-graph solve: upload, solve start, active list,
+    discharge pulses, mask rebuild, flood rounds, the flood check and the solve's end, in
+    launch order with increasing stamps; off, it records nothing."""
+    import _gcut
+    g = synth.make_graph(512, 512, 21)
+    with GraphCut(g.width, g.height) as gc:
+        gc.set_trace(True)
+        gc.upload_capacities(*g.planes())
+        gc.cut()
+        gc.labels()
+        tr = gc.trace()
+        kinds = [k for k, _ in tr]
+        assert kinds[0] == "upload" and kinds[1] == "begin" and kinds[-1] == "labels"
+        assert "end" in kinds and kinds.index("end") < kinds.index("labels")
+        assert kinds.count("discharge") == gc.stats()["pulses"]
+        for k in ("active_list", "masks", "flood_first", "check"):
+            assert k in kinds, k
+        stamps = [t for _, t in tr]
+        assert all(b >= a for a, b in zip(stamps, stamps[1:]))
+        summ = _gcut.trace_summary(tr)
+        assert summ["discharge"][0] == kinds.count("discharge")
+        gc.set_trace(False)
+        gc.upload_capacities(*g.planes())
+        gc.cut()
+        assert gc.trace() == []
