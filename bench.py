@@ -349,8 +349,7 @@ def main():
 
     def step():
         gc.upload_capacities(*dev_planes, stream=stream)
-        gc.cut(stream=stream)
-        gc.labels(out=labels, stream=stream)
+        gc.cut_labels(out=labels, stream=stream)   # solve + labels, one host wait
         return gc.flow
 
     with torch.cuda.stream(stream):
@@ -577,6 +576,9 @@ def main():
                        "l2": "flushed between steps (256 MiB write, outside the timed region)",
                        "parallelism": f"replicas x{world}",
                        "loop": "host-driven" if args.host_driven else "one CUDA graph per solve",
+                       "step": "GraphCut.upload_capacities from device planes, then "
+                               "GraphCut.cut_labels (gc_solve_labels: the solve and the labels "
+                               "into device memory, one host wait)",
                        "solver": {"discharge_iters": gc.opts.discharge_iters,
                                   "pulses_per_relabel": gc.opts.pulses_per_relabel,
                                   "initial_relabel": gc.opts.initial_relabel}},

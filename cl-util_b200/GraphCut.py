@@ -210,6 +210,19 @@ class GraphCut:
         self._solved = True
         return self
 
+    def cut_labels(self, out=None, packed=False, stream=None):
+        """cut() and labels() (or labels_packed() with packed=True) in one call with one host
+        wait: the labels kernel follows the solve on the stream (gc_solve_labels).  Returns
+        the label tensor."""
+        import torch
+        if out is None:
+            shape = (self.height, (self.width + 7) // 8) if packed else (self.height, self.width)
+            out = torch.empty(shape, dtype=torch.uint8, device=self.device)
+        with torch.cuda.device(self.device):
+            check(lib().gc_solve_labels(self._h, ptr(out), int(bool(packed)), stream_handle(stream)))
+        self._solved = True
+        return out
+
     def push(self, stream=None):
         check(lib().gc_push(self._h, stream_handle(stream)))
 

@@ -90,6 +90,7 @@ SIGNATURES = {
     "gc_gmm_fit": [_P, _I, _I, _I, ctypes.c_double, ctypes.c_double, ctypes.c_double, _I,
                    _P, _P],
     "gc_solve": [_P, _P],
+    "gc_solve_labels": [_P, _P, _I, _P],
     "gc_push": [_P, _P],
     "gc_relabel": [_P, _P],
     "gc_start_bfs": [_P, _P],
@@ -147,6 +148,7 @@ SIGNATURES = {
     "gcp_edit_stroke": [_P, _I, _P, _P, _I, _I, _I32, _P],
     "gcp_edit_brush": [_P, _I, _P, _P, _I, _I, _I32, _P],
     "gcp_solve": [_P, _P, _I, _P],
+    "gcp_solve_labels": [_P, _P, _I, _P, _I, _P],
     "gcp_flow": [_P, _I, _P],
     "gcp_labels": [_P, _I, _P, _P],
     "gcp_labels_packed": [_P, _I, _P, _P],

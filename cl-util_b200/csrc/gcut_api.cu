@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -171,6 +172,7 @@ struct Pool {
   char* d_sel = nullptr;
   char* h_sel = nullptr;
   size_t sel_bytes = 0;
+  std::vector<int32_t> sel_key, sel_last;   // a selection; the one last copied to the device
   gc_stats stats{};
   // profiling: event pairs around every launch, tiles processed per kernel kind
   bool prof = false;
@@ -292,8 +294,8 @@ struct Pool {
     c.take(&ktiles, GC_NKERN);
     c.take(&P.trace, 2 * GC_TRACE_MAX);
     c.take(&P.trace_ctl, 2);
-    // look-back slots: the scan uses one per 4096 items, the list rebuild one per 64 tiles
-    const int chunks = scan_chunks(nt) > nt / 64 + 1 ? scan_chunks(nt) : nt / 64 + 1;
+    // look-back slots: the scan uses one per 4096 items, the list rebuild one per 1024 tiles
+    const int chunks = scan_chunks(nt) > nt / 1024 + 1 ? scan_chunks(nt) : nt / 1024 + 1;
     c.take(&scan.st.status, chunks);
     c.take(&scan.st.ticket, 4);
     scan.st.max_chunks = chunks;
@@ -486,28 +488,47 @@ struct Pool {
   // queues its copy to the device.  An image is fresh (mode 1: trivial labelling, no flood
   // before its first pulses) right after its upload, else it continues from its previous
   // flow (mode 2); initial_relabel makes every image mode 2.  *any_warm: some image is mode 2.
+  // Repeated solves of the same images (every solve of a one-image handle) find the
+  // selection already on the device and skip both copies.
   int set_selection(const int* idx, int n, bool* any_warm, cudaStream_t s) {
-    int32_t* cnt = reinterpret_cast<int32_t*>(h_sel);
-    int4* rng = reinterpret_cast<int4*>(h_sel + 16);
-    int32_t* mode = reinterpret_cast<int32_t*>(rng + imgs.size());
+    // n, selected tiles, then per range: first tile, tiles, first selected index, image, mode
+    sel_key.assign(2 + 5 * (size_t)n, 0);
     long long start = 0;
     bool warm = false;
     for (int k = 0; k < n; ++k) {
       const int i = idx[k];
       const ImageDesc& im = imgs[i];
       const int tiles = im.tw * im.th;
-      rng[k] = make_int4(im.tile0, tiles, (int)start, i);
-      mode[k] = (opts.initial_relabel || img_solved[i] || img_edited[i]) ? 2 : 1;
-      warm |= mode[k] == 2;
+      int32_t* e = &sel_key[2 + 5 * (size_t)k];
+      e[0] = im.tile0;
+      e[1] = tiles;
+      e[2] = (int)start;
+      e[3] = i;
+      e[4] = (opts.initial_relabel || img_solved[i] || img_edited[i]) ? 2 : 1;
+      warm |= e[4] == 2;
       start += tiles;
     }
     if (start > nt) return fail(GC_ERR_INTERNAL, "selection larger than the pool");
+    sel_key[0] = n;
+    sel_key[1] = (int)start;
+    *any_warm = warm;
+    if (sel_key == sel_last) return GC_OK;
+    // the previous copy out of the pinned mirror finished with the previous (synchronous) solve
+    int32_t* cnt = reinterpret_cast<int32_t*>(h_sel);
+    int4* rng = reinterpret_cast<int4*>(h_sel + 16);
+    int32_t* mode = reinterpret_cast<int32_t*>(rng + imgs.size());
     cnt[0] = n;
     cnt[1] = (int)start;
-    *any_warm = warm;
+    for (int k = 0; k < n; ++k) {
+      const int32_t* e = &sel_key[2 + 5 * (size_t)k];
+      rng[k] = make_int4(e[0], e[1], e[2], e[3]);
+      mode[k] = e[4];
+    }
     // one copy: counts, the n ranges, then (at their fixed place) the modes
+    sel_last.clear();   // unknown until both copies are queued
     CK(cudaMemcpyAsync(d_sel, h_sel, 16 + sizeof(int4) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(P.sel_mode, mode, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    sel_last.swap(sel_key);
     return GC_OK;
   }
 
@@ -575,15 +596,20 @@ struct Pool {
   }
 
   // Solves every image of a fixed pool.
-  int solve(cudaStream_t s) {
+  // Work queued right behind a solve, before the host waits for it (the labels of
+  // gc_solve_labels): it needs only the solve's device results, so it follows the solve
+  // without a host round trip in between.
+  using After = std::function<int(cudaStream_t)>;
+
+  int solve(cudaStream_t s, const After* after = nullptr) {
     std::vector<int> all(imgs.size());
     for (size_t i = 0; i < imgs.size(); ++i) all[i] = (int)i;
-    return solve_images(all.data(), (int)all.size(), s);
+    return solve_images(all.data(), (int)all.size(), s, after);
   }
 
   // Solves the listed images together (distinct, uploaded); the pool's other images keep
   // their state and results.
-  int solve_images(const int* idx, int n, cudaStream_t s) {
+  int solve_images(const int* idx, int n, cudaStream_t s, const After* after = nullptr) {
     if (n < 1 || !idx) return fail(GC_ERR_INVALID, "no images to solve");
     std::vector<uint8_t> seen(imgs.size(), 0);
     for (int k = 0; k < n; ++k) {
@@ -596,9 +622,14 @@ struct Pool {
     stats = gc_stats{};
     bool warm = false;
     RK(set_selection(idx, n, &warm, s));
-    int r = (prof || collect || !use_graph) ? solve_host(s, warm) : solve_graph(s, warm);
+    const bool host = prof || collect || !use_graph;
+    int r = host ? solve_host(s, warm) : solve_graph(s, warm, after);
     if (r) return r;
-    RK(finish_check(s, idx, n));
+    if (host && after) {   // the host-driven solve has finished: queue the work and wait
+      RK((*after)(s));
+      CK(cudaStreamSynchronize(s));
+    }
+    RK(finish_check(s, idx, n, /*err_in_ctl=*/true));
     for (int k = 0; k < n; ++k) {
       img_solved[idx[k]] = 1;
       img_edited[idx[k]] = 0;
@@ -626,7 +657,7 @@ struct Pool {
       RK(read_ctl(s));
       if (h_ctl[CTL_LEFT] > 0) RK(bfs_phase(s));
     }
-    RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 0, 0, 2, 0, acc, s); }));
+    RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 0, 0, 2, 0, acc, 2 * sms, s); }));
     RK(read_count(s, &n));
     for (int cycle = 0; n > 0; ++cycle) {
       if (cycle >= opts.max_cycles) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
@@ -647,7 +678,7 @@ struct Pool {
       n = 0;
       if (h_ctl[CTL_LEFT] > 0) {
         RK(bfs_phase(s));
-        RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 1, 1, 1, 0, acc, s); }));
+        RK(timed(K_COMPACT, s, [&] { return launch_active_list(P, scan.st, list, counts, 1, 1, 1, 0, acc, 2 * sms, s); }));
         RK(read_count(s, &n));
       }
     }
@@ -756,7 +787,7 @@ struct Pool {
     }
     if (!bump) return GC_OK;   // the first list of a solve follows the IF node
     return capture(bi, Li, [&](cudaStream_t cs) {
-      return launch_active_list(P, scan.st, list, counts, 1, 1, 1, hmain, acc, cs);
+      return launch_active_list(P, scan.st, list, counts, 1, 1, 1, hmain, acc, 2 * sms, cs);
     });
   }
 
@@ -779,7 +810,7 @@ struct Pool {
       RK(graph_cycle_tail(g, L, /*mode=*/3, /*all=*/1, /*bump=*/0, hmain));
     }
     RK(capture(g, L, [&](cudaStream_t cs) {   // the first active list (fresh and live images)
-      return launch_active_list(P, scan.st, list, counts, 0, 0, 2, hmain, acc, cs);
+      return launch_active_list(P, scan.st, list, counts, 0, 0, 2, hmain, acc, 2 * sms, cs);
     }));
     cudaGraph_t bm;
     RK(add_while(g, L, hmain, &bm));
@@ -807,7 +838,7 @@ struct Pool {
   }
 
   // variant 1: some selected image continues from a previous flow (the graph floods first)
-  int solve_graph(cudaStream_t s, bool warm) {
+  int solve_graph(cudaStream_t s, bool warm, const After* after = nullptr) {
     const int v = warm ? 1 : 0;
     if (!gexec[v]) {
       const int r = build_graph(v);
@@ -818,6 +849,7 @@ struct Pool {
     }
     P.ktiles = nullptr;
     CK(cudaGraphLaunch(gexec[v], s));
+    if (after) RK((*after)(s));
     CK(cudaStreamSynchronize(s));
     stats.launches = -1;  // inside the graph; see gc_stats
     return GC_OK;
@@ -835,9 +867,16 @@ struct Pool {
     cap_stream = nullptr;
   }
 
-  // errors and results common to both paths (h_acc / h_ctl are filled and synchronised)
-  int finish_check(cudaStream_t s, const int* idx = nullptr, int n = 0) {
-    RK(check_device_error(s));
+  // errors and results common to both paths (h_acc / h_ctl are filled and synchronised).
+  // err_in_ctl: the solve's active lists brought the scan state's error word back with the
+  // control words, so no separate read (and host round trip) is needed
+  int finish_check(cudaStream_t s, const int* idx = nullptr, int n = 0, bool err_in_ctl = false) {
+    if (!err_in_ctl) {
+      RK(check_device_error(s));
+    } else if (h_ctl[CTL_SCANERR]) {
+      CK(cudaMemsetAsync(scan.st.err, 0, sizeof(int32_t), s));
+      return fail(GC_ERR_INTERNAL, "a bounded device-side wait gave up");
+    }
     if (h_ctl[CTL_ERR] == 1) return fail(GC_ERR_NOT_CONVERGED, "BFS round cap reached");
     if (h_ctl[CTL_ERR] == 2) return fail(GC_ERR_NOT_CONVERGED, "cycle cap reached before the cut was final");
     if (h_ctl[CTL_ERR] == 3) return fail(GC_ERR_INTERNAL, "a bounded wait for a tile copy gave up");
@@ -964,6 +1003,24 @@ struct Pool {
     if (!img_solved[i]) return fail(GC_ERR_STATE, "labels before solve");
     CK(cudaSetDevice(device));
     return timed(K_LABELS, s, [&] { return launch_labels_packed(P, imgs[i], out, s); });
+  }
+
+  // Solves the listed images and writes their labels (bit-packed or one byte per pixel) to
+  // outs[k], with one host wait for both.
+  int solve_labels(const int* idx, int n, uint8_t* const* outs, bool packed, cudaStream_t s) {
+    if (n < 1 || !idx || !outs) return fail(GC_ERR_INVALID, "bad argument");
+    for (int k = 0; k < n; ++k)
+      if (!outs[k]) return fail(GC_ERR_INVALID, "null label buffer");
+    const After after = [&](cudaStream_t cs) {
+      for (int k = 0; k < n; ++k) {
+        const ImageDesc& im = imgs[idx[k]];
+        RK(timed(K_LABELS, cs, [&] {
+          return packed ? launch_labels_packed(P, im, outs[k], cs) : launch_labels_out(P, im, outs[k], cs);
+        }));
+      }
+      return GC_OK;
+    };
+    return solve_images(idx, n, s, &after);
   }
 };
 
@@ -1265,6 +1322,15 @@ int gc_solve(gc_handle* h, void* stream) {
   g_err.clear();
   if (!h) return fail(GC_ERR_INVALID, "null handle");
   const int r = h->pool.solve((cudaStream_t)stream);
+  h->pool.track((cudaStream_t)stream);
+  return r;
+}
+
+int gc_solve_labels(gc_handle* h, uint8_t* labels, int packed, void* stream) {
+  g_err.clear();
+  if (!h || !labels) return fail(GC_ERR_INVALID, "null argument");
+  const int zero = 0;
+  const int r = h->pool.solve_labels(&zero, 1, &labels, packed != 0, (cudaStream_t)stream);
   h->pool.track((cudaStream_t)stream);
   return r;
 }
@@ -1821,6 +1887,16 @@ int gcp_solve(gcp_handle* p, const int* slots, int n, void* stream) {
   if (!p || !slots || n < 1) return fail(GC_ERR_INVALID, "bad argument");
   for (int k = 0; k < n; ++k) RK(gcp_slot(p, slots[k], true));
   const int r = p->pool.solve_images(slots, n, (cudaStream_t)stream);
+  p->pool.track((cudaStream_t)stream);
+  return r;
+}
+
+int gcp_solve_labels(gcp_handle* p, const int* slots, int n, uint8_t* const* labels, int packed,
+                     void* stream) {
+  g_err.clear();
+  if (!p || !slots || !labels || n < 1) return fail(GC_ERR_INVALID, "bad argument");
+  for (int k = 0; k < n; ++k) RK(gcp_slot(p, slots[k], true));
+  const int r = p->pool.solve_labels(slots, n, labels, packed != 0, (cudaStream_t)stream);
   p->pool.track((cudaStream_t)stream);
   return r;
 }

@@ -85,13 +85,14 @@ enum CtlSlot {
   CTL_PULSE = 10,     // discharge launches since the last list rebuild (parity = worklist)
   CTL_DDONE = 11,     // CTAs finished in the current discharge launch
   CTL_BAD = 12,       // first out-of-range worklist value seen by a self-check
-  CTL_BADWHERE = 13,  // 1: worklist append, 2: worklist length, 3: list length, 4: image id,
-                      // 5: frontier append, 6: frontier length, 7: dirty append,
-                      // 8: dirty length
+  CTL_BADWHERE = 13,  // 1: worklist append, 2: worklist length, 3: list length, 4: image id
+                      // (or tile) of the selection, 5: frontier append, 6: frontier length,
+                      // 7: dirty append, 8: dirty length, 9: selection size
   CTL_KDONE = 14,     // CTAs finished in k_masks
   CTL_NCHECK = 15,    // flood checks run (k_flood_check launches)
   CTL_NACT = 16,      // active-list rebuilds run (k_active_list launches)
   CTL_LEFT = 17,      // images still running after the last flood check
+  CTL_SCANERR = 18,   // the scan state's error word, as the last active list saw it
   CTL_N = 64          // the control words fill 256 bytes; the per-image sums follow them
 };
 

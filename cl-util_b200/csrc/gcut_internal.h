@@ -92,10 +92,11 @@ int launch_flood_check(const PoolView& P, int all, cudaGraphConditionalHandle hb
 int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc* acc,
                      cudaStream_t s);
 // over the solve's selected tiles; filter 1: only tiles of the images a flood check kept
-// (img_live == the cycle stamp), 2: those and the tiles of freshly uploaded images
+// (img_live == the cycle stamp), 2: those and the tiles of freshly uploaded images; grid:
+// most CTAs (a few per SM), which loop over the selection's chunks
 int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, int32_t* count,
                        int bump, int count_cycle, int filter, cudaGraphConditionalHandle h,
-                       ImageAcc* acc, cudaStream_t s);
+                       ImageAcc* acc, int grid, cudaStream_t s);
 int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s);
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s);

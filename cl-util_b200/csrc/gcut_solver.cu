@@ -268,11 +268,12 @@ k_upload(PoolView P, ImageDesc im, int img, Source src, int32_t* __restrict__ tl
   if ((threadIdx.x & 31) == 0) wpos[threadIdx.x >> 5] = pos;
   bad = __syncthreads_or(bad);
   anypos = __syncthreads_or(anypos);
-  if ((threadIdx.x & 31) == 0 && pos) atomicAdd(&acc[img].sumpos_t, (unsigned long long)pos);
   if (threadIdx.x == 0) {
     long long tp = 0;
     for (int k = 0; k < DIS_THREADS / 32; ++k) tp += wpos[k];
     P.tpos[t] = tp;
+    // one add per tile: the adds of all of an image's tiles go to one address
+    if (tp) atomicAdd(&acc[img].sumpos_t, (unsigned long long)tp);
     if (bad) atomicAdd(&acc[img].bad_caps, 1);
     P.tact[t] = anypos;
     P.touched[t] = 0;
@@ -976,7 +977,7 @@ __device__ __forceinline__ void frontier_work(const PoolView& P, int first, int 
   const int n = s_n;
   *count = n;
   *nranges = s_nr;
-  const int need = first ? (int)gridDim.x : (n + per_cta - 1) / per_cta;
+  const int need = (n + per_cta - 1) / per_cta;
   *participants = need < 1 ? 1 : (need < (int)gridDim.x ? need : (int)gridDim.x);
 }
 
@@ -1055,11 +1056,26 @@ __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc
 // counts this check as a finished cycle).  Replaces a compaction and a separate stamping
 // launch.  filter: 1 only tiles of the images a flood check kept (img_live == the cycle
 // stamp; a solved image keeps the activity flags of its last relabel), 2 those and the tiles
-// of freshly uploaded images (the first list of a solve).  The grid covers the whole pool;
-// CTAs whose ticket is past the selection's chunks only count themselves done.
+// of freshly uploaded images (the first list of a solve).
+//
+// The grid is a fixed number of CTAs (a few per SM) that take chunk tickets in a loop until
+// the selection's chunks run out, so a pool of millions of tiles costs no more launch work
+// than one image, and a 2048^2 image (4096 tiles) spreads over four CTAs.  Every ticket
+// holder is already running, so a look-back only ever waits for a running CTA.  The image
+// of each item comes from the selection (one range per image), and an image's live stamp,
+// flood sum and sink-reached stamp are written once per warp that holds one of its active
+// tiles rather than once per tile: thousands of stores to one address serialise in L2.
 constexpr int ACT_THREADS = 256;
-constexpr int ACT_ITEMS = 16;
+constexpr int ACT_ITEMS = 4;
 constexpr int ACT_CHUNK = ACT_THREADS * ACT_ITEMS;
+
+__device__ __forceinline__ void stamp_image(const PoolView& P, ImageAcc* acc, int img, int stamp) {
+  P.img_live[img] = stamp;
+  // the image's next flood starts afresh: its sum and its sink-reached stamp (the first
+  // cycle of a warm solve reuses the stamp of the flood before it)
+  acc[img].sumpos_e = 0;
+  P.img_hit[img] = 0;
+}
 
 __global__ void __launch_bounds__(ACT_THREADS)
 k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
@@ -1081,31 +1097,42 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
     s_nr = nr;
   }
   __syncthreads();
-  const int chunk = s_chunk, cur = s_cur, stamp = cur + bump;
+  const int cur = s_cur, stamp = cur + bump;
   const int n = s_n;
   const int nchunks = (n + ACT_CHUNK - 1) / ACT_CHUNK;
-  if (chunk < nchunks) {
+  const int lane = threadIdx.x & 31;
+  for (int chunk = s_chunk; chunk < nchunks;) {
     const int base = chunk * ACT_CHUNK + threadIdx.x * ACT_ITEMS;
     SelCursor cursor(P, s_nr, base < n ? base : 0);
-    int32_t v[ACT_ITEMS], tl[ACT_ITEMS];
+    int32_t v[ACT_ITEMS], tl[ACT_ITEMS], im[ACT_ITEMS];
 #pragma unroll
     for (int k = 0; k < ACT_ITEMS; ++k) {
-      tl[k] = base + k < n ? cursor.tile(base + k) : -1;
-      v[k] = tl[k] >= 0 ? P.tact[tl[k]] != 0 : 0;
+      tl[k] = -1;
+      im[k] = -1;
+      if (base + k < n) {
+        tl[k] = cursor.tile(base + k);
+        im[k] = cursor.image();
+      }
+      v[k] = 0;
+      if ((unsigned)tl[k] < (unsigned)P.nt && (unsigned)im[k] < (unsigned)P.nimg)
+        v[k] = P.tact[tl[k]] != 0;
+      else if (tl[k] >= 0)
+        record_bad(P, 4, (unsigned)im[k] < (unsigned)P.nimg ? tl[k] : im[k]);
     }
     if (filter) {
 #pragma unroll
       for (int k = 0; k < ACT_ITEMS; ++k) {
         if (!v[k]) continue;
-        const int img = P.img_of[tl[k]];
-        if ((unsigned)img >= (unsigned)P.nimg) { v[k] = 0; continue; }
-        const int il = *((volatile int32_t*)&P.img_live[img]);
-        v[k] = il == cur || il == stamp || (filter == 2 && P.img_mode[img] == 1);
+        const int il = *((volatile int32_t*)&P.img_live[im[k]]);
+        v[k] = il == cur || il == stamp || (filter == 2 && P.img_mode[im[k]] == 1);
       }
     }
-    int32_t tsum = 0;
+    int32_t tsum = 0, first = -1;
 #pragma unroll
-    for (int k = 0; k < ACT_ITEMS; ++k) tsum += v[k];
+    for (int k = ACT_ITEMS - 1; k >= 0; --k) {
+      tsum += v[k];
+      if (v[k]) first = im[k];
+    }
     int32_t agg;
     const int32_t tex = block_exclusive_scan(tsum, sm, &agg);
     if (threadIdx.x < 32) {
@@ -1113,27 +1140,29 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
       if (threadIdx.x == 0) s_excl = ex;
     }
     __syncthreads();
+    // one lane per distinct first image in the warp stamps it; the rare later images of a
+    // thread (its items straddle two ranges) are stamped by that thread
+    const unsigned peers = __match_any_sync(0xffffffffu, first);
+    if (first >= 0 && __ffs(peers) - 1 == lane) stamp_image(P, acc, first, stamp);
     int32_t run = s_excl + tex;
+    int last = first;
 #pragma unroll
     for (int k = 0; k < ACT_ITEMS; ++k) {
       if (v[k]) {
-        const int t = tl[k];
-        if ((unsigned)run < (unsigned)P.nt) list[run] = t;
+        if ((unsigned)run < (unsigned)P.nt) list[run] = tl[k];
         else atomicExch(st.err, 2);   // only after a look-back that gave up
-        const int img = P.img_of[t];
-        if ((unsigned)img < (unsigned)P.nimg) {
-          P.img_live[img] = stamp;
-          // the image's next flood starts afresh: its sum and its sink-reached stamp (the
-          // first cycle of a warm solve reuses the stamp of the flood before it)
-          acc[img].sumpos_e = 0;
-          P.img_hit[img] = 0;
-        } else {
-          record_bad(P, 4, img);
+        if (im[k] != last) {
+          stamp_image(P, acc, im[k], stamp);
+          last = im[k];
         }
         ++run;
       }
     }
     if (chunk == nchunks - 1 && threadIdx.x == 0) *count = s_excl + agg;
+    __syncthreads();   // every thread has read s_chunk and s_excl
+    if (threadIdx.x == 0) s_chunk = atomicAdd(st.ticket, 1);
+    __syncthreads();
+    chunk = s_chunk;
   }
   if (threadIdx.x != 0) return;
   __threadfence();
@@ -1154,6 +1183,9 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
   const int cycles = ctl[CTL_CYCLES] + (count_cycle ? 1 : 0);
   ctl[CTL_CYCLES] = cycles;
   ctl[CTL_NACT] = ctl[CTL_NACT] + 1;
+  // a look-back that gave up (here or in an earlier list of this solve) reaches the host
+  // with the control words
+  ctl[CTL_SCANERR] = ctl[CTL_SCANERR] | *((volatile int32_t*)st.err);
   bool more = nact > 0 && ctl[CTL_ERR] < 3;
   if (more && cycles >= ctl[CTL_MAXCYCLES]) {
     ctl[CTL_ERR] = 2;
@@ -1307,6 +1339,8 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
   if ((int)blockIdx.x >= parts) return;
   const int i0 = blockIdx.x * WARPS_PER_CTA + warp;
   SelCursor cursor(P, first ? nr : 0, i0);
+  int wimg = -1;                 // first round: the image whose tile sums this warp holds
+  unsigned long long wsum = 0;
   for (int i = i0; i < n; i += parts * WARPS_PER_CTA) {
     const int t = first ? cursor.tile(i) : P.fq[in][i];
     if (!first && lane == 0) markin[t] = 0;
@@ -1326,9 +1360,17 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
     if (first) {
       R = P.mexc[(long long)t * 32 + lane];
       R0 = 0;
-      // Σ max(excess, 0) of the tile was taken with its masks after the tile last changed
+      // Σ max(excess, 0) of the tile was taken with its masks after the tile last changed;
+      // summed per warp and per CTA before the add to the image's word
       const long long ps = P.tpos[t];
-      if (lane == 0 && ps) atomicAdd(&acc[img].sumpos_e, (unsigned long long)ps);
+      if (lane == 0 && ps) {
+        if (img != wimg) {
+          if (wsum) atomicAdd(&acc[wimg].sumpos_e, wsum);
+          wimg = img;
+          wsum = 0;
+        }
+        wsum += (unsigned long long)ps;
+      }
     } else {
       R = R0 = P.mreach[(long long)t * 32 + lane];
       if (lane == 0 && nb.x >= 0)
@@ -1368,6 +1410,24 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
   if (lane == 0 && done) {
     atomicAdd(&P.rcnt[in], done);
     if (P.ktiles) atomicAdd(&P.ktiles[first ? K_FLOOD_FIRST : K_FLOOD], (unsigned long long)done);
+  }
+  if (first) {   // the CTA's warps that summed the same image add once
+    __shared__ int s_img[WARPS_PER_CTA];
+    __shared__ unsigned long long s_sum[WARPS_PER_CTA];
+    if (lane == 0) {
+      s_img[warp] = wsum ? wimg : -1;
+      s_sum[warp] = wsum;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int a = 0; a < WARPS_PER_CTA; ++a) {
+        if (s_img[a] < 0) continue;
+        unsigned long long v = s_sum[a];
+        for (int b = a + 1; b < WARPS_PER_CTA; ++b)
+          if (s_img[b] == s_img[a]) { v += s_sum[b]; s_img[b] = -1; }
+        atomicAdd(&acc[s_img[a]].sumpos_e, v);
+      }
+    }
   }
   frontier_round_end(P, first, in, CTL_FLOOD_TOTAL, parts, h);
 }
@@ -1713,11 +1773,12 @@ int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc
 
 int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, int32_t* count,
                        int bump, int count_cycle, int filter, cudaGraphConditionalHandle h,
-                       ImageAcc* acc, cudaStream_t s) {
+                       ImageAcc* acc, int grid, cudaStream_t s) {
   const int nch = (P.nt + ACT_CHUNK - 1) / ACT_CHUNK;   // enough for any selection
   if (nch > st.max_chunks) return GC_ERR_INVALID;
-  k_active_list<<<nch > 0 ? nch : 1, ACT_THREADS, 0, s>>>(P, st, list, count, bump, count_cycle,
-                                                          filter, h, acc);
+  grid = grid < nch ? grid : nch;
+  k_active_list<<<grid > 0 ? grid : 1, ACT_THREADS, 0, s>>>(P, st, list, count, bump, count_cycle,
+                                                            filter, h, acc);
   return ok();
 }
 

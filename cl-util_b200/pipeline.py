@@ -110,9 +110,9 @@ class SolvePipeline:
                     self.gc.upload_image(self.stage_img[j], self.stage_exc[j], stream=self.compute,
                                          lamda=self.lamda)
                     self.consumed[j].record(self.compute)
-                    self.gc.cut(stream=self.compute)          # returns when the solve is done
+                    # returns when the solve and the packed labels are done (one host wait)
+                    self.gc.cut_labels(out=self.dbits[j], packed=True, stream=self.compute)
                     flow = self.gc.flow
-                    self.gc.labels_packed(out=self.dbits[j], stream=self.compute)
                     self.packed[j].record(self.compute)
                 with torch.cuda.stream(self.copy):
                     self.copy.wait_event(self.packed[j])

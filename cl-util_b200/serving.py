@@ -713,10 +713,10 @@ class BatchingServer:
                                               stream=self.stream)
                     t1 = time.perf_counter()
                     jobs = images + strokes
-                    self.pool.solve([s.slot for _, _, s in jobs], stream=self.stream)
+                    # the solve and every job's packed labels, one host wait
+                    dev = self.pool.solve_labels([s.slot for _, _, s in jobs], stream=self.stream)
                     t2 = time.perf_counter()
                     flows = [self.pool.flow(s.slot) for _, _, s in jobs]
-                    dev = [self.pool.labels_packed(s.slot, stream=self.stream) for _, _, s in jobs]
                     host = [d.to("cpu", non_blocking=True) for d in dev]
                     self.stream.synchronize()
                 done = time.perf_counter()

@@ -195,6 +195,25 @@ class SessionPool:
         for s in slots:
             self._keep.pop(int(s), None)
 
+    def solve_labels(self, slots, outs=None, packed=True, stream=None):
+        """solve() and every slot's labels (bit-packed by default) with one host wait
+        (gcp_solve_labels); returns the label tensors in the order of `slots`."""
+        torch = self.torch
+        if outs is None:
+            outs = []
+            for s in slots:
+                w, h = self.shape[int(s)]
+                shape = (h, (w + 7) // 8) if packed else (h, w)
+                outs.append(torch.empty(shape, dtype=torch.uint8, device=self.device))
+        arr = (ctypes.c_int * len(slots))(*[int(s) for s in slots])
+        bufs = (ctypes.c_void_p * len(slots))(*[o.data_ptr() for o in outs])
+        with torch.cuda.device(self.device):
+            check(lib().gcp_solve_labels(self._h, arr, len(slots), bufs, int(bool(packed)),
+                                         stream_handle(stream)))
+        for s in slots:
+            self._keep.pop(int(s), None)
+        return outs
+
     def flow(self, slot) -> int:
         f = ctypes.c_int64(0)
         check(lib().gcp_flow(self._h, int(slot), ctypes.byref(f)))

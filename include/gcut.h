@@ -215,8 +215,17 @@ int gc_gmm_fit(const uint32_t* samples, int n, int n_components, int max_iterati
 
 /* Max-flow to the final cut.  Replaces GraphCut.cut (GraphCut.pyx:348-418); warm-starts
    from the current residual graph when called again after gc_edit_tlinks.  Blocks the
-   calling host thread until the solve is done (it polls the active-tile count). */
+   calling host thread until the solve is done (one wait for the solve's CUDA graph; the
+   host-driven path of gc_set_profile / gc_set_collect_stats reads the loop counters between
+   launches). */
 int gc_solve(gc_handle* h, void* stream);
+
+/* gc_solve, then the canonical labels into the DEVICE buffer `labels` (packed != 0: the
+   bit-packed rows of gc_labels_packed, else one byte per pixel as gc_labels), with one host
+   wait for both: the labels kernel is queued behind the solve on `stream` instead of after
+   the host has seen the solve finish.  On an error return the buffer's content is
+   unspecified. */
+int gc_solve_labels(gc_handle* h, uint8_t* labels, int packed, void* stream);
 
 /* Manual stepping, mirroring the reference methods a caller can drive one at a time (the
    GUI buttons of test_GraphCut.py:81-83).  gc_push = one discharge launch over the active
@@ -449,6 +458,10 @@ int gcp_edit_brush(gcp_handle* p, int slot, const int32_t* xs, const int32_t* ys
    uploaded since its last solve starts fresh, an edited or solved one warm-starts from its
    previous flow.  Blocks the calling thread until the solve is done. */
 int gcp_solve(gcp_handle* p, const int* slots, int n, void* stream);
+/* gcp_solve, then every listed slot's labels into the DEVICE buffer labels[k] (packed as in
+   gc_solve_labels), with one host wait for the solve and all the labels. */
+int gcp_solve_labels(gcp_handle* p, const int* slots, int n, uint8_t* const* labels, int packed,
+                     void* stream);
 int gcp_flow(gcp_handle* p, int slot, int64_t* flow);
 /* Canonical labels of a slot's last solve into DEVICE buffers (as gc_labels /
    gc_labels_packed). */

@@ -71,6 +71,26 @@ def test_packed_labels_match_oracle(cuda, oracle, w, h):
     assert np.array_equal(unpack_labels(host, w), l_ref)
 
 
+@pytest.mark.parametrize("w,h,graph", [(1, 1, True), (33, 31, True), (257, 130, True),
+                                       (257, 130, False), (1000, 3, True)])
+def test_cut_labels_matches_cut_then_labels(cuda, oracle, w, h, graph):
+    """gc_solve_labels (solve and labels, one host wait) gives the flow and the labels, packed
+    and one byte per pixel, of gc_solve followed by gc_labels / gc_labels_packed."""
+    from GraphCut import unpack_labels
+    g = synth.random_graph(w, h, 3 * w + h, cap_max=30, tlink_max=60)
+    f_ref, l_ref = oracle.maxflow_bk(*g.planes())
+    with GraphCut(w, h, use_graph=graph) as gc:
+        gc.upload_capacities(*g.planes())
+        lab = gc.cut_labels().cpu().numpy()
+        assert gc.flow == f_ref
+        assert np.array_equal(lab, l_ref)
+        gc.upload_capacities(*g.planes())
+        bits = gc.cut_labels(packed=True).cpu().numpy()
+        assert gc.flow == f_ref
+        assert np.array_equal(unpack_labels(bits, w), l_ref)
+        assert np.array_equal(gc.labels().cpu().numpy(), l_ref)
+
+
 def test_handles_in_caller_memory(cuda, oracle):
     """gc_create_in: handles placed in one caller-owned buffer solve like gc_create, and
     the memory is reused for a handle of another size after gc_destroy."""

@@ -83,3 +83,41 @@ def test_rejects_overlap_and_bad_slots(cuda):
         pool.open(1, 64, 64, 16)
     finally:
         pool.close_pool()
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_solve_labels_matches_solve_then_labels(cuda, oracle, use_graph):
+    """gcp_solve_labels (the solve and every slot's labels with one host wait) gives the
+    flows and labels of gcp_solve followed by gcp_labels / gcp_labels_packed, fresh and
+    warm, packed and one byte per pixel."""
+    torch = cuda
+    from GraphCut import unpack_labels
+    shapes = [(300, 211), (64, 97), (515, 260)]
+    graphs = [synth.make_graph(w, h, 70 + i) for i, (w, h) in enumerate(shapes)]
+    pool = SessionPool(4096, 8, use_graph=use_graph)
+    slots = [5, 1, 2]
+    try:
+        for s, g in zip(slots, graphs):
+            pool.open(s, g.width, g.height, pool.alloc_tiles(g.width, g.height))
+            pool.upload_capacities(s, *[torch.from_numpy(p).cuda() for p in g.planes()])
+        outs = pool.solve_labels(slots, packed=True)
+        for k, g in enumerate(graphs):
+            f, l = oracle.maxflow_bk(*g.planes())
+            assert pool.flow(slots[k]) == f, k
+            assert np.array_equal(unpack_labels(outs[k].cpu().numpy(), g.width), l), k
+        # warm re-solve after strokes, labels one byte per pixel
+        rng = np.random.default_rng(11)
+        ts = [g.excess.copy() for g in graphs]
+        for k in (0, 2):
+            st = strokes.random_stroke(rng, graphs[k].width, graphs[k].height)
+            pool.edit_stroke(slots[k], st.xs, st.ys, st.radius, st.value)
+            ts[k] = strokes.apply(ts[k], st)
+        outs = pool.solve_labels([slots[2], slots[0]], packed=False)
+        for k, out in zip((2, 0), outs):
+            g = graphs[k]
+            f, l = oracle.maxflow_bk(g.up, g.down, g.left, g.right, ts[k])
+            assert pool.flow(slots[k]) == f, k
+            assert np.array_equal(out.cpu().numpy(), l), k
+            assert np.array_equal(pool.labels(slots[k]).cpu().numpy(), l), k
+    finally:
+        pool.close_pool()
