@@ -556,6 +556,12 @@ class BatchingServer:
         self.inflight = 0
         with torch.cuda.device(device):
             self.stream = torch.cuda.Stream()
+            # staging for a tick of tick_pixels (grown on demand, see _reserve)
+            self.dstage = torch.empty(2 * self.tick_pixels, dtype=torch.int32, device=device)
+            nb = self.tick_pixels // 4 + (1 << 20)
+            self.dbits = torch.empty(nb, dtype=torch.uint8, device=device)
+            self.hbits = torch.empty(nb, dtype=torch.uint8, pin_memory=True)
+        self._cursor = 0
         if warm_up:
             self._warm_up()
         self.worker = threading.Thread(target=self._worker, daemon=True)
@@ -704,7 +710,9 @@ class BatchingServer:
                 self.inflight += len(strokes) + len(images)
             try:
                 start = time.perf_counter()
+                jobs = images + strokes
                 with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+                    self._reserve(images, jobs)
                     for req, _, s in images:
                         self.pool.open(s.slot, s.width, s.height, s.tile0, stream=self.stream)
                         self._upload(s, req.planes)
@@ -712,20 +720,26 @@ class BatchingServer:
                         self.pool.edit_stroke(s.slot, req.xs, req.ys, req.radius, req.value,
                                               stream=self.stream)
                     t1 = time.perf_counter()
-                    jobs = images + strokes
-                    # the solve and every job's packed labels, one host wait
-                    dev = self.pool.solve_labels([s.slot for _, _, s in jobs], stream=self.stream)
+                    # the solve and every job's packed labels into one device buffer, one
+                    # host wait; then one copy of that buffer to the pinned staging
+                    outs, spans = self._label_views(jobs)
+                    self.pool.solve_labels([s.slot for _, _, s in jobs], outs=outs,
+                                           stream=self.stream)
                     t2 = time.perf_counter()
                     flows = [self.pool.flow(s.slot) for _, _, s in jobs]
-                    host = [d.to("cpu", non_blocking=True) for d in dev]
+                    total = spans[-1][0] + spans[-1][1]
+                    self.hbits[:total].copy_(self.dbits[:total], non_blocking=True)
                     self.stream.synchronize()
+                    hb = self.hbits.numpy()
+                    host = [hb[off:off + n].reshape(s.height, (s.width + 7) // 8).copy()
+                            for (off, n), (_, _, s) in zip(spans, jobs)]
                 done = time.perf_counter()
                 phases = (1e3 * (t1 - start), 1e3 * (t2 - t1), 1e3 * (done - t2))
                 with self.lock:
                     self.ticks += 1
                     for (req, arr, s), f, bits in zip(jobs, flows, host):
                         kind = "stroke" if isinstance(req, Stroke) else "image"
-                        self.results.append(Result(s.sid, kind, f, bits.numpy(), s.width, arr,
+                        self.results.append(Result(s.sid, kind, f, bits, s.width, arr,
                                                    start, done, s.width * s.height, phases))
                         if kind == "image":
                             self.sessions[s.sid] = s
@@ -750,16 +764,60 @@ class BatchingServer:
                     self.inflight -= len(strokes) + len(images)
                     self.lock.notify_all()
 
+    # ---- staging (worker thread) ------------------------------------------------------
+    # Device memory for the tick's input planes and its packed labels, and pinned host memory
+    # for the labels' copy back: reused tick after tick (the previous tick's work finished
+    # before this one starts) and grown, before the tick's first copy, only when a tick needs
+    # more.  Allocating per request instead (fresh device tensors, a fresh pinned block for
+    # every result) stalled ticks for up to a quarter of a second.
+    @staticmethod
+    def _planes_of(req) -> int:
+        return 2 if len(req.planes) == 2 else 5
+
+    def _reserve(self, images, jobs):
+        torch = self.torch
+        need = sum(self._planes_of(req) * s.width * s.height for req, _, s in images)
+        if need > self.dstage.numel():
+            self.dstage = torch.empty(need + (need >> 2), dtype=torch.int32, device=self.pool.device)
+        nbits = sum(self._bits_span(s) for _, _, s in jobs)
+        if nbits > self.dbits.numel():
+            n = nbits + (nbits >> 2)
+            self.dbits = torch.empty(n, dtype=torch.uint8, device=self.pool.device)
+            self.hbits = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        self._cursor = 0
+
+    @staticmethod
+    def _bits_span(s) -> int:
+        return (s.height * ((s.width + 7) // 8) + 15) & ~15   # 16-byte aligned slices
+
+    def _label_views(self, jobs):
+        outs, spans, off = [], [], 0
+        for _, _, s in jobs:
+            n = s.height * ((s.width + 7) // 8)
+            outs.append(self.dbits[off:off + n].view(s.height, (s.width + 7) // 8))
+            spans.append((off, n))
+            off += self._bits_span(s)
+        return outs, spans
+
+    def _stage(self, n):
+        v = self.dstage[self._cursor:self._cursor + n]
+        self._cursor += n
+        return v
+
     def _upload(self, s, planes):
-        """A new session's inputs (the same three forms as GraphCutServer's) to its slot."""
+        """A new session's inputs (the same three forms as GraphCutServer's) to its slot,
+        through the tick's device staging."""
         torch = self.torch
         w, h = s.width, s.height
+        n = w * h
         if isinstance(planes[-1], tuple):   # (rgba, (fg, bg)): t-links from the models
             import gmm_tlinks
             from GraphCut import _as_rgba32
-            img = torch.from_numpy(np.ascontiguousarray(_as_rgba32(planes[0])).view(np.int32)).to(
-                self.pool.device, non_blocking=True)
-            ex = gmm_tlinks.tlinks(img, *planes[1], stream=self.stream)
+            img = self._stage(n).view(h, w)
+            img.copy_(torch.from_numpy(np.ascontiguousarray(_as_rgba32(planes[0])).view(np.int32)),
+                      non_blocking=True)
+            ex = gmm_tlinks.tlinks(img, *planes[1], out=self._stage(n).view(h, w),
+                                   stream=self.stream)
             self.pool.upload_image(s.slot, img, ex, stream=self.stream)
             return
         dev = []
@@ -767,8 +825,9 @@ class BatchingServer:
             src = np.ascontiguousarray(p)
             if src.dtype == np.uint32:
                 src = src.view(np.int32)
-            dev.append(torch.from_numpy(np.ascontiguousarray(src, dtype=np.int32)).to(
-                self.pool.device, non_blocking=True))
+            d = self._stage(n).view(h, w)
+            d.copy_(torch.from_numpy(np.ascontiguousarray(src, dtype=np.int32)), non_blocking=True)
+            dev.append(d)
         if len(dev) == 2:
             self.pool.upload_image(s.slot, dev[0], dev[1], stream=self.stream)
         else:
