@@ -388,9 +388,11 @@ def main():
         # the graph-mode timeline from the device-side trace (kernel start stamps inside the
         # CUDA graph, which host profilers do not list): one solve, outside the timed region
         import _gcut
+        gc.set_trace(True, stream=stream)
+        step()   # switching the trace on rebuilds the solve graph: not part of the timeline
         flush.fill_(1)
         stream.synchronize()
-        gc.set_trace(True, stream=stream)
+        gc.set_trace(True, stream=stream)   # a fresh trace
         step()
         trace = gc.trace(stream=stream)
         gc.set_trace(False, stream=stream)

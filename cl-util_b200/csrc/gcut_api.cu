@@ -173,6 +173,7 @@ struct Pool {
   char* h_sel = nullptr;
   size_t sel_bytes = 0;
   std::vector<int32_t> sel_key, sel_last;   // a selection; the one last copied to the device
+  int32_t* trace_words = nullptr;   // device: trace on/off and entry count (P.trace_ctl when on)
   gc_stats stats{};
   // profiling: event pairs around every launch, tiles processed per kernel kind
   bool prof = false;
@@ -257,6 +258,7 @@ struct Pool {
     tl = list = counts = stage = pts = nullptr;
     acc = nullptr; lstage = nullptr; h_count = nullptr; h_ctl = nullptr; h_acc = nullptr;
     dsum = nullptr; ntab = nullptr; d_sel = nullptr; h_sel = nullptr;
+    trace_words = nullptr;
   }
 
   // places every device buffer of the pool (see Carve)
@@ -276,8 +278,6 @@ struct Pool {
     c.take(&P.fq[0], nt);
     c.take(&P.fq[1], nt);
     c.take(&P.fcount, 2);
-    c.take(&P.dq, nt);
-    c.take(&P.dcount, 2);
     c.take(&P.img_live, imgs.size());
     c.take(&P.img_hit, imgs.size());
     c.take(&P.img_mode, imgs.size());
@@ -383,6 +383,9 @@ struct Pool {
     if (e) { done_ev = nullptr; release(); return cuda_fail(e, "event"); }
     Carve place{arena, 0};
     layout(place);
+    // tracing starts off: the kernels see a null trace_ctl and skip the mark without a load
+    trace_words = P.trace_ctl;
+    P.trace_ctl = nullptr;
     list = P.queue[0];
     counts = P.qcount;
     scan.st.done = scan.st.ticket + 1;
@@ -651,8 +654,7 @@ struct Pool {
     RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, s));
     int n = 0;
     if (warm) {
-      RK(timed(K_MASKS, s, [&] { return launch_masks(P, grid_warps, s); }));
-      RK(flood_phase(s, /*mode=*/3));
+      RK(flood_phase(s, /*mode=*/3));   // its first round rebuilds the masks of edited tiles
       RK(timed(K_COMPACT, s, [&] { return launch_flood_check(P, 1, 0, 0, s); }));
       RK(read_ctl(s));
       if (h_ctl[CTL_LEFT] > 0) RK(bfs_phase(s));
@@ -671,8 +673,7 @@ struct Pool {
         RK(timed(K_DISCHARGE, s, [&] { return launch_discharge(P, opts.discharge_iters, grid_dis, s); }));
         stats.pulses++;
       }
-      RK(timed(K_MASKS, s, [&] { return launch_masks(P, grid_warps, s); }));
-      RK(flood_phase(s, /*mode=*/2));
+      RK(flood_phase(s, /*mode=*/2));   // its first round rebuilds the masks of changed tiles
       RK(timed(K_COMPACT, s, [&] { return launch_flood_check(P, 0, 0, 0, s); }));
       RK(read_ctl(s));
       n = 0;
@@ -806,7 +807,6 @@ struct Pool {
     RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs); }));
     if (variant) {
       // images that continue from a previous flow: flood them; relabel the ones not solved
-      RK(capture(g, L, [&](cudaStream_t cs) { return launch_masks(P, grid_warps, cs); }));
       RK(graph_cycle_tail(g, L, /*mode=*/3, /*all=*/1, /*bump=*/0, hmain));
     }
     RK(capture(g, L, [&](cudaStream_t cs) {   // the first active list (fresh and live images)
@@ -819,7 +819,7 @@ struct Pool {
       RK(capture(bm, Lm, [&](cudaStream_t cs) {
         for (int p = 0; p < opts.pulses_per_relabel; ++p)
           RK(launch_discharge(P, opts.discharge_iters, grid_dis, cs));
-        return launch_masks(P, grid_warps, cs);
+        return GC_OK;
       }));
       RK(graph_cycle_tail(bm, Lm, /*mode=*/2, /*all=*/0, /*bump=*/1, hmain));
     }
@@ -980,8 +980,16 @@ struct Pool {
     CK(cudaStreamSynchronize(s));   // the words' previous copy has been read
     w[0] = on ? 1 : 0;
     w[1] = 0;
-    CK(cudaMemcpyAsync(P.trace_ctl, w, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(trace_words, w, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
+    // the kernels take the trace words as an argument (null when off, so an untraced solve
+    // pays no load for it): switching rebuilds the solve graphs at their next use
+    int32_t* want = on ? trace_words : nullptr;
+    if (P.trace_ctl != want) {
+      if (done_ev) CK(cudaEventSynchronize(done_ev));   // no solve graph of ours in flight
+      P.trace_ctl = want;
+      release_graphs();
+    }
     return GC_OK;
   }
 
@@ -990,7 +998,7 @@ struct Pool {
     CK(cudaSetDevice(device));
     int32_t cnt[2];
     CK(cudaStreamSynchronize(s));
-    CK(cudaMemcpy(cnt, P.trace_ctl, sizeof(cnt), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cnt, trace_words, sizeof(cnt), cudaMemcpyDeviceToHost));
     const int have = cnt[1] < GC_TRACE_MAX ? cnt[1] : GC_TRACE_MAX;
     *n = cnt[1];
     const int k = have < max ? have : max;

@@ -47,9 +47,7 @@ struct PoolView {
   int32_t* fcount;        // [2] frontier list lengths
   int32_t* tact;          // [nt] tile has an active pixel (excess > 0, height < HINF)
   int32_t* img_of;        // [nt] image index of the tile
-  int32_t* mdirty;        // [nt] the tile is on the dirty list (its masks are stale)
-  int32_t* dq;            // [nt] dirty list: tiles whose masks k_masks rebuilds
-  int32_t* dcount;        // [1] dirty list length
+  int32_t* mdirty;        // [nt] the tile's planes changed after its masks were written
   long long* tpos;        // [nt] sum of max(excess, 0) over the tile (with the masks)
   int nimg;               // images in the pool
   int32_t* img_live;      // [nimg] cycle stamp of images that still have active tiles
@@ -63,7 +61,8 @@ struct PoolView {
   int32_t* nsel;          // [2] ranges, selected tiles in all
   unsigned long long* ktiles;  // [K_COUNT] tiles processed per kernel kind (profiling)
   // device-side trace of the solve: trace_ctl[0] on, trace_ctl[1] entries written; entry i
-  // is (start time in ns of %globaltimer, kind) in trace[2i], trace[2i + 1]
+  // is (start time in ns of %globaltimer, kind) in trace[2i], trace[2i + 1].  trace_ctl is
+  // null while tracing is off, so the kernels skip the mark without a memory access.
   unsigned long long* trace;
   int32_t* trace_ctl;
 };
@@ -87,8 +86,8 @@ enum CtlSlot {
   CTL_BAD = 12,       // first out-of-range worklist value seen by a self-check
   CTL_BADWHERE = 13,  // 1: worklist append, 2: worklist length, 3: list length, 4: image id
                       // (or tile) of the selection, 5: frontier append, 6: frontier length,
-                      // 7: dirty append, 8: dirty length, 9: selection size
-  CTL_KDONE = 14,     // CTAs finished in k_masks
+                      // 9: selection size
+  CTL_RESERVED = 14,
   CTL_NCHECK = 15,    // flood checks run (k_flood_check launches)
   CTL_NACT = 16,      // active-list rebuilds run (k_active_list launches)
   CTL_LEFT = 17,      // images still running after the last flood check

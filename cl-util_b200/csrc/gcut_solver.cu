@@ -33,6 +33,7 @@
 namespace gcut {
 
 constexpr int DIS_THREADS = 256;
+constexpr int WARPS_PER_CTA = 4;   // warp-per-tile kernels (BFS, flood, mask rebuild)
 
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 
@@ -88,15 +89,62 @@ __device__ __forceinline__ void write_tile_masks(const PoolView& P, int t, const
   }
 }
 
-// Queue tile t for a mask rebuild (k_masks) once: its planes changed after its masks were
-// written.  mdirty[t] == 1 exactly while t is on the dirty list.
-__device__ __forceinline__ void mark_dirty(const PoolView& P, int t) {
-  if (*((volatile int32_t*)&P.mdirty[t]) != 0) return;   // common case: already queued
-  if (atomicExch(&P.mdirty[t], 1) == 0) {
-    const int pos = atomicAdd(P.dcount, 1);
-    if (pos < P.nt) P.dq[pos] = t;   // mdirty deduplicates, so pos < nt always holds
-    else record_bad(P, 7, pos);
+// Tile t's planes changed after its masks were written: the first flood round that covers
+// it (or k_masks) rebuilds them.  A plain store: nothing reads the flag until a later kernel.
+__device__ __forceinline__ void mark_dirty(const PoolView& P, int t) { P.mdirty[t] = 1; }
+
+// Row masks of one tile row, as write_tile_masks writes them.
+struct RowMasks { uint32_t up, down, left, right, sink, exc; };
+
+// Rebuilds tile t's row masks and its sum of max(excess, 0) from its planes with one warp:
+// lane c reads column c of four rows at a time (one 128-byte line per row and plane), and a
+// ballot over the lanes is the row's mask.  Writes the masks and the sum, clears the dirty
+// flag, and returns row `lane`'s masks to each lane and the tile's sum to every lane.
+__device__ __forceinline__ RowMasks warp_rebuild_masks(const PoolView& P, int t, int lane,
+                                                       long long* tile_pos) {
+  const unsigned F = 0xffffffffu;
+  const long long base = (long long)t * GC_TILE_PX + lane;
+  RowMasks out{0u, 0u, 0u, 0u, 0u, 0u};
+  long long pos = 0;
+#pragma unroll 1
+  for (int r0 = 0; r0 < GC_TILE; r0 += 4) {
+    int v[4][5];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const long long o = base + (r0 + k) * GC_TILE;
+      v[k][0] = P.exc[o];
+      v[k][1] = P.cap[DUP][o];
+      v[k][2] = P.cap[DDOWN][o];
+      v[k][3] = P.cap[DLEFT][o];
+      v[k][4] = P.cap[DRIGHT][o];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t mu = __ballot_sync(F, v[k][1] > 0), md = __ballot_sync(F, v[k][2] > 0);
+      const uint32_t ml = __ballot_sync(F, v[k][3] > 0), mr = __ballot_sync(F, v[k][4] > 0);
+      const uint32_t ms = __ballot_sync(F, v[k][0] < 0), me = __ballot_sync(F, v[k][0] > 0);
+      if (lane == r0 + k) {
+        out.up = mu; out.down = md; out.left = ml; out.right = mr;
+        out.sink = ms; out.exc = me;
+      }
+      pos += v[k][0] > 0 ? v[k][0] : 0;
+    }
   }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) pos += __shfl_xor_sync(F, pos, o);
+  uint32_t* mc = P.mcan + (long long)t * 128;
+  mc[lane] = out.up;
+  mc[32 + lane] = out.down;
+  mc[64 + lane] = out.left;
+  mc[96 + lane] = out.right;
+  P.msink[(long long)t * 32 + lane] = out.sink;
+  P.mexc[(long long)t * 32 + lane] = out.exc;
+  if (lane == 0) {
+    P.tpos[t] = pos;
+    P.mdirty[t] = 0;
+  }
+  *tile_pos = pos;
+  return out;
 }
 
 // Capacity sources of the upload.  PlaneSource: row-major capacity planes (gc_upload).
@@ -282,67 +330,41 @@ k_upload(PoolView P, ImageDesc im, int img, Source src, int32_t* __restrict__ tl
     P.mark[1][t] = 0;
     P.inq[0][t] = 0;
     P.inq[1][t] = 0;
-    P.img_of[t] = img;   // (a tile still on the dirty list is rebuilt once more: harmless)
+    P.img_of[t] = img;
+    P.mdirty[t] = 0;     // the masks above are current
   }
 }
 
-// Mask rebuild of the tiles on the dirty list (dq[0 .. *dcount)), before a global relabel:
-// one tile per CTA iteration, the 256 threads read the tile's planes with int4 loads (an HBM
-// stream, unlike a per-warp rebuild inside the BFS), write its row masks and its sum of
-// max(excess, 0), and take it off the list.  Only the CTAs the list needs take part; the
-// last of them empties the list.
-__global__ void __launch_bounds__(DIS_THREADS)
+// Mask rebuild of the selected tiles whose planes changed since their masks were written
+// (dirty flag set), one warp per tile.  The solve loops do not need it: their first flood
+// round rebuilds the dirty tiles it covers.  It precedes a global relabel that no flood
+// precedes (gc_start_bfs).
+__global__ void __launch_bounds__(WARPS_PER_CTA * 32)
 k_masks(PoolView P) {
   trace_mark(P, TR_MASKS);
-  __shared__ int s_n;
-  __shared__ long long wpos[DIS_THREADS / 32];
+  __shared__ int s_n, s_nr;
   if (threadIdx.x == 0) {
-    int n = *((volatile int32_t*)P.dcount);
-    if (n < 0 || n > P.nt) {   // self-check: the list holds each tile at most once
-      record_bad(P, 8, n);
-      n = 0;
+    int n = *((volatile int32_t*)&P.nsel[1]), nr = *((volatile int32_t*)&P.nsel[0]);
+    if (n < 0 || n > P.nt || nr < 0 || nr > P.nimg) {   // self-check
+      record_bad(P, 9, n);
+      n = nr = 0;
     }
     s_n = n;
+    s_nr = nr;
   }
   __syncthreads();
   const int n = s_n;
-  const int need = n < 1 ? 1 : n;
-  const int parts = need < (int)gridDim.x ? need : (int)gridDim.x;
-  if ((int)blockIdx.x >= parts) return;
-  const int r = threadIdx.x >> 3, c0 = (threadIdx.x & 7) * 4;
-  const int pix = r * GC_TILE + c0;
-  for (int li = blockIdx.x; li < n; li += parts) {
-    const int t = P.dq[li];
-    const long long off = (long long)t * GC_TILE_PX + pix;
-    int e[4], cu[4], cd[4], cl[4], cr[4];
-    int4 v = *reinterpret_cast<const int4*>(P.exc + off); e[0] = v.x; e[1] = v.y; e[2] = v.z; e[3] = v.w;
-    v = *reinterpret_cast<const int4*>(P.cap[DUP] + off); cu[0] = v.x; cu[1] = v.y; cu[2] = v.z; cu[3] = v.w;
-    v = *reinterpret_cast<const int4*>(P.cap[DDOWN] + off); cd[0] = v.x; cd[1] = v.y; cd[2] = v.z; cd[3] = v.w;
-    v = *reinterpret_cast<const int4*>(P.cap[DLEFT] + off); cl[0] = v.x; cl[1] = v.y; cl[2] = v.z; cl[3] = v.w;
-    v = *reinterpret_cast<const int4*>(P.cap[DRIGHT] + off); cr[0] = v.x; cr[1] = v.y; cr[2] = v.z; cr[3] = v.w;
-    write_tile_masks(P, t, e, cu, cd, cl, cr);
-    long long pos = 0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) pos += e[j] > 0 ? e[j] : 0;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) pos += __shfl_xor_sync(0xffffffffu, pos, o);
-    if ((threadIdx.x & 31) == 0) wpos[threadIdx.x >> 5] = pos;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      long long tp = 0;
-      for (int k = 0; k < DIS_THREADS / 32; ++k) tp += wpos[k];
-      P.tpos[t] = tp;
-      P.mdirty[t] = 0;
-      if (P.ktiles) atomicAdd(&P.ktiles[K_MASKS], 1ull);
-    }
-    __syncthreads();   // wpos is reused by the next tile
+  const int lane = threadIdx.x & 31;
+  const int i0 = blockIdx.x * WARPS_PER_CTA + (threadIdx.x >> 5);
+  const int stride = gridDim.x * WARPS_PER_CTA;
+  SelCursor cursor(P, s_nr, i0 < n ? i0 : 0);
+  for (int i = i0; i < n; i += stride) {
+    const int t = cursor.tile(i);
+    if (P.mdirty[t] == 0) continue;   // the same word for every lane: warp-uniform
+    long long pos;
+    warp_rebuild_masks(P, t, lane, &pos);
+    if (lane == 0 && P.ktiles) atomicAdd(&P.ktiles[K_MASKS], 1ull);
   }
-  if (threadIdx.x != 0) return;
-  __threadfence();
-  if (atomicAdd(&P.ctl[CTL_KDONE], 1) != parts - 1) return;
-  __threadfence();
-  P.ctl[CTL_KDONE] = 0;
-  *P.dcount = 0;
 }
 
 // ------------------------------------------------------------------------------------
@@ -738,7 +760,7 @@ k_discharge(PoolView P, int iters) {
       const int target = tid == 0 ? t : tid == 1 ? nb.x : tid == 2 ? nb.y : tid == 3 ? nb.z : nb.w;
       if (tid == 0 || ((bits >> (tid - 1)) & 1)) {
         P.touched[target] = 1;
-        mark_dirty(P, target);
+        mark_dirty(P, target);   // its masks are rebuilt by the next flood's first round
         if (tid == 0) P.act_int[t] = act_int;
         if (tid != 0 || any_act) worklist_add(P, nxt, target);
         if (tid == 0 && P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
@@ -886,7 +908,6 @@ k_edge_relabel_build(PoolView P, int32_t* list, int32_t* count, ScanState st) {
 // ------------------------------------------------------------------------------------
 // Global relabel: bit-parallel BFS per tile, one warp per tile, lane = row.
 // ------------------------------------------------------------------------------------
-constexpr int WARPS_PER_CTA = 4;
 
 __device__ __forceinline__ int warp_min(int v) {
 #pragma unroll
@@ -981,8 +1002,10 @@ __device__ __forceinline__ void frontier_work(const PoolView& P, int first, int 
   *participants = need < 1 ? 1 : (need < (int)gridDim.x ? need : (int)gridDim.x);
 }
 
-// Queue tile t for the next round (once).
+// Queue tile t for the next round (once).  Within a round the next round's marks only go
+// from 0 to 1, so a set mark read with a plain load needs no atomic.
 __device__ __forceinline__ void frontier_push(const PoolView& P, int out, int t) {
+  if (*((volatile int32_t*)&P.mark[out][t]) != 0) return;
   if (atomicExch(&P.mark[out][t], 1) == 0) {
     const int pos = atomicAdd(&P.fcount[out], 1);
     if (pos < P.nt) P.fq[out][pos] = t;   // the mark deduplicates, so pos < nt always holds
@@ -1159,6 +1182,8 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
       }
     }
     if (chunk == nchunks - 1 && threadIdx.x == 0) *count = s_excl + agg;
+    // the first tickets are 0 .. gridDim.x - 1: when they cover every chunk, none is left
+    if ((int)gridDim.x >= nchunks) break;
     __syncthreads();   // every thread has read s_chunk and s_excl
     if (threadIdx.x == 0) s_chunk = atomicAdd(st.ticket, 1);
     __syncthreads();
@@ -1253,7 +1278,8 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
     ++done;
     const int4 nb = P.nbr[t];
     const long long base = (long long)t * GC_TILE_PX;
-    // the masks are current: k_masks rebuilt every tile that changed since they were written
+    // the masks are current: the flood that precedes every global relabel of a solve (or
+    // k_masks, before gc_start_bfs) rebuilt every tile that changed since they were written
     const uint32_t* mc = P.mcan + (long long)t * 128;
     const uint32_t canU = mc[lane], canD = mc[32 + lane], canL = mc[64 + lane], canR = mc[96 + lane];
     const uint32_t sink = P.msink[(long long)t * 32 + lane];
@@ -1295,12 +1321,12 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
     chL = __any_sync(0xffffffffu, chL); chR = __any_sync(0xffffffffu, chR);
     const uint32_t pos = P.mexc[(long long)t * 32 + lane];
     const int act = __any_sync(0xffffffffu, (pos & fin) != 0);
-    if (lane == 0) {
-      P.tact[t] = act;
-      if (chU && nb.x >= 0) frontier_push(P, out, nb.x);
-      if (chD && nb.y >= 0) frontier_push(P, out, nb.y);
-      if (chL && nb.z >= 0) frontier_push(P, out, nb.z);
-      if (chR && nb.w >= 0) frontier_push(P, out, nb.w);
+    if (lane == 0) P.tact[t] = act;
+    // the neighbours to queue, one lane each (their atomics run in parallel)
+    if (lane < 4) {
+      const int go = lane == 0 ? chU : lane == 1 ? chD : lane == 2 ? chL : chR;
+      const int nt = lane == 0 ? nb.x : lane == 1 ? nb.y : lane == 2 ? nb.z : nb.w;
+      if (go && nt >= 0) frontier_push(P, out, nt);
     }
   }
   if (lane == 0 && done) {
@@ -1354,15 +1380,29 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
     if (mode == 0 && abort_hit && *((volatile int32_t*)&P.img_hit[img]) == stamp) continue;
     ++done;
     const int4 nb = P.nbr[t];
-    const uint32_t* mc = P.mcan + (long long)t * 128;
-    const uint32_t canU = mc[lane], canD = mc[32 + lane], canL = mc[64 + lane], canR = mc[96 + lane];
-    uint32_t R, R0;
+    uint32_t canU, canD, canL, canR, sink, R, R0;
+    long long ps = 0;
+    if (first && P.mdirty[t] != 0) {
+      // the tile changed since its masks were written (a discharge or an edit): rebuild them
+      // here, before anything reads them (every tile of an image this round covers is done
+      // in this round, so the frontier rounds and the global relabel after it see them)
+      const RowMasks m = warp_rebuild_masks(P, t, lane, &ps);
+      canU = m.up; canD = m.down; canL = m.left; canR = m.right;
+      sink = m.sink;
+      R = m.exc;
+    } else {
+      const uint32_t* mc = P.mcan + (long long)t * 128;
+      canU = mc[lane]; canD = mc[32 + lane]; canL = mc[64 + lane]; canR = mc[96 + lane];
+      sink = P.msink[(long long)t * 32 + lane];
+      if (first) {
+        R = P.mexc[(long long)t * 32 + lane];
+        ps = P.tpos[t];
+      }
+    }
     if (first) {
-      R = P.mexc[(long long)t * 32 + lane];
       R0 = 0;
-      // Σ max(excess, 0) of the tile was taken with its masks after the tile last changed;
-      // summed per warp and per CTA before the add to the image's word
-      const long long ps = P.tpos[t];
+      // Σ max(excess, 0) of the tile, taken with its masks; summed per warp and per CTA
+      // before the add to the image's word
       if (lane == 0 && ps) {
         if (img != wimg) {
           if (wsum) atomicAdd(&acc[wimg].sumpos_e, wsum);
@@ -1392,7 +1432,7 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
       R = N;
     }
     P.mreach[(long long)t * 32 + lane] = R;
-    if (__any_sync(0xffffffffu, (R & P.msink[(long long)t * 32 + lane]) != 0) && lane == 0 &&
+    if (__any_sync(0xffffffffu, (R & sink) != 0) && lane == 0 &&
         *((volatile int32_t*)&P.img_hit[img]) != stamp)
       P.img_hit[img] = stamp;
     const uint32_t nw = first ? R : (R & ~R0);
@@ -1400,11 +1440,10 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
     const int sD = __any_sync(0xffffffffu, lane == 31 && (nw & canD));
     const int sL = __any_sync(0xffffffffu, (nw & canL & 1u) != 0);
     const int sR = __any_sync(0xffffffffu, ((nw & canR) >> 31) != 0);
-    if (lane == 0) {
-      if (sU && nb.x >= 0) frontier_push(P, out, nb.x);
-      if (sD && nb.y >= 0) frontier_push(P, out, nb.y);
-      if (sL && nb.z >= 0) frontier_push(P, out, nb.z);
-      if (sR && nb.w >= 0) frontier_push(P, out, nb.w);
+    if (lane < 4) {   // the neighbours to queue, one lane each
+      const int go = lane == 0 ? sU : lane == 1 ? sD : lane == 2 ? sL : sR;
+      const int nt = lane == 0 ? nb.x : lane == 1 ? nb.y : lane == 2 ? nb.z : nb.w;
+      if (go && nt >= 0) frontier_push(P, out, nt);
     }
   }
   if (lane == 0 && done) {
@@ -1720,7 +1759,7 @@ int launch_dsum(const uint32_t* rgba, int W, int H, unsigned long long* sum, int
 }
 
 int launch_masks(const PoolView& P, int grid, cudaStream_t s) {
-  k_masks<<<grid, DIS_THREADS, 0, s>>>(P);
+  k_masks<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P);
   return ok();
 }
 

@@ -308,7 +308,11 @@ const char* gc_kernel_name(int kind);
    round, 9 upload, 10 labels, 11 solve end.  gc_set_trace turns it on or off and empties
    the buffer; gc_get_trace copies up to max_entries entries (two uint64 each) and sets *n
    to the number written since (it may exceed the buffer).  Both synchronise `stream`.
-   No counterpart in the reference (its host loop timed kernels with OpenCL events). */
+   The kernels take the trace as an argument, so an untraced solve pays nothing for it;
+   switching it on or off therefore rebuilds the solve's CUDA graph at the next solve (one
+   graph instantiation; calling gc_set_trace again with the same state only empties the
+   buffer).  No counterpart in the reference (its host loop timed kernels with OpenCL
+   events). */
 #define GC_TRACE_MAX 2048
 int gc_set_trace(gc_handle* h, int on, void* stream);
 int gc_get_trace(gc_handle* h, uint64_t* entries, int max_entries, int* n, void* stream);
