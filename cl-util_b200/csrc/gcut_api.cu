@@ -406,6 +406,13 @@ struct Pool {
     h_count = static_cast<int32_t*>(pin);
     h_ctl = reinterpret_cast<int32_t*>(static_cast<char*>(pin) + 256);
     h_acc = reinterpret_cast<ImageAcc*>(static_cast<char*>(pin) + 512);
+    {   // the kernel that ends a graph solve writes the results here itself (no copy node)
+      void* dptr = nullptr;
+      if (cudaHostGetDevicePointer(&dptr, h_ctl, 0) == cudaSuccess && dptr)
+        P.host_out = static_cast<int32_t*>(dptr);
+      else
+        cudaGetLastError();
+    }
     h_sel = static_cast<char*>(pin) + acc_end;
     // every buffer starts at zero; the look-back tag starts at 1
     CK(cudaMemset(arena, 0, arena_bytes));
@@ -767,14 +774,20 @@ struct Pool {
     cudaGraphConditionalHandle hf, hbfs, hb;
     RK(cond_handle(&hf, g));
     RK(cond_handle(&hbfs, g));
-    RK(capture(g, L, [&](cudaStream_t cs) { return launch_flood_round(P, mode, 1, hf, acc, grid_warps, cs); }));
+    // the round that ends the flood runs the flood check (retires the solved images, sets
+    // the IF condition below and, when none is left, ends the solve loop)
+    const cudaGraphConditionalHandle hm = all ? 0 : hmain;
+    RK(capture(g, L, [&](cudaStream_t cs) {
+      return launch_flood_round(P, mode, 1, hf, acc, grid_warps, cs, all, hbfs, hm);
+    }));
     cudaGraph_t bf;
     RK(add_while(g, L, hf, &bf));
     {
       std::vector<cudaGraphNode_t> Lf;
-      RK(capture(bf, Lf, [&](cudaStream_t cs) { return launch_flood_round(P, 0, 1, hf, acc, grid_warps, cs); }));
+      RK(capture(bf, Lf, [&](cudaStream_t cs) {
+        return launch_flood_round(P, 0, 1, hf, acc, grid_warps, cs, all, hbfs, hm);
+      }));
     }
-    RK(capture(g, L, [&](cudaStream_t cs) { return launch_flood_check(P, all, hbfs, all ? 0 : hmain, cs); }));
     cudaGraph_t bi;
     RK(add_if(g, L, hbfs, &bi));
     std::vector<cudaGraphNode_t> Li;
@@ -823,12 +836,14 @@ struct Pool {
       }));
       RK(graph_cycle_tail(bm, Lm, /*mode=*/2, /*all=*/0, /*bump=*/1, hmain));
     }
-    RK(capture(g, L, [&](cudaStream_t cs) {
-      // control words and per-image sums are adjacent on both sides: one copy
-      CK(cudaMemcpyAsync(h_ctl, P.ctl, sizeof(int32_t) * CTL_N + sizeof(ImageAcc) * imgs.size(),
-                         cudaMemcpyDeviceToHost, cs));
-      return GC_OK;
-    }));
+    if (!P.host_out) {   // else the kernel that ends the solve wrote them already
+      RK(capture(g, L, [&](cudaStream_t cs) {
+        // control words and per-image sums are adjacent on both sides: one copy
+        CK(cudaMemcpyAsync(h_ctl, P.ctl, sizeof(int32_t) * CTL_N + sizeof(ImageAcc) * imgs.size(),
+                           cudaMemcpyDeviceToHost, cs));
+        return GC_OK;
+      }));
+    }
     CK(cudaGraphInstantiate(&gexec[variant], g, 0));
     // upload the executable graph here, under the construction lock, rather than implicitly
     // at its first launch next to other threads' graph work

@@ -65,6 +65,9 @@ struct PoolView {
   // null while tracing is off, so the kernels skip the mark without a memory access.
   unsigned long long* trace;
   int32_t* trace_ctl;
+  // pinned host memory (as the device sees it) that the kernel ending a graph solve writes
+  // the control words and the per-image sums to; null: the graph copies them instead
+  int32_t* host_out;
 };
 
 // Device-side loop control words.  The last CTA of every frontier round advances the round
@@ -138,15 +141,21 @@ enum TraceKind { TR_BEGIN = 0, TR_ACTIVE_LIST, TR_DISCHARGE, TR_MASKS, TR_FLOOD_
 #define GC_TRACE_MAX 2048
 #endif
 
-// Records the start of a kernel in the solve's trace (CTA 0, thread 0, when tracing is on).
-__device__ __forceinline__ void trace_mark(const PoolView& P, int kind) {
-  if (blockIdx.x != 0 || threadIdx.x != 0 || !P.trace_ctl) return;
+// Records an event in the solve's trace when tracing is on (one calling thread).
+__device__ __forceinline__ void trace_record(const PoolView& P, int kind) {
+  if (!P.trace_ctl) return;
   if (*((volatile int32_t*)&P.trace_ctl[0]) == 0) return;
   const int i = atomicAdd(&P.trace_ctl[1], 1);
   if (i < GC_TRACE_MAX) {
     P.trace[2 * i] = global_ns();
     P.trace[2 * i + 1] = (unsigned long long)kind;
   }
+}
+
+// Records the start of a kernel in the solve's trace (CTA 0, thread 0, when tracing is on).
+__device__ __forceinline__ void trace_mark(const PoolView& P, int kind) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  trace_record(P, kind);
 }
 
 // Kernel kinds for profiling (launch counts, event time, tiles processed).

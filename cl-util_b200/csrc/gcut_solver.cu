@@ -1071,6 +1071,20 @@ __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc
   }
 }
 
+// The solve's results (the control words, then the per-image sums: the layout of the host
+// mirror) written straight into pinned host memory by the kernel that ends a graph solve, so
+// the graph needs no copy node after its loops.  Threads 0 .. nthreads-1 take part.
+__device__ __forceinline__ void publish_results(const PoolView& P, const ImageAcc* acc,
+                                                int nthreads) {
+  if (!P.host_out) return;
+  const int na = P.nimg * (int)(sizeof(ImageAcc) / sizeof(int32_t));
+  const volatile int32_t* c = P.ctl;
+  const volatile int32_t* a = reinterpret_cast<const volatile int32_t*>(acc);
+  for (int i = threadIdx.x; i < CTL_N + na; i += nthreads)
+    P.host_out[i] = i < CTL_N ? c[i] : a[i - CTL_N];
+  __threadfence_system();
+}
+
 // The active-tile list after a global relabel, in one launch: a single-pass scan (chunks by
 // arrival ticket, decoupled look-back) of the activity flags of the selected tiles writes the
 // ids of the active tiles in order and stamps their images live for the next cycle (stamp =
@@ -1218,6 +1232,7 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
   }
   __threadfence();
   if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
+  if (h && !more) publish_results(P, acc, 1);   // the graph solve ends here
 }
 
 // After the active-tile compaction: another cycle runs while tiles are active and the cycle
@@ -1336,6 +1351,95 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
   frontier_round_end(P, first, in, CTL_BFS_TOTAL, parts, h);
 }
 
+// After a flood: an image whose flood reached no sink pixel is solved (its flood is the
+// canonical cut, its sums are final) and leaves the live set; the others go on to a global
+// relabel.  all != 0: the images that continue from a previous flow (img_mode == 2; the
+// first check of a solve); else the images live in this cycle.  Sets the condition of the
+// IF node around the relabel (hbfs) and, when no image is left, ends the solve loop (hmain);
+// the last cycle of a solve is counted here.  Every thread of one CTA calls it: k_flood_check,
+// or the last CTA of the flood's last round, which reads what the round's other CTAs wrote
+// (their fence before the round's count orders it), hence the volatile loads.
+__device__ void flood_check_cta(const PoolView& P, int all, cudaGraphConditionalHandle hbfs,
+                                cudaGraphConditionalHandle hmain, const ImageAcc* acc) {
+  __shared__ int s_left, s_n;
+  if (threadIdx.x == 0) {
+    s_left = 0;
+    trace_record(P, TR_CHECK);
+  }
+  __syncthreads();
+  volatile int32_t* ctl = P.ctl;
+  const int stamp = ctl[CTL_CYCLES] + 1;
+  int left = 0;
+  for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) {
+    const bool part = all ? *((volatile int32_t*)&P.img_mode[i]) == 2
+                          : *((volatile int32_t*)&P.img_live[i]) == stamp;
+    if (!part) continue;
+    if (*((volatile int32_t*)&P.img_hit[i]) == stamp) {
+      P.img_live[i] = stamp;
+      ++left;
+    } else {
+      P.img_live[i] = 0;   // solved: no later stamp equals 0
+    }
+  }
+  if (left) atomicAdd(&s_left, left);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int n = s_left;
+    if (ctl[CTL_ERR] != 0) n = 0;   // a cap or a self-check ends the loops
+    ctl[CTL_LEFT] = n;
+    ctl[CTL_NCHECK] = ctl[CTL_NCHECK] + 1;
+    if (n == 0 && !all) ctl[CTL_CYCLES] = ctl[CTL_CYCLES] + 1;
+    __threadfence();
+    if (hbfs) cudaGraphSetConditional(hbfs, n > 0 ? 1u : 0u);
+    if (hmain && n == 0) cudaGraphSetConditional(hmain, 0u);
+    if (n == 0) trace_record(P, TR_END);
+    s_n = n;
+  }
+  __syncthreads();
+  if (s_n == 0 && hmain) publish_results(P, acc, blockDim.x);   // the graph solve ends here
+}
+
+// End of a flood round: frontier_round_end's bookkeeping by the round's last CTA; when the
+// flood is over (no frontier left, or a cap), that CTA runs the flood check too (check >= 0
+// is its `all`), so the solve graph needs no separate check launch.  Every thread calls it.
+__device__ __forceinline__ void flood_round_end(const PoolView& P, int first, int in, int parts,
+                                                cudaGraphConditionalHandle h, int check,
+                                                cudaGraphConditionalHandle hbfs,
+                                                cudaGraphConditionalHandle hmain,
+                                                const ImageAcc* acc) {
+  __shared__ int s_last, s_more;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&P.ctl[CTL_DONE], 1) == parts - 1;
+    if (s_last) {
+      __threadfence();
+      volatile int32_t* ctl = P.ctl;
+      const int out = in ^ 1;
+      P.rcnt[in] = 0;
+      const int next = *((volatile int32_t*)&P.fcount[out]);
+      P.fcount[in] = 0;   // this round's list is consumed
+      ctl[CTL_LASTCNT] = next;
+      ctl[CTL_RND] = first ? 1 : ctl[CTL_RND] + 1;
+      const int rounds = first ? 1 : ctl[CTL_ROUNDS] + 1;
+      ctl[CTL_ROUNDS] = rounds;
+      ctl[CTL_FLOOD_TOTAL] = ctl[CTL_FLOOD_TOTAL] + 1;
+      ctl[CTL_DONE] = 0;
+      bool more = next > 0 && ctl[CTL_ERR] < 3;   // a copy or self-check error ends the loop
+      if (more && rounds >= ctl[CTL_MAXROUNDS]) {
+        ctl[CTL_ERR] = 1;
+        more = false;
+      }
+      __threadfence();
+      if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
+      s_more = more;
+    }
+  }
+  __syncthreads();
+  if (!s_last || check < 0 || s_more) return;
+  flood_check_cta(P, check, hbfs, hmain, acc);
+}
+
 // ------------------------------------------------------------------------------------
 // Canonical cut: flood from excess pixels over residual edges (forward direction).
 // The first flood round also sums max(excess, 0) per image for the flow value.
@@ -1352,7 +1456,8 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
 // stamped (their flood is redone in a later cycle).
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
-k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h, ImageAcc* acc) {
+k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h, ImageAcc* acc,
+              int check, cudaGraphConditionalHandle hbfs, cudaGraphConditionalHandle hmain) {
   trace_mark(P, mode ? TR_FLOOD_FIRST : TR_FLOOD);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int first = mode != 0;
@@ -1468,45 +1573,14 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
       }
     }
   }
-  frontier_round_end(P, first, in, CTL_FLOOD_TOTAL, parts, h);
+  flood_round_end(P, first, in, parts, h, check, hbfs, hmain, acc);
 }
 
-// After a flood: an image whose flood reached no sink pixel is solved (its flood is the
-// canonical cut, its sums are final) and leaves the live set; the others go on to a global
-// relabel.  all != 0: the images that continue from a previous flow (img_mode == 2; the
-// first check of a solve); else the images live in this cycle.  Sets the condition of the
-// IF node around the relabel (hbfs) and, when no image is left, ends the solve loop (hmain);
-// the last cycle of a solve is counted here.  One CTA.
+// After a flood (host-driven loops; the solve graph runs the check at the end of its last
+// flood round instead): see flood_check_cta.  One CTA.
 __global__ void k_flood_check(PoolView P, int all, cudaGraphConditionalHandle hbfs,
                               cudaGraphConditionalHandle hmain) {
-  trace_mark(P, TR_CHECK);
-  __shared__ int s_left;
-  if (threadIdx.x == 0) s_left = 0;
-  __syncthreads();
-  volatile int32_t* ctl = P.ctl;
-  const int stamp = ctl[CTL_CYCLES] + 1;
-  int left = 0;
-  for (int i = threadIdx.x; i < P.nimg; i += blockDim.x) {
-    if (all ? P.img_mode[i] != 2 : P.img_live[i] != stamp) continue;
-    if (P.img_hit[i] == stamp) {
-      P.img_live[i] = stamp;
-      ++left;
-    } else {
-      P.img_live[i] = 0;   // solved: no later stamp equals 0
-    }
-  }
-  if (left) atomicAdd(&s_left, left);
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  int n = s_left;
-  if (ctl[CTL_ERR] != 0) n = 0;   // a cap or a self-check ends the loops
-  ctl[CTL_LEFT] = n;
-  ctl[CTL_NCHECK] = ctl[CTL_NCHECK] + 1;
-  if (n == 0 && !all) ctl[CTL_CYCLES] = ctl[CTL_CYCLES] + 1;
-  __threadfence();
-  if (hbfs) cudaGraphSetConditional(hbfs, n > 0 ? 1u : 0u);
-  if (hmain && n == 0) cudaGraphSetConditional(hmain, 0u);
-  if (n == 0) trace_mark(P, TR_END);
+  flood_check_cta(P, all, hbfs, hmain, nullptr);
 }
 
 // Neighbour tile ids and image index of one image's tiles (row-major from im.tile0), for an
@@ -1783,8 +1857,9 @@ int launch_bfs_round(const PoolView& P, int first, cudaGraphConditionalHandle h,
 }
 
 int launch_flood_round(const PoolView& P, int mode, int abort_hit, cudaGraphConditionalHandle h,
-                       ImageAcc* acc, int grid, cudaStream_t s) {
-  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, mode, abort_hit, h, acc);
+                       ImageAcc* acc, int grid, cudaStream_t s, int check,
+                       cudaGraphConditionalHandle hbfs, cudaGraphConditionalHandle hmain) {
+  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, mode, abort_hit, h, acc, check, hbfs, hmain);
   return ok();
 }
 
