@@ -817,14 +817,21 @@ struct Pool {
     std::vector<cudaGraphNode_t> L;
     cudaGraphConditionalHandle hmain;
     RK(cond_handle(&hmain, g));
-    RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs); }));
-    if (variant) {
-      // images that continue from a previous flow: flood them; relabel the ones not solved
-      RK(graph_cycle_tail(g, L, /*mode=*/3, /*all=*/1, /*bump=*/0, hmain));
+    if (!variant && nt <= begin_list_max_tiles()) {
+      // fresh images only, a small pool: the prologue and the first active list in one CTA
+      RK(capture(g, L, [&](cudaStream_t cs) {
+        return launch_begin_list(P, opts.max_bfs_rounds, opts.max_cycles, acc, list, counts, hmain, cs);
+      }));
+    } else {
+      RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs); }));
+      if (variant) {
+        // images that continue from a previous flow: flood them; relabel the ones not solved
+        RK(graph_cycle_tail(g, L, /*mode=*/3, /*all=*/1, /*bump=*/0, hmain));
+      }
+      RK(capture(g, L, [&](cudaStream_t cs) {   // the first active list (fresh and live images)
+        return launch_active_list(P, scan.st, list, counts, 0, 0, 2, hmain, acc, 2 * sms, cs);
+      }));
     }
-    RK(capture(g, L, [&](cudaStream_t cs) {   // the first active list (fresh and live images)
-      return launch_active_list(P, scan.st, list, counts, 0, 0, 2, hmain, acc, 2 * sms, cs);
-    }));
     cudaGraph_t bm;
     RK(add_while(g, L, hmain, &bm));
     {

@@ -100,6 +100,11 @@ int launch_ctl_begin(const PoolView& P, int max_rounds, int max_cycles, ImageAcc
 int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, int32_t* count,
                        int bump, int count_cycle, int filter, cudaGraphConditionalHandle h,
                        ImageAcc* acc, int grid, cudaStream_t s);
+// launch_ctl_begin followed by the first launch_active_list (filter 2, no flood before it) in
+// one single-CTA launch, for pools of at most begin_list_max_tiles() tiles
+int begin_list_max_tiles();
+int launch_begin_list(const PoolView& P, int max_rounds, int max_cycles, ImageAcc* acc,
+                      int32_t* list, int32_t* count, cudaGraphConditionalHandle h, cudaStream_t s);
 int launch_acc_reset(ImageAcc* acc, int n, cudaStream_t s);
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s);

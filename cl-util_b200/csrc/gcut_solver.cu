@@ -1235,6 +1235,107 @@ k_active_list(PoolView P, ScanState st, int32_t* list, int32_t* count, int bump,
   if (h && !more) publish_results(P, acc, 1);   // the graph solve ends here
 }
 
+// k_ctl_begin and the first active-tile list of a solve of fresh images only (no flood
+// precedes that list), in one CTA for pools of at most BL_MAX tiles: the reset, a barrier,
+// then the list with a block-wide scan instead of a look-back, and the list's cycle check.
+// One launch instead of two, and none of the multi-CTA list's tickets and waits.
+constexpr int BL_THREADS = 1024;
+constexpr int BL_ITEMS = 4;
+constexpr int BL_MAX = BL_THREADS * BL_ITEMS;
+
+__global__ void __launch_bounds__(BL_THREADS)
+k_begin_list(PoolView P, int max_rounds, int max_cycles, ImageAcc* acc, int32_t* list,
+             int32_t* count, cudaGraphConditionalHandle h) {
+  trace_mark(P, TR_BEGIN);
+  __shared__ int32_t sm[32];
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int i = tid; i < CTL_N; i += BL_THREADS) P.ctl[i] = 0;
+  for (int i = tid; i < P.nimg; i += BL_THREADS) {
+    P.img_live[i] = 0;
+    P.img_hit[i] = 0;
+    P.img_mode[i] = 0;
+  }
+  __syncthreads();
+  int nr = *((volatile int32_t*)&P.nsel[0]), n = *((volatile int32_t*)&P.nsel[1]);
+  if (n < 0 || n > P.nt || n > BL_MAX || nr < 0 || nr > P.nimg) {   // self-check
+    if (tid == 0) record_bad(P, 9, n);
+    n = nr = 0;
+  }
+  for (int k = tid; k < nr; k += BL_THREADS) {
+    const int img = P.sel[k].w;
+    if ((unsigned)img >= (unsigned)P.nimg) continue;
+    P.img_mode[img] = P.sel_mode[k];
+    acc[img].sumpos_e = 0;   // the floods of this solve accumulate it
+  }
+  if (tid == 0) {
+    P.ctl[CTL_MAXROUNDS] = max_rounds;
+    P.ctl[CTL_MAXCYCLES] = max_cycles;
+    P.rcnt[0] = 0;
+    P.rcnt[1] = 0;
+    P.fcount[0] = 0;
+    P.fcount[1] = 0;
+    trace_record(P, TR_ACTIVE_LIST);
+  }
+  __syncthreads();   // the modes above are visible to every thread
+  // the list: active tiles of the fresh images (cycle stamp 1)
+  const int stamp = 1;
+  const int base = tid * BL_ITEMS;
+  SelCursor cursor(P, nr, base < n ? base : 0);
+  int32_t v[BL_ITEMS], tl[BL_ITEMS], im[BL_ITEMS];
+#pragma unroll
+  for (int k = 0; k < BL_ITEMS; ++k) {
+    tl[k] = -1;
+    im[k] = -1;
+    if (base + k < n) {
+      tl[k] = cursor.tile(base + k);
+      im[k] = cursor.image();
+    }
+    v[k] = 0;
+    if ((unsigned)tl[k] < (unsigned)P.nt && (unsigned)im[k] < (unsigned)P.nimg)
+      v[k] = P.tact[tl[k]] != 0 && P.img_mode[im[k]] == 1;
+    else if (tl[k] >= 0)
+      record_bad(P, 4, (unsigned)im[k] < (unsigned)P.nimg ? tl[k] : im[k]);
+  }
+  int32_t tsum = 0, first = -1;
+#pragma unroll
+  for (int k = BL_ITEMS - 1; k >= 0; --k) {
+    tsum += v[k];
+    if (v[k]) first = im[k];
+  }
+  int32_t agg;
+  int32_t run = block_exclusive_scan(tsum, sm, &agg);
+  const unsigned peers = __match_any_sync(0xffffffffu, first);
+  if (first >= 0 && __ffs(peers) - 1 == lane) stamp_image(P, acc, first, stamp);
+  int last = first;
+#pragma unroll
+  for (int k = 0; k < BL_ITEMS; ++k) {
+    if (v[k]) {
+      if ((unsigned)run < (unsigned)P.nt) list[run] = tl[k];
+      if (im[k] != last) {
+        stamp_image(P, acc, im[k], stamp);
+        last = im[k];
+      }
+      ++run;
+    }
+  }
+  if (tid != 0) return;
+  // the cycle check of k_active_list (count_cycle 0: no cycle has run yet)
+  *count = agg;
+  volatile int32_t* ctl = P.ctl;
+  ctl[CTL_PULSE] = 0;   // the list sits in queue[0]
+  ctl[CTL_DDONE] = 0;
+  P.qcount[1] = 0;
+  ctl[CTL_NACT] = 1;
+  bool more = agg > 0 && ctl[CTL_ERR] < 3;
+  if (more && ctl[CTL_MAXCYCLES] <= 0) {
+    ctl[CTL_ERR] = 2;
+    more = false;
+  }
+  __threadfence();
+  if (h) cudaGraphSetConditional(h, more ? 1u : 0u);
+  if (h && !more) publish_results(P, acc, 1);   // the graph solve ends here
+}
+
 // After the active-tile compaction: another cycle runs while tiles are active and the cycle
 // cap is not reached (`count_cycle` counts this check as a finished cycle).
 __global__ void k_ctl_cycle(PoolView P, const int32_t* count, int count_cycle,
@@ -1896,6 +1997,15 @@ int launch_active_list(const PoolView& P, const ScanState& st, int32_t* list, in
   return ok();
 }
 
+int begin_list_max_tiles() { return BL_MAX; }
+
+int launch_begin_list(const PoolView& P, int max_rounds, int max_cycles, ImageAcc* acc,
+                      int32_t* list, int32_t* count, cudaGraphConditionalHandle h, cudaStream_t s) {
+  if (P.nt > BL_MAX) return GC_ERR_INVALID;
+  k_begin_list<<<1, BL_THREADS, 0, s>>>(P, max_rounds, max_cycles, acc, list, count, h);
+  return ok();
+}
+
 int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s) {
   k_ctl_cycle<<<1, 32, 0, s>>>(P, count, count_cycle, h);
@@ -2000,7 +2110,8 @@ void preload_kernels() {
       (const void*)k_nlink_table,
       (const void*)k_masks, (const void*)k_discharge, (const void*)k_edge_relabel_build,
       (const void*)k_bfs_round, (const void*)k_flood_round, (const void*)k_ctl_begin,
-      (const void*)k_active_list, (const void*)k_ctl_cycle, (const void*)k_flood_check,
+      (const void*)k_active_list, (const void*)k_begin_list, (const void*)k_ctl_cycle,
+      (const void*)k_flood_check,
       (const void*)k_image_tiles,
       (const void*)k_acc_reset, (const void*)k_labels_out, (const void*)k_labels_packed,
       (const void*)k_state_out, (const void*)k_edit, (const void*)k_stroke,
