@@ -87,6 +87,10 @@ def parse():
                     help="warm up, then run one host-driven solve of the --size grid inside the "
                          "NVTX range 'profiled_solve' and print its per-kernel launches and "
                          "tiles (the command the ncu summaries are made from)")
+    ap.add_argument("--profile-graph", action="store_true",
+                    help="with --profile-solve: the profiled solve is the benchmark step itself "
+                         "(upload, then one CUDA-graph solve with its labels, cut_labels), so ncu "
+                         "lists the graph's kernel nodes")
     ap.add_argument("--profile-models", action="store_true",
                     help="one gc_tlinks_gmm launch on the --size image (two 2-component "
                          "full-covariance models) and one gc_gmm_fit launch (10000 samples, 4 "
@@ -627,23 +631,25 @@ def run_profile_solve(args):
     labels = torch.empty((H, W), dtype=torch.uint8, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.Stream()
-    gc = GraphCut(W, H, use_graph=False)
+    graph = bool(args.profile_graph)
+    gc = GraphCut(W, H, use_graph=graph)
     with torch.cuda.stream(stream):
         for _ in range(max(1, args.warmup)):
             gc.upload_capacities(*planes, stream=stream)
-            gc.cut(stream=stream)
+            gc.cut_labels(out=labels, stream=stream)
         flush.fill_(1)
         stream.synchronize()
-        gc.set_profile(True)
+        if not graph:
+            gc.set_profile(True)
         torch.cuda.nvtx.range_push("profiled_solve")
         gc.upload_capacities(*planes, stream=stream)
-        gc.cut(stream=stream)
-        gc.labels(out=labels, stream=stream)
+        gc.cut_labels(out=labels, stream=stream)
         stream.synchronize()
         torch.cuda.nvtx.range_pop()
-        prof = gc.profile()
+        prof = {} if graph else gc.profile()
         gc.set_profile(False)
-    print(json.dumps({"workload": f"{W}x{H} synthetic grid, seed 1, one host-driven solve",
+    how = "one CUDA-graph solve (the benchmark step)" if graph else "one host-driven solve"
+    print(json.dumps({"workload": f"{W}x{H} synthetic grid, seed 1, {how}",
                       "flow": gc.flow, "stats": gc.stats(),
                       "kernels": {k: v for k, v in prof.items() if v["launches"]}}), flush=True)
     gc.close()
