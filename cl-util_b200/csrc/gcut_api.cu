@@ -174,6 +174,7 @@ struct Pool {
   size_t sel_bytes = 0;
   std::vector<int32_t> sel_key, sel_last;   // a selection; the one last copied to the device
   int32_t* trace_words = nullptr;   // device: trace on/off and entry count (P.trace_ctl when on)
+  bool graph_warm = false;          // the last graph solve ran the warm variant
   gc_stats stats{};
   // profiling: event pairs around every launch, tiles processed per kernel kind
   bool prof = false;
@@ -870,6 +871,7 @@ struct Pool {
       }
     }
     P.ktiles = nullptr;
+    graph_warm = warm;
     CK(cudaGraphLaunch(gexec[v], s));
     if (after) RK((*after)(s));
     CK(cudaStreamSynchronize(s));
@@ -915,9 +917,10 @@ struct Pool {
     if (stats.launches < 0) {  // graph solve: count the kernel nodes that ran
       stats.cycles = h_ctl[CTL_CYCLES];
       stats.pulses = stats.cycles * opts.pulses_per_relabel;
-      // ctl_begin, the pulses, one mask rebuild per flood check, the checks, the active
-      // lists and every BFS / flood round
-      stats.launches = 1 + stats.pulses + 2LL * h_ctl[CTL_NCHECK] + h_ctl[CTL_NACT] +
+      // the prologue (k_begin_list also builds the first active list), the active lists,
+      // the pulses and every BFS / flood round (the flood check runs inside the last round)
+      const bool begin_list = !graph_warm && nt <= begin_list_max_tiles();
+      stats.launches = (begin_list ? 0 : 1) + h_ctl[CTL_NACT] + stats.pulses +
                        stats.bfs_rounds + stats.flood_rounds;
     }
     for (int k = 0; k < (idx ? n : (int)imgs.size()); ++k) {

@@ -147,6 +147,11 @@ def test_device_trace_of_a_graph_solve(cuda):
         assert all(b >= a for a, b in zip(stamps, stamps[1:]))
         summ = _gcut.trace_summary(tr)
         assert summ["discharge"][0] == kinds.count("discharge")
+        # every solver kernel of the graph marks its start once; the fresh solve of a pool
+        # this small begins with the one launch that also builds the first active list
+        kernel_marks = sum(kinds.count(k) for k in ("begin", "active_list", "discharge",
+                                                    "flood_first", "flood", "bfs_first", "bfs"))
+        assert gc.stats()["launches"] == kernel_marks - 1
         gc.set_trace(False)
         gc.upload_capacities(*g.planes())
         gc.cut()
