@@ -37,6 +37,16 @@ def _as_i32_device(a, device):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.int32)).to(device)
 
 
+def _device_guard(device):
+    """torch.cuda.device(device), or nothing when `device` is already current: the library
+    selects the device itself, and the guard only restores the caller's afterwards."""
+    import contextlib
+    import torch
+    if torch.cuda.current_device() == device.index:
+        return contextlib.nullcontext()
+    return torch.cuda.device(device)
+
+
 def _on(stream):
     """Makes `stream` torch's current stream (no-op for None), so that torch copies made for
     a call are ordered before the library's kernels on that stream."""
@@ -141,8 +151,12 @@ class GraphCut:
             if tuple(p.shape) != (self.height, self.width):
                 raise ValueError(f"plane shape {tuple(p.shape)} != {(self.height, self.width)}")
         if all(isinstance(p, torch.Tensor) and p.is_cuda for p in planes):
-            with _on(stream):   # conversions are ordered before the upload kernel
-                dev = [_as_i32_device(p, self.device) for p in planes]
+            if all(p.dtype == torch.int32 and p.device == self.device and p.is_contiguous()
+                   for p in planes):
+                dev = planes      # read in place: no conversion to order before the kernel
+            else:
+                with _on(stream):   # conversions are ordered before the upload kernel
+                    dev = [_as_i32_device(p, self.device) for p in planes]
             check(lib().gc_upload(self._h, *[ptr(d) for d in dev], stream_handle(stream)))
             self._keep = dev  # the upload kernel reads them asynchronously
         else:
@@ -205,7 +219,7 @@ class GraphCut:
     # ---- solve ------------------------------------------------------------------
     def cut(self, stream=None):
         """Runs push-relabel to the final cut (GraphCut.cut, GraphCut.pyx:348-418)."""
-        with __import__("torch").cuda.device(self.device):
+        with _device_guard(self.device):
             check(lib().gc_solve(self._h, stream_handle(stream)))
         self._solved = True
         return self
@@ -218,7 +232,7 @@ class GraphCut:
         if out is None:
             shape = (self.height, (self.width + 7) // 8) if packed else (self.height, self.width)
             out = torch.empty(shape, dtype=torch.uint8, device=self.device)
-        with torch.cuda.device(self.device):
+        with _device_guard(self.device):
             check(lib().gc_solve_labels(self._h, ptr(out), int(bool(packed)), stream_handle(stream)))
         self._solved = True
         return out
