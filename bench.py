@@ -601,6 +601,8 @@ def main():
             "roofline": {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
+                         # against the nominal HBM3e figure (8 TB/s), for context
+                         "nominal_peak": 8000.0, "frac_of_nominal": achieved / 8000.0,
                          "algo_bytes_per_launch": algo_bytes / max(1, d["launches"]),
                          "avg_launch_us": 1000 * d["ms"] / max(1, d["launches"])},
             "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 4), "tiles": v["tiles"]}
