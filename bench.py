@@ -87,10 +87,6 @@ def parse():
                     help="warm up, then run one host-driven solve of the --size grid inside the "
                          "NVTX range 'profiled_solve' and print its per-kernel launches and "
                          "tiles (the command the ncu summaries are made from)")
-    ap.add_argument("--profile-graph", action="store_true",
-                    help="with --profile-solve: the profiled solve is the benchmark step itself "
-                         "(upload, then one CUDA-graph solve with its labels, cut_labels), so ncu "
-                         "lists the graph's kernel nodes")
     ap.add_argument("--profile-models", action="store_true",
                     help="one gc_tlinks_gmm launch on the --size image (two 2-component "
                          "full-covariance models) and one gc_gmm_fit launch (10000 samples, 4 "
@@ -633,25 +629,22 @@ def run_profile_solve(args):
     labels = torch.empty((H, W), dtype=torch.uint8, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.Stream()
-    graph = bool(args.profile_graph)
-    gc = GraphCut(W, H, use_graph=graph)
+    gc = GraphCut(W, H, use_graph=False)
     with torch.cuda.stream(stream):
         for _ in range(max(1, args.warmup)):
             gc.upload_capacities(*planes, stream=stream)
             gc.cut_labels(out=labels, stream=stream)
         flush.fill_(1)
         stream.synchronize()
-        if not graph:
-            gc.set_profile(True)
+        gc.set_profile(True)
         torch.cuda.nvtx.range_push("profiled_solve")
         gc.upload_capacities(*planes, stream=stream)
         gc.cut_labels(out=labels, stream=stream)
         stream.synchronize()
         torch.cuda.nvtx.range_pop()
-        prof = {} if graph else gc.profile()
+        prof = gc.profile()
         gc.set_profile(False)
-    how = "one CUDA-graph solve (the benchmark step)" if graph else "one host-driven solve"
-    print(json.dumps({"workload": f"{W}x{H} synthetic grid, seed 1, {how}",
+    print(json.dumps({"workload": f"{W}x{H} synthetic grid, seed 1, one host-driven solve",
                       "flow": gc.flow, "stats": gc.stats(),
                       "kernels": {k: v for k, v in prof.items() if v["launches"]}}), flush=True)
     gc.close()

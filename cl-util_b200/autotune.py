@@ -48,11 +48,11 @@ RUNTIME_GRID = {
 SIZE_CLASSES = ((1 << 18, 384), (1 << 20, 768), (1 << 22, 1536), (None, 4096))
 
 # built-in choices (offline tuning on synthetic grids) used until a class is tuned: one grid
-# 3 x 2 is within a few percent of the best up to 2048^2; 4 x 1 is faster from 4096^2 on;
-# pools of many grids 4 x 2
+# 3 x 2 is the best of the 72 candidates at 2048^2 (0.259 ms against 0.287 for 4 x 2) and at
+# 4096^2 (1.10 ms against 1.21 for 4 x 2; 4 x 1 is not among the best six), and within a few
+# percent of the best on smaller grids; pools of many grids 4 x 2
 BUILTIN = {
-    "single": [dict(discharge_iters=3, pulses_per_relabel=2, initial_relabel=0)] * 3 +
-              [dict(discharge_iters=4, pulses_per_relabel=1, initial_relabel=0)],
+    "single": [dict(discharge_iters=3, pulses_per_relabel=2, initial_relabel=0)] * 4,
     "batch": [dict(discharge_iters=4, pulses_per_relabel=2, initial_relabel=0)] * 4,
 }
 

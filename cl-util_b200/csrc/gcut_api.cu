@@ -1193,8 +1193,8 @@ int gc_opts_default(gc_opts* o) {
   if (!o) return fail(GC_ERR_INVALID, "null opts");
   o->device = 0;
   // autotuned (cl-util_b200/autotune.py) on synthetic grids: 3 in-tile iterations x 2
-  // discharge launches between exact global relabels is within a few percent of the best
-  // from 256^2 to 2048^2 (4 x 1 wins by 19 % at 4096^2 but loses on grids below 2048^2)
+  // discharge launches between exact global relabels is the best of the offline grid at
+  // 2048^2 and 4096^2 and within a few percent of the best on smaller grids
   o->discharge_iters = 3;
   o->pulses_per_relabel = 2;
   o->initial_relabel = 0;

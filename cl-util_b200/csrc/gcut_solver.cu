@@ -1071,17 +1071,26 @@ __global__ void k_ctl_begin(PoolView P, int max_rounds, int max_cycles, ImageAcc
   }
 }
 
-// The solve's results (the control words, then the per-image sums: the layout of the host
-// mirror) written straight into pinned host memory by the kernel that ends a graph solve, so
-// the graph needs no copy node after its loops.  Threads 0 .. nthreads-1 take part.
+// The solve's results written straight into pinned host memory by the kernel that ends a
+// graph solve, so the graph needs no copy node after its loops: the control words, then the
+// sums of the solve's images at their places in the host mirror (the other images' sums have
+// not changed since their own solves).  Threads 0 .. nthreads-1 take part.
 __device__ __forceinline__ void publish_results(const PoolView& P, const ImageAcc* acc,
                                                 int nthreads) {
   if (!P.host_out) return;
-  const int na = P.nimg * (int)(sizeof(ImageAcc) / sizeof(int32_t));
+  constexpr int AW = (int)(sizeof(ImageAcc) / sizeof(int32_t));
+  int nr = *((volatile int32_t*)&P.nsel[0]);
+  nr = nr < 0 ? 0 : nr > P.nimg ? P.nimg : nr;
   const volatile int32_t* c = P.ctl;
   const volatile int32_t* a = reinterpret_cast<const volatile int32_t*>(acc);
-  for (int i = threadIdx.x; i < CTL_N + na; i += nthreads)
-    P.host_out[i] = i < CTL_N ? c[i] : a[i - CTL_N];
+  for (int i = threadIdx.x; i < CTL_N + AW * nr; i += nthreads) {
+    if (i < CTL_N) {
+      P.host_out[i] = c[i];
+    } else {
+      const int img = P.sel[(i - CTL_N) / AW].w, w = (i - CTL_N) % AW;
+      if ((unsigned)img < (unsigned)P.nimg) P.host_out[CTL_N + AW * img + w] = a[AW * img + w];
+    }
+  }
   __threadfence_system();
 }
 
