@@ -186,7 +186,7 @@ struct Pool {
   template <class F>
   int timed(int kind, cudaStream_t s, F&& launch) {
     kprof[kind].launches++;
-    stats.launches++;
+    if (kind != K_LABELS) stats.launches++;   // the labels are not a kernel of the solve
     if (!prof) return launch();
     size_t i = ev_used.size() * 2;
     while (ev_pool.size() < i + 2) {

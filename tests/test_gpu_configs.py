@@ -153,7 +153,7 @@ def test_device_trace_of_a_graph_solve(cuda):
         # this small begins with the one launch that also builds the first active list
         kernel_marks = sum(kinds.count(k) for k in ("begin", "active_list", "discharge",
                                                     "flood_first", "flood", "bfs_first", "bfs"))
-        assert gc.stats()["launches"] == kernel_marks - 1, (kinds, gc.stats())
+        assert gc.stats()["launches"] == kernel_marks - 1, (" ".join(kinds), gc.stats())
         gc.set_trace(False)
         gc.upload_capacities(*g.planes())
         gc.cut()
