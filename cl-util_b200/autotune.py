@@ -50,7 +50,9 @@ SIZE_CLASSES = ((1 << 18, 384), (1 << 20, 768), (1 << 22, 1536), (None, 4096))
 # built-in choices (offline tuning on synthetic grids) used until a class is tuned: one grid
 # 3 x 2 is the best of the 72 candidates at 2048^2 (0.259 ms against 0.287 for 4 x 2) and at
 # 4096^2 (1.10 ms against 1.21 for 4 x 2; 4 x 1 is not among the best six), and within a few
-# percent of the best on smaller grids; pools of many grids 4 x 2
+# percent of the best on smaller grids; pools of many grids 4 x 2 (the pool choice depends on
+# the instance: on one sample of 64 grids of 256^2 to 1536^2 the tuner preferred 3 x 4, 8.82
+# against 10.57 ms, while the benchmark's 64 grids take 5.97 ms with 3 x 4 and 5.33 with 4 x 2)
 BUILTIN = {
     "single": [dict(discharge_iters=3, pulses_per_relabel=2, initial_relabel=0)] * 4,
     "batch": [dict(discharge_iters=4, pulses_per_relabel=2, initial_relabel=0)] * 4,
