@@ -365,6 +365,24 @@ class GraphCut:
         check(lib().gc_download_state(self._h, *args, stream_handle(None)))
         return out
 
+    _PLANES = {"excess": 0, "height": 1, "up": 2, "down": 3, "left": 4, "right": 5}
+
+    def execute(self, input):
+        """GraphCut.execute (GraphCut.pyx:423-437, filter_transpose graphcut.cl:1134-1170): the
+        reference turns one of its planes (its left / right capacities are stored
+        tile-transposed) into image layout as float32 for display.  Every plane here
+        (dExcess, dHeight, dUp, dDown, dLeft, dRight) is already in image layout, so this
+        returns `input` as a float32 [H, W] device tensor; a plane name ("excess", "height",
+        "up", "down", "left", "right") reads that plane first."""
+        import torch
+        if isinstance(input, str):
+            if input not in self._PLANES:
+                raise ValueError(f"plane must be one of {sorted(self._PLANES)}")
+            input = self._plane(self._PLANES[input])
+        if tuple(input.shape) != (self.height, self.width):
+            raise ValueError(f"plane shape {tuple(input.shape)} != {(self.height, self.width)}")
+        return torch.as_tensor(input, device=self.device).to(torch.float32)
+
     @property
     def dExcess(self):
         return self._plane(0)

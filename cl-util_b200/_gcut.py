@@ -128,6 +128,7 @@ SIGNATURES = {
     "gc_tiles_incorporate": [_P, _P, _I, _I32, _I, _I32, _I, _I32, _I, _P],
     "gc_tiles_fill": [_P, _I32, _I, _P],
     "gc_tiles_view": [_P, _I, _I, _I, _I, _I32, _I, _I, _P, _P],
+    "gc_view_colorize": [_P, _I, _I, _I, _I, _I, _I, _P, _P, _P, _P],
     "gcb_create": [_I, _P, _P, _P, _P],
     "gcb_destroy": [_P],
     "gcb_upload": [_P, _I] + [_P] * 5 + [_P],

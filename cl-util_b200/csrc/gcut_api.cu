@@ -1698,6 +1698,22 @@ int gc_tiles_fill(int32_t* tiles, int32_t value, int n, void* stream) {
   return launch_fill(tiles, n, value, (cudaStream_t)stream);
 }
 
+int gc_view_colorize(const int32_t* values, int values_w, int values_h, int cell_w, int cell_h,
+                     int width, int height, const float* ramp, const uint32_t* base,
+                     uint32_t* out, void* stream) {
+  g_err.clear();
+  if (values_w < 0 || values_h < 0 || cell_w < 1 || cell_h < 1 || width < 0 || height < 0)
+    return fail(GC_ERR_INVALID, "gc_view_colorize: bad size");
+  if (!ramp) return fail(GC_ERR_INVALID, "gc_view_colorize: null ramp");
+  for (int k = 0; k < 9; ++k)
+    if (!std::isfinite(ramp[k])) return fail(GC_ERR_INVALID, "gc_view_colorize: ramp not finite");
+  if ((long long)width * height > 0 && (!out || ((long long)values_w * values_h > 0 && !values)))
+    return fail(GC_ERR_INVALID, "gc_view_colorize: null pointer");
+  const int r = launch_view_colorize(values, values_w, values_h, cell_w, cell_h, width, height,
+                                     ramp, base, out, (cudaStream_t)stream);
+  return r == GC_OK ? GC_OK : fail(r, "gc_view_colorize: launch failed");
+}
+
 int gc_tiles_view(const int32_t* tiles, int tiles_w, int tiles_h, int tile_w, int tile_h,
                   int32_t iteration, int width, int height, uint32_t* out, void* stream) {
   g_err.clear();

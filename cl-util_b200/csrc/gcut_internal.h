@@ -129,6 +129,10 @@ int launch_brush(const PoolView& P, const ImageDesc& im, int img, const int32_t*
 // first handle creation and the first stand-alone primitive on a device).
 void preload_kernels();
 void preload_scan_kernels();
+// gc_view_colorize; ramp9: range lo, hi, hue lo, hi, saturation lo, hi, value lo, hi, opacity
+int launch_view_colorize(const int32_t* values, int values_w, int values_h, int cell_w,
+                         int cell_h, int width, int height, const float* ramp9,
+                         const uint32_t* base, uint32_t* out, cudaStream_t s);
 int occupancy_discharge(int device);
 int occupancy_warps(int device);
 

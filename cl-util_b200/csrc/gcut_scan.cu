@@ -174,6 +174,92 @@ __global__ void k_tiles_view(const int32_t* __restrict__ tiles, int tiles_w, int
   }
 }
 
+// Headless counterpart of the reference's display filters (graphcut_filter.cl:5-155: colorizef,
+// HSVtoRGB and the tranpose / tilelist / tilelist_growcut kernels): each pixel takes the int32
+// value of its cell (cell_w x cell_h pixels share one value: 1 x 1 for a pixel plane, the tile
+// size for a tile map), maps it through an HSV ramp and blends the colour over the base image:
+// out = base + (colour - base) * opacity per channel, every channel in [0, 1] (byte / 255).
+// Below the range the colour is black (tested first, as colorizef, graphcut_filter.cl:29-48,
+// does), above it white, inside it the hue, saturation and value run linearly between the
+// ends (a range of one value maps it to the start, where the reference divides 0 by 0); its
+// alpha is 0, as the reference's.  The arithmetic is float32
+// with every rounding written out (no contraction), and the result is rounded to the nearest
+// byte (ties to even).  Pixels outside the cell grid keep the base.
+struct ViewRamp { float lo, hi, h0, h1, s0, s1, v0, v1, opacity; };
+
+__device__ __forceinline__ float ramp_at(float a, float b, float t) {
+  return __fadd_rn(a, __fmul_rn(t, __fsub_rn(b, a)));
+}
+__device__ __forceinline__ uint32_t unorm8(float f) {
+  f = fminf(fmaxf(f, 0.0f), 1.0f);
+  return (uint32_t)__float2int_rn(__fmul_rn(f, 255.0f));
+}
+
+__global__ void k_view_colorize(const int32_t* __restrict__ values, int values_w, int values_h,
+                                int cell_w, int cell_h, int width, long long n, ViewRamp R,
+                                const uint32_t* __restrict__ base, uint32_t* __restrict__ out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i / width);
+    const int x = (int)(i - (long long)y * width);
+    const int cx = x / cell_w, cy = y / cell_h;
+    const uint32_t b = base ? base[i] : 0u;
+    if (cx >= values_w || cy >= values_h) { out[i] = b; continue; }
+    const float v = __int2float_rn(values[(long long)cy * values_w + cx]);
+    float H = 0.0f, S = 0.0f, V = 0.0f;
+    if (v < R.lo) {
+      // below the range: black
+    } else if (v > R.hi) {
+      V = 1.0f;
+    } else {
+      const float t = R.hi > R.lo ? __fdiv_rn(__fsub_rn(v, R.lo), __fsub_rn(R.hi, R.lo)) : 0.0f;
+      H = ramp_at(R.h0, R.h1, t);
+      S = ramp_at(R.s0, R.s1, t);
+      V = ramp_at(R.v0, R.v1, t);
+    }
+    // HSV -> RGB over the sectors of the hue circle; sector 4 takes sector 5's (v, p, q) as the
+    // reference's HSVtoRGB does, so hues 4/6..5/6 show as it shows them
+    float c[3] = {0.0f, 0.0f, 0.0f};
+    if (V != 0.0f) {
+      const float h6 = __fmul_rn(H, 6.0f);
+      const int sector = (int)__fsub_rn(h6, 1e-6f);   // truncated toward zero
+      const float f = __fsub_rn(h6, (float)sector);
+      const float p = __fmul_rn(V, __fsub_rn(1.0f, S));
+      const float q = __fmul_rn(V, __fsub_rn(1.0f, __fmul_rn(S, f)));
+      const float u = __fmul_rn(V, __fsub_rn(1.0f, __fmul_rn(S, __fsub_rn(1.0f, f))));
+      switch (sector) {
+        case 0: c[0] = V; c[1] = u; c[2] = p; break;
+        case 1: c[0] = q; c[1] = V; c[2] = p; break;
+        case 2: c[0] = p; c[1] = V; c[2] = u; break;
+        case 3: c[0] = p; c[1] = q; c[2] = V; break;
+        default: c[0] = V; c[1] = p; c[2] = q; break;
+      }
+    }
+    uint32_t w = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float cb = __fdiv_rn((float)((b >> (8 * k)) & 0xffu), 255.0f);
+      const float co = k < 3 ? c[k] : 0.0f;
+      w |= unorm8(__fadd_rn(cb, __fmul_rn(__fsub_rn(co, cb), R.opacity))) << (8 * k);
+    }
+    out[i] = w;
+  }
+}
+
+int launch_view_colorize(const int32_t* values, int values_w, int values_h, int cell_w,
+                         int cell_h, int width, int height, const float* ramp9,
+                         const uint32_t* base, uint32_t* out, cudaStream_t s) {
+  const long long n = (long long)width * height;
+  if (n <= 0) return GC_OK;
+  const ViewRamp R{ramp9[0], ramp9[1], ramp9[2], ramp9[3], ramp9[4], ramp9[5], ramp9[6],
+                   ramp9[7], ramp9[8]};
+  const long long blocks = (n + 255) / 256;
+  const unsigned grid = (unsigned)(blocks < (1LL << 30) ? blocks : (1LL << 30));
+  k_view_colorize<<<grid, 256, 0, s>>>(values, values_w, values_h, cell_w, cell_h, width, n, R,
+                                       base, out);
+  return cudaGetLastError() == cudaSuccess ? GC_OK : GC_ERR_CUDA;
+}
+
 int launch_lookback_selftest(const ScanState& st, cudaStream_t s) {
   if (st.max_chunks < 2) return GC_ERR_INVALID;
   if (cudaMemsetAsync(st.status, 0, sizeof(unsigned long long), s) != cudaSuccess) return GC_ERR_CUDA;
@@ -188,6 +274,7 @@ void preload_scan_kernels() {
   cudaFuncGetAttributes(&a, (const void*)k_increment_logical);
   cudaFuncGetAttributes(&a, (const void*)k_fill);
   cudaFuncGetAttributes(&a, (const void*)k_tiles_view);
+  cudaFuncGetAttributes(&a, (const void*)k_view_colorize);
 }
 
 int scan_chunks(int n) { return n <= 0 ? 1 : (n + SCAN_CHUNK - 1) / SCAN_CHUNK; }

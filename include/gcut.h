@@ -407,6 +407,25 @@ int gc_tiles_fill(int32_t* tiles, int32_t value, int n, void* stream);
    tiles_w x tiles_h tile grid are black (the reference reads past its tile array there). */
 int gc_tiles_view(const int32_t* tiles, int tiles_w, int tiles_h, int tile_w, int tile_h,
                   int32_t iteration, int width, int height, uint32_t* out, void* stream);
+/* The reference's display filters without a graphics stack (graphcut_filter.cl:5-155:
+   colorizef, HSVtoRGB, and the tranpose / tilelist / tilelist_growcut kernels that paint a
+   plane or a tile map over the displayed image).  Pixel (x, y) of the width x height output
+   takes v = values[(y / cell_h) * values_w + x / cell_w] (1 x 1 cells: a pixel plane such as
+   GraphCut's heights; the tile size: a tile map), converted to float.
+   - ramp (HOST, 9 floats, all finite): range lo, hi; hue lo, hi; saturation lo, hi; value lo,
+     hi; opacity.
+   - Colour: black for v < lo, white for v > hi; inside the range, hue, saturation and value
+     run linearly from their lo to their hi ends (t = (v - lo) / (hi - lo), 0 when hi == lo),
+     then HSV -> RGB by the hue sectors of the reference's HSVtoRGB (its sector 4 repeats
+     sector 5's (v, p, q), and so does this one). Its alpha is 0, as the reference's. The
+     reference's double literals (1.0, 0.000001) are taken as float here.
+   - out = base + (colour - base) * opacity per channel, channels read as byte / 255; float32
+     arithmetic, rounded to the nearest byte, ties to even. base may be NULL (all zero).
+   - Pixels outside the values_w x values_h cell grid keep the base.
+   values, base, out: DEVICE; base and out are RGBA words, R in the low byte. */
+int gc_view_colorize(const int32_t* values, int values_w, int values_h, int cell_w, int cell_h,
+                     int width, int height, const float* ramp, const uint32_t* base,
+                     uint32_t* out, void* stream);
 
 /* ---- batched solver: many independent grids in one tile pool ------------------------ */
 typedef struct gcb_handle gcb_handle;

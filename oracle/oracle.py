@@ -22,6 +22,7 @@ this module to check results; the product never imports it.
                       integer arithmetic; ``weight_reference_float32`` is the reference's own
                       float evaluation it is pinned against.
 * ``brush_pixels``    the pixel set of a brush stroke (brush.pyx:138-161).
+* ``view_colorize``   the display filters' colour ramp and blend (graphcut_filter.cl:5-155).
 """
 from __future__ import annotations
 
@@ -453,3 +454,62 @@ def brush_pixels(xs, ys, radius, width, height):
     xx = (lc[:, None] + odc[None, :]).reshape(-1)
     keep = (yy >= 0) & (yy < height) & (xx >= 0) & (xx < width)
     return np.unique(yy[keep] * width + xx[keep])
+
+
+def view_colorize(values, cell_w, cell_h, width, height, ramp, base=None):
+    """The display layer of graphcut_filter.cl:5-155 (colorizef, HSVtoRGB, and the blend of the
+    tranpose / tilelist kernels) in float32, each operation rounded as the device does it (no
+    fused multiply-add).  Sector 4 of the hue circle repeats sector 5's (v, p, q) as
+    HSVtoRGB (graphcut_filter.cl:17-22) does; below the range is tested before above it
+    (colorizef, :32-35); a range of one value maps it to the ramp's start (the reference
+    divides 0 by 0 there).  values: int32 [rows, cols] cells; ramp: range lo, hi, hue lo,
+    hi, saturation lo, hi, value lo, hi, opacity; base: uint32 RGBA words [height, width] or
+    None.  Returns uint32 RGBA words [height, width], R in the low byte."""
+    f32 = np.float32
+    values = np.asarray(values, dtype=np.int32)
+    rows, cols = values.shape
+    lo, hi, h0, h1, s0, s1, v0, v1, op = [f32(x) for x in ramp]
+    base = np.zeros((height, width), np.uint32) if base is None else \
+        np.asarray(base).view(np.uint32).reshape(height, width)
+    ys, xs = np.mgrid[0:height, 0:width]
+    cx, cy = xs // cell_w, ys // cell_h
+    inside = (cx < cols) & (cy < rows)
+    v = np.zeros((height, width), f32)
+    v[inside] = values[cy[inside], cx[inside]].astype(f32)
+    H = np.zeros_like(v)
+    S = np.zeros_like(v)
+    V = np.zeros_like(v)
+    below = v < lo
+    above = ~below & (v > hi)
+    mid = ~below & ~above
+    V[above] = f32(1)
+    with np.errstate(all="ignore"):
+        t = (v - lo) / (hi - lo) if hi > lo else np.zeros_like(v)
+    t = t.astype(f32)
+    for arr, a, b in ((H, h0, h1), (S, s0, s1), (V, v0, v1)):
+        arr[mid] = (a + t * (b - a)).astype(f32)[mid]
+    h6 = (H * f32(6)).astype(f32)
+    sector = np.trunc((h6 - f32(1e-6)).astype(f32)).astype(np.int64)
+    f = (h6 - sector.astype(f32)).astype(f32)
+    p = (V * (f32(1) - S)).astype(f32)
+    q = (V * (f32(1) - S * f)).astype(f32)
+    u = (V * (f32(1) - S * (f32(1) - f))).astype(f32)
+    rgb = np.zeros((3, height, width), f32)
+    table = {0: (V, u, p), 1: (q, V, p), 2: (p, V, u), 3: (p, q, V)}
+    lit = V != 0
+    for sec, chans in table.items():
+        m = (sector == sec) & lit
+        for k in range(3):
+            rgb[k][m] = chans[k][m]
+    m = ((sector < 0) | (sector > 3)) & lit     # every other sector: (v, p, q)
+    for k, chan in enumerate((V, p, q)):
+        rgb[k][m] = chan[m]
+    out = np.zeros((height, width), np.uint32)
+    for k in range(4):
+        cb = ((base >> np.uint32(8 * k)) & np.uint32(0xFF)).astype(f32) / f32(255)
+        co = rgb[k] if k < 3 else np.zeros_like(cb)
+        c = (cb + (co - cb) * op).astype(f32)
+        c = np.clip(c, f32(0), f32(1))
+        out |= np.rint(c * f32(255)).astype(np.uint32) << np.uint32(8 * k)
+    out[~inside] = base[~inside]
+    return out

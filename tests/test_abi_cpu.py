@@ -55,6 +55,12 @@ def test_calls_without_gpu_fail_cleanly(libgcut):
     # invalid arguments are rejected before any CUDA call
     assert L.gc_create(0, 64, None, ctypes.byref(h)) == _gcut.GC_ERR_INVALID
     assert L.gc_solve(None, None) == _gcut.GC_ERR_INVALID
+    ramp = (ctypes.c_float * 9)(0, 1, 0, 1, 1, 1, 1, 1, 1)
+    assert L.gc_view_colorize(None, 1, 1, 0, 1, 4, 4, ramp, None, None, None) \
+        == _gcut.GC_ERR_INVALID                               # cell width 0
+    ramp[8] = float("nan")
+    assert L.gc_view_colorize(None, 1, 1, 1, 1, 4, 4, ramp, None, None, None) \
+        == _gcut.GC_ERR_INVALID                               # opacity not finite
     o = _gcut.GcOpts()
     assert L.gc_opts_default(ctypes.byref(o)) == 0 and o.discharge_iters > 0
 
