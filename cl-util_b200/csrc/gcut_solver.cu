@@ -6,17 +6,20 @@
 // relabels the whole image with a Jacobi pass (:538-577) and computes the global relabel
 // with init_bfs/bfs_intratile/bfs_intertile (:582-1016) over compacted tile lists.  Here:
 //
-//  * k_discharge   one CTA per active tile (persistent over the device-side list): the tile's
-//                  excess, height and four residual planes are loaded with int4 loads into
-//                  registers/shared memory together with the halo heights, and the CTA runs
-//                  `iters` rounds of {push along every admissible edge (all 4 directions),
-//                  Jacobi relabel of interior pixels}.  Flow leaving the tile is added to
-//                  the neighbour's excess and reverse residual with atomics (no border
-//                  buffer, no add_border launch).  Tile-edge pixels keep their height during
-//                  the launch, so every cross-tile push sees the true height of its target.
+//  * k_discharge   one CTA of 256 threads per listed tile (persistent over the device-side
+//                  list): the tile's excess, height and four residual planes arrive in shared
+//                  memory by bulk copy (the next tile's copy overlaps this tile's work), with
+//                  the halo heights, and the CTA runs `iters` rounds of {push along every
+//                  admissible edge (all 4 directions), Jacobi relabel}.  Flow leaving the tile
+//                  is added to the neighbour's excess and reverse residual with atomics (no
+//                  border buffer, no add_border launch); tile-edge pixels rise at most 2 per
+//                  launch, so the labelling stays valid whether a neighbouring CTA saw a
+//                  pixel's start or final height.  Each finished
+//                  tile's bookkeeping (next list, dirty flags) is settled in batches.
 //  * k_edge_relabel_build   relabels the active tile-edge pixels (Jacobi) and rebuilds the
 //                  active-tile list with the single-pass decoupled look-back compaction in
-//                  the same launch (IncrementalTileList.build + StreamCompact + PrefixSum).
+//                  the same launch (IncrementalTileList.build + StreamCompact + PrefixSum);
+//                  the manual relabel step (GraphCut.relabel) only.
 //  * k_bfs_round   exact global relabel: per tile, one warp runs a bit-parallel multi-source
 //                  BFS (32-bit row masks of residual edges, lane = row) seeded by sink
 //                  pixels and by the halo distances, and marks neighbours whose edge
@@ -33,6 +36,7 @@
 namespace gcut {
 
 constexpr int DIS_THREADS = 256;
+constexpr int DIS_LOG = 32;       // tiles per bookkeeping flush in k_discharge (<= DIS_THREADS / 5)
 constexpr int WARPS_PER_CTA = 4;   // warp-per-tile kernels (BFS, flood, mask rebuild)
 
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
@@ -488,6 +492,29 @@ k_discharge(PoolView P, int iters) {
   }
   __syncthreads();
   const int cur = s_cur, nxt = cur ^ 1;
+  // Bookkeeping log: each finished tile leaves (tile, neighbours, flags) here, and the CTA's
+  // threads settle up to DIS_LOG tiles at once (its list entry, and the list entries and
+  // dirty flags of the neighbours it sent flow to), so the dependent L2 round trips of that
+  // bookkeeping are paid once per flush, not once per tile.  Nothing in this launch reads
+  // what it writes: the next list, the dirty flags and act_int are read by later kernels.
+  __shared__ int s_logt[DIS_LOG], s_logf[DIS_LOG];
+  __shared__ int4 s_lognb[DIS_LOG];
+  int nlog = 0;   // the same in every thread
+  auto flush_log = [&](int cnt) {
+    for (int w = tid; w < cnt * 5; w += DIS_THREADS) {
+      const int i = w / 5, k = w - i * 5;       // k = 0: the tile; 1..4: up, down, left, right
+      const int tt = s_logt[i], f = s_logf[i];
+      const int4 nbb = s_lognb[i];
+      const int target = k == 0 ? tt : k == 1 ? nbb.x : k == 2 ? nbb.y : k == 3 ? nbb.z : nbb.w;
+      if (k == 0 || ((f >> (k - 1)) & 1)) {
+        P.touched[target] = 1;
+        mark_dirty(P, target);   // its masks are rebuilt by the next flood's first round
+        if (k == 0) P.act_int[tt] = (f >> 5) & 1;
+        if (k != 0 || ((f >> 4) & 1)) worklist_add(P, nxt, target);
+        if (k == 0 && P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
+      }
+    }
+  };
   int n = s_n;
   if (n < 0 || n > P.nt) {   // self-check: a list never holds more than every tile once
     if (tid == 0 && blockIdx.x == 0) record_bad(P, 2, n);
@@ -754,19 +781,17 @@ k_discharge(PoolView P, int iters) {
     // the block-wide reductions also order every read of this buffer before its reuse
     const int any_act = __syncthreads_or(act);
     act_int = __syncthreads_or(act_int);
-    // the tile itself (lane 0) and the neighbours that received flow (lanes 1-4), in parallel
-    if (tid < 5) {
-      const int bits = s_sent;
-      const int target = tid == 0 ? t : tid == 1 ? nb.x : tid == 2 ? nb.y : tid == 3 ? nb.z : nb.w;
-      if (tid == 0 || ((bits >> (tid - 1)) & 1)) {
-        P.touched[target] = 1;
-        mark_dirty(P, target);   // its masks are rebuilt by the next flood's first round
-        if (tid == 0) P.act_int[t] = act_int;
-        if (tid != 0 || any_act) worklist_add(P, nxt, target);
-        if (tid == 0 && P.ktiles) atomicAdd(&P.ktiles[K_DISCHARGE], 1ull);
-      }
+    // log the tile's bookkeeping; a full log is settled now (the barrier makes the entries
+    // visible; the next write of an entry follows several more barriers)
+    if (tid == 0) {
+      s_logt[nlog] = t;
+      s_lognb[nlog] = nb;
+      s_logf[nlog] = (s_sent & 15) | (any_act ? 16 : 0) | (act_int ? 32 : 0);
     }
+    if (++nlog == DIS_LOG) { __syncthreads(); flush_log(nlog); nlog = 0; }
   }
+  __syncthreads();
+  flush_log(nlog);
   if (failed) {
     // a bulk copy did not complete in time: record it, let our copy drain, stop
     if (tid == 0) {
