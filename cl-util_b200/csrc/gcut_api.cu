@@ -769,24 +769,30 @@ struct Pool {
   }
 
   // Appends to g: flood first round (mode) + WHILE(frontier rounds) + the check, then
-  // IF(images left) { global relabel [+ active list (bump = count_cycle = 1), in the loop] }.
+  // IF(images left) { global relabel [+ the next cycle's active list (bump = count_cycle =
+  // 1)] }.  all: the warm prologue's flood (the solve does not end at its check; the first
+  // active list that follows decides).  first_cycle: the first cycle of a fresh solve, which
+  // runs ahead of the solve loop: the loop and its handle sit inside the IF body, after the
+  // list, so a solve that ends after one cycle never enters or leaves a loop node (each
+  // conditional node a solve passes costs several microseconds of device time).
   int graph_cycle_tail(cudaGraph_t g, std::vector<cudaGraphNode_t>& L, int mode, int all,
-                       int bump, cudaGraphConditionalHandle hmain) {
+                       int bump, cudaGraphConditionalHandle hmain, bool first_cycle = false) {
     cudaGraphConditionalHandle hf, hbfs, hb;
     RK(cond_handle(&hf, g));
     RK(cond_handle(&hbfs, g));
     // the round that ends the flood runs the flood check (retires the solved images, sets
-    // the IF condition below and, when none is left, ends the solve loop)
+    // the IF condition below and, when none is left, ends the solve loop and publishes)
     const cudaGraphConditionalHandle hm = all ? 0 : hmain;
+    const int publish = all ? 0 : 1;
     RK(capture(g, L, [&](cudaStream_t cs) {
-      return launch_flood_round(P, mode, 1, hf, acc, grid_warps, cs, all, hbfs, hm);
+      return launch_flood_round(P, mode, 1, hf, acc, grid_warps, cs, all, hbfs, hm, publish);
     }));
     cudaGraph_t bf;
     RK(add_while(g, L, hf, &bf));
     {
       std::vector<cudaGraphNode_t> Lf;
       RK(capture(bf, Lf, [&](cudaStream_t cs) {
-        return launch_flood_round(P, 0, 1, hf, acc, grid_warps, cs, all, hbfs, hm);
+        return launch_flood_round(P, 0, 1, hf, acc, grid_warps, cs, all, hbfs, hm, publish);
       }));
     }
     cudaGraph_t bi;
@@ -801,9 +807,29 @@ struct Pool {
       RK(capture(bb, Lb, [&](cudaStream_t cs) { return launch_bfs_round(P, 0, hb, grid_warps, cs); }));
     }
     if (!bump) return GC_OK;   // the first list of a solve follows the IF node
-    return capture(bi, Li, [&](cudaStream_t cs) {
-      return launch_active_list(P, scan.st, list, counts, 1, 1, 1, hmain, acc, 2 * sms, cs);
-    });
+    cudaGraphConditionalHandle hl = hmain;
+    if (first_cycle) RK(cond_handle(&hl, bi));   // the solve loop's handle, in the IF body
+    RK(capture(bi, Li, [&](cudaStream_t cs) {
+      return launch_active_list(P, scan.st, list, counts, 1, 1, 1, hl, acc, 2 * sms, cs);
+    }));
+    return first_cycle ? add_solve_loop(bi, Li, hl) : GC_OK;
+  }
+
+  // WHILE(hloop) { pulses x discharge, then the cycle's flood, check and relabel, and the
+  // next active list, which sets hloop }
+  int add_solve_loop(cudaGraph_t g, std::vector<cudaGraphNode_t>& L,
+                     cudaGraphConditionalHandle hloop) {
+    cudaGraph_t bm;
+    RK(add_while(g, L, hloop, &bm));
+    std::vector<cudaGraphNode_t> Lm;
+    RK(capture(bm, Lm, [&](cudaStream_t cs) { return launch_pulses(cs); }));
+    return graph_cycle_tail(bm, Lm, /*mode=*/2, /*all=*/0, /*bump=*/1, hloop);
+  }
+
+  int launch_pulses(cudaStream_t s) {
+    for (int p = 0; p < opts.pulses_per_relabel; ++p)
+      RK(launch_discharge(P, opts.discharge_iters, grid_dis, s));
+    return GC_OK;
   }
 
   int build_graph(int variant) {
@@ -816,33 +842,33 @@ struct Pool {
     CK(cudaGraphCreate(&g, 0));
     graph[variant] = g;
     std::vector<cudaGraphNode_t> L;
-    cudaGraphConditionalHandle hmain;
-    RK(cond_handle(&hmain, g));
-    if (!variant && nt <= begin_list_max_tiles()) {
-      // fresh images only, a small pool: the prologue and the first active list in one CTA
-      RK(capture(g, L, [&](cudaStream_t cs) {
-        return launch_begin_list(P, opts.max_bfs_rounds, opts.max_cycles, acc, list, counts, hmain, cs);
-      }));
-    } else {
-      RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs); }));
-      if (variant) {
-        // images that continue from a previous flow: flood them; relabel the ones not solved
-        RK(graph_cycle_tail(g, L, /*mode=*/3, /*all=*/1, /*bump=*/0, hmain));
+    if (!variant) {
+      // fresh images only: the prologue and the first active list (one CTA for a small
+      // pool), then the first cycle unrolled, with the solve loop inside its IF node.  The
+      // list sets no condition: an empty one leaves nothing for the pulses, the flood finds
+      // no live image and its check ends the solve.
+      if (nt <= begin_list_max_tiles()) {
+        RK(capture(g, L, [&](cudaStream_t cs) {
+          return launch_begin_list(P, opts.max_bfs_rounds, opts.max_cycles, acc, list, counts, 0, cs);
+        }));
+      } else {
+        RK(capture(g, L, [&](cudaStream_t cs) {
+          RK(launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs));
+          return launch_active_list(P, scan.st, list, counts, 0, 0, 2, 0, acc, 2 * sms, cs);
+        }));
       }
+      RK(capture(g, L, [&](cudaStream_t cs) { return launch_pulses(cs); }));
+      RK(graph_cycle_tail(g, L, /*mode=*/2, /*all=*/0, /*bump=*/1, 0, /*first_cycle=*/true));
+    } else {
+      cudaGraphConditionalHandle hmain;
+      RK(cond_handle(&hmain, g));
+      RK(capture(g, L, [&](cudaStream_t cs) { return launch_ctl_begin(P, opts.max_bfs_rounds, opts.max_cycles, acc, cs); }));
+      // images that continue from a previous flow: flood them; relabel the ones not solved
+      RK(graph_cycle_tail(g, L, /*mode=*/3, /*all=*/1, /*bump=*/0, hmain));
       RK(capture(g, L, [&](cudaStream_t cs) {   // the first active list (fresh and live images)
         return launch_active_list(P, scan.st, list, counts, 0, 0, 2, hmain, acc, 2 * sms, cs);
       }));
-    }
-    cudaGraph_t bm;
-    RK(add_while(g, L, hmain, &bm));
-    {
-      std::vector<cudaGraphNode_t> Lm;
-      RK(capture(bm, Lm, [&](cudaStream_t cs) {
-        for (int p = 0; p < opts.pulses_per_relabel; ++p)
-          RK(launch_discharge(P, opts.discharge_iters, grid_dis, cs));
-        return GC_OK;
-      }));
-      RK(graph_cycle_tail(bm, Lm, /*mode=*/2, /*all=*/0, /*bump=*/1, hmain));
+      RK(add_solve_loop(g, L, hmain));
     }
     if (!P.host_out) {   // else the kernel that ends the solve wrote them already
       RK(capture(g, L, [&](cudaStream_t cs) {

@@ -85,10 +85,12 @@ int launch_bfs_round(const PoolView& P, int first, cudaGraphConditionalHandle h,
 // mode: 0 frontier round, 1 first round over every tile, 2 first round over the tiles of the
 // images live in this cycle; abort_hit: frontier rounds skip images that reached a sink
 // check >= 0: the round that ends the flood also runs the flood check (its `all`), with the
-// IF / WHILE handles of launch_flood_check
+// IF / WHILE handles of launch_flood_check; publish: a check that finds no image left writes
+// the results to the handle's pinned host block (the graph solve ends there)
 int launch_flood_round(const PoolView& P, int mode, int abort_hit, cudaGraphConditionalHandle h,
                        ImageAcc* acc, int grid, cudaStream_t s, int check = -1,
-                       cudaGraphConditionalHandle hbfs = 0, cudaGraphConditionalHandle hmain = 0);
+                       cudaGraphConditionalHandle hbfs = 0, cudaGraphConditionalHandle hmain = 0,
+                       int publish = 0);
 // retires the images whose flood reached no sink; all: every image takes part
 int launch_flood_check(const PoolView& P, int all, cudaGraphConditionalHandle hbfs,
                        cudaGraphConditionalHandle hmain, cudaStream_t s);

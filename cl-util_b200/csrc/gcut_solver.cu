@@ -1490,12 +1490,14 @@ k_bfs_round(PoolView P, int first, cudaGraphConditionalHandle h) {
 // canonical cut, its sums are final) and leaves the live set; the others go on to a global
 // relabel.  all != 0: the images that continue from a previous flow (img_mode == 2; the
 // first check of a solve); else the images live in this cycle.  Sets the condition of the
-// IF node around the relabel (hbfs) and, when no image is left, ends the solve loop (hmain);
-// the last cycle of a solve is counted here.  Every thread of one CTA calls it: k_flood_check,
+// IF node around the relabel (hbfs) and, when no image is left, ends the solve loop (hmain,
+// 0 outside the loop) and, with `publish`, writes the results to the host (the graph solve
+// ends here); the last cycle of a solve is counted here.  Every thread of one CTA calls it: k_flood_check,
 // or the last CTA of the flood's last round, which reads what the round's other CTAs wrote
 // (their fence before the round's count orders it), hence the volatile loads.
 __device__ void flood_check_cta(const PoolView& P, int all, cudaGraphConditionalHandle hbfs,
-                                cudaGraphConditionalHandle hmain, const ImageAcc* acc) {
+                                cudaGraphConditionalHandle hmain, int publish,
+                                const ImageAcc* acc) {
   __shared__ int s_left, s_n;
   if (threadIdx.x == 0) {
     s_left = 0;
@@ -1531,7 +1533,7 @@ __device__ void flood_check_cta(const PoolView& P, int all, cudaGraphConditional
     s_n = n;
   }
   __syncthreads();
-  if (s_n == 0 && hmain) publish_results(P, acc, blockDim.x);   // the graph solve ends here
+  if (s_n == 0 && publish) publish_results(P, acc, blockDim.x);   // the graph solve ends here
 }
 
 // End of a flood round: frontier_round_end's bookkeeping by the round's last CTA; when the
@@ -1540,7 +1542,7 @@ __device__ void flood_check_cta(const PoolView& P, int all, cudaGraphConditional
 __device__ __forceinline__ void flood_round_end(const PoolView& P, int first, int in, int parts,
                                                 cudaGraphConditionalHandle h, int check,
                                                 cudaGraphConditionalHandle hbfs,
-                                                cudaGraphConditionalHandle hmain,
+                                                cudaGraphConditionalHandle hmain, int publish,
                                                 const ImageAcc* acc) {
   __shared__ int s_last, s_more;
   __syncthreads();
@@ -1572,7 +1574,7 @@ __device__ __forceinline__ void flood_round_end(const PoolView& P, int first, in
   }
   __syncthreads();
   if (!s_last || check < 0 || s_more) return;
-  flood_check_cta(P, check, hbfs, hmain, acc);
+  flood_check_cta(P, check, hbfs, hmain, publish, acc);
 }
 
 // ------------------------------------------------------------------------------------
@@ -1592,7 +1594,8 @@ __device__ __forceinline__ void flood_round_end(const PoolView& P, int first, in
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(WARPS_PER_CTA * 32)
 k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h, ImageAcc* acc,
-              int check, cudaGraphConditionalHandle hbfs, cudaGraphConditionalHandle hmain) {
+              int check, cudaGraphConditionalHandle hbfs, cudaGraphConditionalHandle hmain,
+              int publish) {
   trace_mark(P, mode ? TR_FLOOD_FIRST : TR_FLOOD);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int first = mode != 0;
@@ -1708,14 +1711,14 @@ k_flood_round(PoolView P, int mode, int abort_hit, cudaGraphConditionalHandle h,
       }
     }
   }
-  flood_round_end(P, first, in, parts, h, check, hbfs, hmain, acc);
+  flood_round_end(P, first, in, parts, h, check, hbfs, hmain, publish, acc);
 }
 
 // After a flood (host-driven loops; the solve graph runs the check at the end of its last
 // flood round instead): see flood_check_cta.  One CTA.
 __global__ void k_flood_check(PoolView P, int all, cudaGraphConditionalHandle hbfs,
                               cudaGraphConditionalHandle hmain) {
-  flood_check_cta(P, all, hbfs, hmain, nullptr);
+  flood_check_cta(P, all, hbfs, hmain, 0, nullptr);
 }
 
 // Neighbour tile ids and image index of one image's tiles (row-major from im.tile0), for an
@@ -1993,8 +1996,10 @@ int launch_bfs_round(const PoolView& P, int first, cudaGraphConditionalHandle h,
 
 int launch_flood_round(const PoolView& P, int mode, int abort_hit, cudaGraphConditionalHandle h,
                        ImageAcc* acc, int grid, cudaStream_t s, int check,
-                       cudaGraphConditionalHandle hbfs, cudaGraphConditionalHandle hmain) {
-  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, mode, abort_hit, h, acc, check, hbfs, hmain);
+                       cudaGraphConditionalHandle hbfs, cudaGraphConditionalHandle hmain,
+                       int publish) {
+  k_flood_round<<<grid, WARPS_PER_CTA * 32, 0, s>>>(P, mode, abort_hit, h, acc, check, hbfs, hmain,
+                                                    publish);
   return ok();
 }
 
