@@ -158,6 +158,9 @@ struct Pool {
   size_t pin_bytes = 0;
   int32_t* h_count = nullptr;  // pinned
   int32_t* h_ctl = nullptr;    // pinned copy of the control words
+  unsigned long long* lab_slot = nullptr;     // device: output buffer of the in-graph labels
+  unsigned long long* h_labslot = nullptr;    // pinned: its source word (inside h_count's slot)
+  uint8_t* lab_slot_val = nullptr;            // what lab_slot holds
   bool use_graph = true;
   ImageAcc* h_acc = nullptr;   // pinned
   int grid_dis = 0, grid_warps = 0, sms = 1;
@@ -259,6 +262,7 @@ struct Pool {
     tl = list = counts = stage = pts = nullptr;
     acc = nullptr; lstage = nullptr; h_count = nullptr; h_ctl = nullptr; h_acc = nullptr;
     dsum = nullptr; ntab = nullptr; d_sel = nullptr; h_sel = nullptr;
+    lab_slot = nullptr; h_labslot = nullptr; lab_slot_val = nullptr;
     trace_words = nullptr;
   }
 
@@ -303,6 +307,7 @@ struct Pool {
     c.take(&pts, 2 * 1024);
     c.take(&dsum, 1);
     c.take(&ntab, GC_NLINK_LEVELS);
+    c.take(&lab_slot, 1);
     if (imgs.size() == 1) c.take(&lstage, (size_t)imgs[0].W * imgs[0].H);
   }
 
@@ -405,6 +410,7 @@ struct Pool {
     pin = pinned_take(pin_bytes);
     if (!pin) { release(); return fail(GC_ERR_OOM, "pinned host allocation failed"); }
     h_count = static_cast<int32_t*>(pin);
+    h_labslot = reinterpret_cast<unsigned long long*>(static_cast<char*>(pin) + 128);
     h_ctl = reinterpret_cast<int32_t*>(static_cast<char*>(pin) + 256);
     h_acc = reinterpret_cast<ImageAcc*>(static_cast<char*>(pin) + 512);
     {   // the kernel that ends a graph solve writes the results here itself (no copy node)
@@ -620,7 +626,8 @@ struct Pool {
 
   // Solves the listed images together (distinct, uploaded); the pool's other images keep
   // their state and results.
-  int solve_images(const int* idx, int n, cudaStream_t s, const After* after = nullptr) {
+  int solve_images(const int* idx, int n, cudaStream_t s, const After* after = nullptr,
+                   int lmode = 0, uint8_t* lbuf = nullptr) {
     if (n < 1 || !idx) return fail(GC_ERR_INVALID, "no images to solve");
     std::vector<uint8_t> seen(imgs.size(), 0);
     for (int k = 0; k < n; ++k) {
@@ -634,7 +641,7 @@ struct Pool {
     bool warm = false;
     RK(set_selection(idx, n, &warm, s));
     const bool host = prof || collect || !use_graph;
-    int r = host ? solve_host(s, warm) : solve_graph(s, warm, after);
+    int r = host ? solve_host(s, warm) : solve_graph(s, warm, after, lmode, lbuf);
     if (r) return r;
     if (host && after) {   // the host-driven solve has finished: queue the work and wait
       RK((*after)(s));
@@ -715,6 +722,14 @@ struct Pool {
   cudaStream_t cap_stream = nullptr;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};   // [relabel_first]
   cudaGraph_t graph[2] = {nullptr, nullptr};
+  // Solve graphs that end with the labels of a pool's one image (gc_solve_labels), [warm]
+  // [packed]: the labels start right after the solve's last kernel instead of after the
+  // graph has left its loop nodes and ended.  Their kernels read the output buffer from a
+  // device word (lab_slot), which is set from the pinned h_labslot when the caller's buffer
+  // changes, so the graphs stay as built.
+  cudaGraphExec_t lexec[2][2] = {};
+  cudaGraph_t lgraph[2][2] = {};
+  int bl_mode = 0;   // during a build: the labels the graph ends with (0 none, 1 bytes, 2 packed)
 
   template <class F>
   int capture(cudaGraph_t g, std::vector<cudaGraphNode_t>& leaves, F&& fn) {
@@ -768,6 +783,15 @@ struct Pool {
     return fail(GC_ERR_INTERNAL, "cudaGraphConditionalHandleCreate gave only handle 0");
   }
 
+  // A labels node of the pool's one image, into the buffer held in lab_slot.  first: the
+  // node after the first cycle's flood (it writes only when that cycle ended the solve).
+  int capture_labels(cudaGraph_t g, std::vector<cudaGraphNode_t>& L, int first) {
+    return capture(g, L, [&](cudaStream_t cs) {
+      return bl_mode == 2 ? launch_labels_packed(P, imgs[0], nullptr, cs, first, lab_slot, 4 * sms)
+                          : launch_labels_out(P, imgs[0], nullptr, cs, first, lab_slot, 4 * sms);
+    });
+  }
+
   // Appends to g: flood first round (mode) + WHILE(frontier rounds) + the check, then
   // IF(images left) { global relabel [+ the next cycle's active list (bump = count_cycle =
   // 1)] }.  all: the warm prologue's flood (the solve does not end at its check; the first
@@ -795,8 +819,13 @@ struct Pool {
         return launch_flood_round(P, 0, 1, hf, acc, grid_warps, cs, all, hbfs, hm, publish);
       }));
     }
+    // a graph that ends with the labels: they follow the first cycle's flood on a branch of
+    // their own (writing only when its check ended the solve), beside the IF node
+    std::vector<cudaGraphNode_t> Lq = L;
+    if (first_cycle && bl_mode) RK(capture_labels(g, Lq, 1));
     cudaGraph_t bi;
     RK(add_if(g, L, hbfs, &bi));
+    if (first_cycle && bl_mode) L.push_back(Lq[0]);   // what follows waits for both
     std::vector<cudaGraphNode_t> Li;
     RK(cond_handle(&hb, bi));
     RK(capture(bi, Li, [&](cudaStream_t cs) { return launch_bfs_round(P, 2, hb, grid_warps, cs); }));
@@ -812,7 +841,10 @@ struct Pool {
     RK(capture(bi, Li, [&](cudaStream_t cs) {
       return launch_active_list(P, scan.st, list, counts, 1, 1, 1, hl, acc, 2 * sms, cs);
     }));
-    return first_cycle ? add_solve_loop(bi, Li, hl) : GC_OK;
+    if (!first_cycle) return GC_OK;
+    RK(add_solve_loop(bi, Li, hl));
+    // the labels of a solve that went on past its first cycle, after its loop
+    return bl_mode ? capture_labels(bi, Li, 0) : GC_OK;
   }
 
   // WHILE(hloop) { pulses x discharge, then the cycle's flood, check and relabel, and the
@@ -832,7 +864,9 @@ struct Pool {
     return GC_OK;
   }
 
-  int build_graph(int variant) {
+  // Builds the solve graph of a variant into *gout / *eout; with bl_mode set, the graph
+  // ends with the labels of the pool's one image.
+  int build_graph(int variant, cudaGraph_t* gout, cudaGraphExec_t* eout) {
     // One graph construction at a time in the process (building, instantiating and
     // destroying graphs with nested conditional nodes from several threads at once was the
     // suspected trigger of an intermittent fault under concurrent serving).
@@ -840,7 +874,7 @@ struct Pool {
     if (!cap_stream) CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
     cudaGraph_t g;
     CK(cudaGraphCreate(&g, 0));
-    graph[variant] = g;
+    *gout = g;
     std::vector<cudaGraphNode_t> L;
     if (!variant) {
       // fresh images only: the prologue and the first active list (one CTA for a small
@@ -870,6 +904,7 @@ struct Pool {
       }));
       RK(add_solve_loop(g, L, hmain));
     }
+    if (bl_mode && variant) RK(capture_labels(g, L, 0));   // (fresh: inside the IF node)
     if (!P.host_out) {   // else the kernel that ends the solve wrote them already
       RK(capture(g, L, [&](cudaStream_t cs) {
         // control words and per-image sums are adjacent on both sides: one copy
@@ -878,27 +913,41 @@ struct Pool {
         return GC_OK;
       }));
     }
-    CK(cudaGraphInstantiate(&gexec[variant], g, 0));
+    CK(cudaGraphInstantiate(eout, g, 0));
     // upload the executable graph here, under the construction lock, rather than implicitly
     // at its first launch next to other threads' graph work
-    CK(cudaGraphUpload(gexec[variant], cap_stream));
+    CK(cudaGraphUpload(*eout, cap_stream));
     CK(cudaStreamSynchronize(cap_stream));
     return GC_OK;
   }
 
-  // variant 1: some selected image continues from a previous flow (the graph floods first)
-  int solve_graph(cudaStream_t s, bool warm, const After* after = nullptr) {
+
+  // variant 1: some selected image continues from a previous flow (the graph floods first).
+  // lmode 1 / 2: the graph that ends with the labels (bytes / packed) of the pool's one
+  // image, into lbuf.
+  int solve_graph(cudaStream_t s, bool warm, const After* after = nullptr, int lmode = 0,
+                  uint8_t* lbuf = nullptr) {
     const int v = warm ? 1 : 0;
-    if (!gexec[v]) {
-      const int r = build_graph(v);
+    cudaGraphExec_t* ex = lmode ? &lexec[v][lmode - 1] : &gexec[v];
+    cudaGraph_t* gr = lmode ? &lgraph[v][lmode - 1] : &graph[v];
+    if (!*ex) {
+      bl_mode = lmode;
+      const int r = build_graph(v, gr, ex);
+      bl_mode = 0;
       if (r) {
-        if (graph[v]) { cudaGraphDestroy(graph[v]); graph[v] = nullptr; }
+        if (*ex) { cudaGraphExecDestroy(*ex); *ex = nullptr; }
+        if (*gr) { cudaGraphDestroy(*gr); *gr = nullptr; }
         return r;
       }
     }
+    if (lmode && lab_slot_val != lbuf) {   // the labels kernels read their buffer from here
+      *h_labslot = (unsigned long long)(uintptr_t)lbuf;
+      CK(cudaMemcpyAsync(lab_slot, h_labslot, sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
+      lab_slot_val = lbuf;
+    }
     P.ktiles = nullptr;
     graph_warm = warm;
-    CK(cudaGraphLaunch(gexec[v], s));
+    CK(cudaGraphLaunch(*ex, s));
     if (after) RK((*after)(s));
     CK(cudaStreamSynchronize(s));
     stats.launches = -1;  // inside the graph; see gc_stats
@@ -912,6 +961,12 @@ struct Pool {
       if (graph[v]) cudaGraphDestroy(graph[v]);
       gexec[v] = nullptr;
       graph[v] = nullptr;
+      for (int m = 0; m < 2; ++m) {
+        if (lexec[v][m]) cudaGraphExecDestroy(lexec[v][m]);
+        if (lgraph[v][m]) cudaGraphDestroy(lgraph[v][m]);
+        lexec[v][m] = nullptr;
+        lgraph[v][m] = nullptr;
+      }
     }
     if (cap_stream) cudaStreamDestroy(cap_stream);
     cap_stream = nullptr;
@@ -1070,6 +1125,9 @@ struct Pool {
     if (n < 1 || !idx || !outs) return fail(GC_ERR_INVALID, "bad argument");
     for (int k = 0; k < n; ++k)
       if (!outs[k]) return fail(GC_ERR_INVALID, "null label buffer");
+    // a pool of one image solved by graph: the solve graph itself ends with the labels
+    if (n == 1 && imgs.size() == 1 && idx[0] == 0 && use_graph && !prof && !collect)
+      return solve_images(idx, n, s, nullptr, packed ? 2 : 1, outs[0]);
     const After after = [&](cudaStream_t cs) {
       for (int k = 0; k < n; ++k) {
         const ImageDesc& im = imgs[idx[k]];

@@ -112,8 +112,14 @@ int launch_ctl_cycle(const PoolView& P, const int32_t* count, int count_cycle,
                      cudaGraphConditionalHandle h, cudaStream_t s);
 // neighbour ids and image index of the tiles of image img (a session-pool slot)
 int launch_image_tiles(const PoolView& P, const ImageDesc& im, int img, cudaStream_t s);
-int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s);
-int launch_labels_packed(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s);
+// Inside a solve graph that ends with the labels: first = 1 for the launch after the first
+// cycle's flood (it writes only when that cycle ended the solve); slot: the device word that
+// holds the output buffer (out is then ignored); grid_cap > 0 caps the CTAs.
+int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s,
+                      int first = 0, const unsigned long long* slot = nullptr, int grid_cap = 0);
+int launch_labels_packed(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s,
+                         int first = 0, const unsigned long long* slot = nullptr,
+                         int grid_cap = 0);
 int launch_state_out(const PoolView& P, const ImageDesc& im, const int32_t* plane,
                      int32_t* out, cudaStream_t s);
 int launch_edit(const PoolView& P, const ImageDesc& im, int img, const int32_t* idx,

@@ -1732,46 +1732,69 @@ __global__ void k_image_tiles(PoolView P, ImageDesc im, int img) {
   P.img_of[t] = img;
 }
 
+// The labels kernels inside a solve graph that ends with the labels of its one image:
+// `first`: the launch that follows the first cycle's flood writes only when that cycle's
+// check left no image (the solve ended there; otherwise the launch at the end of the relabel
+// IF node writes them).  `slot`: the output buffer is read from this device word, which the
+// host sets when the caller's buffer changes, so the graph never changes.  Every thread
+// reads words that earlier launches (or copies) wrote.
+__device__ __forceinline__ bool labels_skip(const PoolView& P, int first) {
+  return first && *((volatile int32_t*)&P.ctl[CTL_LEFT]) != 0;
+}
+__device__ __forceinline__ uint8_t* labels_dest(uint8_t* out, const unsigned long long* slot) {
+  return slot ? reinterpret_cast<uint8_t*>(*((const volatile unsigned long long*)slot)) : out;
+}
+
 // Labels of one image, row-major, padding excluded.  One thread writes the 32 pixels of
 // one tile row (one mask word); consecutive threads take consecutive tiles of an image row.
-__global__ void k_labels_out(PoolView P, ImageDesc im, uint8_t* __restrict__ out) {
+__global__ void k_labels_out(PoolView P, ImageDesc im, uint8_t* __restrict__ out_arg, int first,
+                             const unsigned long long* slot) {
+  if (labels_skip(P, first)) return;
   trace_mark(P, TR_LABELS);
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)im.H * im.tw) return;
-  const int y = (int)(i / im.tw), tx = (int)(i % im.tw);
-  const int t = im.tile0 + (y >> 5) * im.tw + tx;
-  const uint32_t m = P.mreach[(long long)t * 32 + (y & 31)];
-  const int x0 = tx * GC_TILE;
-  uint8_t* row = out + (long long)y * im.W + x0;
-  if (x0 + GC_TILE <= im.W && (((uintptr_t)row) & 3) == 0) {
+  uint8_t* const out = labels_dest(out_arg, slot);
+  const long long n = (long long)im.H * im.tw;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i / im.tw), tx = (int)(i % im.tw);
+    const int t = im.tile0 + (y >> 5) * im.tw + tx;
+    const uint32_t m = P.mreach[(long long)t * 32 + (y & 31)];
+    const int x0 = tx * GC_TILE;
+    uint8_t* row = out + (long long)y * im.W + x0;
+    if (x0 + GC_TILE <= im.W && (((uintptr_t)row) & 3) == 0) {
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const uint32_t b = (m >> (4 * k)) & 0xfu;
-      const uint32_t w = (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21);
-      reinterpret_cast<uint32_t*>(row)[k] = w;
+      for (int k = 0; k < 8; ++k) {
+        const uint32_t b = (m >> (4 * k)) & 0xfu;
+        const uint32_t w = (b & 1u) | ((b & 2u) << 7) | ((b & 4u) << 14) | ((b & 8u) << 21);
+        reinterpret_cast<uint32_t*>(row)[k] = w;
+      }
+    } else {
+      for (int c = 0; c < GC_TILE && x0 + c < im.W; ++c) row[c] = (uint8_t)((m >> c) & 1u);
     }
-  } else {
-    for (int c = 0; c < GC_TILE && x0 + c < im.W; ++c) row[c] = (uint8_t)((m >> c) & 1u);
   }
 }
 
 // Bit-packed labels: thread (y, tx) writes the up to four bytes of tile column tx in row y
 // (row stride (W + 7) / 8 bytes, little bit order).  Pixels of a ragged tile beyond the
 // image have no capacities and no excess, so their reach bits are 0.
-__global__ void k_labels_packed(PoolView P, ImageDesc im, uint8_t* __restrict__ out) {
+__global__ void k_labels_packed(PoolView P, ImageDesc im, uint8_t* __restrict__ out_arg,
+                                int first, const unsigned long long* slot) {
+  if (labels_skip(P, first)) return;
   trace_mark(P, TR_LABELS);
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)im.H * im.tw) return;
-  const int y = (int)(i / im.tw), tx = (int)(i % im.tw);
-  const int t = im.tile0 + (y >> 5) * im.tw + tx;
-  const uint32_t m = P.mreach[(long long)t * 32 + (y & 31)];
+  uint8_t* const out = labels_dest(out_arg, slot);
+  const long long n = (long long)im.H * im.tw;
   const int stride = (im.W + 7) >> 3;
-  uint8_t* row = out + (long long)y * stride + 4 * tx;
-  const int nb = stride - 4 * tx < 4 ? stride - 4 * tx : 4;
-  if (nb == 4 && (((uintptr_t)row) & 3) == 0) {
-    *reinterpret_cast<uint32_t*>(row) = m;
-  } else {
-    for (int k = 0; k < nb; ++k) row[k] = (uint8_t)(m >> (8 * k));
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(i / im.tw), tx = (int)(i % im.tw);
+    const int t = im.tile0 + (y >> 5) * im.tw + tx;
+    const uint32_t m = P.mreach[(long long)t * 32 + (y & 31)];
+    uint8_t* row = out + (long long)y * stride + 4 * tx;
+    const int nb = stride - 4 * tx < 4 ? stride - 4 * tx : 4;
+    if (nb == 4 && (((uintptr_t)row) & 3) == 0) {
+      *reinterpret_cast<uint32_t*>(row) = m;
+    } else {
+      for (int k = 0; k < nb; ++k) row[k] = (uint8_t)(m >> (8 * k));
+    }
   }
 }
 
@@ -2058,17 +2081,22 @@ int launch_image_tiles(const PoolView& P, const ImageDesc& im, int img, cudaStre
   return ok();
 }
 
-int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s) {
-  const long long n = (long long)im.W * im.H;
-  const long long segs = (long long)im.H * im.tw;
-  (void)n;
-  k_labels_out<<<(unsigned)((segs + 255) / 256), 256, 0, s>>>(P, im, out);
+// one thread per tile row of the image; grid_cap > 0 caps the CTAs (they stride over rows)
+static unsigned labels_grid(const ImageDesc& im, int grid_cap) {
+  const long long need = ((long long)im.H * im.tw + 255) / 256;
+  const long long g = grid_cap > 0 && need > grid_cap ? grid_cap : need;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+int launch_labels_out(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s,
+                      int first, const unsigned long long* slot, int grid_cap) {
+  k_labels_out<<<labels_grid(im, grid_cap), 256, 0, s>>>(P, im, out, first, slot);
   return ok();
 }
 
-int launch_labels_packed(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s) {
-  const long long segs = (long long)im.H * im.tw;
-  k_labels_packed<<<(unsigned)((segs + 255) / 256), 256, 0, s>>>(P, im, out);
+int launch_labels_packed(const PoolView& P, const ImageDesc& im, uint8_t* out, cudaStream_t s,
+                         int first, const unsigned long long* slot, int grid_cap) {
+  k_labels_packed<<<labels_grid(im, grid_cap), 256, 0, s>>>(P, im, out, first, slot);
   return ok();
 }
 

@@ -91,6 +91,43 @@ def test_cut_labels_matches_cut_then_labels(cuda, oracle, w, h, graph):
         assert np.array_equal(gc.labels().cpu().numpy(), l_ref)
 
 
+def test_cut_labels_graph_follows_buffers_fresh_and_warm(cuda, oracle):
+    """The solve graph that ends with the labels: its labels nodes follow the caller's buffer
+    from call to call (two buffers alternate, bytes and packed), on a synthetic image and on
+    random capacities, fresh and warm (after stroke edits), each equal to the exact cut."""
+    import torch
+    from GraphCut import unpack_labels
+    rng = np.random.default_rng(5)
+    for g in (synth.make_graph(300, 200, 4), synth.random_graph(300, 200, 6, cap_max=30,
+                                                                tlink_max=60)):
+        w, h = g.width, g.height
+        bufs = [torch.empty((h, w), dtype=torch.uint8, device="cuda") for _ in range(2)]
+        pbufs = [torch.empty((h, (w + 7) // 8), dtype=torch.uint8, device="cuda")
+                 for _ in range(2)]
+        t = g.excess.copy()
+        with GraphCut(w, h) as gc:
+            gc.upload_capacities(*g.planes())
+            for k in range(6):
+                if k >= 2:   # warm: the graph variant that floods the previous flow first
+                    s = strokes.random_stroke(rng, w, h)
+                    gc.edit_stroke(s.xs, s.ys, s.radius, s.value)
+                    t = strokes.apply(t, s)
+                f_ref, l_ref = oracle.maxflow_bk(g.up, g.down, g.left, g.right, t)
+                for b in (bufs[k % 2], bufs[(k + 1) % 2]):
+                    b.fill_(7)
+                    gc.cut_labels(out=b)
+                    assert gc.flow == f_ref, k
+                    assert np.array_equal(b.cpu().numpy(), l_ref), k
+                    if k < 2:
+                        gc.upload_capacities(*g.planes())
+                pb = pbufs[k % 2]
+                pb.fill_(0xFF)
+                gc.cut_labels(out=pb, packed=True)
+                assert np.array_equal(unpack_labels(pb.cpu().numpy(), w), l_ref), k
+                if k < 2:
+                    gc.upload_capacities(*g.planes())
+
+
 def test_handles_in_caller_memory(cuda, oracle):
     """gc_create_in: handles placed in one caller-owned buffer solve like gc_create, and
     the memory is reused for a handle of another size after gc_destroy."""
