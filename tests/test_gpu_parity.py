@@ -128,6 +128,24 @@ def test_cut_labels_graph_follows_buffers_fresh_and_warm(cuda, oracle):
                     gc.upload_capacities(*g.planes())
 
 
+def test_cut_labels_graph_strides_over_a_large_image(cuda, oracle):
+    """2500^2: the labels kernels inside the solve graph cap their grid at 4 CTAs per SM and
+    stride over the tile rows (2500 rows x 79 tiles need 771 CTAs of 256 threads), bytes and
+    packed, equal to the exact cut."""
+    from GraphCut import unpack_labels
+    g = synth.make_graph(2500, 2500, 7)
+    f_ref, l_ref = oracle.maxflow_bk(*g.planes())
+    with GraphCut(g.width, g.height) as gc:
+        gc.upload_capacities(*g.planes())
+        lab = gc.cut_labels().cpu().numpy()
+        assert gc.flow == f_ref
+        assert np.array_equal(lab, l_ref)
+        gc.upload_capacities(*g.planes())
+        bits = gc.cut_labels(packed=True).cpu().numpy()
+        assert gc.flow == f_ref
+        assert np.array_equal(unpack_labels(bits, g.width), l_ref)
+
+
 def test_handles_in_caller_memory(cuda, oracle):
     """gc_create_in: handles placed in one caller-owned buffer solve like gc_create, and
     the memory is reused for a handle of another size after gc_destroy."""
