@@ -48,8 +48,9 @@ RUNTIME_GRID = {
 SIZE_CLASSES = ((1 << 18, 384), (1 << 20, 768), (1 << 22, 1536), (None, 4096))
 
 # built-in choices (offline tuning on synthetic grids) used until a class is tuned: one grid
-# 3 x 2 is the best of the 72 candidates at 2048^2 (0.259 ms against 0.287 for 4 x 2) and at
-# 4096^2 (1.10 ms against 1.21 for 4 x 2; 4 x 1 is not among the best six), and within a few
+# 3 x 2 is the best candidate at 2048^2 (0.257 ms against 0.281 for 4 x 2, upload and solve
+# of seed 1000) and at 4096^2 (1.09 ms against 1.21 for 4 x 2; 4 x 1 is not among the best
+# six), and within a few
 # percent of the best on smaller grids; pools of many grids 4 x 2 (the pool choice depends on
 # the instance: on one sample of 64 grids of 256^2 to 1536^2 the tuner preferred 3 x 4, 8.82
 # against 10.57 ms, while the benchmark's 64 grids take 5.97 ms with 3 x 4 and 5.33 with 4 x 2)
