@@ -1,0 +1,97 @@
+"""The reference's own graph-cut kernels on the host.  TEST INFRASTRUCTURE ONLY.
+
+``oracle/_ref/librefcl.so`` holds graphcut.cl compiled unchanged as C, with the reference's
+host loop (GraphCut.cut, GraphCut.pyx:348-418) around it; ``refcl_host.c`` says how it is
+run.  The library is built only where the reference checkout is present (``make -C oracle
+ref REF=<checkout>``), and ``available()`` is false elsewhere.  The parity tests use it to
+pin the oracle to the reference's own kernels; ``tests/golden/make_refcl_golden.py`` writes
+its answers into fixtures, which pin the oracle and the CUDA path where the checkout is
+absent.
+
+The kernels' image size is fixed in their source (graphcut.cl:15-16): 800 x 608.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_PATH = os.path.join(_HERE, "_ref", "librefcl.so")
+_LIB = None
+
+WIDTH, HEIGHT = 800, 608
+STAT_NAMES = ("iterations", "relabels", "bfs_rounds", "launches", "guard_bytes_dirty",
+              "barriers_without_fibers", "divergent_barrier_passes", "non_integral_values")
+
+
+def build(reference_dir: str) -> bool:
+    """Build the library from the reference checkout; False when it is not there."""
+    if not os.path.exists(os.path.join(reference_dir, "graphcut.cl")):
+        return False
+    subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={reference_dir}"], check=True)
+    return os.path.exists(_PATH)
+
+
+def available() -> bool:
+    return os.path.exists(_PATH)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not available():
+            raise FileNotFoundError(f"{_PATH} is not built (make -C oracle ref REF=<checkout>)")
+        L = ctypes.CDLL(_PATH)
+        P = ctypes.c_void_p
+        L.refcl_cut.argtypes = ([P] * 5 + [ctypes.c_int, ctypes.c_longlong] + [P] * 6 +
+                                [ctypes.c_int, P])
+        L.refcl_cut.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+SCHEDULE_LOCKSTEP, SCHEDULE_SERIAL = 0, 1
+
+
+def cut(up, down, left, right, excess, bfs: int = 5, max_iters: int = 100_000,
+        schedule: int = SCHEDULE_LOCKSTEP):
+    """Run GraphCut.cut with the reference's kernels on an 800 x 608 integer graph.
+
+    schedule: SCHEDULE_LOCKSTEP (the work-items of a group make each access to
+    bfs_intratile's loop flag together -- all test, all reset, then the changed ones set --
+    as a GPU warp's lanes do) or SCHEDULE_SERIAL (work-items strictly one after another
+    between barriers, as a CPU OpenCL runtime runs them; the race on that flag,
+    graphcut.cl:925-990, then ends the in-tile BFS early).
+
+    Returns a dict: the final residual planes ``up``/``down``/``left``/``right`` and
+    ``excess`` (int32, row-major, true residuals: tiles never loaded get their capacities
+    added), ``height``, and ``stats`` (a dict over STAT_NAMES).  Raises on a bad argument
+    or when max_iters push iterations do not finish."""
+    planes = [np.ascontiguousarray(a, dtype=np.int32) for a in (up, down, left, right, excess)]
+    for a in planes:
+        if a.shape != (HEIGHT, WIDTH):
+            raise ValueError(f"the reference kernels take {HEIGHT}x{WIDTH} planes, got {a.shape}")
+    out = [np.zeros((HEIGHT, WIDTH), np.int32) for _ in range(6)]
+    stats = np.zeros(len(STAT_NAMES), np.int64)
+    rc = lib().refcl_cut(*[_p(a) for a in planes], int(bfs), int(max_iters),
+                         *[_p(a) for a in out], int(schedule), _p(stats))
+    if rc == 1:
+        raise ValueError("refcl_cut: bad argument (capacities must be in [0, 2^24), "
+                         "|excess| < 2^24)")
+    if rc == 2:
+        raise MemoryError("refcl_cut: out of memory")
+    if rc == 3:
+        raise RuntimeError(f"refcl_cut: not finished after {max_iters} push iterations")
+    if rc != 0:
+        raise RuntimeError(f"refcl_cut failed ({rc})")
+    names = ("up", "down", "left", "right", "excess", "height")
+    res = dict(zip(names, out))
+    res["stats"] = {k: int(v) for k, v in zip(STAT_NAMES, stats)}
+    return res

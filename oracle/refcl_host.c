@@ -1,0 +1,728 @@
+/* The reference's own graph-cut kernels, run on the host.  TEST INFRASTRUCTURE ONLY: the
+ * parity tests and the script that writes the reference-kernel golden fixtures use it to
+ * check the oracle; nothing in the product links or loads it.
+ *
+ * The reference's graph-cut kernels (graphcut.cl) are compiled unchanged from where they
+ * lie (the Makefile passes the path as REF_GRAPHCUT_CL; the build output goes to
+ * oracle/_ref/ only), with the options GraphCut.__init__ gives them (GraphCut.pyx:85-96).
+ * refcl_clc.h supplies the OpenCL C built-ins; this file supplies the work-group runtime
+ * (fibers switched at barrier(), see refcl_clc.h) and the host side: GraphCut.cut / push /
+ * relabel / startBfs / isCompleted (GraphCut.pyx:155-418) and IncrementalTileList.reset /
+ * increment / build / incorporate (IncrementalTileList.pyx:101-189), each launch with the
+ * reference's own global and local sizes and argument lists.
+ *
+ * Four things differ from the reference's host code, all outside graphcut.cl:
+ *   - The tile lists' one-line kernels (init_incremental, flag, increment_logical,
+ *     incremental_tile_list.cl:26-154) are restated below: that file's display kernel
+ *     (`filter`) uses OpenCL vector literals, which C cannot parse, so the file is not
+ *     included.
+ *   - load_tiles (graphcut.cl:1033-1132) derives float capacities from an RGBA image.
+ *     Here the capacities are given as integer planes, and loading a tile adds them to the
+ *     tile's residual planes: up/down as they are, left/right in the kernels' tile-transposed
+ *     layout (plane row ty*32 + x', column tx*32 + y' holds pixel (tx*32 + x', ty*32 + y')).
+ *     load_tiles itself adds for every edge except two that it assigns (:1104, :1130); the
+ *     image-edge capacities it zeroes are zero in the given planes already.
+ *   - StreamCompact.compact (StreamCompact.pyx) becomes a host loop: the indices of the
+ *     non-zero flags in ascending order.  The reference's compaction kernels are pinned to
+ *     their own known answers elsewhere in the tests.
+ *   - dHeight, which the reference never clears, starts at zero; every device buffer starts
+ *     at zero, inside zero-filled guard bands (the kernels read up to one image row before
+ *     the first tile row and after the last).  The harness reports a guard band that no
+ *     longer holds zero, and a barrier() reached by a kernel run without fibers.
+ *
+ * The integer planes are exact in the kernels' float32 buffers while every capacity and
+ * excess stays below 2^24 in magnitude; refcl_cut refuses larger inputs and reports any
+ * final value that is not a whole number.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "refcl_clc.h"
+
+/* ---------------------------------------------------------------------------------------
+ * The reference kernels.  GraphCut.__init__ (GraphCut.pyx:85-96) builds graphcut.cl with
+ * MAX_HEIGHT = W * H, LAMBDA, EPSILON, TILESW and TILESH; the image size itself is fixed
+ * in the source (graphcut.cl:15-16: 800 x 608).
+ *
+ * bfs_intratile keeps its loop flag in local memory (_l_didChange, graphcut.cl:925-990):
+ * every work-item tests it, resets it and, when its pixels changed, sets it, with no barrier
+ * between the test and the reset or between the reset and the set.  The lanes of a GPU warp
+ * make each of these accesses together, so all reset before any sets.  Compiled here, the
+ * flag's name stands for a call into the harness, and under the default (lockstep)
+ * schedule every access to it is a scheduling point: the work-items of the group make each
+ * access in turn before any makes the next -- all test, then all reset, then those that
+ * changed set it.  Under the serial schedule (a CPU OpenCL runtime's order: each work-item
+ * runs on until a barrier) later work-items see the flag another has reset, or reset it
+ * after another set it, and the in-tile BFS ends early.  Nothing else in the kernels is
+ * shared between work-items without a barrier between a write and a read.
+ * ------------------------------------------------------------------------------------- */
+#define MAX_HEIGHT (800 * 608)
+#define LAMBDA 60
+#define EPSILON 0.05
+#define TILESW 25
+#define TILESH 19
+#define _l_didChange refcl_loop_flag()
+#include REF_GRAPHCUT_CL
+#undef _l_didChange
+
+/* IncrementalTileList's kernels, restated from incremental_tile_list.cl: init_incremental
+ * (:26-38), flag (:40-64) and increment_logical (:110-154: tiles[i] = iteration where the
+ * two comparisons, combined by AND or OR, hold).  Operators: 0 ==, 1 >, 2 <, 3 >=, 4 <=. */
+static int tl_test(int v, int op, int operand) {
+  switch (op) {
+    case 0: return v == operand;
+    case 1: return v > operand;
+    case 2: return v < operand;
+    case 3: return v >= operand;
+    case 4: return v <= operand;
+  }
+  return 0;
+}
+
+static void init_incremental(int* tiles, int2 dim, int iteration) {
+  int gx = get_global_id(0), gy = get_global_id(1);
+  if (gx > dim.x - 1 || gy > dim.y - 1) return;
+  tiles[gy * dim.x + gx] = iteration;
+}
+
+static void flag(int* in, int* out, int length, int op, int operand) {
+  int gx = get_global_id(0);
+  if (gx > length - 1) return;
+  out[gx] = tl_test(in[gx], op, operand);
+}
+
+static void increment_logical(int* in1, int* in2, int* out, int length, int op1, int op2,
+                              int a1, int a2, int logical, int iteration) {
+  int gx = get_global_id(0);
+  if (gx > length - 1) return;
+  int f1 = tl_test(in1[gx], op1, a1), f2 = tl_test(in2[gx], op2, a2);
+  int f = logical == 0 ? (f1 && f2) : (f1 || f2);
+  if (f) out[gx] = iteration;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * Work-group runtime.  A work-item switches back to the scheduler at a barrier, at an
+ * access to bfs_intratile's loop flag (lockstep schedule only) and when it ends.  The scheduler resumes, in local-id order,
+ * every work-item not waiting at a barrier, pass after pass; when every work-item still
+ * running waits at the barrier, it releases them all.  Work-items that ended before a
+ * barrier are not waited for (a GPU drops exited threads from a barrier the same way); the
+ * harness counts such releases.
+ * ------------------------------------------------------------------------------------- */
+enum { MAX_ITEMS = 256, STACK_BYTES = 64 * 1024, MAX_LOCAL = 8 };
+enum { ST_RUN = 0, ST_BARRIER = 1, ST_DONE = 2 };
+
+typedef struct {
+  void* sp;
+  int lid[2];
+  int state;
+} Item;
+
+static struct {
+  int lsz[2], ngrp[2], grp[2];
+  Item* cur;
+  void* sched_sp;
+  void (*body)(void);
+  int fibers, lockstep;
+  Item items[MAX_ITEMS];
+  char* stacks;
+  void* loc[MAX_LOCAL];
+  size_t locsz[MAX_LOCAL];
+  int nloc;
+  long long launches, divergent, bad_barrier;
+} R;
+
+/* Stack switch (x86-64 System V): save the callee-saved registers on the current stack,
+ * store the stack pointer in *save, load `to` and restore the registers saved there. */
+__asm__(
+    ".text\n"
+    ".p2align 4\n"
+    ".globl refcl_swap\n"
+    ".hidden refcl_swap\n"
+    ".type refcl_swap, @function\n"
+    "refcl_swap:\n"
+    "  pushq %rbp\n"
+    "  pushq %rbx\n"
+    "  pushq %r12\n"
+    "  pushq %r13\n"
+    "  pushq %r14\n"
+    "  pushq %r15\n"
+    "  movq %rsp, (%rdi)\n"
+    "  movq %rsi, %rsp\n"
+    "  popq %r15\n"
+    "  popq %r14\n"
+    "  popq %r13\n"
+    "  popq %r12\n"
+    "  popq %rbx\n"
+    "  popq %rbp\n"
+    "  ret\n"
+    ".size refcl_swap, .-refcl_swap\n");
+void refcl_swap(void** save, void* to);
+
+static void fiber_entry(void) {
+  R.body();
+  R.cur->state = ST_DONE;
+  refcl_swap(&R.cur->sp, R.sched_sp);
+  abort(); /* a finished work-item is never resumed */
+}
+
+/* A fresh fiber's stack: six zero registers for refcl_swap to pop, then fiber_entry as the
+ * return address, placed so that fiber_entry starts with the stack aligned as after a call. */
+static void* fiber_stack(int i) {
+  uintptr_t top = ((uintptr_t)(R.stacks + (size_t)(i + 1) * STACK_BYTES)) & ~(uintptr_t)15;
+  uintptr_t* sp = (uintptr_t*)top;
+  *--sp = 0;
+  *--sp = (uintptr_t)fiber_entry;
+  for (int k = 0; k < 6; ++k) *--sp = 0;
+  return sp;
+}
+
+size_t get_local_id(uint d) { return d < 2 ? (size_t)R.cur->lid[d] : 0; }
+size_t get_group_id(uint d) { return d < 2 ? (size_t)R.grp[d] : 0; }
+size_t get_local_size(uint d) { return d < 2 ? (size_t)R.lsz[d] : 1; }
+size_t get_num_groups(uint d) { return d < 2 ? (size_t)R.ngrp[d] : 1; }
+size_t get_global_size(uint d) { return d < 2 ? (size_t)R.ngrp[d] * R.lsz[d] : 1; }
+size_t get_global_id(uint d) {
+  return d < 2 ? (size_t)R.grp[d] * R.lsz[d] + (size_t)R.cur->lid[d] : 0;
+}
+
+void barrier(int fence) {
+  (void)fence;
+  if (!R.fibers) {
+    R.bad_barrier++;
+    return;
+  }
+  R.cur->state = ST_BARRIER;
+  refcl_swap(&R.cur->sp, R.sched_sp);
+}
+
+/* bfs_intratile's loop flag: local-memory slot 1 of its launch (intratile_gaps). */
+static int* loop_flag_access(void) {
+  if (R.fibers && R.lockstep) refcl_swap(&R.cur->sp, R.sched_sp);
+  return (int*)R.loc[1];
+}
+
+static void set_local(int n, const size_t* bytes) {
+  for (int k = 0; k < n; ++k) {
+    free(R.loc[k]);
+    R.loc[k] = calloc(1, bytes[k] ? bytes[k] : 1);
+    R.locsz[k] = bytes[k];
+  }
+  R.nloc = n;
+}
+
+/* One NDRange launch: global size g0 x g1, work-group size l0 x l1.  Kernels that reach a
+ * barrier run as fibers; the others run each work-item as a plain call.  Local memory is
+ * cleared before every work-group. */
+static int launch(void (*body)(void), int g0, int g1, int l0, int l1, int fibers) {
+  if (g0 < 0 || g1 < 0 || l0 <= 0 || l1 <= 0 || g0 % l0 || g1 % l1 || l0 * l1 > MAX_ITEMS)
+    return 1;
+  R.launches++;
+  if (g0 == 0 || g1 == 0) return 0;
+  R.lsz[0] = l0;
+  R.lsz[1] = l1;
+  R.ngrp[0] = g0 / l0;
+  R.ngrp[1] = g1 / l1;
+  R.body = body;
+  R.fibers = fibers;
+  const int n = l0 * l1;
+  for (int gy = 0; gy < R.ngrp[1]; ++gy)
+    for (int gx = 0; gx < R.ngrp[0]; ++gx) {
+      R.grp[0] = gx;
+      R.grp[1] = gy;
+      for (int k = 0; k < R.nloc; ++k) memset(R.loc[k], 0, R.locsz[k]);
+      if (!fibers) {
+        Item it = {0};
+        R.cur = &it;
+        for (int ly = 0; ly < l1; ++ly)
+          for (int lx = 0; lx < l0; ++lx) {
+            it.lid[0] = lx;
+            it.lid[1] = ly;
+            body();
+          }
+        continue;
+      }
+      for (int i = 0; i < n; ++i) {
+        R.items[i].lid[0] = i % l0;
+        R.items[i].lid[1] = i / l0;
+        R.items[i].state = ST_RUN;
+        R.items[i].sp = fiber_stack(i);
+      }
+      int live = n, ended_since_release = 0;
+      while (live > 0) {
+        int waiting = 0;
+        for (int i = 0; i < n; ++i) {
+          Item* it = &R.items[i];
+          if (it->state == ST_RUN) {
+            R.cur = it;
+            refcl_swap(&R.sched_sp, it->sp);
+            if (it->state == ST_DONE) {
+              live--;
+              ended_since_release++;
+            }
+          }
+          waiting += it->state == ST_BARRIER;
+        }
+        if (live > 0 && waiting == live) {
+          if (ended_since_release) R.divergent++;
+          ended_since_release = 0;
+          for (int i = 0; i < n; ++i)
+            if (R.items[i].state == ST_BARRIER) R.items[i].state = ST_RUN;
+        }
+      }
+    }
+  return 0;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * Kernel arguments (one set per kernel; every work-item gets the same) and the per-kernel
+ * entry the runtime calls for each work-item.
+ * ------------------------------------------------------------------------------------- */
+#define L(T, k) ((T*)R.loc[k])
+static struct {
+  float *up, *down, *left, *right, *excess, *border;
+  int *height, *height2;
+  uint *can_up, *can_down, *can_left, *can_right;
+  int* list;
+  int* tiles;
+  int* tiles2;
+  int* flags;
+  int* is_completed;
+  int iteration, direction, length, op1, op2, a1, a2, logical;
+  int2 dim;
+} A;
+
+static void k_init_gc(void) {
+  init_gc(A.up, A.down, A.left, A.right, A.excess, L(int, 0), A.tiles, A.iteration);
+}
+static void k_init_bfs(void) {
+  init_bfs(A.list, A.excess, L(float, 0), A.height, L(int, 1), A.down, A.up, A.right, A.left,
+           A.can_down, A.can_up, A.can_right, A.can_left, L(uchar, 2), L(uchar, 3),
+           L(uchar, 4), L(uchar, 5), A.tiles, A.iteration);
+}
+static void k_bfs_intratile(void) {
+  bfs_intratile(A.list, A.height, L(int, 0), A.can_down, A.can_up, A.can_right, A.can_left,
+                loop_flag_access, A.tiles, A.iteration);
+}
+static void k_bfs_intertile(void) {
+  bfs_intertile(A.list, L(int, 0), A.height, A.can_down, A.can_up, A.can_right, A.can_left,
+                A.iteration, A.tiles);
+}
+static void k_relabel(void) {
+  relabel(A.down, A.right, A.up, A.left, A.excess, A.height, A.height2);
+}
+static void k_push_down(void) {
+  push_down(A.list, A.down, A.up, A.height, A.excess, A.border, L(int, 0), A.tiles,
+            A.iteration);
+}
+static void k_push_up(void) {
+  push_up(A.list, A.down, A.up, A.height, A.excess, A.border, L(int, 0), A.tiles, A.iteration);
+}
+static void k_push_right(void) {
+  push_right(A.list, A.excess, L(float, 0), A.height, L(int, 1), A.right, A.left, A.border,
+             L(int, 2), A.tiles, A.iteration);
+}
+static void k_push_left(void) {
+  push_left(A.list, A.excess, L(float, 0), A.height, L(int, 1), A.right, A.left, A.border,
+            L(int, 2), A.tiles, A.iteration);
+}
+static void k_add_border(void) { add_border(A.list, A.border, A.excess, A.direction); }
+static void k_check_completion(void) {
+  check_completion(A.list, A.excess, A.height, L(int, 0), A.is_completed);
+}
+static void k_init_incremental(void) { init_incremental(A.tiles, A.dim, A.iteration); }
+static void k_flag(void) { flag(A.tiles, A.flags, A.length, A.op1, A.a1); }
+static void k_increment_logical(void) {
+  increment_logical(A.tiles, A.tiles2, A.tiles, A.length, A.op1, A.op2, A.a1, A.a2, A.logical,
+                    A.iteration);
+}
+
+static int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+/* ---------------------------------------------------------------------------------------
+ * Device buffers: zero-filled, inside zero-filled guard bands.
+ * ------------------------------------------------------------------------------------- */
+enum { WW = 800, HH = 608, TW = TILESW, TH = TILESH, NT = TILESW * TILESH, GUARD = 8 * WW };
+enum { NPIX = WW * HH, NWAVE = WW * (HH / 32) };
+
+typedef struct {
+  char* base;
+  size_t elem, n;
+} Buf;
+
+static Buf g_bufs[32];
+static int g_nbufs;
+
+static void* buf_new(size_t n, size_t elem) {
+  Buf* b = &g_bufs[g_nbufs++];
+  b->elem = elem;
+  b->n = n;
+  b->base = calloc(n + 2 * GUARD, elem);
+  return b->base ? b->base + GUARD * elem : NULL;
+}
+
+static long long guards_dirty(void) {
+  long long bad = 0;
+  for (int k = 0; k < g_nbufs; ++k) {
+    const Buf* b = &g_bufs[k];
+    const char* lo = b->base;
+    const char* hi = b->base + (GUARD + b->n) * b->elem;
+    for (size_t i = 0; i < GUARD * b->elem; ++i) bad += (lo[i] != 0) + (hi[i] != 0);
+  }
+  return bad;
+}
+
+static void bufs_free(void) {
+  for (int k = 0; k < g_nbufs; ++k) free(g_bufs[k].base);
+  g_nbufs = 0;
+}
+
+/* ---------------------------------------------------------------------------------------
+ * IncrementalTileList (IncrementalTileList.pyx:60-189), tile grid 25 x 19.
+ * ------------------------------------------------------------------------------------- */
+typedef struct {
+  int *tiles, *flags, *list;
+  int length, iteration;
+} TileList;
+
+enum { OP_EQUAL = 0, OP_GT = 1, OP_LT = 2, OP_GTE = 3, OP_LTE = 4, LOGIC_AND = 0 };
+
+static int tl_init(TileList* t) {
+  t->tiles = buf_new(NT, sizeof(int));
+  t->flags = buf_new(NT, sizeof(int));
+  t->list = buf_new(NT, sizeof(int));
+  if (!t->tiles || !t->flags || !t->list) return 1;
+  /* reset(): iteration = init_iteration + 1, every stamp = init_iteration = -1 */
+  t->iteration = 0;
+  t->length = 0;
+  A.tiles = t->tiles;
+  A.dim.x = TW;
+  A.dim.y = TH;
+  A.iteration = -1;
+  set_local(0, NULL);
+  return launch(k_init_incremental, round_up(TW, 16), round_up(TH, 16), 16, 16, 0);
+}
+
+static int tl_increment(TileList* t) { return ++t->iteration; }
+
+/* build(operator, operand): the flag kernel, then an order-keeping compaction */
+static int tl_build(TileList* t, int op, int operand) {
+  A.tiles = t->tiles;
+  A.flags = t->flags;
+  A.length = NT;
+  A.op1 = op;
+  A.a1 = operand;
+  set_local(0, NULL);
+  int rc = launch(k_flag, round_up(NT, 256), 1, 256, 1, 0);
+  int n = 0;
+  for (int i = 0; i < NT; ++i)
+    if (t->flags[i]) t->list[n++] = i;
+  t->length = n;
+  return rc;
+}
+
+static int tl_incorporate(TileList* t, const int* tiles2, int op1, int a1, int op2, int a2,
+                          int logical) {
+  A.tiles = t->tiles;
+  A.tiles2 = (int*)tiles2;
+  A.length = NT;
+  A.op1 = op1;
+  A.op2 = op2;
+  A.a1 = a1;
+  A.a2 = a2;
+  A.logical = logical;
+  A.iteration = t->iteration;
+  set_local(0, NULL);
+  return launch(k_increment_logical, round_up(NT, 256), 1, 256, 1, 0);
+}
+
+/* ---------------------------------------------------------------------------------------
+ * GraphCut (GraphCut.pyx).
+ * ------------------------------------------------------------------------------------- */
+typedef struct {
+  float *up, *down, *left, *right, *excess, *border;
+  int *height, *height2;
+  uint *can_up, *can_down, *can_left, *can_right;
+  int is_completed;
+  TileList load, bfs, edges, brd;
+  const int32_t* src[4]; /* up, down, left, right: integer capacities, row-major */
+  long long iterations, relabels, bfs_rounds;
+  int err;
+} GC;
+
+static void bind_planes(const GC* g) {
+  A.up = g->up;
+  A.down = g->down;
+  A.left = g->left;
+  A.right = g->right;
+  A.excess = g->excess;
+  A.border = g->border;
+  A.height = g->height;
+  A.height2 = g->height2;
+  A.can_up = g->can_up;
+  A.can_down = g->can_down;
+  A.can_left = g->can_left;
+  A.can_right = g->can_right;
+}
+
+/* Index of pixel (x, y)'s left/right capacity in the kernels' tile-transposed planes. */
+static long tpos(int x, int y) {
+  return (long)((y / 32) * 32 + x % 32) * WW + (x / 32) * 32 + y % 32;
+}
+
+/* In place of load_tiles (graphcut.cl:1033-1132): add the given capacities of the listed
+ * tiles to their residual planes. */
+static void load_listed(GC* g) {
+  for (int k = 0; k < g->load.length; ++k) {
+    const int t = g->load.list[k], tx = t % TW, ty = t / TW;
+    for (int y = ty * 32; y < ty * 32 + 32; ++y)
+      for (int x = tx * 32; x < tx * 32 + 32; ++x) {
+        const long i = (long)y * WW + x;
+        g->up[i] += (float)g->src[0][i];
+        g->down[i] += (float)g->src[1][i];
+        g->left[tpos(x, y)] += (float)g->src[2][i];
+        g->right[tpos(x, y)] += (float)g->src[3][i];
+      }
+  }
+}
+
+static void chk(GC* g, int rc) {
+  if (rc && !g->err) g->err = rc;
+}
+
+/* intratile_gaps (GraphCut.pyx:155-170) */
+static void intratile_gaps(GC* g) {
+  bind_planes(g);
+  A.list = g->bfs.list;
+  A.tiles = g->edges.tiles;
+  A.iteration = tl_increment(&g->edges);
+  const size_t loc[2] = {4 * (32 + 2) * (8 * 4 + 2), 4};
+  set_local(2, loc);
+  chk(g, launch(k_bfs_intratile, 32 * g->bfs.length, 8, 32, 4, 1));
+}
+
+/* intertile_gaps (GraphCut.pyx:172-185) */
+static void intertile_gaps(GC* g) {
+  bind_planes(g);
+  A.list = g->edges.list;
+  A.iteration = tl_increment(&g->bfs);
+  A.tiles = g->bfs.tiles;
+  const size_t loc[1] = {4 * 3};
+  set_local(1, loc);
+  chk(g, launch(k_bfs_intertile, 32 * g->edges.length, 1, 32, 1, 1));
+}
+
+/* startBfs (GraphCut.pyx:187-222) */
+static void start_bfs(GC* g) {
+  bind_planes(g);
+  A.list = g->load.list;
+  A.tiles = g->bfs.tiles;
+  A.iteration = tl_increment(&g->bfs);
+  const size_t loc[6] = {4 * 32 * 32, 4 * 6, 32 * 4, 32 * 4, 32 * 4, 32 * 4};
+  set_local(6, loc);
+  chk(g, launch(k_init_bfs, 32 * g->load.length, 4, 32, 4, 1));
+  for (;;) {
+    chk(g, tl_build(&g->bfs, OP_EQUAL, g->bfs.iteration));
+    if (g->bfs.length > 0) {
+      g->bfs_rounds++;
+      intratile_gaps(g);
+    } else {
+      break;
+    }
+    chk(g, tl_build(&g->edges, OP_EQUAL, g->edges.iteration));
+    if (g->edges.length > 0)
+      intertile_gaps(g);
+    else
+      break;
+  }
+}
+
+/* relabel (GraphCut.pyx:224-241): the Jacobi pass, then the two height buffers swap */
+static void relabel_pass(GC* g) {
+  bind_planes(g);
+  set_local(0, NULL);
+  chk(g, launch(k_relabel, round_up(WW, 16), round_up(HH, 16), 16, 16, 0));
+  int* t = g->height;
+  g->height = g->height2;
+  g->height2 = t;
+}
+
+static void add_border_pass(GC* g, int direction) {
+  chk(g, tl_build(&g->brd, OP_EQUAL, g->brd.iteration));
+  if (!g->brd.length) return;
+  bind_planes(g);
+  A.list = g->brd.list;
+  A.direction = direction;
+  set_local(0, NULL);
+  chk(g, launch(k_add_border, 32 * g->brd.length, 1, 32, 1, 0));
+}
+
+/* push (GraphCut.pyx:243-326): down, up, right, left, each followed by add_border */
+static void push(GC* g) {
+  const size_t loc_ud[1] = {4};
+  const size_t loc_lr[3] = {4 * 32 * 33, 4 * 32 * 33, 4};
+  void (*const body[4])(void) = {k_push_down, k_push_up, k_push_right, k_push_left};
+  for (int d = 0; d < 4; ++d) {
+    bind_planes(g);
+    A.list = g->load.list;
+    A.tiles = g->brd.tiles;
+    A.iteration = tl_increment(&g->brd);
+    if (d < 2)
+      set_local(1, loc_ud);
+    else
+      set_local(3, loc_lr);
+    chk(g, launch(body[d], 32 * g->load.length, 4, 32, 4, 1));
+    add_border_pass(g, d);
+  }
+}
+
+/* isCompleted (GraphCut.pyx:328-346) */
+static int is_completed(GC* g) {
+  g->is_completed = 1;
+  bind_planes(g);
+  A.list = g->load.list;
+  A.is_completed = &g->is_completed;
+  const size_t loc[1] = {4};
+  set_local(1, loc);
+  chk(g, launch(k_check_completion, 32 * g->load.length, 4, 32, 4, 1));
+  return g->is_completed != 0;
+}
+
+/* cut (GraphCut.pyx:348-418), with an iteration cap (the reference loops until done) */
+static int cut(GC* g, int bfs_period, long long max_iters) {
+  const int load_iteration = g->load.iteration;
+  bind_planes(g);
+  A.tiles = g->load.tiles;
+  A.iteration = tl_increment(&g->load);
+  const size_t loc[1] = {4};
+  set_local(1, loc);
+  chk(g, launch(k_init_gc, WW, HH / 8, 32, 4, 1));
+  chk(g, tl_build(&g->load, OP_EQUAL, g->load.iteration));
+  load_listed(g);
+  start_bfs(g);
+  for (long long iteration = 1;; ++iteration) {
+    if (g->err) return g->err;
+    if (iteration > max_iters) return 3;
+    push(g);
+    g->iterations++;
+    if (iteration % bfs_period == 0) {
+      tl_increment(&g->load);
+      chk(g, tl_incorporate(&g->load, g->brd.tiles, OP_LTE, load_iteration, OP_GTE,
+                            g->brd.iteration - bfs_period * 4, LOGIC_AND));
+      chk(g, tl_build(&g->load, OP_EQUAL, g->load.iteration));
+      if (g->load.length > 0) load_listed(g);
+      chk(g, tl_build(&g->load, OP_GT, load_iteration));
+      start_bfs(g);
+      if (is_completed(g)) return g->err;
+    } else {
+      relabel_pass(g);
+      g->relabels++;
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------------------------
+ * C entry point.
+ *
+ * up/down/left/right/excess: int32 row-major [608][800] planes (capacity of the edge from
+ * a pixel to that neighbour; excess = signed t-link, positive = source capacity).
+ * Out: the final residual planes and excess in the same layout (tiles never loaded get
+ * their given capacities added, so the planes are the true residual graph), the final
+ * heights, and stats[8] = {push iterations, relabel passes, BFS rounds, launches, guard
+ * bytes found non-zero, barrier() calls without fibers, barrier releases with work-items
+ * that had ended before it, final values that are not whole numbers}.  schedule: 0 =
+ * the work-items of a group access bfs_intratile's loop flag in lockstep (a warp's order),
+ * 1 = strictly one after another (a CPU OpenCL runtime's order).
+ * Returns 0 when cut() finished, 1 for a bad argument, 2 for out of memory, 3 when
+ * max_iters push iterations did not finish.
+ * ------------------------------------------------------------------------------------- */
+int refcl_width(void) { return WW; }
+int refcl_height(void) { return HH; }
+
+int refcl_cut(const int32_t* up, const int32_t* down, const int32_t* left,
+              const int32_t* right, const int32_t* excess, int bfs_period, long long max_iters,
+              int32_t* r_up, int32_t* r_down, int32_t* r_left, int32_t* r_right,
+              int32_t* r_excess, int32_t* r_height, int schedule, long long* stats) {
+  if (!up || !down || !left || !right || !excess || bfs_period <= 0 || schedule < 0 ||
+      schedule > 1)
+    return 1;
+  const int32_t lim = 1 << 24;
+  for (long i = 0; i < NPIX; ++i)
+    if (up[i] < 0 || down[i] < 0 || left[i] < 0 || right[i] < 0 || up[i] >= lim ||
+        down[i] >= lim || left[i] >= lim || right[i] >= lim || excess[i] >= lim ||
+        excess[i] <= -lim)
+      return 1;
+  memset(&R, 0, sizeof(R));
+  memset(&A, 0, sizeof(A));
+  R.lockstep = schedule == 0;
+  GC g;
+  memset(&g, 0, sizeof(g));
+  int rc = 0;
+  R.stacks = malloc((size_t)MAX_ITEMS * STACK_BYTES);
+  g.up = buf_new(NPIX, 4);
+  g.down = buf_new(NPIX, 4);
+  g.left = buf_new(NPIX, 4);
+  g.right = buf_new(NPIX, 4);
+  g.excess = buf_new(NPIX, 4);
+  g.height = buf_new(NPIX, 4);
+  g.height2 = buf_new(NPIX, 4);
+  g.border = buf_new(NWAVE, 4);
+  g.can_up = buf_new(NWAVE, 4);
+  g.can_down = buf_new(NWAVE, 4);
+  g.can_left = buf_new(NWAVE, 4);
+  g.can_right = buf_new(NWAVE, 4);
+  if (!R.stacks || !g.up || !g.down || !g.left || !g.right || !g.excess || !g.height ||
+      !g.height2 || !g.border || !g.can_up || !g.can_down || !g.can_left || !g.can_right) {
+    rc = 2;
+    goto done;
+  }
+  if (tl_init(&g.load) || tl_init(&g.bfs) || tl_init(&g.edges) || tl_init(&g.brd)) {
+    rc = 2;
+    goto done;
+  }
+  g.src[0] = up;
+  g.src[1] = down;
+  g.src[2] = left;
+  g.src[3] = right;
+  for (long i = 0; i < NPIX; ++i) g.excess[i] = (float)excess[i];
+  rc = cut(&g, bfs_period, max_iters);
+
+  {
+    /* tiles never loaded hold only the reverse flow pushed into them */
+    uint8_t loaded[NT];
+    for (int t = 0; t < NT; ++t) loaded[t] = g.load.tiles[t] > 0;
+    long long frac = 0;
+    for (int y = 0; y < HH; ++y)
+      for (int x = 0; x < WW; ++x) {
+        const long i = (long)y * WW + x, j = tpos(x, y);
+        const int t = (y / 32) * TW + x / 32;
+        float v[6] = {g.up[i], g.down[i], g.left[j], g.right[j], g.excess[i], 0.f};
+        if (!loaded[t])
+          for (int d = 0; d < 4; ++d) v[d] += (float)g.src[d][i];
+        int32_t* out[5] = {r_up, r_down, r_left, r_right, r_excess};
+        for (int d = 0; d < 5; ++d) {
+          if ((float)(int32_t)v[d] != v[d]) frac++;
+          if (out[d]) out[d][i] = (int32_t)v[d];
+        }
+        if (r_height) r_height[i] = g.height[i];
+      }
+    if (stats) {
+      stats[0] = g.iterations;
+      stats[1] = g.relabels;
+      stats[2] = g.bfs_rounds;
+      stats[3] = R.launches;
+      stats[4] = guards_dirty();
+      stats[5] = R.bad_barrier;
+      stats[6] = R.divergent;
+      stats[7] = frac;
+    }
+  }
+done:
+  for (int k = 0; k < MAX_LOCAL; ++k) {
+    free(R.loc[k]);
+    R.loc[k] = NULL;
+  }
+  free(R.stacks);
+  bufs_free();
+  return rc;
+}
