@@ -19,10 +19,13 @@
 //                        baseline (OpenMP over tiles) and a second independent solver.
 //
 // Parity status: the flow value of a graph is unique, and so is its canonical cut (the
-// minimal source set), so orc_maxflow_bk pins both for any correct solver.  The reference's
-// own kernels were not run here (they need an OpenCL runtime; the image has none), and its
-// graph-cut test asserts no outputs, so parity with the reference's kernels themselves is
-// unpinned; the primitives (scan, compaction, tile lists) are pinned against the
+// minimal source set), so orc_maxflow_bk pins both for any correct solver.  Both parts are
+// pinned to the reference's own kernels: graphcut.cl, compiled unchanged for the host and
+// run under the reference's host loop (refcl_host.c), gives orc_maxflow_bk's flow and cut
+// on the golden graphs (tests/golden/refcl_*.npz, among them the reference's own test
+// input), and orc_ref_tiled ends in the kernels' cut after the kernels' push iterations
+// and relabel passes on every graph tried, including one where both stop short of the
+// maximum flow.  The primitives (scan, compaction, tile lists) are pinned against the
 // reference's own test vectors.
 //
 // Plane layout: row-major int32 [H][W]; up/down/left/right hold the residual capacity of

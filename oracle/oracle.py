@@ -23,6 +23,10 @@ this module to check results; the product never imports it.
                       float evaluation it is pinned against.
 * ``brush_pixels``    the pixel set of a brush stroke (brush.pyx:138-161).
 * ``view_colorize``   the display filters' colour ramp and blend (graphcut_filter.cl:5-155).
+
+``oracle/refcl.py`` runs the reference's own graph-cut kernels (graphcut.cl, compiled for
+the host) under its host loop; ``tests/test_refcl_golden.py`` pins ``maxflow_bk`` and
+``ref_tiled`` to them.
 """
 from __future__ import annotations
 

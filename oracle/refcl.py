@@ -27,11 +27,19 @@ STAT_NAMES = ("iterations", "relabels", "bfs_rounds", "launches", "guard_bytes_d
               "barriers_without_fibers", "divergent_barrier_passes", "non_integral_values")
 
 
-def build(reference_dir: str) -> bool:
-    """Build the library from the reference checkout; False when it is not there."""
-    if not os.path.exists(os.path.join(reference_dir, "graphcut.cl")):
-        return False
-    subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={reference_dir}"], check=True)
+def build(reference_dir: str | None = None) -> bool:
+    """Build the library from the reference checkout (the Makefile's default location when
+    reference_dir is None); False when the checkout's graphcut.cl is not there."""
+    cmd = ["make", "-s", "-C", _HERE, "ref"]
+    if reference_dir is not None:
+        if not os.path.exists(os.path.join(reference_dir, "graphcut.cl")):
+            return False
+        cmd.append(f"REF={reference_dir}")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        if "No rule to make target" in r.stderr and "graphcut.cl" in r.stderr:
+            return False
+        raise RuntimeError(f"building {_PATH} failed:\n{r.stderr}")
     return os.path.exists(_PATH)
 
 
