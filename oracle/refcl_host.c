@@ -354,6 +354,7 @@ static Buf g_bufs[32];
 static int g_nbufs;
 
 static void* buf_new(size_t n, size_t elem) {
+  if (g_nbufs >= (int)(sizeof(g_bufs) / sizeof(g_bufs[0]))) return NULL;
   Buf* b = &g_bufs[g_nbufs++];
   b->elem = elem;
   b->n = n;
@@ -634,7 +635,8 @@ static int cut(GC* g, int bfs_period, long long max_iters) {
  * the work-items of a group access bfs_intratile's loop flag in lockstep (a warp's order),
  * 1 = strictly one after another (a CPU OpenCL runtime's order).
  * Returns 0 when cut() finished, 1 for a bad argument, 2 for out of memory, 3 when
- * max_iters push iterations did not finish.
+ * max_iters push iterations did not finish.  The harness keeps its state in file-scope
+ * variables: one call at a time per process.
  * ------------------------------------------------------------------------------------- */
 int refcl_width(void) { return WW; }
 int refcl_height(void) { return HH; }
