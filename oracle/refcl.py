@@ -8,7 +8,9 @@ pin the oracle to the reference's own kernels; ``tests/golden/make_refcl_golden.
 its answers into fixtures, which pin the oracle and the CUDA path where the checkout is
 absent.
 
-The kernels' image size is fixed in their source (graphcut.cl:15-16): 800 x 608.
+The kernels' image size is fixed in their source (graphcut.cl:15-16): 800 x 608.  A second
+library, ``librefcl_512x512.so``, is built from a copy with those two lines set to 512 x 512
+(the reference's CPU-sized configuration); ``cut`` picks the library by the planes' shape.
 """
 from __future__ import annotations
 
@@ -20,9 +22,12 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _PATH = os.path.join(_HERE, "_ref", "librefcl.so")
-_LIB = None
+_PATHS = {(800, 608): _PATH,
+          (512, 512): os.path.join(_HERE, "_ref", "librefcl_512x512.so")}
+_LIBS = {}
 
-WIDTH, HEIGHT = 800, 608
+WIDTH, HEIGHT = 800, 608     # the size fixed in graphcut.cl
+SIZES = tuple(_PATHS)        # (width, height) of every library
 STAT_NAMES = ("iterations", "relabels", "bfs_rounds", "launches", "guard_bytes_dirty",
               "barriers_without_fibers", "divergent_barrier_passes", "non_integral_values")
 
@@ -39,26 +44,29 @@ def build(reference_dir: str | None = None) -> bool:
     if r.returncode != 0:
         if "No rule to make target" in r.stderr and "graphcut.cl" in r.stderr:
             return False
-        raise RuntimeError(f"building {_PATH} failed:\n{r.stderr}")
-    return os.path.exists(_PATH)
+        raise RuntimeError(f"building the reference kernels failed:\n{r.stderr}")
+    return all(os.path.exists(p) for p in _PATHS.values())
 
 
-def available() -> bool:
-    return os.path.exists(_PATH)
+def available(size=(WIDTH, HEIGHT)) -> bool:
+    return os.path.exists(_PATHS[tuple(size)])
 
 
-def lib():
-    global _LIB
-    if _LIB is None:
-        if not available():
-            raise FileNotFoundError(f"{_PATH} is not built (make -C oracle ref REF=<checkout>)")
-        L = ctypes.CDLL(_PATH)
+def lib(size=(WIDTH, HEIGHT)):
+    size = tuple(size)
+    if size not in _LIBS:
+        path = _PATHS[size]
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (make -C oracle ref REF=<checkout>)")
+        L = ctypes.CDLL(path)
         P = ctypes.c_void_p
         L.refcl_cut.argtypes = ([P] * 5 + [ctypes.c_int, ctypes.c_longlong] + [P] * 6 +
                                 [ctypes.c_int, P])
         L.refcl_cut.restype = ctypes.c_int
-        _LIB = L
-    return _LIB
+        if (L.refcl_width(), L.refcl_height()) != size:
+            raise RuntimeError(f"{path} was built for another size")
+        _LIBS[size] = L
+    return _LIBS[size]
 
 
 def _p(a):
@@ -70,7 +78,8 @@ SCHEDULE_LOCKSTEP, SCHEDULE_SERIAL = 0, 1
 
 def cut(up, down, left, right, excess, bfs: int = 5, max_iters: int = 100_000,
         schedule: int = SCHEDULE_LOCKSTEP):
-    """Run GraphCut.cut with the reference's kernels on an 800 x 608 integer graph.
+    """Run GraphCut.cut with the reference's kernels on an integer graph of one of SIZES
+    (800 x 608, the kernels' own size, or 512 x 512).
 
     schedule: SCHEDULE_LOCKSTEP (the work-items of a group make each access to
     bfs_intratile's loop flag together -- all test, all reset, then the changed ones set --
@@ -83,12 +92,14 @@ def cut(up, down, left, right, excess, bfs: int = 5, max_iters: int = 100_000,
     added), ``height``, and ``stats`` (a dict over STAT_NAMES).  Raises on a bad argument
     or when max_iters push iterations do not finish."""
     planes = [np.ascontiguousarray(a, dtype=np.int32) for a in (up, down, left, right, excess)]
-    for a in planes:
-        if a.shape != (HEIGHT, WIDTH):
-            raise ValueError(f"the reference kernels take {HEIGHT}x{WIDTH} planes, got {a.shape}")
-    out = [np.zeros((HEIGHT, WIDTH), np.int32) for _ in range(6)]
+    shape = planes[4].shape
+    size = (shape[1], shape[0]) if len(shape) == 2 else None
+    if size not in _PATHS or any(a.shape != shape for a in planes):
+        raise ValueError(f"the reference kernels take planes of one of {SIZES} "
+                         f"(width, height), got {[a.shape for a in planes]}")
+    out = [np.zeros(shape, np.int32) for _ in range(6)]
     stats = np.zeros(len(STAT_NAMES), np.int64)
-    rc = lib().refcl_cut(*[_p(a) for a in planes], int(bfs), int(max_iters),
+    rc = lib(size).refcl_cut(*[_p(a) for a in planes], int(bfs), int(max_iters),
                          *[_p(a) for a in out], int(schedule), _p(stats))
     if rc == 1:
         raise ValueError("refcl_cut: bad argument (capacities must be in [0, 2^24), "

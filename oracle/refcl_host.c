@@ -43,7 +43,9 @@
 /* ---------------------------------------------------------------------------------------
  * The reference kernels.  GraphCut.__init__ (GraphCut.pyx:85-96) builds graphcut.cl with
  * MAX_HEIGHT = W * H, LAMBDA, EPSILON, TILESW and TILESH; the image size itself is fixed
- * in the source (graphcut.cl:15-16: 800 x 608).
+ * in the source (graphcut.cl:15-16: 800 x 608).  REFCL_W / REFCL_H name the size the
+ * kernels were built for: 800 x 608 for the source as it is, or the size the Makefile
+ * wrote into a generated copy whose two #define lines it rewrote (nothing else changes).
  *
  * bfs_intratile keeps its loop flag in local memory (_l_didChange, graphcut.cl:925-990):
  * every work-item tests it, resets it and, when its pixels changed, sets it, with no barrier
@@ -57,11 +59,15 @@
  * after another set it, and the in-tile BFS ends early.  Nothing else in the kernels is
  * shared between work-items without a barrier between a write and a read.
  * ------------------------------------------------------------------------------------- */
-#define MAX_HEIGHT (800 * 608)
+#ifndef REFCL_W
+#define REFCL_W 800
+#define REFCL_H 608
+#endif
+#define MAX_HEIGHT (REFCL_W * REFCL_H)
 #define LAMBDA 60
 #define EPSILON 0.05
-#define TILESW 25
-#define TILESH 19
+#define TILESW (REFCL_W / 32)
+#define TILESH (REFCL_H / 32)
 #define _l_didChange refcl_loop_flag()
 #include REF_GRAPHCUT_CL
 #undef _l_didChange
@@ -342,7 +348,9 @@ static int round_up(int v, int m) { return (v + m - 1) / m * m; }
 /* ---------------------------------------------------------------------------------------
  * Device buffers: zero-filled, inside zero-filled guard bands.
  * ------------------------------------------------------------------------------------- */
-enum { WW = 800, HH = 608, TW = TILESW, TH = TILESH, NT = TILESW * TILESH, GUARD = 8 * WW };
+_Static_assert(IMAGEW == REFCL_W && IMAGEH == REFCL_H, "kernels built for another size");
+_Static_assert(REFCL_W % 32 == 0 && REFCL_H % 32 == 0, "whole 32 x 32 tiles");
+enum { WW = REFCL_W, HH = REFCL_H, TW = TILESW, TH = TILESH, NT = TILESW * TILESH, GUARD = 8 * WW };
 enum { NPIX = WW * HH, NWAVE = WW * (HH / 32) };
 
 typedef struct {
@@ -625,8 +633,10 @@ static int cut(GC* g, int bfs_period, long long max_iters) {
 /* ---------------------------------------------------------------------------------------
  * C entry point.
  *
- * up/down/left/right/excess: int32 row-major [608][800] planes (capacity of the edge from
- * a pixel to that neighbour; excess = signed t-link, positive = source capacity).
+ * up/down/left/right/excess: int32 row-major [H][W] planes, where W x H is the size the
+ * kernels were built for (refcl_width / refcl_height).  up/down/left/right hold the
+ * capacity of the edge from a pixel to that neighbour; excess is the signed t-link
+ * (positive = source capacity).
  * Out: the final residual planes and excess in the same layout (tiles never loaded get
  * their given capacities added, so the planes are the true residual graph), the final
  * heights, and stats[8] = {push iterations, relabel passes, BFS rounds, launches, guard

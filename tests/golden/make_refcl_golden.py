@@ -2,7 +2,9 @@
 
 ``oracle/refcl.py`` runs graphcut.cl, compiled unchanged as C, under the reference's host
 loop (GraphCut.cut, GraphCut.pyx:348-418) on 800 x 608 integer graphs (the kernels' fixed
-image size, graphcut.cl:15-16).  This script runs it on six graphs and writes, for each,
+image size, graphcut.cl:15-16), and at 512 x 512 from a copy with those two lines
+rewritten (the reference's CPU-sized configuration).  This script runs it on eight graphs
+and writes, for each,
 ``tests/golden/refcl_<name>.npz``: the flow value, the canonical minimum cut of the
 kernels' final residual graph (pixels reachable from excess > 0, bit-packed rows), and the
 kernels' step counts (push iterations, relabel passes, BFS rounds).  Each answer is checked
@@ -21,11 +23,13 @@ The graphs:
 * ``directed``: independent random capacities in all four directions and random t-links.
 * ``sparse_sources``: sink pixels everywhere except six blocks of sources, so that most
   tiles start unloaded and are loaded as flow reaches them (GraphCut.pyx:394-405).
+* ``config0_seed1``, ``config0_seed2``: the 512 x 512 synthetic graphs of the CPU-sized
+  configuration.
 
 Inputs other than ``scores`` are regenerated from their seeds by ``graph()``; each fixture
 holds a SHA-256 of its input planes, so a test notices a generator that changed.
 
-    python tests/golden/make_refcl_golden.py REFERENCE_DIR
+    python tests/golden/make_refcl_golden.py REFERENCE_DIR [NAME ...]
 """
 from __future__ import annotations
 
@@ -42,8 +46,16 @@ for p in (os.path.join(ROOT, "cl-util_b200"), ROOT, HERE):
         sys.path.insert(0, p)
 
 W, H = 800, 608
-NAMES = ("scores", "synth1", "synth2", "synth3", "directed", "sparse_sources")
+NAMES = ("scores", "synth1", "synth2", "synth3", "directed", "sparse_sources",
+         "config0_seed1", "config0_seed2")
+
+
 STEP_NAMES = ("iterations", "relabels", "bfs_rounds")
+
+
+def size(name: str):
+    """(width, height) of a fixture's graph."""
+    return (512, 512) if name.startswith("config0") else (W, H)
 
 
 def planes_sha256(planes) -> str:
@@ -63,6 +75,9 @@ def graph(name: str, excess=None):
     if name.startswith("synth"):
         import synth
         return synth.make_graph(W, H, int(name[len("synth"):])).planes()
+    if name.startswith("config0_seed"):
+        import synth
+        return synth.make_graph(512, 512, int(name[len("config0_seed"):])).planes()
     rng = np.random.default_rng({"directed": 5, "sparse_sources": 6}[name])
     up, down, left, right = (rng.integers(0, 60, (H, W)).astype(np.int32) for _ in range(4))
     up[0, :] = 0
@@ -78,7 +93,7 @@ def graph(name: str, excess=None):
     return up, down, left, right, ex
 
 
-def main(ref_root):
+def main(ref_root, names=NAMES):
     from make_golden import tlinks
     from oracle import oracle as O
     from oracle import refcl
@@ -86,7 +101,7 @@ def main(ref_root):
         sys.exit(f"graphcut.cl not found under {ref_root}")
     fg = np.load(os.path.join(ref_root, "scoreFg.npy")).reshape(H, W)
     bg = np.load(os.path.join(ref_root, "scoreBg.npy")).reshape(H, W)
-    for name in NAMES:
+    for name in names:
         excess = tlinks(fg, bg) if name == "scores" else None
         planes = graph(name, excess)
         r = refcl.cut(*planes)
@@ -112,7 +127,8 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    if len(sys.argv) != 2:
-        sys.exit("usage: python tests/golden/make_refcl_golden.py REFERENCE_DIR  (the checkout "
-                 "of rheiland/cl-util holding graphcut.cl, scoreFg.npy and scoreBg.npy)")
-    main(sys.argv[1])
+    if len(sys.argv) < 2 or any(n not in NAMES for n in sys.argv[2:]):
+        sys.exit("usage: python tests/golden/make_refcl_golden.py REFERENCE_DIR [NAME ...]  "
+                 "(the checkout of rheiland/cl-util holding graphcut.cl, scoreFg.npy and "
+                 f"scoreBg.npy; names from {', '.join(NAMES)}; default all)")
+    main(sys.argv[1], tuple(sys.argv[2:]) or NAMES)

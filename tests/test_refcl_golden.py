@@ -1,10 +1,12 @@
 """Parity with the reference's own graph-cut kernels.
 
-The fixtures in tests/golden/refcl_*.npz hold what graphcut.cl computes, run unchanged
-under the reference's host loop (oracle/refcl.py, oracle/refcl_host.c), on six 800 x 608
-graphs: the reference's own test input (scoreBg - scoreFg, test_GraphCut.py:44-47), the
-benchmark's synthetic graphs, random directed capacities, and a graph whose tiles load as
-flow reaches them.  They are written by tests/golden/make_refcl_golden.py.
+The fixtures in tests/golden/refcl_*.npz hold what graphcut.cl computes under the
+reference's host loop (oracle/refcl.py, oracle/refcl_host.c) on eight graphs.  Six are
+800 x 608, the size fixed in the kernels' source, and run on it unchanged: the reference's
+own test input (scoreBg - scoreFg, test_GraphCut.py:44-47), the benchmark's synthetic
+graphs, random directed capacities, and a graph whose tiles load as flow reaches them.  Two
+are the 512 x 512 graphs of the CPU-sized configuration, run on a copy with only the two
+size lines rewritten.  tests/golden/make_refcl_golden.py writes them.
 
 * CPU, always: the oracle's exact solver gives each fixture's flow and cut, and the
   restated reference schedule takes the fixture's steps (push iterations, relabel passes,
@@ -19,7 +21,7 @@ import os
 import numpy as np
 import pytest
 
-from golden.make_refcl_golden import NAMES, STEP_NAMES, W, H, graph, planes_sha256
+from golden.make_refcl_golden import NAMES, STEP_NAMES, W, H, graph, planes_sha256, size
 
 HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -28,14 +30,14 @@ def load(name):
     z = np.load(os.path.join(HERE, f"refcl_{name}.npz"))
     planes = graph(name, z["excess"] if "excess" in z.files else None)
     assert planes_sha256(planes) == str(z["planes_sha256"]), "an input generator changed"
-    labels = np.unpackbits(z["labels_packed"], axis=1, bitorder="little", count=W)
+    labels = np.unpackbits(z["labels_packed"], axis=1, bitorder="little", count=size(name)[0])
     return planes, int(z["flow"]), labels, z["steps"], int(z["serial_flow"])
 
 
 @pytest.fixture(scope="module")
 def refcl():
     from oracle import refcl as R
-    if not (R.available() or R.build()):
+    if not (all(R.available(sz) for sz in R.SIZES) or R.build()):
         pytest.skip("the reference checkout is not present: its kernels cannot be built")
     return R
 
@@ -140,7 +142,8 @@ def test_reference_kernels_refuse_values_float32_cannot_hold(refcl):
 def test_cuda_gives_the_reference_kernels_answer(cuda, name):
     from GraphCut import GraphCut
     planes, flow, labels, _, _ = load(name)
-    with GraphCut(W, H) as gc:
+    w, h = size(name)
+    with GraphCut(w, h) as gc:
         gc.upload_capacities(*planes)
         gc.cut()
         assert gc.flow == flow
