@@ -1,8 +1,8 @@
-"""IncrementalTileList, StreamCompact and PrefixSum on libgcut's single-pass scan.
+"""IncrementalTileList on libgcut's single-pass scan; StreamCompact and PrefixSum live in
+their own modules, as in the reference, and are re-exported here.
 
-Mirrors of the reference classes beneath GraphCut (IncrementalTileList.pyx:26-208,
-StreamCompact.pyx:22-82, PrefixSum.pyx:121-226) with the same method names, argument
-meaning and ValueError on capacity overflow.  Buffers are torch int32 CUDA tensors; every
+A mirror of the reference class beneath GraphCut (IncrementalTileList.pyx:26-208) with the
+same method names and argument meaning.  Buffers are torch int32 CUDA tensors; every
 build / compact / scan is one kernel launch (decoupled look-back) instead of the
 reference's flag + copy + 1-3 scan launches + scatter.  Each object owns its look-back
 state (as each reference object owns its buffers), so objects on different streams do not
@@ -11,10 +11,10 @@ compacted length of -1 (a wait that gave up) raises when `length` is read.
 """
 from __future__ import annotations
 
-import ctypes
-
 import _gcut
 from _gcut import ScanState, check, lib, ptr, stream_handle
+from PrefixSum import PrefixSum, _i32  # noqa: F401  (PrefixSum re-exported)
+from StreamCompact import StreamCompact  # noqa: F401  (re-exported)
 
 
 class Operator:
@@ -30,79 +30,6 @@ class Logical:
     """Combination of two predicates (IncrementalTileList.pyx:33-35)."""
     AND = 0
     OR = 1
-
-
-def _i32(n, device):
-    import torch
-    return torch.zeros(max(1, n), dtype=torch.int32, device=device)
-
-
-def _pow2gt(x: int) -> int:
-    """Smallest power of two >= x (clutil.pyx:15-20)."""
-    i = 1
-    while i < x:
-        i <<= 1
-    return i
-
-
-class PrefixSum:
-    """Exclusive int32 scan (PrefixSum.pyx:121-226, prefixsum.cl)."""
-
-    def __init__(self, capacity: int, device=0):
-        import torch
-        self.capacity = int(capacity)
-        self.device = torch.device("cuda", device) if isinstance(device, int) else device
-        self.state = ScanState(self.device.index or 0, self.capacity)
-
-    def factory(self, length=None):
-        """A scan buffer; its size is rounded up to a power of two (PrefixSum.pyx:168-176)."""
-        if length is None:
-            length = self.capacity
-        elif length > self.capacity:
-            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
-        return _i32(_pow2gt(length), self.device)
-
-    def scan(self, dArray, dTotal, length=None, stream=None):
-        """In-place exclusive scan of dArray[:length]; the sum goes to dTotal[0]."""
-        if length is None:
-            length = dArray.numel()
-        if length > self.capacity:
-            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
-        check(lib().gc_scan_exclusive(self.state.handle, ptr(dArray), ptr(dArray), ptr(dTotal),
-                                      int(length), stream_handle(stream)))
-
-
-class StreamCompact:
-    """Stream compaction of int32 flags (StreamCompact.pyx:22-82)."""
-
-    def __init__(self, capacity: int, device=0):
-        import torch
-        self.capacity = int(capacity)
-        self.device = torch.device("cuda", device) if isinstance(device, int) else device
-        self.state = ScanState(self.device.index or 0, self.capacity)
-
-    def flagFactory(self, length=None):
-        if length is None:
-            length = self.capacity
-        elif length > self.capacity:
-            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
-        return _i32(length, self.device)
-
-    def listFactory(self, length=None):
-        if length is None:
-            length = self.capacity
-        elif length > self.capacity:
-            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
-        return _i32(_pow2gt(length), self.device)
-
-    def compact(self, dFlags, dList, dLength, length=None, stream=None):
-        """dList[:n] = indices of the non-zero flags (increasing), dLength[0] = n."""
-        if length is None:
-            length = dFlags.numel()
-        elif length > self.capacity:
-            raise ValueError(f"length > self.capacity: {length}, {self.capacity}")
-        check(lib().gc_compact(self.state.handle, ptr(dFlags), ptr(dList), ptr(dLength),
-                               int(length), stream_handle(stream)))
 
 
 class IncrementalTileList:
