@@ -127,6 +127,41 @@ def test_reference_kernels_agree_with_the_restated_schedule(oracle, refcl, seed)
         assert np.array_equal(lab, l_bk)
 
 
+def walled_graph_512(seed):
+    """512 x 512 random capacities with a random share (0-40 %) of zero-capacity edges."""
+    rng = np.random.default_rng(seed)
+    cap = int(rng.integers(5, 200))
+    wall = float(rng.uniform(0.0, 0.4))
+    up, down, left, right = (rng.integers(0, cap, (512, 512)).astype(np.int32) for _ in range(4))
+    for a in (up, down, left, right):
+        a[rng.random((512, 512)) < wall] = 0
+    up[0, :] = 0
+    down[-1, :] = 0
+    left[:, 0] = 0
+    right[:, -1] = 0
+    ex = rng.integers(-4 * cap, 4 * cap, (512, 512)).astype(np.int32)
+    return up, down, left, right, ex
+
+
+@pytest.mark.parametrize("seed", [100, 101, 102, 103, 104, 105, 106, 107, 122, 125])
+def test_reference_kernels_agree_with_the_restated_schedule_512(oracle, refcl, seed):
+    """The 512 x 512 build of the kernels, on random graphs with walls: the same cut after
+    the same push and relabel steps as the restatement.  On seed 122 the BFS takes two more
+    rounds in the kernels (the restatement fixes init_bfs's left case, graphcut.cl:746); on
+    seed 125 both stop 4 units short of the maximum flow (a tile-corner path, as on the
+    800 x 608 seed 29)."""
+    planes = walled_graph_512(seed)
+    r = refcl.cut(*planes)
+    f, lab = oracle.canonical(r["up"], r["down"], r["left"], r["right"], r["excess"], planes[4])
+    f_t, l_t, st_t = oracle.ref_tiled(*planes)
+    assert f == f_t and np.array_equal(lab, l_t)
+    steps = [r["stats"][k] for k in STEP_NAMES]
+    assert steps[:2] == st_t[:2].tolist()
+    assert (steps[2] - st_t[2]) == (2 if seed == 122 else 0)
+    f_bk, _ = oracle.maxflow_bk(*planes)
+    assert f_bk - f == (4 if seed == 125 else 0)
+
+
 def test_reference_kernels_refuse_values_float32_cannot_hold(refcl):
     z = np.zeros((H, W), np.int32)
     ex = z.copy()
