@@ -183,3 +183,19 @@ def test_cuda_gives_the_reference_kernels_answer(cuda, name):
         gc.cut()
         assert gc.flow == flow
         assert np.array_equal(gc.labels_host(), labels)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["walled_800x608_seed29", "walled_512_seed125"])
+def test_cuda_is_exact_where_the_reference_stops_short(cuda, oracle, case):
+    """The two graphs on which the reference's kernels (and the restated schedule) end 4
+    units short of the maximum flow: the CUDA solver gives the exact flow and cut."""
+    from GraphCut import GraphCut
+    planes = walled_graph(29) if case.startswith("walled_800") else walled_graph_512(125)
+    h, w = planes[4].shape
+    f_bk, l_bk = oracle.maxflow_bk(*planes)
+    with GraphCut(w, h) as gc:
+        gc.upload_capacities(*planes)
+        gc.cut()
+        assert gc.flow == f_bk
+        assert np.array_equal(gc.labels_host(), l_bk)
