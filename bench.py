@@ -227,6 +227,11 @@ def _cpu_build():
         "-O3 -march=x86-64-v2 (portable build)"
 
 
+# What pins the port to the reference's own code (tests/test_refcl_golden.py).
+PORT_PINNED = ("ends in the same cut after the same push iterations and relabel passes as "
+               "the reference's graphcut.cl run under its host loop")
+
+
 def cpu_baseline(graph, threads, budget_s=12.0):
     """The reference schedule restated (oracle ref_tiled) on the host cores, built for this
     host's CPU."""
@@ -240,7 +245,7 @@ def cpu_baseline(graph, threads, budget_s=12.0):
         reps += 1
     mpix = graph.width * graph.height / 1e6
     return {"value": reps * mpix / t_total, "unit": UNIT, "cores": threads, "kind": "port",
-            "build": build,
+            "build": build, "pinned": PORT_PINNED,
             "sample": f"{reps} full solves of the {graph.width}x{graph.height} grid "
                       f"({t_total:.1f} s), oracle ref_tiled (GraphCut.cut + graphcut.cl "
                       f"restated, int32, OpenMP)"}
@@ -274,7 +279,7 @@ def run_reference(args):
                    "impl": "oracle ref_tiled: the reference schedule (GraphCut.pyx:348-418 + "
                            "graphcut.cl) restated in int32 C++, OpenMP over tiles"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "build": build,
+                         "build": build, "pinned": PORT_PINNED,
                          "sample": f"{args.steps} full solves of the {args.size}^2 grid"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
