@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import re
 import subprocess
 
 import numpy as np
@@ -33,8 +34,8 @@ STAT_NAMES = ("iterations", "relabels", "bfs_rounds", "launches", "guard_bytes_d
 
 
 def build(reference_dir: str | None = None) -> bool:
-    """Build the library from the reference checkout (the Makefile's default location when
-    reference_dir is None); False when the checkout's graphcut.cl is not there."""
+    """Build the libraries from the reference checkout (the Makefile's default location
+    when reference_dir is None); False when the checkout's kernel sources are not there."""
     cmd = ["make", "-s", "-C", _HERE, "ref"]
     if reference_dir is not None:
         if not os.path.exists(os.path.join(reference_dir, "graphcut.cl")):
@@ -42,10 +43,10 @@ def build(reference_dir: str | None = None) -> bool:
         cmd.append(f"REF={reference_dir}")
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        if "No rule to make target" in r.stderr and "graphcut.cl" in r.stderr:
-            return False
+        if re.search(r"No rule to make target '[^']*\.cl'", r.stderr):
+            return False   # a reference kernel source is missing: no checkout here
         raise RuntimeError(f"building the reference kernels failed:\n{r.stderr}")
-    return all(os.path.exists(p) for p in _PATHS.values())
+    return all(os.path.exists(p) for p in _PATHS.values()) and scan_available()
 
 
 def available(size=(WIDTH, HEIGHT)) -> bool:
@@ -114,3 +115,67 @@ def cut(up, down, left, right, excess, bfs: int = 5, max_iters: int = 100_000,
     res = dict(zip(names, out))
     res["stats"] = {k: int(v) for k, v in zip(STAT_NAMES, stats)}
     return res
+
+
+# ---------------------------------------------------------------------------------------
+# The reference's scan and compaction kernels (prefixsum.cl, streamcompact.cl) under the
+# restated PrefixSum / StreamCompact host code (refcl_scan.c).
+# ---------------------------------------------------------------------------------------
+_SCAN_PATH = os.path.join(_HERE, "_ref", "librefcl_scan.so")
+SCAN_STAT_NAMES = ("launches", "guard_bytes_dirty", "barriers_without_fibers")
+
+
+def scan_available() -> bool:
+    return os.path.exists(_SCAN_PATH)
+
+
+def _scan_lib():
+    if "scan" not in _LIBS:
+        if not scan_available():
+            raise FileNotFoundError(f"{_SCAN_PATH} is not built (make -C oracle ref REF=<checkout>)")
+        L = ctypes.CDLL(_SCAN_PATH)
+        P = ctypes.c_void_p
+        for name in ("refcl_scan", "refcl_compact"):
+            f = getattr(L, name)
+            f.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P]
+            f.restype = ctypes.c_int
+        _LIBS["scan"] = L
+    return _LIBS["scan"]
+
+
+def _scan_rc(rc, what):
+    if rc == 1:
+        raise ValueError(f"{what}: bad argument (length >= 1 and capacity >= length)")
+    if rc == 2:
+        raise MemoryError(f"{what}: out of memory")
+    if rc == 4:
+        raise IndexError(f"{what}: the reference's host code indexes a partial-sum level "
+                         "that does not exist")
+    if rc != 0:
+        raise RuntimeError(f"{what} failed ({rc})")
+
+
+def scan(values, capacity=None):
+    """PrefixSum(capacity).scan on the reference's kernels: (exclusive scan, total, stats).
+    The reference cannot scan an empty array, so len(values) >= 1."""
+    a = np.ascontiguousarray(values, dtype=np.int32).ravel()
+    out = np.zeros_like(a)
+    total = np.zeros(1, np.int32)
+    stats = np.zeros(len(SCAN_STAT_NAMES), np.int64)
+    cap = a.size if capacity is None else int(capacity)
+    _scan_rc(_scan_lib().refcl_scan(_p(a), a.size, cap, _p(out), _p(total), _p(stats)),
+             "refcl_scan")
+    return out, int(total[0]), {k: int(v) for k, v in zip(SCAN_STAT_NAMES, stats)}
+
+
+def compact(flags, capacity=None):
+    """StreamCompact(capacity).compact on the reference's kernels: (list, length, stats)."""
+    a = np.ascontiguousarray(flags, dtype=np.int32).ravel()
+    lst = np.zeros_like(a)
+    length = np.zeros(1, np.int32)
+    stats = np.zeros(len(SCAN_STAT_NAMES), np.int64)
+    cap = a.size if capacity is None else int(capacity)
+    _scan_rc(_scan_lib().refcl_compact(_p(a), a.size, cap, _p(lst), _p(length), _p(stats)),
+             "refcl_compact")
+    n = int(length[0])
+    return lst[:n], n, {k: int(v) for k, v in zip(SCAN_STAT_NAMES, stats)}

@@ -1,0 +1,79 @@
+"""The reference's own scan and compaction kernels (prefixsum.cl, streamcompact.cl), run on
+the host under its PrefixSum / StreamCompact host code restated (oracle/refcl_scan.c), where
+the reference checkout is present to build them (skipped elsewhere).
+
+* The reference's own test scenarios (test_PrefixSum.py: 65536 values in [0, 20), total ==
+  sum; test_StreamCompact.py: 65536 random flags, list == np.where(flags == 1)) pass on its
+  kernels, element by element, and the oracle's restatements give the same answers.
+* Exact at every length up to 512^2 - 1.
+* From 512^2 elements on, the reference's host code picks a partial-sum buffer too short for
+  the pass (PrefixSum.pyx:103-105: level int(log(n)/log(512)) - 1 holds capacity / 512^2
+  entries, the pass writes n / 512), and the kernels write past it: the harness's guard
+  bands catch the writes, which on a GPU would land in another buffer.  libgcut's scan has
+  no such limit.
+"""
+import numpy as np
+import pytest
+
+
+@pytest.fixture(scope="module")
+def refcl():
+    from oracle import refcl as R
+    if not (R.scan_available() or R.build()):
+        pytest.skip("the reference checkout is not present: its kernels cannot be built")
+    return R
+
+
+def exclusive(v):
+    return np.concatenate([[0], np.cumsum(v, dtype=np.int64)[:-1]]).astype(np.int32)
+
+
+def test_reference_prefix_sum_scenario(refcl, oracle):
+    """test_PrefixSum.py:16-34: 65536 values in [0, 20); its check is total == sum."""
+    v = np.random.default_rng(35).integers(0, 20, 65536).astype(np.int32)
+    out, total, st = refcl.scan(v)
+    assert total == int(v.sum())
+    assert np.array_equal(out, exclusive(v))
+    assert st["guard_bytes_dirty"] == 0 and st["barriers_without_fibers"] == 0
+    scan, tot = oracle.exclusive_scan(v)
+    assert np.array_equal(np.asarray(scan)[:v.size], out) and int(tot) == total
+
+
+def test_reference_stream_compact_scenario(refcl, oracle):
+    """test_StreamCompact.py:19-41: 65536 random flags; its check is
+    list[:length] == np.where(flags == 1)."""
+    f = np.random.default_rng(41).integers(0, 2, 65536).astype(np.int32)
+    lst, n, st = refcl.compact(f)
+    assert n == int(f.sum())
+    assert np.array_equal(lst, np.where(f == 1)[0])
+    assert st["guard_bytes_dirty"] == 0
+    o_list, o_n = oracle.compact(f)
+    assert int(o_n) == n and np.array_equal(np.asarray(o_list)[:n], lst)
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 255, 511, 512, 513, 1000, 16384, 100003, 262143])
+def test_reference_scan_and_compaction_exact_below_512_squared(refcl, n):
+    rng = np.random.default_rng(n)
+    v = rng.integers(0, 1000, n).astype(np.int32)
+    out, total, st = refcl.scan(v)
+    assert total == int(v.sum()) and np.array_equal(out, exclusive(v))
+    assert st["guard_bytes_dirty"] == 0
+    f = (rng.random(n) < 0.4).astype(np.int32)
+    lst, m, st = refcl.compact(f)
+    assert m == int(f.sum()) and np.array_equal(lst, np.flatnonzero(f))
+    assert st["guard_bytes_dirty"] == 0
+
+
+@pytest.mark.parametrize("n", [262144, 300000])
+def test_reference_scan_writes_past_its_partial_sums_from_512_squared(refcl, n):
+    v = np.random.default_rng(n).integers(1, 1000, n).astype(np.int32)
+    out, total, st = refcl.scan(v)
+    assert st["guard_bytes_dirty"] > 0
+    # the writes landed in the guard band and were read back from there, so the values
+    # themselves come out right here
+    assert total == int(v.sum()) and np.array_equal(out, exclusive(v))
+
+
+def test_reference_cannot_scan_an_empty_array(refcl):
+    with pytest.raises(ValueError):
+        refcl.scan(np.zeros(0, np.int32))
