@@ -24,9 +24,10 @@ this module to check results; the product never imports it.
 * ``brush_pixels``    the pixel set of a brush stroke (brush.pyx:138-161).
 * ``view_colorize``   the display filters' colour ramp and blend (graphcut_filter.cl:5-155).
 
-``oracle/refcl.py`` runs the reference's own graph-cut kernels (graphcut.cl, compiled for
-the host) under its host loop; ``tests/test_refcl_golden.py`` pins ``maxflow_bk`` and
-``ref_tiled`` to them.
+``oracle/refcl.py`` runs the reference's own kernels, compiled for the host, under its host
+code: graphcut.cl (``tests/test_refcl_golden.py`` pins ``maxflow_bk`` and ``ref_tiled`` to
+it) and prefixsum.cl / streamcompact.cl (``tests/test_refcl_scan.py`` pins
+``exclusive_scan`` and ``compact``).
 """
 from __future__ import annotations
 
