@@ -5,17 +5,18 @@
  * The reference's graph-cut kernels (graphcut.cl) are compiled unchanged from where they
  * lie (the Makefile passes the path as REF_GRAPHCUT_CL; the build output goes to
  * oracle/_ref/ only), with the options GraphCut.__init__ gives them (GraphCut.pyx:85-96).
- * refcl_clc.h supplies the OpenCL C built-ins; this file supplies the work-group runtime
- * (fibers switched at barrier(), see refcl_clc.h) and the host side: GraphCut.cut / push /
+ * refcl_clc.h supplies the OpenCL C built-ins, refcl_runtime.h the work-group runtime
+ * (fibers switched at barrier()), and this file the host side: GraphCut.cut / push /
  * relabel / startBfs / isCompleted (GraphCut.pyx:155-418) and IncrementalTileList.reset /
  * increment / build / incorporate (IncrementalTileList.pyx:101-189), each launch with the
  * reference's own global and local sizes and argument lists.
  *
- * Four things differ from the reference's host code, all outside graphcut.cl:
- *   - The tile lists' one-line kernels (init_incremental, flag, increment_logical,
- *     incremental_tile_list.cl:26-154) are restated below: that file's display kernel
- *     (`filter`) uses OpenCL vector literals, which C cannot parse, so the file is not
- *     included.
+ * The tile lists' kernels (init_incremental, flag, increment_logical) are the reference's
+ * too: the Makefile compiles incremental_tile_list.cl (REF_TILELIST_CL) from a copy without
+ * its last kernel, `filter` (the display view, :156-175), whose OpenCL vector literals C
+ * cannot parse.
+ *
+ * Three things differ from the reference's host code, all on the input side:
  *   - load_tiles (graphcut.cl:1033-1132) derives float capacities from an RGBA image.
  *     Here the capacities are given as integer planes, and loading a tile adds them to the
  *     tile's residual planes: up/down as they are, left/right in the kernels' tile-transposed
@@ -23,8 +24,8 @@
  *     load_tiles itself adds for every edge except two that it assigns (:1104, :1130); the
  *     image-edge capacities it zeroes are zero in the given planes already.
  *   - StreamCompact.compact (StreamCompact.pyx) becomes a host loop: the indices of the
- *     non-zero flags in ascending order.  The reference's compaction kernels are pinned to
- *     their own known answers elsewhere in the tests.
+ *     non-zero flags in ascending order.  The reference's own scan and compaction kernels
+ *     give exactly that at the tile lists' lengths (refcl_scan.c, tests/test_refcl_scan.py).
  *   - dHeight, which the reference never clears, starts at zero; every device buffer starts
  *     at zero, inside zero-filled guard bands (the kernels read up to one image row before
  *     the first tile row and after the last).  The harness reports a guard band that no
@@ -72,40 +73,9 @@
 #include REF_GRAPHCUT_CL
 #undef _l_didChange
 
-/* IncrementalTileList's kernels, restated from incremental_tile_list.cl: init_incremental
- * (:26-38), flag (:40-64) and increment_logical (:110-154: tiles[i] = iteration where the
- * two comparisons, combined by AND or OR, hold).  Operators: 0 ==, 1 >, 2 <, 3 >=, 4 <=. */
-static int tl_test(int v, int op, int operand) {
-  switch (op) {
-    case 0: return v == operand;
-    case 1: return v > operand;
-    case 2: return v < operand;
-    case 3: return v >= operand;
-    case 4: return v <= operand;
-  }
-  return 0;
-}
-
-static void init_incremental(int* tiles, int2 dim, int iteration) {
-  int gx = get_global_id(0), gy = get_global_id(1);
-  if (gx > dim.x - 1 || gy > dim.y - 1) return;
-  tiles[gy * dim.x + gx] = iteration;
-}
-
-static void flag(int* in, int* out, int length, int op, int operand) {
-  int gx = get_global_id(0);
-  if (gx > length - 1) return;
-  out[gx] = tl_test(in[gx], op, operand);
-}
-
-static void increment_logical(int* in1, int* in2, int* out, int length, int op1, int op2,
-                              int a1, int a2, int logical, int iteration) {
-  int gx = get_global_id(0);
-  if (gx > length - 1) return;
-  int f1 = tl_test(in1[gx], op1, a1), f2 = tl_test(in2[gx], op2, a2);
-  int f = logical == 0 ? (f1 && f2) : (f1 || f2);
-  if (f) out[gx] = iteration;
-}
+/* IncrementalTileList's kernels (IncrementalTileList.pyx:82-87 builds them with the tile
+ * grid's sizes, which only the omitted `filter` kernel reads). */
+#include REF_TILELIST_CL
 
 #include "refcl_runtime.h"
 
