@@ -16,16 +16,15 @@
  * its last kernel, `filter` (the display view, :156-175), whose OpenCL vector literals C
  * cannot parse.
  *
- * Three things differ from the reference's host code, all on the input side:
+ * The tile lists compact with the reference's StreamCompact / PrefixSum kernels under their
+ * host code (refcl_prefixsum.h).  Two things differ from the reference, both on the input
+ * side:
  *   - load_tiles (graphcut.cl:1033-1132) derives float capacities from an RGBA image.
  *     Here the capacities are given as integer planes, and loading a tile adds them to the
  *     tile's residual planes: up/down as they are, left/right in the kernels' tile-transposed
  *     layout (plane row ty*32 + x', column tx*32 + y' holds pixel (tx*32 + x', ty*32 + y')).
  *     load_tiles itself adds for every edge except two that it assigns (:1104, :1130); the
  *     image-edge capacities it zeroes are zero in the given planes already.
- *   - StreamCompact.compact (StreamCompact.pyx) becomes a host loop: the indices of the
- *     non-zero flags in ascending order.  The reference's own scan and compaction kernels
- *     give exactly that at the tile lists' lengths (refcl_scan.c, tests/test_refcl_scan.py).
  *   - dHeight, which the reference never clears, starts at zero; every device buffer starts
  *     at zero, inside zero-filled guard bands (the kernels read up to one image row before
  *     the first tile row and after the last).  The harness reports a guard band that no
@@ -77,7 +76,16 @@
  * grid's sizes, which only the omitted `filter` kernel reads). */
 #include REF_TILELIST_CL
 
+/* StreamCompact / PrefixSum's kernels, under which IncrementalTileList.build compacts
+ * (IncrementalTileList.pyx:119-136).  prefixsum.cl's helpers are C99 `inline` functions
+ * without an external definition; here they become file-local. */
+#define inline static inline
+#include REF_PREFIXSUM_CL
+#undef inline
+#include REF_STREAMCOMPACT_CL
+
 #include "refcl_runtime.h"
+#include "refcl_prefixsum.h"
 
 /* bfs_intratile's loop flag: local-memory slot 1 of its launch (intratile_gaps). */
 static int* loop_flag_access(void) {
@@ -197,6 +205,8 @@ static void bufs_free(void) {
 typedef struct {
   int *tiles, *flags, *list;
   int length, iteration;
+  PrefixSum ps;  /* its StreamCompact's scan (IncrementalTileList.pyx:64-65) */
+  int* d_length;
 } TileList;
 
 enum { OP_EQUAL = 0, OP_GT = 1, OP_LT = 2, OP_GTE = 3, OP_LTE = 4, LOGIC_AND = 0 };
@@ -205,7 +215,9 @@ static int tl_init(TileList* t) {
   t->tiles = buf_new(NT, sizeof(int));
   t->flags = buf_new(NT, sizeof(int));
   t->list = buf_new(NT, sizeof(int));
-  if (!t->tiles || !t->flags || !t->list) return 1;
+  t->d_length = gbuf_new(1, 1);
+  if (!t->tiles || !t->flags || !t->list || !t->d_length) return 1;
+  if (ps_init(&t->ps, NT)) return 1;
   /* reset(): iteration = init_iteration + 1, every stamp = init_iteration = -1 */
   t->iteration = 0;
   t->length = 0;
@@ -219,7 +231,7 @@ static int tl_init(TileList* t) {
 
 static int tl_increment(TileList* t) { return ++t->iteration; }
 
-/* build(operator, operand): the flag kernel, then an order-keeping compaction */
+/* build(operator, operand): the flag kernel, then StreamCompact.compact */
 static int tl_build(TileList* t, int op, int operand) {
   A.tiles = t->tiles;
   A.flags = t->flags;
@@ -228,10 +240,9 @@ static int tl_build(TileList* t, int op, int operand) {
   A.a1 = operand;
   set_local(0, NULL);
   int rc = launch(k_flag, round_up(NT, 256), 1, 256, 1, 0);
-  int n = 0;
-  for (int i = 0; i < NT; ++i)
-    if (t->flags[i]) t->list[n++] = i;
-  t->length = n;
+  if (rc) return rc;
+  rc = sc_compact(&t->ps, t->flags, t->list, t->d_length, NT);
+  t->length = *t->d_length;
   return rc;
 }
 
@@ -471,6 +482,7 @@ int refcl_cut(const int32_t* up, const int32_t* down, const int32_t* left,
       return 1;
   memset(&R, 0, sizeof(R));
   memset(&A, 0, sizeof(A));
+  memset(&S, 0, sizeof(S));
   R.lockstep = schedule == 0;
   GC g;
   memset(&g, 0, sizeof(g));
@@ -528,7 +540,7 @@ int refcl_cut(const int32_t* up, const int32_t* down, const int32_t* left,
       stats[1] = g.relabels;
       stats[2] = g.bfs_rounds;
       stats[3] = R.launches;
-      stats[4] = guards_dirty();
+      stats[4] = guards_dirty() + gbufs_dirty();
       stats[5] = R.bad_barrier;
       stats[6] = R.divergent;
       stats[7] = frac;
@@ -541,5 +553,6 @@ done:
   }
   free(R.stacks);
   bufs_free();
+  gbufs_free();
   return rc;
 }
