@@ -77,3 +77,12 @@ def test_reference_scan_writes_past_its_partial_sums_from_512_squared(refcl, n):
 def test_reference_cannot_scan_an_empty_array(refcl):
     with pytest.raises(ValueError):
         refcl.scan(np.zeros(0, np.int32))
+
+
+def test_build_leaves_only_libraries_under_ref(refcl):
+    """The recipe compiles the reference's sources from the checkout, or from a copy that
+    it deletes after compiling; nothing of the reference's source stays in the tree."""
+    import os
+    ref_dir = os.path.join(os.path.dirname(refcl.__file__), "_ref")
+    leftovers = [f for f in os.listdir(ref_dir) if not f.endswith(".so")]
+    assert leftovers == []
